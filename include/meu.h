@@ -1,0 +1,192 @@
+/*
+ * meu.h -- C-ABI of the B200 (sm_100a) time step of MEUMAPPS-SS.
+ *
+ * One call of meu_run() replaces the body of the reference time loop
+ *   Multi_MEUMAPPS.f:548-1106  ("4 continue ... if(step.lt.Nt) go to 4"),
+ * i.e. the spectral gradients (:575-615), the KKS driving force (:634-845),
+ * the elasticity solve `eldis`/`elener` (ModElastic.f:11-691), the
+ * semi-implicit Cahn-Hilliard/diffusion update (:910-949), the TDGL update
+ * (:955-1001) and the post-step clip and reductions (:1008-1065, :885-908).
+ * The data_save I/O (:1074-1100) stays with the caller.
+ *
+ * All entry points take plain C types, return an int status (never exit the
+ * process) and are synchronous on return.  A handle owns its device memory and
+ * its CUDA stream; one handle must not be used by two host threads at once.
+ *
+ * Array layout at the boundary is the reference's Fortran layout, component
+ * index fastest:  Cons(numel,Nx,Ny,Nz), phi(vartot,Nx,Ny,Nz)
+ * (Multi_MEUMAPPS.f:260,267), el_en(Nx,Ny,Nz) and each displacement field
+ * u1..u3 / grad_j_ui as (Nx,Ny,Nz) (:279-293).  The library converts to its
+ * own structure-of-arrays layout on upload and back on download.
+ */
+#ifndef MEU_H
+#define MEU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MEU_MAX_VAR 16 /* variants (vartot) */
+#define MEU_MAX_PH 4   /* phases including the matrix (numph) */
+#define MEU_MAX_EL 3   /* solutes (numel after Multi_MEUMAPPS.f:153) */
+#define MEU_MAX_GP (2 * MEU_MAX_EL + 1) /* rows of Gparams (pmax, :155) */
+
+/* model */
+#define MEU_MODEL_KKS 0    /* the reference's KKS model, Multi_MEUMAPPS.f:634-845 */
+#define MEU_MODEL_LANDAU 1 /* Landau polynomial in c and eta (configuration decks) */
+
+/* arithmetic of the bulk fields and transforms */
+#define MEU_PREC_F64 0 /* plain FP64 everywhere */
+#define MEU_PREC_F32 1 /* FP32 fields/FFTs; FP64 for Omega(k), k=0, reductions */
+
+/* elasticity */
+#define MEU_ELAST_NONE 0
+#define MEU_ELAST_HOMOG 1  /* Landau only: homogeneous moduli, Green operator */
+#define MEU_ELAST_HETERO 2 /* eldis fixed-point iteration (KKS always uses it) */
+
+/* Landau eigenstrain coupling theta(eta) */
+#define MEU_EIG_ETA2 0 /* theta = eta^2 */
+#define MEU_EIG_H 1    /* theta = eta^3 (6 eta^2 - 15 eta + 10) */
+
+/* status codes; 2,3,4,6,20 are the reference's err_flag values (ModFunc.f:55-67,
+ * set at Multi_MEUMAPPS.f:690, ModElastic.f:187,270,599, ModInitials.f:98) and 7
+ * is the elastic "newfac is too small" stop (ModElastic.f:446-450). */
+#define MEU_OK 0
+#define MEU_ERR_Z_SINGULAR 2
+#define MEU_ERR_Q_SINGULAR 3
+#define MEU_ERR_C_SINGULAR 4
+#define MEU_ERR_C_ELENER_SINGULAR 6
+#define MEU_ERR_NOT_CONVERGED 7
+#define MEU_ERR_SETUP_SINGULAR 20
+#define MEU_ERR_BADARG 100
+#define MEU_ERR_CUDA 101
+#define MEU_ERR_NOMEM 102
+#define MEU_ERR_UNSUPPORTED 103
+#define MEU_ERR_NOT_FINITE 104
+
+/*
+ * Parameters consumed by the step (ModGparams.f:59-90 after the setup of
+ * Multi_MEUMAPPS.f:153-156,218-236,354-405).  Matrices are stored exactly as
+ * the Fortran module holds them (column-major), so a bind(C) copy is a flat
+ * assignment:
+ *   grad_coeff[v][(j-1)*3+(i-1)] = grad_coeff(i,j,v+1)   (already / del_N**2)
+ *   trans_ppt[v][i-1]            = trans_ppt(i,v+1)
+ *   cela[n][(j-1)*6+(i-1)]       = CEla(i,j,n+1), sela likewise (SEla)
+ *   gparams[n][j-1]              = Gparams(j,n+1)         (after / 1.055e-5)
+ */
+typedef struct meu_params {
+  int64_t step;       /* `step` at entry; incremented once per time step */
+  int64_t elastep0;   /* first elastic step (KKS; Landau uses it too) */
+  int64_t noise_step; /* phi_noise is kept while step <= noise_step */
+  int32_t nx, ny, nz;
+  int32_t model;      /* MEU_MODEL_* */
+  int32_t precision;  /* MEU_PREC_* */
+  int32_t nvar;       /* vartot */
+  int32_t numel;      /* solutes E */
+  int32_t numph;      /* phases (matrix = 1) */
+  int32_t nvar_ph[MEU_MAX_PH]; /* Nvar(1..numph); Nvar(1) = 1 */
+  int32_t elastic;      /* MEU_ELAST_* */
+  int32_t eig_coupling; /* MEU_EIG_* (Landau) */
+  int32_t el_min_iter;  /* 4 in the reference (ModElastic.f:469) */
+  int32_t el_max_iter;  /* 10 in the reference (ModElastic.f:462) */
+  int32_t clip_phi;     /* 1: clip phi to [0,1] after each step (:1034-1035) */
+  int32_t diag_energy;  /* 1: compute the fort.98 energies every step */
+  int32_t reserved0;
+  double dt;            /* t_step */
+  double b_mob;         /* L */
+  double cmobs[MEU_MAX_EL]; /* Cmobs = diff_coeff/del_N**2 (M for Landau) */
+  double el_tol;        /* 1e-7 in the reference (ModElastic.f:435) */
+  double e_mean[6];     /* applied mean strain */
+  double grad_coeff[MEU_MAX_VAR][9];
+  double trans_ppt[MEU_MAX_VAR][6];
+  double cela[MEU_MAX_PH][36];
+  double sela[MEU_MAX_PH][36];
+  double gparams[MEU_MAX_PH][MEU_MAX_GP];
+  double wellph[MEU_MAX_PH];
+  /* Landau free energy f = A/2 (c-c1)^2 + B/2 (c2-c) sum eta^2 - C/4 sum eta^4
+   * + D/6 sum eta^6 + cross_w sum_{u!=v} eta_u^2 eta_v^2, gradient kappa_c/2 |grad c|^2
+   * (kappa_eta enters through grad_coeff, L through b_mob, M through cmobs[0]). */
+  double lan_a, lan_b, lan_c, lan_d, lan_c1, lan_c2, kappa_c, cross_w;
+} meu_params;
+
+/*
+ * One row of per-step diagnostics: the fort.98 line (Multi_MEUMAPPS.f:903-906,
+ * format :1113) and the fort.99 line (:1064).  glob_min, glob_max, phi_max and
+ * solid are reported as the reference writes them, i.e. the values reduced at
+ * the end of the PREVIOUS step (:1057-1062, :891 precede the next write);
+ * cmin..solid_now are this step's end-of-step values.
+ */
+typedef struct meu_diag {
+  int64_t step;      /* value of `step` on this fort.98 line */
+  int32_t el_iters;  /* elastic fixed-point iterations run in this step */
+  int32_t status;
+  double fint, fw, fch, elen, etot;
+  double glob_min, glob_max, phi_max, solid;
+  double cmin, cmax, phimax, solid_now;
+  double cavg[MEU_MAX_EL];
+} meu_diag;
+
+typedef struct meu_handle meu_handle;
+
+/* Create a step engine on the current CUDA device.  Replaces the per-step
+ * state allocation of Multi_MEUMAPPS.f:254-332 and k_space (ModInitials.f:348). */
+int meu_create(const meu_params* params, meu_handle** out);
+
+/* Upload fields.  cons: Cons(numel,Nx,Ny,Nz); phi: phi(vartot,Nx,Ny,Nz);
+ * u_state: NULL (zero) or 12 consecutive (Nx,Ny,Nz) arrays in the data_save
+ * record order u1,u2,u3, grad_1_u1,grad_1_u2,grad_1_u3, grad_2_u1,..,
+ * grad_3_u3 (Multi_MEUMAPPS.f:474-480).  Landau: cons holds c, phi holds eta. */
+int meu_set_fields(meu_handle* h, const double* cons, const double* phi, const double* u_state);
+
+/* Add a host-generated Langevin increment phi(vartot,Nx,Ny,Nz) to phi_noise
+ * (Multi_MEUMAPPS.f:552-566; the generator ran_2/langevin stays on the host). */
+int meu_add_noise(meu_handle* h, const double* incr);
+
+/* Run nsteps time steps.  diag: NULL or nsteps rows. */
+int meu_run(meu_handle* h, int32_t nsteps, meu_diag* diag);
+
+/* Download fields (any pointer may be NULL).  u_state as in meu_set_fields. */
+int meu_get_fields(meu_handle* h, double* cons, double* phi, double* el_en, double* u_state);
+
+/* Current `step` counter. */
+int64_t meu_get_step(const meu_handle* h);
+
+/* Message of the last failing call on this handle (static storage). */
+const char* meu_last_error(const meu_handle* h);
+
+int meu_destroy(meu_handle* h);
+
+/* Host-side helpers (no GPU work). ------------------------------------- */
+
+/* State of the reference's ran_2 (ran_2.f:1-42), whose SAVE variables
+ * iv, iy, idum2 become explicit fields.  Initialise with meu_ran2_init. */
+typedef struct meu_ran2_state {
+  int32_t idum, idum2, iy, iv[32];
+} meu_ran2_state;
+
+void meu_ran2_init(meu_ran2_state* s, int32_t iseed);
+double meu_ran2(meu_ran2_state* s);
+/* langevin (ModFunc.f:77-100): one N(0,sd) draw by the polar method. */
+double meu_langevin(meu_ran2_state* s, double sd);
+
+/* Uniform-noise initial fields for the Landau decks: per voxel in Fortran
+ * order (x fastest), c = c0 + c_amp*(2u-1), then for each variant
+ * eta_v = eta_amp*(2u-1), u = ran_2 draws.  Layout as meu_set_fields. */
+void meu_init_uniform(meu_ran2_state* s, int32_t nx, int32_t ny, int32_t nz, int32_t nvar,
+                      double c0, double c_amp, double eta_amp, double* cons, double* phi);
+
+/* Diagnostics. --------------------------------------------------------- */
+
+/* One f_trans / inv_trans pair (ModFunc.f:15-40) of a real (Nx,Ny,Nz) field on
+ * the GPU, for transform tests: spec_out receives the scaled half spectrum
+ * [z][y][kx] as interleaved re,im doubles (Nz*Ny*(Nx/2+1) complex), back_out
+ * the unscaled inverse of that spectrum (equal to the input up to round-off). */
+int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t precision, const double* in, double* spec_out,
+                      double* back_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEU_H */

@@ -1,0 +1,66 @@
+// common.cuh -- complex arithmetic, launch helpers and error handling shared by
+// the MEUMAPPS-SS step kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace meu {
+
+template <typename R> struct CplxOf;
+template <> struct CplxOf<float> { using type = float2; };
+template <> struct CplxOf<double> { using type = double2; };
+template <typename R> using cplx = typename CplxOf<R>::type;
+
+__host__ __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+__host__ __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
+  return mk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { return mk(a.x, -a.y); }
+template <typename C, typename R> __host__ __device__ __forceinline__ C cscale(C a, R s) {
+  return mk(a.x * s, a.y * s);
+}
+// multiply by i*s (s = +1 or -1)
+template <int S, typename C> __host__ __device__ __forceinline__ C cmul_is(C a) {
+  return S > 0 ? mk(-a.y, a.x) : mk(a.y, -a.x);
+}
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+
+#define MEU_CUDA(x)                                                                              \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess)                                                                       \
+      throw ::meu::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_) + " at " __FILE__ ":" \
+                                 + std::to_string(__LINE__),                                     \
+                             101);                                                               \
+  } while (0)
+
+#define MEU_CHECK_LAUNCH() MEU_CUDA(cudaGetLastError())
+
+inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 16) {
+  int64_t g = (n + block - 1) / block;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+// Up to MAXF field pointers passed by value to batched kernels.
+constexpr int MAXF = 32;
+template <typename T> struct PtrList {
+  T* p[MAXF];
+};
+
+}  // namespace meu

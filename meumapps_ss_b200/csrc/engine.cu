@@ -1,0 +1,841 @@
+// engine.cu -- the step engine behind include/meu.h.
+//
+// One Engine owns the device state of one grid: fields, spectra, the elastic
+// state (u^ and the engineering strain), reduction buffers and a CUDA stream.
+// Engine<R>::run() executes the reference time loop body
+// (Multi_MEUMAPPS.f:548-1106) for the KKS model, or the Landau step, as a
+// sequence of kernels on that stream.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fft.cuh"
+#include "step_kernels.cuh"
+
+namespace meu {
+
+__global__ void k_finalize(const double* __restrict__ partials, int nb, const int* __restrict__ ops, double* out) {
+  const int q = blockIdx.x, op = ops[q];
+  double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    const double v = partials[(int64_t)q * nb + i];
+    acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
+  }
+  block_reduce_store(acc, op, out + q);
+}
+
+// AoS (component fastest, double) <-> SoA (R)
+template <typename R>
+__global__ void k_aos_to_soa(const double* __restrict__ src, R* __restrict__ dst, int ncomp, int64_t v0, int64_t nv,
+                             int64_t n3, int add) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv * ncomp; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t vox = i / ncomp;
+    const int c = (int)(i - vox * ncomp);
+    R* d = dst + (int64_t)c * n3 + v0 + vox;
+    if (add) *d = (R)((double)*d + src[i]);
+    else *d = (R)src[i];
+  }
+}
+template <typename R>
+__global__ void k_soa_to_aos(const R* __restrict__ src, double* __restrict__ dst, int ncomp, int64_t v0, int64_t nv,
+                             int64_t n3) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv * ncomp; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t vox = i / ncomp;
+    const int c = (int)(i - vox * ncomp);
+    dst[i] = (double)src[(int64_t)c * n3 + v0 + vox];
+  }
+}
+template <typename R>
+__global__ void k_convert(const R* __restrict__ src, double* __restrict__ dst, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+template <typename R>
+__global__ void k_convert_in(const double* __restrict__ src, R* __restrict__ dst, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (R)src[i];
+}
+// engineering strain from the 9 gradients grad_j_ui (data_save order (j-1)*3+(i-1))
+// gu holds nv voxels of each gradient back to back; strain is offset to the chunk
+template <typename R>
+__global__ void k_grads_to_strain(const double* __restrict__ gu, R* __restrict__ strain, int64_t nv, int64_t n3) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+    auto G = [&](int ui, int dj) { return gu[(int64_t)((dj - 1) * 3 + (ui - 1)) * nv + i]; };
+    strain[0 * n3 + i] = (R)G(1, 1);
+    strain[1 * n3 + i] = (R)G(2, 2);
+    strain[2 * n3 + i] = (R)G(3, 3);
+    strain[3 * n3 + i] = (R)(G(3, 2) + G(2, 3));
+    strain[4 * n3 + i] = (R)(G(3, 1) + G(1, 3));
+    strain[5 * n3 + i] = (R)(G(2, 1) + G(1, 2));
+  }
+}
+// u^ -> [u_i^ (3), kf_j u_i^ (9)] in data_save order
+template <typename R>
+__global__ void k_u_spectra(const DevConst* __restrict__ Kp, const cplx<R>* __restrict__ uk, PtrList<cplx<R>> out) {
+  const DevConst& K = *Kp;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    for (int i = 0; i < 3; ++i) {
+      double re, im;
+      ld2(uk[(int64_t)i * K.nk + id], re, im);
+      out.p[i][id] = mk((R)re, (R)im);
+      for (int j = 0; j < 3; ++j) out.p[3 + j * 3 + i][id] = mk((R)(-b[j] * im), (R)(b[j] * re));
+    }
+  }
+}
+
+// ==========================================================================
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual void set_fields(const double* cons, const double* phi, const double* ustate) = 0;
+  virtual void add_noise(const double* incr) = 0;
+  virtual void run(int nsteps, meu_diag* diag) = 0;
+  virtual void get_fields(double* cons, double* phi, double* el_en, double* ustate) = 0;
+  int64_t step = 0;
+  std::string err;
+};
+
+template <typename R>
+class Engine : public EngineBase {
+  using C = cplx<R>;
+
+ public:
+  explicit Engine(const meu_params& p);
+  ~Engine() override;
+  void set_fields(const double* cons, const double* phi, const double* ustate) override;
+  void add_noise(const double* incr) override;
+  void run(int nsteps, meu_diag* diag) override;
+  void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
+
+ private:
+  meu_params P;
+  DevConst hK;
+  DevConst* dK = nullptr;
+  std::unique_ptr<FFT3> fft;
+  cudaStream_t st = nullptr;
+  int V, E;
+  int64_t n3, nk;
+  // device buffers
+  R *c = nullptr, *c2 = nullptr, *phi = nullptr, *noise = nullptr, *pphi = nullptr, *wr = nullptr, *fd = nullptr,
+    *fc = nullptr, *el_en = nullptr, *strain = nullptr, *xs = nullptr;
+  C *sp = nullptr, *uk = nullptr;
+  int NS = 0, NWR = 0;
+  double *partials = nullptr, *results = nullptr, *h_results = nullptr;
+  int* d_ops = nullptr;
+  int* d_err = nullptr;
+  int* h_err = nullptr;
+  double* stage = nullptr;  // AoS staging (double)
+  int64_t stage_elems = 0;
+  std::vector<void*> allocs;
+  // reference quirk state: values written on the next fort.98 line
+  double prev_min = 1.0, prev_max = 0.0, prev_phimax = 0.0, prev_solid = 0.0;
+  bool el_ready = false;  // u^ / strain hold a valid elastic state
+  int last_iters = 0;
+
+  template <typename T> T* dalloc(int64_t n) {
+    void* ptr = nullptr;
+    MEU_CUDA(cudaMalloc(&ptr, (size_t)std::max<int64_t>(n, 1) * sizeof(T)));
+    allocs.push_back(ptr);
+    return (T*)ptr;
+  }
+  R* field(R* base, int f) const { return base + (int64_t)f * n3; }
+  C* spec(int f) const { return sp + (int64_t)f * nk; }
+  unsigned gridk() const { return grid_for(nk, 256); }
+  unsigned gridr() const { return grid_for(n3, 256); }
+
+  void fwd(std::initializer_list<const R*> in, int s0) {
+    PtrList<const R> a{};
+    PtrList<C> b{};
+    int n = 0;
+    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
+    fft->forward<R>(a, b, n, st);
+  }
+  void fwd_list(const std::vector<const R*>& in, int s0) {
+    PtrList<const R> a{};
+    PtrList<C> b{};
+    int n = 0;
+    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
+    fft->forward<R>(a, b, n, st);
+  }
+  void inv_list(int s0, const std::vector<R*>& out) {
+    PtrList<C> a{};
+    PtrList<R> b{};
+    int n = 0;
+    for (R* q : out) { a.p[n] = spec(s0 + n); b.p[n] = q; ++n; }
+    fft->inverse<R>(a, b, n, st);
+  }
+  PtrList<C> specs(int s0, int n) const {
+    PtrList<C> l{};
+    for (int i = 0; i < n; ++i) l.p[i] = spec(s0 + i);
+    return l;
+  }
+  void check_err();
+  void finalize(int q0, int nq);
+  void elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only);
+  void kks_step(meu_diag* d);
+  void landau_step(meu_diag* d);
+  void end_step(meu_diag* d, int clip);
+};
+
+template <typename R>
+Engine<R>::Engine(const meu_params& p) : P(p) {
+  V = p.nvar;
+  E = p.numel;
+  if (p.nx < 4 || p.ny < 2 || p.nz < 2 || V < 1 || V > MEU_MAX_VAR || E < 1 || E > MEU_MAX_EL || p.numph < 2 ||
+      p.numph > MEU_MAX_PH || p.numph * p.numel > 12)
+    throw CudaError("parameters out of range", MEU_ERR_BADARG);
+  if (p.model == MEU_MODEL_LANDAU && (E != 1 || p.numph != 2))
+    throw CudaError("Landau decks have one solute and two phases", MEU_ERR_BADARG);
+  if (!fft_size_ok(p.nx, true) || !fft_size_ok(p.ny, false) || !fft_size_ok(p.nz, false))
+    throw CudaError("grid sizes must be 2^a 3^b with Nx even", MEU_ERR_UNSUPPORTED);
+  int sum = 0;
+  for (int n = 0; n < p.numph; ++n) sum += p.nvar_ph[n];
+  if (V + 1 - sum != 0) throw CudaError("variant numbers (initerr 1)", MEU_ERR_BADARG);
+  step = p.step;
+  MEU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  fft.reset(new FFT3(p.nx, p.ny, p.nz, sizeof(R) == 8));
+  n3 = fft->n3();
+  nk = fft->nk();
+  // ---- device constants
+  memset(&hK, 0, sizeof(hK));
+  hK.p = p;
+  hK.nx = p.nx; hK.ny = p.ny; hK.nz = p.nz; hK.nxh = p.nx / 2 + 1;
+  hK.n3 = n3; hK.nk = nk;
+  {
+    int ivn = 0;
+    for (int n = 2; n <= p.numph; ++n) {
+      ivn += p.nvar_ph[n - 2];
+      int fvn = ivn + p.nvar_ph[n - 1] - 1;
+      hK.ph_lo[n] = ivn - 1;
+      hK.ph_hi[n] = fvn;
+      for (int v = ivn - 1; v < fvn; ++v) hK.var_phase[v] = n;
+    }
+  }
+  hK.zdim = p.numph * p.numel;
+  if (p.model == MEU_MODEL_KKS) {
+    const int numel = p.numel, numph = p.numph, zdim = hK.zdim;
+    for (int e = 1; e <= numel; ++e) {
+      const int i1 = e + numel + 1;
+      for (int n = 1; n <= numph - 1; ++n) {
+        const int i0 = (numph - 1) * (e - 1) + n, j0 = numph * (e - 1) + n;
+        hK.zconst[(i0 - 1) + (j0 - 1) * zdim] = p.gparams[n - 1][e - 1];
+        hK.zconst[(i0 - 1) + j0 * zdim] = -p.gparams[n][e - 1];
+        hK.zr_const[i0 - 1] = p.gparams[n - 1][e - 1] * p.gparams[n - 1][i1 - 1] - p.gparams[n][e - 1] * p.gparams[n][i1 - 1];
+      }
+    }
+  }
+  for (int i = 0; i < 36; ++i) hK.c0m[i] = p.cela[1][i];
+  auto vg = [](int i, int j) { return i == j ? i : 9 - i - j; };
+  for (int v = 0; v < V; ++v) {
+    const int n = hK.var_phase[v];
+    for (int ij = 1; ij <= 6; ++ij) {
+      double acc = 0;
+      for (int k = 1; k <= 3; ++k)
+        for (int l = 1; l <= 3; ++l) acc += p.trans_ppt[v][vg(k, l) - 1] * p.cela[n - 1][(ij - 1) + (vg(k, l) - 1) * 6];
+      hK.sig0[v][ij - 1] = acc;
+    }
+    for (int m = 0; m < 6; ++m) hK.eps_eng[v][m] = (m < 3 ? 1.0 : 2.0) * p.trans_ppt[v][m];
+    double ts = 0;
+    for (int m = 0; m < 6; ++m) ts += p.trans_ppt[v][m];
+    hK.use_var[v] = (p.model == MEU_MODEL_LANDAU) ? 1 : (ts > (double)1.e-9f ? 1 : 0);
+    double se = 0;
+    for (int m = 0; m < 6; ++m) se += (m < 3 ? 1.0 : 2.0) * hK.sig0[v][m] * p.e_mean[m];
+    hK.sig0_ebar[v] = se;
+  }
+  for (int v = 0; v < V; ++v)
+    for (int q = 0; q < V; ++q) {
+      double acc = 0;
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) acc += hK.eps_eng[v][i] * p.cela[1][i + j * 6] * hK.eps_eng[q][j];
+      hK.A[v][q] = acc;
+    }
+  for (int m = 0; m < 6; ++m) hK.ebar_eng[m] = (m < 3 ? 1.0 : 2.0) * p.e_mean[m];
+  if (p.model == MEU_MODEL_LANDAU && p.elastic == MEU_ELAST_HOMOG) {
+    for (int i = 0; i < 36; ++i)
+      if (std::fabs(p.cela[0][i] - p.cela[1][i]) > 1e-12 * (std::fabs(p.cela[1][i]) + 1e-300))
+        throw CudaError("MEU_ELAST_HOMOG needs equal matrix and precipitate moduli", MEU_ERR_BADARG);
+  }
+  if (p.model == MEU_MODEL_KKS && sizeof(R) != 8)
+    throw CudaError("the KKS model runs in plain FP64 only", MEU_ERR_UNSUPPORTED);
+  // ---- buffers
+  c = dalloc<R>(E * n3);
+  c2 = dalloc<R>(E * n3);
+  phi = dalloc<R>(V * n3);
+  pphi = dalloc<R>(V * n3);
+  fd = dalloc<R>(V * n3);
+  el_en = dalloc<R>(n3);
+  const bool elast = p.elastic != MEU_ELAST_NONE;
+  const bool het = (p.model == MEU_MODEL_KKS) || p.elastic == MEU_ELAST_HETERO;
+  if (p.model == MEU_MODEL_KKS) {
+    noise = dalloc<R>(V * n3);
+    fc = dalloc<R>(3 * E * n3);
+    NWR = 4 * V;
+    NS = std::max(5 * V, 4 * E);
+  } else {
+    NWR = 2 * V + 1;
+    NS = 2 * V + 2;
+  }
+  if (elast && het) {
+    strain = dalloc<R>(6 * n3);
+    xs = dalloc<R>(6 * n3);
+    uk = dalloc<C>(3 * nk);
+    NS = std::max(NS, V + 6);
+  }
+  NS = std::max(NS, 12);  // u_state download uses 12 spectra
+  NWR = std::max(NWR, 1);
+  wr = dalloc<R>((int64_t)NWR * n3);
+  sp = dalloc<C>((int64_t)NS * nk);
+  partials = dalloc<double>((int64_t)Q_TOTAL * RED_BLOCKS);
+  results = dalloc<double>(Q_TOTAL);
+  d_ops = dalloc<int>(Q_TOTAL);
+  d_err = dalloc<int>(1);
+  dK = dalloc<DevConst>(1);
+  MEU_CUDA(cudaHostAlloc((void**)&h_results, sizeof(double) * Q_TOTAL, cudaHostAllocDefault));
+  MEU_CUDA(cudaHostAlloc((void**)&h_err, sizeof(int), cudaHostAllocDefault));
+  int ops[Q_TOTAL];
+  for (int q = 0; q < Q_TOTAL; ++q) ops[q] = 0;
+  ops[Q_CMIN] = 2;
+  ops[Q_CMAX] = 1;
+  ops[Q_PHIMAX] = 1;
+  MEU_CUDA(cudaMemcpy(d_ops, ops, sizeof(ops), cudaMemcpyHostToDevice));
+  MEU_CUDA(cudaMemcpy(dK, &hK, sizeof(DevConst), cudaMemcpyHostToDevice));
+  MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+  MEU_CUDA(cudaMemset(c, 0, sizeof(R) * E * n3));
+  MEU_CUDA(cudaMemset(phi, 0, sizeof(R) * V * n3));
+  if (noise) MEU_CUDA(cudaMemset(noise, 0, sizeof(R) * V * n3));
+  MEU_CUDA(cudaMemset(el_en, 0, sizeof(R) * n3));
+  if (strain) MEU_CUDA(cudaMemset(strain, 0, sizeof(R) * 6 * n3));
+  if (uk) MEU_CUDA(cudaMemset(uk, 0, sizeof(C) * 3 * nk));
+  stage_elems = std::min<int64_t>(n3 * std::max(std::max(V, E), 1), (int64_t)32 << 20);
+  stage = dalloc<double>(stage_elems);
+}
+
+template <typename R>
+Engine<R>::~Engine() {
+  if (st) cudaStreamSynchronize(st);
+  for (void* q : allocs) cudaFree(q);
+  if (h_results) cudaFreeHost(h_results);
+  if (h_err) cudaFreeHost(h_err);
+  fft.reset();
+  if (st) cudaStreamDestroy(st);
+}
+
+template <typename R>
+void Engine<R>::check_err() {
+  MEU_CUDA(cudaMemcpyAsync(h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MEU_CUDA(cudaStreamSynchronize(st));
+  if (*h_err) {
+    int code = *h_err;
+    MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    throw CudaError("singular matrix in the step (reference err_flag " + std::to_string(code) + ")", code);
+  }
+}
+
+template <typename R>
+void Engine<R>::finalize(int q0, int nq) {
+  k_finalize<<<nq, 256, 0, st>>>(partials + (int64_t)q0 * RED_BLOCKS, RED_BLOCKS, d_ops + q0, results + q0);
+  MEU_CHECK_LAUNCH();
+}
+
+// ---- host-side AoS conversion in chunks through the staging buffer
+template <typename R>
+void Engine<R>::set_fields(const double* cons, const double* phi_in, const double* ustate) {
+  auto up = [&](const double* src, R* dst, int ncomp, int add) {
+    const int64_t chunk = std::max<int64_t>(stage_elems / ncomp, 1);
+    for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+      const int64_t nv = std::min(chunk, n3 - v0);
+      MEU_CUDA(cudaMemcpyAsync(stage, src + v0 * ncomp, sizeof(double) * nv * ncomp, cudaMemcpyHostToDevice, st));
+      k_aos_to_soa<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(stage, dst, ncomp, v0, nv, n3, add);
+      MEU_CHECK_LAUNCH();
+    }
+  };
+  if (cons) up(cons, c, E, 0);
+  if (phi_in) up(phi_in, phi, V, 0);
+  // conserved mean per solute (k = 0 mode), FP64
+  if (cons) {
+    for (int e = 0; e < E; ++e) {
+      long double s = 0;
+      for (int64_t i = 0; i < n3; ++i) s += cons[i * E + e];
+      hK.c_mean[e] = (double)(s / (long double)n3);
+    }
+    MEU_CUDA(cudaMemcpyAsync(dK, &hK, sizeof(DevConst), cudaMemcpyHostToDevice, st));
+  }
+  if (strain) {
+    if (ustate) {
+      // u (3 x n3) -> u^ ; grads (9 x n3) -> engineering strain
+      for (int i = 0; i < 3; ++i) {
+        const int64_t chunk = stage_elems;
+        for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+          const int64_t nv = std::min(chunk, n3 - v0);
+          MEU_CUDA(cudaMemcpyAsync(stage, ustate + i * n3 + v0, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+          k_convert_in<R><<<grid_for(nv, 256), 256, 0, st>>>(stage, wr + v0, nv);
+          MEU_CHECK_LAUNCH();
+        }
+        PtrList<const R> a{};
+        PtrList<C> b{};
+        a.p[0] = wr;
+        b.p[0] = uk + (int64_t)i * nk;
+        fft->forward<R>(a, b, 1, st);
+      }
+      // the 9 gradients, chunked through the staging buffer
+      const int64_t chunk = std::max<int64_t>(stage_elems / 9, 1);
+      for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+        const int64_t nv = std::min(chunk, n3 - v0);
+        for (int g = 0; g < 9; ++g)
+          MEU_CUDA(cudaMemcpyAsync(stage + (int64_t)g * nv, ustate + (int64_t)(3 + g) * n3 + v0, sizeof(double) * nv,
+                                   cudaMemcpyHostToDevice, st));
+        k_grads_to_strain<R><<<grid_for(nv, 256), 256, 0, st>>>(stage, strain + v0, nv, n3);
+        MEU_CHECK_LAUNCH();
+      }
+      el_ready = true;
+    } else {
+      MEU_CUDA(cudaMemsetAsync(strain, 0, sizeof(R) * 6 * n3, st));
+      MEU_CUDA(cudaMemsetAsync(uk, 0, sizeof(C) * 3 * nk, st));
+      el_ready = false;
+    }
+  }
+  MEU_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename R>
+void Engine<R>::add_noise(const double* incr) {
+  if (!noise) return;
+  const int64_t chunk = std::max<int64_t>(stage_elems / V, 1);
+  for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+    const int64_t nv = std::min(chunk, n3 - v0);
+    MEU_CUDA(cudaMemcpyAsync(stage, incr + v0 * V, sizeof(double) * nv * V, cudaMemcpyHostToDevice, st));
+    k_aos_to_soa<R><<<grid_for(nv * V, 256), 256, 0, st>>>(stage, noise, V, v0, nv, n3, 1);
+    MEU_CHECK_LAUNCH();
+  }
+  MEU_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename R>
+void Engine<R>::get_fields(double* cons, double* phi_out, double* el_out, double* ustate) {
+  auto down = [&](const R* src, double* dst, int ncomp) {
+    const int64_t chunk = std::max<int64_t>(stage_elems / ncomp, 1);
+    for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+      const int64_t nv = std::min(chunk, n3 - v0);
+      k_soa_to_aos<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(src, stage, ncomp, v0, nv, n3);
+      MEU_CHECK_LAUNCH();
+      MEU_CUDA(cudaMemcpyAsync(dst + v0 * ncomp, stage, sizeof(double) * nv * ncomp, cudaMemcpyDeviceToHost, st));
+    }
+  };
+  if (cons) down(c, cons, E);
+  if (phi_out) down(phi, phi_out, V);
+  if (el_out) down(el_en, el_out, 1);
+  if (ustate) {
+    if (uk) {
+      k_u_spectra<R><<<gridk(), 256, 0, st>>>(dK, uk, specs(0, 12));
+      MEU_CHECK_LAUNCH();
+      for (int f = 0; f < 12; ++f) {
+        PtrList<C> a{};
+        PtrList<R> b{};
+        a.p[0] = spec(f);
+        b.p[0] = wr;
+        fft->inverse<R>(a, b, 1, st);
+        down(wr, ustate + (int64_t)f * n3, 1);
+      }
+    } else {
+      memset(ustate, 0, sizeof(double) * 12 * n3);
+    }
+  }
+  MEU_CUDA(cudaStreamSynchronize(st));
+}
+
+// ---------------------------------------------------------------- elasticity
+// eldis (ModElastic.f:11-489) + elener (:493-691).  P_phi in pphi.
+template <typename R>
+void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only) {
+  const bool first = zeroth_only || step == P.elastep0 || !el_ready;
+  // the reference computes the zeroth order only at step == elastep0; a run that
+  // enters later without an uploaded state starts from u = 0 like the reference.
+  const bool do_zeroth = zeroth_only || step == P.elastep0;
+  (void)first;
+  if (do_zeroth) {
+    std::vector<const R*> in;
+    for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
+    fwd_list(in, 0);
+    k_el_zeroth<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, uk, specs(V, 6), d_err);
+    MEU_CHECK_LAUNCH();
+    std::vector<R*> out;
+    for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
+    inv_list(V, out);
+  }
+  el_ready = true;
+  int total = 0;
+  if (!zeroth_only) {
+    double newfac = 0.5, cfac = 1.0, err_old[6] = {0, 0, 0, 0, 0, 0};
+    int niter = 0;
+    bool converged = false;
+    for (;;) {
+      niter += 1;
+      total += 1;
+      if (total > 100000) throw CudaError("elastic iteration runaway", MEU_ERR_NOT_CONVERGED);
+      k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err);
+      MEU_CHECK_LAUNCH();
+      std::vector<const R*> in;
+      for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
+      fwd_list(in, 0);
+      k_el_k<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 6), uk, partials, d_err);
+      MEU_CHECK_LAUNCH();
+      std::vector<R*> out;
+      for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
+      inv_list(0, out);
+      finalize(Q_ERR0, 6);
+      MEU_CUDA(cudaMemcpyAsync(h_results + Q_ERR0, results + Q_ERR0, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
+      check_err();  // synchronises
+      double err[6];
+      for (int q = 0; q < 6; ++q) err[q] = h_results[Q_ERR0 + q] * (double)n3;
+      const double tol = P.el_tol;
+      if (err[0] / err[1] < tol && err[2] / err[3] < tol && err[4] / err[5] < tol) converged = true;
+      if (niter > 1 && !converged) {
+        if (err[0] / err[1] > err_old[0] / err_old[1] || err[2] / err[3] > err_old[2] / err_old[3] ||
+            err[4] / err[5] > err_old[4] / err_old[5]) {
+          cfac = cfac * newfac;
+          newfac = newfac * 0.5;
+          if (newfac < 1e-7) throw CudaError("newfac is too small ... trouble converging", MEU_ERR_NOT_CONVERGED);
+          niter = 0;
+          converged = false;
+          continue;
+        }
+      }
+      memcpy(err_old, err, sizeof(err));
+      if (niter == P.el_max_iter) converged = true;
+      if (!converged || niter < P.el_min_iter) continue;
+      if (cfac < 1.0 - 1e-6) {
+        cfac = cfac + 0.1;
+        if (cfac > 1.0) cfac = 1.0;
+        niter = 0;
+        converged = false;
+        continue;
+      }
+      break;
+    }
+  }
+  last_iters = total;
+  k_elener<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+                                                  (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
+                                                  partials, d_err);
+  MEU_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------------- KKS step
+template <typename R>
+void Engine<R>::kks_step(meu_diag* d) {
+  MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * RED_BLOCKS, st));
+  if (!(step <= P.noise_step)) MEU_CUDA(cudaMemsetAsync(noise, 0, sizeof(R) * V * n3, st));
+  // spectral gradients (:575-615)
+  {
+    std::vector<const R*> in;
+    for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
+    fwd_list(in, 0);
+    k_kks_grad<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), specs(V, 4 * V), V);
+    MEU_CHECK_LAUNCH();
+    std::vector<R*> out;
+    for (int f = 0; f < 4 * V; ++f) out.push_back(field(wr, f));
+    inv_list(V, out);
+  }
+  // local driving force (:619-845)
+  k_kks_point<<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, (const double*)phi, (const double*)c, (const double*)wr,
+                                                  (double*)pphi, (double*)fd, (double*)fc, partials, d_err);
+  MEU_CHECK_LAUNCH();
+  // elasticity (:851-880)
+  last_iters = 0;
+  if (step >= P.elastep0 && P.elastic != MEU_ELAST_NONE) {
+    elastic(phi, fd, 0, false);
+  } else {
+    MEU_CUDA(cudaMemsetAsync(el_en, 0, sizeof(R) * n3, st));
+  }
+  // diffusion (:910-949)
+  for (int e = 0; e < E; ++e) {
+    fwd({field(c, e), field(fc, 3 * e), field(fc, 3 * e + 1), field(fc, 3 * e + 2)}, 0);
+    k_kks_ch<R><<<gridk(), 256, 0, st>>>(dK, spec(0), spec(1), spec(2), spec(3), P.dt * P.cmobs[e]);
+    MEU_CHECK_LAUNCH();
+    inv_list(0, {field(c, e)});
+  }
+  // TDGL (:955-1001)
+  k_tdgl_pre<R><<<grid_for((int64_t)V * n3, 256), 256, 0, st>>>(phi, fd, noise, wr, (int64_t)V * n3, P.dt * P.b_mob, P.dt);
+  MEU_CHECK_LAUNCH();
+  {
+    std::vector<const R*> in;
+    for (int v = 0; v < V; ++v) in.push_back(field(wr, v));
+    fwd_list(in, 0);
+    k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob);
+    MEU_CHECK_LAUNCH();
+    std::vector<R*> out;
+    for (int v = 0; v < V; ++v) out.push_back(field(phi, v));
+    inv_list(0, out);
+  }
+  end_step(d, 1);
+}
+
+// ---------------------------------------------------------------- Landau step
+template <typename R>
+void Engine<R>::landau_step(meu_diag* d) {
+  MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * RED_BLOCKS, st));
+  const bool elast = P.elastic != MEU_ELAST_NONE && step >= P.elastep0;
+  const bool homog = elast && P.elastic == MEU_ELAST_HOMOG;
+  const bool het = elast && P.elastic == MEU_ELAST_HETERO;
+  R* mu = field(wr, 0);
+  k_lan_a<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, pphi, mu, partials);
+  MEU_CHECK_LAUNCH();
+  // [theta_v, mu, c, eta_v]
+  {
+    std::vector<const R*> in;
+    for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
+    in.push_back(mu);
+    in.push_back(c);
+    for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
+    fwd_list(in, 0);
+  }
+  k_lan_k1<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 2 * V + 2), V, homog ? 1 : 0, P.diag_energy, partials, d_err);
+  MEU_CHECK_LAUNCH();
+  R* phel = field(wr, 1);  // V fields: strain interaction (homog) or el_grad (hetero)
+  {
+    std::vector<R*> out;
+    if (homog) {
+      for (int v = 0; v < V; ++v) out.push_back(field(phel, v));
+      out.push_back(c2);
+      // spectra 0..V-1 then V+1: move c^ next to them
+      MEU_CUDA(cudaMemcpyAsync(spec(V), spec(V + 1), sizeof(C) * nk, cudaMemcpyDeviceToDevice, st));
+      inv_list(0, out);
+    } else {
+      inv_list(V + 1, {c2});
+    }
+  }
+  last_iters = 0;
+  if (het) {
+    // P_phi = theta (already in pphi), elener gives el_grad into phel
+    elastic(phi, phel, 1, false);
+  } else if (!homog) {
+    MEU_CUDA(cudaMemsetAsync(el_en, 0, sizeof(R) * n3, st));
+  }
+  k_lan_b<R><<<gridr(), 256, 0, st>>>(dK, c, phi, elast ? phel : nullptr, homog ? 1 : 0, pphi);
+  MEU_CHECK_LAUNCH();
+  {
+    std::vector<const R*> in;
+    for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
+    fwd_list(in, 0);
+    k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob);
+    MEU_CHECK_LAUNCH();
+    std::vector<R*> out;
+    for (int v = 0; v < V; ++v) out.push_back(field(phi, v));
+    inv_list(0, out);
+  }
+  std::swap(c, c2);
+  end_step(d, P.clip_phi);
+}
+
+template <typename R>
+void Engine<R>::end_step(meu_diag* d, int clip) {
+  k_stats<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, clip, partials);
+  MEU_CHECK_LAUNCH();
+  finalize(0, Q_STEP_COUNT);
+  MEU_CUDA(cudaMemcpyAsync(h_results, results, sizeof(double) * Q_STEP_COUNT, cudaMemcpyDeviceToHost, st));
+  if (d) {
+    check_err();
+    const double* r = h_results;
+    const double sn3 = (double)n3;
+    d->step = step;
+    d->el_iters = last_iters;
+    d->status = 0;
+    const bool lan = P.model == MEU_MODEL_LANDAU;
+    d->fint = lan ? r[Q_FINT] * sn3 : r[Q_FINT];
+    d->fw = r[Q_FW];
+    d->fch = r[Q_FCH];
+    d->elen = (lan && P.elastic == MEU_ELAST_HOMOG) ? r[Q_ELEN] * sn3 : r[Q_ELEN];
+    d->etot = d->fint + d->fch + d->elen + d->fw;
+    d->glob_min = prev_min;
+    d->glob_max = prev_max;
+    d->phi_max = prev_phimax;
+    d->solid = prev_solid / sn3;
+    d->cmin = r[Q_CMIN];
+    d->cmax = r[Q_CMAX];
+    d->phimax = r[Q_PHIMAX];
+    d->solid_now = r[Q_SOLID] / sn3;
+    for (int e = 0; e < MEU_MAX_EL; ++e) d->cavg[e] = e < E ? r[Q_CSUM0 + e] / sn3 : 0.0;
+    prev_min = r[Q_CMIN];
+    prev_max = r[Q_CMAX];
+    prev_phimax = r[Q_PHIMAX];
+    prev_solid = r[Q_SOLID];
+    if (!std::isfinite(d->etot) || !std::isfinite(d->cavg[0]))
+      throw CudaError("non-finite field values", MEU_ERR_NOT_FINITE);
+  }
+  step += 1;
+}
+
+template <typename R>
+void Engine<R>::run(int nsteps, meu_diag* diag) {
+  for (int i = 0; i < nsteps; ++i) {
+    meu_diag* d = diag ? diag + i : nullptr;
+    if (P.model == MEU_MODEL_KKS) kks_step(d);
+    else landau_step(d);
+  }
+  check_err();
+  if (!diag && nsteps > 0) {
+    const double* r = h_results;
+    prev_min = r[Q_CMIN];
+    prev_max = r[Q_CMAX];
+    prev_phimax = r[Q_PHIMAX];
+    prev_solid = r[Q_SOLID];
+  }
+}
+
+template class Engine<double>;
+template class Engine<float>;
+
+}  // namespace meu
+
+// =============================================================== C-ABI
+struct meu_handle {
+  std::unique_ptr<meu::EngineBase> eng;
+  std::string err;
+};
+
+static int fail(meu_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define MEU_TRY(h, body)                                              \
+  try {                                                               \
+    body;                                                             \
+  } catch (const meu::CudaError& e) {                                 \
+    return fail(h, e.code, e.what());                                 \
+  } catch (const std::bad_alloc&) {                                   \
+    return fail(h, MEU_ERR_NOMEM, "host allocation failed");          \
+  } catch (const std::exception& e) {                                 \
+    return fail(h, MEU_ERR_CUDA, e.what());                           \
+  }
+
+extern "C" {
+
+static thread_local std::string g_create_err;
+
+int meu_create(const meu_params* params, meu_handle** out) {
+  if (!params || !out) return MEU_ERR_BADARG;
+  *out = nullptr;
+  meu_handle* h = new (std::nothrow) meu_handle();
+  if (!h) return MEU_ERR_NOMEM;
+  try {
+    if (params->precision == MEU_PREC_F64) h->eng.reset(new meu::Engine<double>(*params));
+    else if (params->precision == MEU_PREC_F32) h->eng.reset(new meu::Engine<float>(*params));
+    else throw meu::CudaError("unknown precision", MEU_ERR_BADARG);
+  } catch (const meu::CudaError& e) {
+    g_create_err = e.what();
+    delete h;
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_err = e.what();
+    delete h;
+    return MEU_ERR_CUDA;
+  }
+  *out = h;
+  return MEU_OK;
+}
+
+int meu_set_fields(meu_handle* h, const double* cons, const double* phi, const double* u_state) {
+  if (!h) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->set_fields(cons, phi, u_state));
+  return MEU_OK;
+}
+
+int meu_add_noise(meu_handle* h, const double* incr) {
+  if (!h || !incr) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->add_noise(incr));
+  return MEU_OK;
+}
+
+int meu_run(meu_handle* h, int32_t nsteps, meu_diag* diag) {
+  if (!h || nsteps < 0) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->run(nsteps, diag));
+  return MEU_OK;
+}
+
+int meu_get_fields(meu_handle* h, double* cons, double* phi, double* el_en, double* u_state) {
+  if (!h) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->get_fields(cons, phi, el_en, u_state));
+  return MEU_OK;
+}
+
+int64_t meu_get_step(const meu_handle* h) { return h ? h->eng->step : -1; }
+
+const char* meu_last_error(const meu_handle* h) {
+  if (!h) return g_create_err.c_str();
+  return h->err.c_str();
+}
+
+int meu_destroy(meu_handle* h) {
+  if (!h) return MEU_ERR_BADARG;
+  delete h;
+  return MEU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------- diagnostics
+extern "C" int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t precision, const double* in,
+                                 double* spec_out, double* back_out) {
+  using namespace meu;
+  try {
+    if (!fft_size_ok(nx, true) || !fft_size_ok(ny, false) || !fft_size_ok(nz, false)) return MEU_ERR_UNSUPPORTED;
+    const bool f64 = precision == MEU_PREC_F64;
+    FFT3 f(nx, ny, nz, f64);
+    const int64_t n3 = f.n3(), nk = f.nk();
+    double* d_in = nullptr;
+    double* d_spec = nullptr;
+    MEU_CUDA(cudaMalloc(&d_in, sizeof(double) * n3));
+    MEU_CUDA(cudaMalloc(&d_spec, sizeof(double) * 2 * nk));
+    MEU_CUDA(cudaMemcpy(d_in, in, sizeof(double) * n3, cudaMemcpyHostToDevice));
+    cudaStream_t st = 0;
+    if (f64) {
+      PtrList<const double> a{};
+      PtrList<double2> b{};
+      a.p[0] = d_in;
+      b.p[0] = (double2*)d_spec;
+      f.forward<double>(a, b, 1, st);
+      MEU_CUDA(cudaMemcpy(spec_out, d_spec, sizeof(double) * 2 * nk, cudaMemcpyDeviceToHost));
+      PtrList<double2> c{};
+      PtrList<double> d{};
+      c.p[0] = (double2*)d_spec;
+      d.p[0] = d_in;
+      f.inverse<double>(c, d, 1, st);
+      MEU_CUDA(cudaMemcpy(back_out, d_in, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+    } else {
+      float* fin = nullptr;
+      float2* fsp = nullptr;
+      MEU_CUDA(cudaMalloc(&fin, sizeof(float) * n3));
+      MEU_CUDA(cudaMalloc(&fsp, sizeof(float2) * nk));
+      k_convert_in<float><<<grid_for(n3, 256), 256>>>(d_in, fin, n3);
+      PtrList<const float> a{};
+      PtrList<float2> b{};
+      a.p[0] = fin;
+      b.p[0] = fsp;
+      f.forward<float>(a, b, 1, st);
+      k_convert<float><<<grid_for(2 * nk, 256), 256>>>((const float*)fsp, d_spec, 2 * nk);
+      MEU_CUDA(cudaMemcpy(spec_out, d_spec, sizeof(double) * 2 * nk, cudaMemcpyDeviceToHost));
+      PtrList<float2> c{};
+      PtrList<float> d{};
+      c.p[0] = fsp;
+      d.p[0] = fin;
+      f.inverse<float>(c, d, 1, st);
+      k_convert<float><<<grid_for(n3, 256), 256>>>(fin, d_in, n3);
+      MEU_CUDA(cudaMemcpy(back_out, d_in, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+      cudaFree(fin);
+      cudaFree(fsp);
+    }
+    cudaFree(d_in);
+    cudaFree(d_spec);
+    MEU_CUDA(cudaDeviceSynchronize());
+  } catch (const CudaError& e) {
+    return e.code;
+  }
+  return MEU_OK;
+}

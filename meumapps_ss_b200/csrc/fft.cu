@@ -1,0 +1,334 @@
+// fft.cu -- batched 3-D R2C / C2R transforms (see fft.cuh).
+#include <cmath>
+#include <vector>
+
+#include "fft.cuh"
+
+namespace meu {
+
+static bool factor_23(int n, std::vector<int>& r) {
+  r.clear();
+  while (n % 8 == 0 && n > 8) { r.push_back(8); n /= 8; }
+  if (n % 8 == 0) { r.push_back(8); n /= 8; }
+  if (n % 4 == 0) { r.push_back(4); n /= 4; }
+  if (n % 2 == 0) { r.push_back(2); n /= 2; }
+  while (n % 3 == 0) { r.push_back(3); n /= 3; }
+  return n == 1;
+}
+
+bool fft_size_ok(int n, bool is_x) {
+  std::vector<int> r;
+  if (is_x) return n >= 4 && n % 2 == 0 && n <= 2048 && factor_23(n / 2, r);
+  return n >= 2 && n <= 1024 && factor_23(n, r);
+}
+
+// digit-reversal map of the DIF stage order (position p -> frequency k)
+static std::vector<int> rev_table(int L, const std::vector<int>& rad) {
+  std::vector<int> out(L);
+  std::vector<int> m(rad.size());
+  int span = L;
+  for (size_t s = 0; s < rad.size(); ++s) { span /= rad[s]; m[s] = span; }
+  for (int k = 0; k < L; ++k) {
+    // k = q0 + R0*(q1 + R1*(q2 + ...)) ; p = sum q_s * m_s
+    int kk = k, p = 0;
+    for (size_t s = 0; s < rad.size(); ++s) {
+      int q = kk % rad[s];
+      kk /= rad[s];
+      p += q * m[s];
+    }
+    out[p] = k;
+  }
+  return out;
+}
+
+// exp(-2 pi i n / L) with long-double argument reduction; exact at multiples of L/4
+static void twiddle(int n, int L, long double& c, long double& s) {
+  n %= L;
+  if (4 * n % L == 0) {
+    int q = 4 * n / L;
+    c = (q == 0) ? 1 : (q == 2) ? -1 : 0;
+    s = (q == 1) ? -1 : (q == 3) ? 1 : 0;
+    return;
+  }
+  const long double pi = 3.141592653589793238462643383279502884L;
+  long double a = -2.0L * pi * (long double)n / (long double)L;
+  c = cosl(a);
+  s = sinl(a);
+}
+
+FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_) : nx(nx_), ny(ny_), nz(nz_), nxh(nx_ / 2 + 1), fp64(fp64_) {
+  std::vector<int> rx, ry, rz;
+  if (!(nx % 2 == 0 && factor_23(nx / 2, rx) && factor_23(ny, ry) && factor_23(nz, rz)))
+    throw CudaError("grid sizes must be 2^a 3^b (Nx even)", 100);
+  const int Lx = nx / 2;
+  auto rvx = rev_table(Lx, rx), rvy = rev_table(ny, ry), rvz = rev_table(nz, rz);
+  const size_t csz = fp64 ? sizeof(double2) : sizeof(float2);
+  // layout: twx[Lx] twy[ny] twz[nz] post[nxh] | revx revy revz
+  size_t ntw = (size_t)Lx + ny + nz + nxh;
+  size_t bytes_tw = ntw * csz;
+  size_t bytes = bytes_tw + sizeof(int) * ((size_t)Lx + ny + nz) + 256;
+  std::vector<unsigned char> host(bytes, 0);
+  auto put = [&](size_t idx, long double c, long double s) {
+    if (fp64) {
+      double2 v = make_double2((double)c, (double)s);
+      memcpy(host.data() + idx * csz, &v, csz);
+    } else {
+      float2 v = make_float2((float)(double)c, (float)(double)s);
+      memcpy(host.data() + idx * csz, &v, csz);
+    }
+  };
+  size_t off = 0;
+  long double c, s;
+  for (int n = 0; n < Lx; ++n) { twiddle(n, Lx, c, s); put(off + n, c, s); }
+  off += Lx;
+  for (int n = 0; n < ny; ++n) { twiddle(n, ny, c, s); put(off + n, c, s); }
+  off += ny;
+  for (int n = 0; n < nz; ++n) { twiddle(n, nz, c, s); put(off + n, c, s); }
+  off += nz;
+  for (int n = 0; n < nxh; ++n) { twiddle(n, nx, c, s); put(off + n, c, s); }
+  int* ri = (int*)(host.data() + bytes_tw);
+  memcpy(ri, rvx.data(), sizeof(int) * Lx);
+  memcpy(ri + Lx, rvy.data(), sizeof(int) * ny);
+  memcpy(ri + Lx + ny, rvz.data(), sizeof(int) * nz);
+  MEU_CUDA(cudaMalloc(&dev_mem, bytes));
+  MEU_CUDA(cudaMemcpy(dev_mem, host.data(), bytes, cudaMemcpyHostToDevice));
+  unsigned char* d = (unsigned char*)dev_mem;
+  const int* dr = (const int*)(d + bytes_tw);
+  auto fill = [](LinePlan& p, int L, const std::vector<int>& r, const void* tw, const int* rev) {
+    p.L = L;
+    p.ns = (int)r.size();
+    for (int i = 0; i < 12; ++i) p.r[i] = i < (int)r.size() ? r[i] : 1;
+    p.tw = tw;
+    p.rev = rev;
+  };
+  fill(px, Lx, rx, d, dr);
+  fill(py, ny, ry, d + (size_t)Lx * csz, dr + Lx);
+  fill(pz, nz, rz, d + (size_t)(Lx + ny) * csz, dr + Lx + ny);
+  post_tw = d + (size_t)(Lx + ny + nz) * csz;
+}
+
+FFT3::~FFT3() {
+  if (dev_mem) cudaFree(dev_mem);
+}
+
+// ------------------------------------------------------------------ kernels
+__host__ __device__ inline int odd_pitch(int L) { return (L & 1) ? L : L + 1; }
+__host__ __device__ inline int rows_per_block(int L) {
+  int r = 2048 / L;
+  return r < 1 ? 1 : (r > 64 ? 64 : r);
+}
+
+// x transform: rows of nx reals -> rows of nx/2+1 complex (unscaled)
+template <typename R>
+__global__ void __launch_bounds__(256) k_rows_r2c(PtrList<const R> in, PtrList<cplx<R>> out, int nx, int64_t nrows,
+                                                  LinePlan pl, const cplx<R>* __restrict__ post) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  const int L = pl.L, pitch = odd_pitch(L), nxh = L + 1;
+  const int rpb = rows_per_block(L);
+  const int64_t row0 = (int64_t)blockIdx.x * rpb;
+  const int nr = (int)min((int64_t)rpb, nrows - row0);
+  const R* src = in.p[blockIdx.y] + row0 * nx;
+  C* dst = out.p[blockIdx.y] + row0 * nxh;
+  for (int i = threadIdx.x; i < nr * L; i += blockDim.x) {
+    int r = i / L, n = i - r * L;
+    buf[r * pitch + n] = ((const C*)(src + (int64_t)r * nx))[n];
+  }
+  __syncthreads();
+  fft_dif(buf, pl, nr, pitch, 1);
+  // split: X[k] = E + W^k O with E = (Z[k] + conj Z[L-k])/2, O = -i (Z[k] - conj Z[L-k])/2
+  const int* rev = pl.rev;
+  const int npair = L / 2 + 1;
+  __shared__ int posk[1024];
+  for (int i = threadIdx.x; i < L; i += blockDim.x) posk[rev[i]] = i;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nr * npair; i += blockDim.x) {
+    int r = i / npair, k = i - r * npair;
+    int k2 = (L - k) % L;
+    C zk = buf[r * pitch + posk[k % L]], zm = buf[r * pitch + posk[k2]];
+    C* drow = dst + (int64_t)r * nxh;
+    {
+      C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
+      C o = cscale(csub(zk, cconj(zm)), (R)0.5);
+      o = mk(o.y, -o.x);
+      drow[k] = cadd(e, cmul(post[k], o));
+    }
+    if (k != L - k) {
+      C e = cscale(cadd(zm, cconj(zk)), (R)0.5);
+      C o = cscale(csub(zm, cconj(zk)), (R)0.5);
+      o = mk(o.y, -o.x);
+      drow[L - k] = cadd(e, cmul(post[L - k], o));
+    }
+  }
+}
+
+// x inverse: rows of nx/2+1 complex -> rows of nx reals (unscaled c2r)
+template <typename R>
+__global__ void __launch_bounds__(256) k_rows_c2r(PtrList<const cplx<R>> in, PtrList<R> out, int nx, int64_t nrows,
+                                                  LinePlan pl, const cplx<R>* __restrict__ post) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  const int L = pl.L, pitch = odd_pitch(L), nxh = L + 1;
+  const int rpb = rows_per_block(L);
+  const int64_t row0 = (int64_t)blockIdx.x * rpb;
+  const int nr = (int)min((int64_t)rpb, nrows - row0);
+  const C* src = in.p[blockIdx.y] + row0 * nxh;
+  R* dst = out.p[blockIdx.y] + row0 * nx;
+  __shared__ int posk[1024];
+  for (int i = threadIdx.x; i < L; i += blockDim.x) posk[pl.rev[i]] = i;
+  __syncthreads();
+  const int npair = L / 2 + 1;
+  for (int i = threadIdx.x; i < nr * npair; i += blockDim.x) {
+    int r = i / npair, k = i - r * npair;
+    const C* srow = src + (int64_t)r * nxh;
+    C xk = srow[k], xm = srow[L - k];
+    if (k == 0) { xk.y = 0; xm.y = 0; }
+    // Z[k] = (X[k] + conj X[L-k]) + i (X[k] - conj X[L-k]) W^-k
+    {
+      C ex = cadd(xk, cconj(xm));
+      C ox = cmulc(csub(xk, cconj(xm)), post[k]);
+      buf[r * pitch + posk[k % L]] = cadd(ex, mk(-ox.y, ox.x));
+    }
+    if (k != 0 && k != L - k) {
+      C ex = cadd(xm, cconj(xk));
+      C ox = cmulc(csub(xm, cconj(xk)), post[L - k]);
+      buf[r * pitch + posk[L - k]] = cadd(ex, mk(-ox.y, ox.x));
+    }
+  }
+  __syncthreads();
+  fft_dit(buf, pl, nr, pitch, 1);
+  for (int i = threadIdx.x; i < nr * L; i += blockDim.x) {
+    int r = i / L, n = i - r * L;
+    ((C*)(dst + (int64_t)r * nx))[n] = buf[r * pitch + n];
+  }
+}
+
+// strided columns: element l of column (o, c) at base + o*ostride + l*inner + c.
+// FWD: natural in -> natural out (DIF + reversed store), scaled.
+// INV: natural in -> natural out (reversed load + DIT).
+template <typename R, bool FWD>
+__global__ void __launch_bounds__(256) k_cols(PtrList<cplx<R>> in, PtrList<cplx<R>> out, int inner, int64_t ostride,
+                                              int tm, LinePlan pl, R scale) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  const int L = pl.L;
+  const int tiles = (inner + tm - 1) / tm;
+  const int o = blockIdx.x / tiles, t = blockIdx.x - o * tiles;
+  const int c0 = t * tm, nc = min(tm, inner - c0);
+  const C* src = in.p[blockIdx.y] + (int64_t)o * ostride + c0;
+  C* dst = out.p[blockIdx.y] + (int64_t)o * ostride + c0;
+  const int* rev = pl.rev;
+  for (int i = threadIdx.x; i < L * nc; i += blockDim.x) {
+    int l = i / nc, c = i - l * nc;
+    int gl = FWD ? l : rev[l];
+    buf[l * tm + c] = src[(int64_t)gl * inner + c];
+  }
+  __syncthreads();
+  if (FWD) fft_dif(buf, pl, nc, 1, tm);
+  else fft_dit(buf, pl, nc, 1, tm);
+  for (int i = threadIdx.x; i < L * nc; i += blockDim.x) {
+    int l = i / nc, c = i - l * nc;
+    int gl = FWD ? rev[l] : l;
+    C v = buf[l * tm + c];
+    if (FWD) v = cscale(v, scale);
+    dst[(int64_t)gl * inner + c] = v;
+  }
+}
+
+// Raise a kernel's dynamic shared-memory limit to the opt-in maximum once
+// (227 KB per block on sm_100 minus the kernel's static shared memory).
+template <typename R>
+static void set_smem(const void* fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static thread_local std::vector<const void*> done;
+  for (const void* f : done)
+    if (f == fn) return;
+  int dev = 0, optin = 0;
+  MEU_CUDA(cudaGetDevice(&dev));
+  MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  MEU_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const int lim = optin - (int)fa.sharedSizeBytes;
+  if ((int)bytes > lim) throw CudaError("transform tile exceeds shared memory", 103);
+  MEU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  done.push_back(fn);
+}
+
+static inline int col_tile(int L, bool fp64) {
+  if (fp64) return L >= 256 ? 8 : 16;
+  return 16;
+}
+
+template <typename R>
+void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const {
+  using C = cplx<R>;
+  const int Lx = px.L;
+  const int64_t nrows = (int64_t)ny * nz;
+  const int rpb = rows_per_block(Lx);
+  size_t sm = (size_t)rpb * odd_pitch(Lx) * sizeof(C);
+  set_smem<R>((const void*)k_rows_r2c<R>, sm);
+  dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
+  k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw);
+  MEU_CHECK_LAUNCH();
+  // y columns: outer = z, inner = nxh
+  {
+    int tm = col_tile(ny, sizeof(R) == 8);
+    size_t s2 = (size_t)ny * tm * sizeof(C);
+    set_smem<R>((const void*)k_cols<R, true>, s2);
+    dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
+    k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1);
+    MEU_CHECK_LAUNCH();
+  }
+  // z columns: outer = 1, inner = ny*nxh
+  {
+    int tm = col_tile(nz, sizeof(R) == 8);
+    size_t s3 = (size_t)nz * tm * sizeof(C);
+    set_smem<R>((const void*)k_cols<R, true>, s3);
+    int inner = ny * nxh;
+    dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
+    k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, (R)(1.0 / ((double)nx * ny * nz)));
+    MEU_CHECK_LAUNCH();
+  }
+}
+
+template <typename R>
+void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const {
+  using C = cplx<R>;
+  {
+    int tm = col_tile(nz, sizeof(R) == 8);
+    size_t s3 = (size_t)nz * tm * sizeof(C);
+    set_smem<R>((const void*)k_cols<R, false>, s3);
+    int inner = ny * nxh;
+    dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
+    k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    int tm = col_tile(ny, sizeof(R) == 8);
+    size_t s2 = (size_t)ny * tm * sizeof(C);
+    set_smem<R>((const void*)k_cols<R, false>, s2);
+    dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
+    k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1);
+    MEU_CHECK_LAUNCH();
+  }
+  const int Lx = px.L;
+  const int64_t nrows = (int64_t)ny * nz;
+  const int rpb = rows_per_block(Lx);
+  size_t sm = (size_t)rpb * odd_pitch(Lx) * sizeof(C);
+  set_smem<R>((const void*)k_rows_c2r<R>, sm);
+  PtrList<const C> cin;
+  for (int f = 0; f < MAXF; ++f) cin.p[f] = in.p[f];
+  dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
+  k_rows_c2r<R><<<g, 256, sm, st>>>(cin, out, nx, nrows, px, (const C*)post_tw);
+  MEU_CHECK_LAUNCH();
+}
+
+template void FFT3::forward<float>(const PtrList<const float>&, const PtrList<float2>&, int, cudaStream_t) const;
+template void FFT3::forward<double>(const PtrList<const double>&, const PtrList<double2>&, int, cudaStream_t) const;
+template void FFT3::inverse<float>(const PtrList<float2>&, const PtrList<float>&, int, cudaStream_t) const;
+template void FFT3::inverse<double>(const PtrList<double2>&, const PtrList<double>&, int, cudaStream_t) const;
+
+}  // namespace meu

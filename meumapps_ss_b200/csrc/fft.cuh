@@ -1,0 +1,191 @@
+// fft.cuh -- shared-memory batched 3-D real FFT for sm_100a.
+//
+// Replaces the P3DFFT calls of the reference's f_trans / inv_trans
+// (ModFunc.f:15-40): forward = R2C scaled by 1/(Nx Ny Nz), inverse = C2R
+// unscaled.  The spectrum is stored [z][y][kx] with kx in [0, Nx/2].
+//
+// Each 1-D transform runs in shared memory as in-place mixed-radix stages
+// (radix 8/4/2/3).  Forward = decimation in frequency (natural order in,
+// digit-reversed order out); inverse = decimation in time (digit-reversed in,
+// natural out).  The digit reversal is folded into the global-memory
+// addressing of the load/store, so no permutation pass exists.  The x
+// transform of N reals is a complex transform of length N/2 plus a split
+// step; the C2R split discards Im X(0) and Im X(N/2) like FFTW's c2r.
+#pragma once
+#include "common.cuh"
+
+namespace meu {
+
+struct LinePlan {
+  int L;       // transform length
+  int ns;      // number of stages
+  int r[12];   // radix of each DIF stage (product = L)
+  const void* tw;   // cplx<R>[L], tw[n] = exp(-2 pi i n / L)
+  const int* rev;   // rev[p] = frequency index held at position p after DIF
+};
+
+// ---------------------------------------------------------------- butterflies
+// y_q = sum_r x_r exp(S * 2 pi i r q / R), in place.
+template <int R, int S, typename C> struct Dft;
+
+template <int S, typename C> struct Dft<2, S, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    C a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+  }
+};
+template <int S, typename C> struct Dft<4, S, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    C a = cadd(x[0], x[2]), b = csub(x[0], x[2]);
+    C c = cadd(x[1], x[3]), d = cmul_is<S>(csub(x[1], x[3]));
+    x[0] = cadd(a, c);
+    x[2] = csub(a, c);
+    x[1] = cadd(b, d);
+    x[3] = csub(b, d);
+  }
+};
+template <int S, typename C> struct Dft<3, S, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    using R = decltype(x[0].x);
+    const R h = (R)0.5, s3 = (R)0.86602540378443864676372317075293618;
+    C t = cadd(x[1], x[2]);
+    C u = cmul_is<S>(cscale(csub(x[1], x[2]), s3));
+    C m = csub(x[0], cscale(t, h));
+    x[0] = cadd(x[0], t);
+    x[1] = cadd(m, u);
+    x[2] = csub(m, u);
+  }
+};
+template <int S, typename C> struct Dft<8, S, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    using R = decltype(x[0].x);
+    const R r2 = (R)0.70710678118654752440084436210484904;
+    C a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      a[r] = cadd(x[r], x[r + 4]);
+      b[r] = csub(x[r], x[r + 4]);
+    }
+    // b_r *= W8^r, W8 = exp(S 2 pi i / 8)
+    b[1] = cscale(cadd(b[1], cmul_is<S>(b[1])), r2);
+    b[2] = cmul_is<S>(b[2]);
+    b[3] = cscale(csub(cmul_is<S>(b[3]), b[3]), r2);
+    Dft<4, S, C>::run(a);
+    Dft<4, S, C>::run(b);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      x[2 * q] = a[q];
+      x[2 * q + 1] = b[q];
+    }
+  }
+};
+
+// ----------------------------------------------------------------- stages
+// Lines of a batch: element e of line l sits at buf[l*ls + e*es].
+template <typename C, int R>
+__device__ __forceinline__ void dif_stage(C* buf, int span, int L, int nlines, int ls, int es, const C* __restrict__ tw) {
+  const int m = span / R, nbf = nlines * (L / R), tws = L / span;
+  for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
+    const int line = t % nlines, u = t / nlines, j = u % m, b = u / m;
+    C* base = buf + line * ls + (b * span + j) * es;
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = base[r * m * es];
+    Dft<R, -1, C>::run(x);
+#pragma unroll
+    for (int q = 1; q < R; ++q) x[q] = cmul(x[q], tw[j * q * tws]);
+#pragma unroll
+    for (int q = 0; q < R; ++q) base[q * m * es] = x[q];
+  }
+}
+
+template <typename C, int R>
+__device__ __forceinline__ void dit_stage(C* buf, int span, int L, int nlines, int ls, int es, const C* __restrict__ tw) {
+  const int m = span / R, nbf = nlines * (L / R), tws = L / span;
+  for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
+    const int line = t % nlines, u = t / nlines, j = u % m, b = u / m;
+    C* base = buf + line * ls + (b * span + j) * es;
+    C x[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) x[q] = base[q * m * es];
+#pragma unroll
+    for (int q = 1; q < R; ++q) x[q] = cmulc(x[q], tw[j * q * tws]);
+    Dft<R, 1, C>::run(x);
+#pragma unroll
+    for (int r = 0; r < R; ++r) base[r * m * es] = x[r];
+  }
+}
+
+// Forward (DIF): natural -> digit reversed.  Caller syncs before; this syncs after.
+template <typename C>
+__device__ void fft_dif(C* buf, const LinePlan& pl, int nlines, int ls, int es) {
+  const C* tw = (const C*)pl.tw;
+  int span = pl.L;
+  for (int s = 0; s < pl.ns; ++s) {
+    switch (pl.r[s]) {
+      case 8: dif_stage<C, 8>(buf, span, pl.L, nlines, ls, es, tw); break;
+      case 4: dif_stage<C, 4>(buf, span, pl.L, nlines, ls, es, tw); break;
+      case 3: dif_stage<C, 3>(buf, span, pl.L, nlines, ls, es, tw); break;
+      default: dif_stage<C, 2>(buf, span, pl.L, nlines, ls, es, tw); break;
+    }
+    span /= pl.r[s];
+    __syncthreads();
+  }
+}
+
+// Inverse (DIT, unscaled): digit reversed -> natural.
+template <typename C>
+__device__ void fft_dit(C* buf, const LinePlan& pl, int nlines, int ls, int es) {
+  const C* tw = (const C*)pl.tw;
+  int spans[12];
+  int span = pl.L;
+  for (int s = 0; s < pl.ns; ++s) {
+    spans[s] = span;
+    span /= pl.r[s];
+  }
+  for (int s = pl.ns - 1; s >= 0; --s) {
+    switch (pl.r[s]) {
+      case 8: dit_stage<C, 8>(buf, spans[s], pl.L, nlines, ls, es, tw); break;
+      case 4: dit_stage<C, 4>(buf, spans[s], pl.L, nlines, ls, es, tw); break;
+      case 3: dit_stage<C, 3>(buf, spans[s], pl.L, nlines, ls, es, tw); break;
+      default: dit_stage<C, 2>(buf, spans[s], pl.L, nlines, ls, es, tw); break;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ host side
+struct FFTPlan3;  // defined in fft.cu
+
+// Plan of a 3-D real transform of one grid (twiddle tables live on the device).
+class FFT3 {
+ public:
+  FFT3(int nx, int ny, int nz, bool fp64);
+  ~FFT3();
+  FFT3(const FFT3&) = delete;
+  FFT3& operator=(const FFT3&) = delete;
+
+  int nx, ny, nz, nxh;
+  int64_t n3() const { return (int64_t)nx * ny * nz; }
+  int64_t nk() const { return (int64_t)nz * ny * nxh; }
+
+  // f_trans on nf fields: real in[f] -> spectrum out[f] (scaled by 1/n3).
+  template <typename R>
+  void forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const;
+  // inv_trans on nf fields: spectrum in[f] -> real out[f].  in[f] is used as
+  // scratch and holds garbage afterwards.
+  template <typename R>
+  void inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
+
+  LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
+  const void* post_tw;  // cplx<R>[nx/2+1]: exp(-2 pi i k / nx)
+  bool fp64;
+
+ private:
+  void* dev_mem = nullptr;
+};
+
+bool fft_size_ok(int n, bool is_x);
+
+}  // namespace meu

@@ -1,0 +1,78 @@
+// host.cu -- host-side helpers of the C-ABI (no GPU work): the reference's
+// ran_2 generator (ran_2.f:1-42) with its SAVE state made explicit, the
+// langevin draw (ModFunc.f:77-100) and the uniform-noise initialiser of the
+// Landau decks.
+#include <cmath>
+#include <cstring>
+
+#include "../../include/meu.h"
+
+namespace {
+constexpr int32_t kIm1 = 2147483563, kIm2 = 2147483399, kImm1 = kIm1 - 1;
+constexpr int32_t kIa1 = 40014, kIa2 = 40692, kIq1 = 53668, kIq2 = 52774, kIr1 = 12211, kIr2 = 3791;
+constexpr int32_t kNtab = 32, kNdiv = 1 + kImm1 / kNtab;
+
+// One Schrage step of a multiplicative congruential generator (a*x mod m
+// without overflow): x <- a*(x - k*q) - k*r, then wrap into [0, m).
+inline int32_t schrage(int32_t x, int32_t a, int32_t q, int32_t r, int32_t m) {
+  const int32_t k = x / q;
+  int32_t y = a * (x - k * q) - k * r;
+  if (y < 0) y += m;
+  return y;
+}
+}  // namespace
+
+extern "C" {
+
+void meu_ran2_init(meu_ran2_state* s, int32_t iseed) {
+  std::memset(s, 0, sizeof(*s));
+  s->idum = iseed;
+  s->idum2 = 123456789;
+}
+
+double meu_ran2(meu_ran2_state* s) {
+  // am = 1./im1 is single precision in the reference: float(im1) rounds to
+  // 2^31 - 128 and the quotient is rounded to single before widening
+  const double am = (double)(1.0f / (float)kIm1);
+  const double rnmx = 1.0 - 1.2e-7;
+  if (s->idum <= 0) {
+    s->idum = (-s->idum > 1) ? -s->idum : 1;
+    s->idum2 = s->idum;
+    for (int j = kNtab + 8; j >= 1; --j) {
+      s->idum = schrage(s->idum, kIa1, kIq1, kIr1, kIm1);
+      if (j <= kNtab) s->iv[j - 1] = s->idum;
+    }
+    s->iy = s->iv[0];
+  }
+  s->idum = schrage(s->idum, kIa1, kIq1, kIr1, kIm1);
+  s->idum2 = schrage(s->idum2, kIa2, kIq2, kIr2, kIm2);
+  const int j = s->iy / kNdiv;  // 0-based slot of the shuffle table
+  s->iy = s->iv[j] - s->idum2;
+  s->iv[j] = s->idum;
+  if (s->iy < 1) s->iy += kImm1;
+  const double v = am * (double)s->iy;
+  return v < rnmx ? v : rnmx;
+}
+
+double meu_langevin(meu_ran2_state* s, double sd) {
+  for (;;) {
+    const double v1 = 2.0 * meu_ran2(s) - 1.0;
+    const double v2 = 2.0 * meu_ran2(s) - 1.0;
+    double rsq = v1 * v1 + v2 * v2;
+    if (rsq > 0.0 && rsq < 1.0) {
+      rsq = std::sqrt(-2.0 * std::log(rsq) / rsq);
+      return v2 * rsq * sd;
+    }
+  }
+}
+
+void meu_init_uniform(meu_ran2_state* s, int32_t nx, int32_t ny, int32_t nz, int32_t nvar, double c0, double c_amp,
+                      double eta_amp, double* cons, double* phi) {
+  const int64_t n3 = (int64_t)nx * ny * nz;
+  for (int64_t i = 0; i < n3; ++i) {
+    cons[i] = c0 + c_amp * (2.0 * meu_ran2(s) - 1.0);
+    for (int v = 0; v < nvar; ++v) phi[i * nvar + v] = eta_amp * (2.0 * meu_ran2(s) - 1.0);
+  }
+}
+
+}  // extern "C"

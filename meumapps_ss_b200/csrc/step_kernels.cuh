@@ -1,0 +1,668 @@
+// step_kernels.cuh -- the kernels of one time step (templated on the bulk
+// precision R: double for the plain FP64 path, float for the FP32 path; every
+// per-k operator and every reduction computes in FP64).
+#pragma once
+#include "kernels.cuh"
+
+namespace meu {
+
+enum RedQ : int {
+  Q_FCH = 0, Q_FW, Q_FINT, Q_ELEN, Q_CMIN, Q_CMAX, Q_PHIMAX, Q_SOLID, Q_CSUM0,
+  Q_STEP_COUNT = Q_CSUM0 + MEU_MAX_EL,
+  // elastic convergence sums, separate finalisation
+  Q_ERR0 = Q_STEP_COUNT, Q_TOTAL = Q_ERR0 + 6
+};
+
+__device__ __forceinline__ void set_err(int* err, int code) {
+  if (code) atomicMax(err, code);
+}
+
+template <typename C>
+__device__ __forceinline__ void ld2(const C& v, double& re, double& im) {
+  re = (double)v.x;
+  im = (double)v.y;
+}
+
+// ------------------------------------------------------------ KKS: gradients
+// dft_grad_{x,y,z} = kf * phi^, dft_k_del_sq = phi^ * (grad_coeff multiplier)
+// (Multi_MEUMAPPS.f:581-605).  out[4v+c].
+template <typename R>
+__global__ void __launch_bounds__(256) k_kks_grad(const DevConst* __restrict__ Kp, PtrList<cplx<R>> in,
+                                                  PtrList<cplx<R>> out, int V) {
+  const DevConst& K = *Kp;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    for (int v = 0; v < V; ++v) {
+      const cplx<R> val = in.p[v][id];
+      const double re = val.x, im = val.y;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) out.p[4 * v + c][id] = mk((R)(-b[c] * im), (R)(b[c] * re));
+      const double m = -kkappak(K.p.grad_coeff[v], a, b);
+      out.p[4 * v + 3][id] = mk((R)(re * m), (R)(im * m));
+    }
+  }
+}
+
+// ------------------------------------------------- KKS: local driving force
+// Multi_MEUMAPPS.f:634-845 per voxel.  g4 = [gx_v, gy_v, gz_v, kds_v] per v.
+__global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __restrict__ Kp, const double* __restrict__ phi,
+                                                           const double* __restrict__ cons, const double* __restrict__ g4,
+                                                           double* __restrict__ pphi, double* __restrict__ fdiff,
+                                                           double* __restrict__ fc, double* partials, int* err) {
+  const DevConst& K = *Kp;
+  const meu_params& p = K.p;
+  const int V = p.nvar, numel = p.numel, numph = p.numph, zdim = K.zdim;
+  const int64_t n3 = K.n3;
+  double fch = 0, fw = 0, fint = 0;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    double Pph[MEU_MAX_PH], Gph[MEU_MAX_PH], Ppr[MEU_MAX_VAR], fgrad[MEU_MAX_VAR], ph[MEU_MAX_VAR];
+    for (int n = 0; n < MEU_MAX_PH; ++n) { Pph[n] = 0; Gph[n] = 0; }
+    for (int v = 0; v < V; ++v) ph[v] = phi[v * n3 + id];
+    for (int n = 2; n <= numph; ++n)
+      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+        const double fi = ph[v], fi_sq = fi * fi;
+        const double pl = fi_sq * fi * (6.0 * fi_sq - 15.0 * fi + 10.0);
+        pphi[v * n3 + id] = pl;
+        Ppr[v] = 30.0 * fi_sq * (fi_sq - 2.0 * fi + 1.0);
+        Pph[0] += pl;
+        Pph[n - 1] += pl;
+        Gph[n - 1] += fi_sq * (1.0 - fi) * (1.0 - fi);
+        for (int u = 0; u < V; ++u)
+          if (u != v) Gph[0] += fi_sq * ph[u] * ph[u];
+      }
+    Pph[0] = 1.0 - Pph[0];
+    // interface compositions (:677-710)
+    double Z[144], Zr[12], X[MEU_MAX_EL][MEU_MAX_PH], Gib[MEU_MAX_PH], MuC[MEU_MAX_EL];
+    for (int i = 0; i < zdim * zdim; ++i) Z[i] = K.zconst[i];
+    for (int i = 0; i < zdim; ++i) Zr[i] = K.zr_const[i];
+    for (int e = 1; e <= numel; ++e) {
+      const int i0 = zdim - numel + e;
+      Zr[i0 - 1] = cons[(e - 1) * n3 + id];
+      for (int n = 1; n <= numph; ++n) Z[(i0 - 1) + (numph * (e - 1) + n - 1) * zdim] = Pph[n - 1];
+    }
+    set_err(err, invert_small<12>(Z, zdim, MEU_ERR_Z_SINGULAR));
+    for (int n = 1; n <= numph; ++n)
+      for (int e = 1; e <= numel; ++e) {
+        const int i0 = numph * (e - 1) + n;
+        double acc = 0;
+        for (int j0 = 1; j0 <= zdim; ++j0) acc += Z[(i0 - 1) + (j0 - 1) * zdim] * Zr[j0 - 1];
+        X[e - 1][n - 1] = acc;
+      }
+#define GP(j, n) p.gparams[(n) - 1][(j) - 1]
+    for (int n = 1; n <= numph; ++n) {
+      double g = 0;
+      for (int e = 1; e <= numel; ++e) {
+        const double d = X[e - 1][n - 1] - GP(e + numel + 1, n);
+        g += GP(e, n) * d * d;
+      }
+      Gib[n - 1] = g + GP(numel + 1, n);
+    }
+    for (int e = 1; e <= numel; ++e) MuC[e - 1] = 2.0 * GP(e, 1) * (X[e - 1][0] - GP(e + numel + 1, 1));
+#undef GP
+    double fchloc = Pph[0] * Gib[0], fwloc = p.wellph[0] * Gph[0];
+    double fcl[3 * MEU_MAX_EL];
+    for (int i = 0; i < 3 * numel; ++i) fcl[i] = 0;
+    for (int n = 2; n <= numph; ++n) {
+      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+        const double* g = p.grad_coeff[v];
+        const double gx = g4[(4 * v + 0) * n3 + id], gy = g4[(4 * v + 1) * n3 + id], gz = g4[(4 * v + 2) * n3 + id];
+        const double term = g[0] * gx * gx + g[4] * gy * gy + g[8] * gz * gz + (g[3] + g[1]) * gx * gy +
+                            (g[6] + g[2]) * gx * gz + (g[7] + g[5]) * gy * gz;
+        fint += 0.5 * term;
+        const double fi = ph[v];
+        double termch = Gib[n - 1] - Gib[0];
+        for (int e = 0; e < numel; ++e) {
+          const double xd = X[e][0] - X[e][n - 1];
+          termch += MuC[e] * xd;
+          const double t = Ppr[v] * xd;
+          fcl[3 * e + 0] += t * gx;
+          fcl[3 * e + 1] += t * gy;
+          fcl[3 * e + 2] += t * gz;
+        }
+        double well = 2.0 * p.wellph[n - 1] * fi * (1.0 - fi) * (1.0 - 2.0 * fi);
+        for (int u = 0; u < V; ++u)
+          if (u != v) well += 4.0 * p.wellph[0] * fi * ph[u] * ph[u];
+        fgrad[v] = termch * Ppr[v] + well;
+      }
+      fchloc += Pph[n - 1] * Gib[n - 1];
+      fwloc += p.wellph[n - 1] * Gph[n - 1];
+    }
+    fch += fchloc;
+    fw += fwloc;
+    for (int i = 0; i < 3 * numel; ++i) fc[(int64_t)i * n3 + id] = fcl[i];
+    // n_tilda projection (:824-841)
+    for (int jv = 0; jv < V; ++jv) {
+      double term11 = 0;
+      int nt = 1;
+      if (ph[jv] > 0.0)
+        for (int iv = 0; iv < V; ++iv)
+          if (ph[iv] > 0.0 && iv != jv) {
+            term11 += fgrad[iv] - g4[(4 * iv + 3) * n3 + id];
+            nt += 1;
+          }
+      fdiff[jv * n3 + id] = fgrad[jv] - term11 / (double)nt;
+    }
+  }
+  block_reduce_store(fch, 0, partials + Q_FCH * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(fw, 0, partials + Q_FW * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(fint, 0, partials + Q_FINT * RED_BLOCKS + blockIdx.x);
+}
+
+// ------------------------------------------------------ elastic: zeroth order
+// ModElastic.f:115-236: u^ = Q^-1 R, R_i = sum_j kf_j sum_v P^_v sig0_v(ij); the
+// engineering strain gamma^ of u^ goes to g[0..6).
+template <typename R>
+__global__ void __launch_bounds__(256) k_el_zeroth(const DevConst* __restrict__ Kp, PtrList<cplx<R>> pk, int V,
+                                                   cplx<R>* __restrict__ uk, PtrList<cplx<R>> g, int* err) {
+  const DevConst& K = *Kp;
+  const int64_t nk = K.nk;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    double sr[6] = {0, 0, 0, 0, 0, 0}, si[6] = {0, 0, 0, 0, 0, 0};
+    for (int v = 0; v < V; ++v) {
+      double re, im;
+      ld2(pk.p[v][id], re, im);
+#pragma unroll
+      for (int m = 0; m < 6; ++m) { sr[m] += re * K.sig0[v][m]; si[m] += im * K.sig0[v][m]; }
+    }
+    // R_i = i sum_j b_j S_ij  (S symmetric, Voigt m = voigt(i,j))
+    double Rr[3], Ri[3];
+#pragma unroll
+    for (int i = 1; i <= 3; ++i) {
+      double tr = 0, ti = 0;
+#pragma unroll
+      for (int j = 1; j <= 3; ++j) { const int m = voigt(i, j) - 1; tr += b[j - 1] * sr[m]; ti += b[j - 1] * si[m]; }
+      Rr[i - 1] = -ti;
+      Ri[i - 1] = tr;
+    }
+    double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+    if (id != 0) {
+      double Q[9];
+      build_q(K, a, b, Q);
+      set_err(err, invert3(Q, MEU_ERR_Q_SINGULAR));
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        ur[i] = Q[i] * Rr[0] + Q[i + 3] * Rr[1] + Q[i + 6] * Rr[2];
+        ui[i] = Q[i] * Ri[0] + Q[i + 3] * Ri[1] + Q[i + 6] * Ri[2];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) uk[(int64_t)i * nk + id] = mk((R)ur[i], (R)ui[i]);
+    // gamma = i*(b (x) u) symmetrised, engineering Voigt order 11,22,33,23,13,12
+    const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const int i = I1[m], j = J1[m];
+      double gr, gi;
+      if (m < 3) { gr = -b[i] * ui[i]; gi = b[i] * ur[i]; }
+      else { gr = -(b[i] * ui[j] + b[j] * ui[i]); gi = b[i] * ur[j] + b[j] * ur[i]; }
+      g.p[m][id] = mk((R)gr, (R)gi);
+    }
+  }
+}
+
+// --------------------------------------------------- elastic: polarisation x
+// ModElastic.f:248-327.  strain = engineering gamma (6), xs out (6).
+template <typename R>
+__global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
+                                              const R* __restrict__ strain, R* __restrict__ xs, double cfac, int* err) {
+  const DevConst& K = *Kp;
+  const meu_params& p = K.p;
+  const int64_t n3 = K.n3;
+  const int V = p.nvar;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    double Cm[36], e0[6] = {0, 0, 0, 0, 0, 0}, psum = 0;
+#pragma unroll
+    for (int i = 0; i < 36; ++i) Cm[i] = 0;
+    for (int n = 2; n <= p.numph; ++n)
+      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+        const double pv = (double)pphi[v * n3 + id];
+        psum += pv;
+#pragma unroll
+        for (int i = 0; i < 36; ++i) Cm[i] += pv * p.sela[n - 1][i];
+      }
+    for (int v = 0; v < V; ++v) {
+      const double pv = (double)pphi[v * n3 + id];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) e0[m] += pv * K.eps_eng[v][m];
+    }
+    if (psum < 1.0) {
+#pragma unroll
+      for (int i = 0; i < 36; ++i) Cm[i] += (1.0 - psum) * p.sela[0][i];
+    }
+    set_err(err, invert_small<6>(Cm, 6, MEU_ERR_C_SINGULAR));
+    double gam[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) gam[m] = (double)strain[(int64_t)m * n3 + id] + K.ebar_eng[m];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double s = 0;
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        const double c = Cm[r + m * 6];
+        s += cfac * (K.c0m[r + m * 6] - c) * gam[m] + c * e0[m];
+      }
+      xs[(int64_t)r * n3 + id] = (R)s;
+    }
+  }
+}
+
+// ------------------------------------------------- elastic: Green operator
+// ModElastic.f:340-394: u^ = Qinv (kf . x^), gamma^ of u^ written over x^.
+// Convergence sums (ModElastic.f:413-430) by Parseval against the previous u^.
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict__ Kp, PtrList<cplx<R>> xk,
+                                                      cplx<R>* __restrict__ uk, double* partials, int* err) {
+  const DevConst& K = *Kp;
+  const int64_t nk = K.nk;
+  double e[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    double xr[6], xi[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) ld2(xk.p[m][id], xr[m], xi[m]);
+    // R = kf . x (Voigt 1..6 -> x1 x2 x3 x4 x5 x6)
+    const double tr1 = xr[0] * b[0] + xr[5] * b[1] + xr[4] * b[2], ti1 = xi[0] * b[0] + xi[5] * b[1] + xi[4] * b[2];
+    const double tr2 = xr[5] * b[0] + xr[1] * b[1] + xr[3] * b[2], ti2 = xi[5] * b[0] + xi[1] * b[1] + xi[3] * b[2];
+    const double tr3 = xr[4] * b[0] + xr[3] * b[1] + xr[2] * b[2], ti3 = xi[4] * b[0] + xi[3] * b[1] + xi[2] * b[2];
+    const double Rr[3] = {-ti1, -ti2, -ti3}, Ri[3] = {tr1, tr2, tr3};
+    double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+    if (id != 0) {
+      double Q[9];
+      build_q(K, a, b, Q);
+      set_err(err, invert3(Q, MEU_ERR_Q_SINGULAR));
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        ur[i] = Q[i] * Rr[0] + Q[i + 3] * Rr[1] + Q[i + 6] * Rr[2];
+        ui[i] = Q[i] * Ri[0] + Q[i + 3] * Ri[1] + Q[i + 6] * Ri[2];
+      }
+    }
+    const double w = hweight(K, kx);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double orr, oi;
+      ld2(uk[(int64_t)i * nk + id], orr, oi);
+      const double dr = ur[i] - orr, di = ui[i] - oi;
+      e[2 * i] += w * (dr * dr + di * di);
+      e[2 * i + 1] += w * (orr * orr + oi * oi);
+      uk[(int64_t)i * nk + id] = mk((R)ur[i], (R)ui[i]);
+    }
+    const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const int i = I1[m], j = J1[m];
+      double gr, gi;
+      if (m < 3) { gr = -b[i] * ui[i]; gi = b[i] * ur[i]; }
+      else { gr = -(b[i] * ui[j] + b[j] * ui[i]); gi = b[i] * ur[j] + b[j] * ur[i]; }
+      xk.p[m][id] = mk((R)gr, (R)gi);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) block_reduce_store(e[q], 0, partials + (Q_ERR0 + q) * RED_BLOCKS + blockIdx.x);
+}
+
+// -------------------------------------------------------------- elener
+// ModElastic.f:540-687.  mode 0 (KKS): fdiff += el_grad; mode 1 (Landau): elg = el_grad.
+// theta' = 30 f^2 (f^2 - 2f + 1) (KKS and Landau h coupling) or 2 eta (eta^2 coupling).
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
+                                                        const R* __restrict__ pphi, const R* __restrict__ strain,
+                                                        R* __restrict__ el_en, R* __restrict__ elg, int mode, int eta2,
+                                                        double* partials, int* err) {
+  const DevConst& K = *Kp;
+  const meu_params& p = K.p;
+  const int64_t n3 = K.n3;
+  const int V = p.nvar;
+  double esum = 0;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    double te[6] = {0, 0, 0, 0, 0, 0}, psum = 0, P[MEU_MAX_VAR];
+    for (int v = 0; v < V; ++v) {
+      P[v] = (double)pphi[v * n3 + id];
+      psum += P[v];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) te[m] += P[v] * p.trans_ppt[v][m];
+    }
+    double eps[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const double gm = (double)strain[(int64_t)m * n3 + id];
+      eps[m] = (m < 3) ? (p.e_mean[m] + gm - te[m]) : (2.0 * p.e_mean[m] + gm - 2.0 * te[m]);
+    }
+    double Cm[36];
+#pragma unroll
+    for (int i = 0; i < 36; ++i) Cm[i] = (1.0 - psum) * p.sela[0][i];
+    for (int n = 2; n <= p.numph; ++n)
+      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+#pragma unroll
+        for (int i = 0; i < 36; ++i) Cm[i] += P[v] * p.sela[n - 1][i];
+      }
+    set_err(err, invert_small<6>(Cm, 6, MEU_ERR_C_ELENER_SINGULAR));
+    double sig[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double s = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) s += Cm[i + j * 6] * eps[j];
+      sig[i] = s;
+    }
+    double elmat = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double em = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) em += p.sela[0][i + j * 6] * sig[j];
+      elmat += sig[i] * em;
+    }
+    elmat *= 0.5;
+    double en = (1.0 - psum) * elmat;
+    for (int n = 2; n <= p.numph; ++n)
+      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+        if (!K.use_var[v]) continue;
+        double elp = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          double ep = 0;
+#pragma unroll
+          for (int j = 0; j < 6; ++j) ep += p.sela[n - 1][i + j * 6] * sig[j];
+          elp += sig[i] * ep;
+        }
+        elp *= 0.5;
+        en += elp * P[v];
+        const double* t = p.trans_ppt[v];
+        const double g = sig[0] * t[0] + sig[1] * t[1] + sig[2] * t[2] + 2.0 * (sig[3] * t[3] + sig[4] * t[4] + sig[5] * t[5]);
+        const double f = (double)phi[v * n3 + id];
+        const double pr = eta2 ? 2.0 * f : 30.0 * f * f * (f * f - 2.0 * f + 1.0);
+        const double eg = pr * (elmat - elp) - g * pr;
+        if (mode == 0) elg[v * n3 + id] += (R)eg;
+        else elg[v * n3 + id] = (R)eg;
+      }
+    el_en[id] = (R)en;
+    esum += en;
+  }
+  block_reduce_store(esum, 0, partials + Q_ELEN * RED_BLOCKS + blockIdx.x);
+}
+
+// --------------------------------------------------- KKS: diffusion update
+// Multi_MEUMAPPS.f:924-943 on spectra [c, fx, fy, fz] of one solute.
+template <typename R>
+__global__ void __launch_bounds__(256) k_kks_ch(const DevConst* __restrict__ Kp, cplx<R>* __restrict__ ck,
+                                                const cplx<R>* __restrict__ fx, const cplx<R>* __restrict__ fy,
+                                                const cplx<R>* __restrict__ fz, double dm) {
+  const DevConst& K = *Kp;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    const double ksq = -a[0] * a[0] - a[1] * a[1] - a[2] * a[2];
+    double cr, ci, xr, xi, yr, yi, zr, zi;
+    ld2(ck[id], cr, ci);
+    ld2(fx[id], xr, xi);
+    ld2(fy[id], yr, yi);
+    ld2(fz[id], zr, zi);
+    // term1 = i (b . F)
+    const double t1r = -(b[0] * xi + b[1] * yi + b[2] * zi), t1i = b[0] * xr + b[1] * yr + b[2] * zr;
+    const double term2 = 1.0 - dm * ksq;
+    ck[id] = mk((R)((cr + dm * t1r) / term2), (R)((ci + dm * t1i) / term2));
+  }
+}
+
+// TDGL right-hand side in real space: w = phi - dt L f_diff + dt noise
+// (by linearity equal to the three transforms of Multi_MEUMAPPS.f:957-987).
+template <typename R>
+__global__ void k_tdgl_pre(const R* __restrict__ phi, const R* __restrict__ fdiff, const R* __restrict__ noise,
+                           R* __restrict__ w, int64_t n, double dtl, double dt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    w[i] = (R)((double)phi[i] - dtl * (double)fdiff[i] + dt * (double)noise[i]);
+}
+
+// TDGL divide (Multi_MEUMAPPS.f:979-987): w^ /= 1 + dt L k.kappa.k
+template <typename R>
+__global__ void __launch_bounds__(256) k_tdgl(const DevConst* __restrict__ Kp, PtrList<cplx<R>> sp, int V, double dtl) {
+  const DevConst& K = *Kp;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    for (int v = 0; v < V; ++v) {
+      const double den = 1.0 + dtl * kkappak(K.p.grad_coeff[v], a, b);
+      double re, im;
+      ld2(sp.p[v][id], re, im);
+      sp.p[v][id] = mk((R)(re / den), (R)(im / den));
+    }
+  }
+}
+
+// -------------------------------------------------------------- Landau
+// theta_v, mu_c and the bulk free energy
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_lan_a(const DevConst* __restrict__ Kp, const R* __restrict__ c,
+                                                       const R* __restrict__ eta, R* __restrict__ theta,
+                                                       R* __restrict__ mu, double* partials) {
+  const DevConst& K = *Kp;
+  const meu_params& p = K.p;
+  const int64_t n3 = K.n3;
+  const int V = p.nvar;
+  const int hcp = p.eig_coupling == MEU_EIG_H;
+  double fch = 0;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    const double cv = (double)c[id];
+    double s2 = 0, s4 = 0, s6 = 0;
+    for (int v = 0; v < V; ++v) {
+      const double e = (double)eta[v * n3 + id], e2 = e * e;
+      s2 += e2; s4 += e2 * e2; s6 += e2 * e2 * e2;
+      theta[v * n3 + id] = (R)(hcp ? e2 * e * (6.0 * e2 - 15.0 * e + 10.0) : e2);
+    }
+    // sum_{u != v} eta_u^2 eta_v^2 = s2^2 - s4
+    const double cross = s2 * s2 - s4;
+    fch += 0.5 * p.lan_a * (cv - p.lan_c1) * (cv - p.lan_c1) + 0.5 * p.lan_b * (p.lan_c2 - cv) * s2 - 0.25 * p.lan_c * s4 +
+           p.lan_d / 6.0 * s6 + p.cross_w * cross;
+    mu[id] = (R)(p.lan_a * (cv - p.lan_c1) - 0.5 * p.lan_b * s2);
+  }
+  block_reduce_store(fch, 0, partials + Q_FCH * RED_BLOCKS + blockIdx.x);
+}
+
+// Landau k-space kernel: gradient energy (Parseval), homogeneous Green
+// operator phi^_p = sum_q (sig0_p b).Omega.(sig0_q b) theta^_q with
+// Omega = -Q^-1 (the reference's Q, ModElastic.f:119-158), its exact elastic
+// energy, and the Cahn-Hilliard update
+//   c^ <- (c^ - dt M k^2 mu^) / (1 + dt M kappa_c k^4),  c^(0) = conserved mean.
+// sp: [theta_0..V-1, mu, c, eta_0..V-1]
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_lan_k1(const DevConst* __restrict__ Kp, PtrList<cplx<R>> sp, int V,
+                                                        int homog, int energy, double* partials, int* err) {
+  const DevConst& K = *Kp;
+  const meu_params& p = K.p;
+  const int64_t nk = K.nk;
+  const double dm = p.dt * p.cmobs[0];
+  double fint = 0, elen = 0;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    const double w = hweight(K, kx);
+    double cr, ci, mr, mi;
+    ld2(sp.p[V + 1][id], cr, ci);
+    ld2(sp.p[V][id], mr, mi);
+    if (energy) {
+      const double bb = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+      double f = p.kappa_c * bb * (cr * cr + ci * ci);
+      for (int v = 0; v < V; ++v) {
+        double er, ei;
+        ld2(sp.p[V + 2 + v][id], er, ei);
+        f += kkappak_b(p.grad_coeff[v], b) * (er * er + ei * ei);
+      }
+      fint += 0.5 * w * f;
+    }
+    if (homog) {
+      double tr[MEU_MAX_VAR], ti[MEU_MAX_VAR];
+      double sr[6] = {0, 0, 0, 0, 0, 0}, si[6] = {0, 0, 0, 0, 0, 0};
+      for (int v = 0; v < V; ++v) {
+        ld2(sp.p[v][id], tr[v], ti[v]);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) { sr[m] += tr[v] * K.sig0[v][m]; si[m] += ti[v] * K.sig0[v][m]; }
+      }
+      double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+      if (id != 0) {
+        double Rr[3], Ri[3];
+#pragma unroll
+        for (int i = 1; i <= 3; ++i) {
+          double t_r = 0, t_i = 0;
+#pragma unroll
+          for (int j = 1; j <= 3; ++j) { const int m = voigt(i, j) - 1; t_r += b[j - 1] * sr[m]; t_i += b[j - 1] * si[m]; }
+          Rr[i - 1] = -t_i;
+          Ri[i - 1] = t_r;
+        }
+        double Q[9];
+        build_q(K, a, b, Q);
+        set_err(err, invert3(Q, MEU_ERR_Q_SINGULAR));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          ur[i] = Q[i] * Rr[0] + Q[i + 3] * Rr[1] + Q[i + 6] * Rr[2];
+          ui[i] = Q[i] * Ri[0] + Q[i + 3] * Ri[1] + Q[i + 6] * Ri[2];
+        }
+      }
+      // phi^_p = sig0_p : sym(i b (x) u^) = i (sig0_p b) . u^
+      for (int v = 0; v < V; ++v) {
+        double sb[3];
+#pragma unroll
+        for (int i = 1; i <= 3; ++i) {
+          double t = 0;
+#pragma unroll
+          for (int j = 1; j <= 3; ++j) t += K.sig0[v][voigt(i, j) - 1] * b[j - 1];
+          sb[i - 1] = t;
+        }
+        const double dr = sb[0] * ur[0] + sb[1] * ur[1] + sb[2] * ur[2];
+        const double di = sb[0] * ui[0] + sb[1] * ui[1] + sb[2] * ui[2];
+        sp.p[v][id] = mk((R)(-di), (R)dr);
+      }
+      if (energy) {
+        // engineering elastic strain e = gamma(u^) - sum_q theta^_q eps0_q (+ e_mean at k = 0)
+        const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+        double er[6], ei[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          const int i = I1[m], j = J1[m];
+          double gr, gi;
+          if (m < 3) { gr = -b[i] * ui[i]; gi = b[i] * ur[i]; }
+          else { gr = -(b[i] * ui[j] + b[j] * ui[i]); gi = b[i] * ur[j] + b[j] * ur[i]; }
+          for (int v = 0; v < V; ++v) { gr -= tr[v] * K.eps_eng[v][m]; gi -= ti[v] * K.eps_eng[v][m]; }
+          if (id == 0) gr += K.ebar_eng[m];
+          er[m] = gr;
+          ei[m] = gi;
+        }
+        double q = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          double cr2 = 0, ci2 = 0;
+#pragma unroll
+          for (int j = 0; j < 6; ++j) { cr2 += K.c0m[i + j * 6] * er[j]; ci2 += K.c0m[i + j * 6] * ei[j]; }
+          q += er[i] * cr2 + ei[i] * ci2;
+        }
+        elen += 0.5 * w * q;
+      }
+    }
+    // Cahn-Hilliard
+    const double k2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+    double nr, ni;
+    if (id == 0) { nr = K.c_mean[0]; ni = 0.0; }
+    else {
+      const double den = 1.0 + dm * p.kappa_c * k2 * k2;
+      nr = (cr - dm * k2 * mr) / den;
+      ni = (ci - dm * k2 * mi) / den;
+    }
+    sp.p[V + 1][id] = mk((R)nr, (R)ni);
+  }
+  block_reduce_store(fint, 0, partials + Q_FINT * RED_BLOCKS + blockIdx.x);
+  if (homog) block_reduce_store(elen, 0, partials + Q_ELEN * RED_BLOCKS + blockIdx.x);
+}
+
+// Landau TDGL right-hand side w_v = eta_v - dt L (df/deta_v + el_grad_v)
+// homog: el_grad_v = -theta'_v (sig0_v:e_mean + phi_v - sum_q A_vq theta_q); else el from elener.
+template <typename R>
+__global__ void __launch_bounds__(256) k_lan_b(const DevConst* __restrict__ Kp, const R* __restrict__ c,
+                                               const R* __restrict__ eta, const R* __restrict__ el, int homog,
+                                               R* __restrict__ w) {
+  const DevConst& K = *Kp;
+  const meu_params& p = K.p;
+  const int64_t n3 = K.n3;
+  const int V = p.nvar;
+  const int hcp = p.eig_coupling == MEU_EIG_H;
+  const double dtl = p.dt * p.b_mob;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    const double cv = (double)c[id];
+    double e[MEU_MAX_VAR], th[MEU_MAX_VAR], s2 = 0;
+    for (int v = 0; v < V; ++v) {
+      e[v] = (double)eta[v * n3 + id];
+      const double e2 = e[v] * e[v];
+      s2 += e2;
+      th[v] = hcp ? e2 * e[v] * (6.0 * e2 - 15.0 * e[v] + 10.0) : e2;
+    }
+    for (int v = 0; v < V; ++v) {
+      const double ev = e[v], e2 = ev * ev;
+      double g = p.lan_b * (p.lan_c2 - cv) * ev - p.lan_c * e2 * ev + p.lan_d * e2 * e2 * ev +
+                 4.0 * p.cross_w * ev * (s2 - e2);
+      if (el) {
+        if (homog) {
+          const double tp = hcp ? 30.0 * e2 * (e2 - 2.0 * ev + 1.0) : 2.0 * ev;
+          double s = K.sig0_ebar[v] + (double)el[v * n3 + id];
+          for (int q = 0; q < V; ++q) s -= K.A[v][q] * th[q];
+          g += -tp * s;
+        } else {
+          g += (double)el[v * n3 + id];
+        }
+      }
+      w[v * n3 + id] = (R)(ev - dtl * g);
+    }
+  }
+}
+
+// ---------------------------------------------------- end-of-step reductions
+// Multi_MEUMAPPS.f:1008-1043: clip phi (KKS), min/max C (initial 1.0 / 0.0),
+// max phi (initial 0.0), solid fraction (sum of phi>0; Landau: sum eta^2), sum C.
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_stats(const DevConst* __restrict__ Kp, const R* __restrict__ c,
+                                                       R* __restrict__ phi, int clip, double* partials) {
+  const DevConst& K = *Kp;
+  const int64_t n3 = K.n3;
+  const int V = K.p.nvar, E = K.p.numel;
+  double cmin = 1.0, cmax = 0.0, pmax = 0.0, solid = 0.0, cs[MEU_MAX_EL] = {0, 0, 0};
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    for (int e = 0; e < E; ++e) {
+      const double v = (double)c[(int64_t)e * n3 + id];
+      cmin = fmin(cmin, v);
+      cmax = fmax(cmax, v);
+      cs[e] += v;
+    }
+    for (int v = 0; v < V; ++v) {
+      double f = (double)phi[v * n3 + id];
+      if (clip) {
+        if (f < 0.0) f = 0.0;
+        if (f > 1.0) f = 1.0;
+        phi[v * n3 + id] = (R)f;
+        if (f > 0.0) solid += f;
+      } else {
+        solid += f * f;
+      }
+      pmax = fmax(pmax, f);
+    }
+  }
+  block_reduce_store(cmin, 2, partials + Q_CMIN * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(cmax, 1, partials + Q_CMAX * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(pmax, 1, partials + Q_PHIMAX * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(solid, 0, partials + Q_SOLID * RED_BLOCKS + blockIdx.x);
+  for (int e = 0; e < MEU_MAX_EL; ++e) block_reduce_store(cs[e], 0, partials + (Q_CSUM0 + e) * RED_BLOCKS + blockIdx.x);
+}
+
+}  // namespace meu

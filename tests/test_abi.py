@@ -1,0 +1,50 @@
+"""C-ABI surface (CPU): the library loads without a GPU, exports every
+function include/meu.h declares, and the ctypes mirrors of meu_params /
+meu_diag have the C layout."""
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+from meumapps_ss_b200 import _lib
+from meumapps_ss_b200 import params as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_header_symbols():
+    L = _lib.lib()
+    names = _lib.header_functions()
+    assert "meu_run" in names and "meu_create" in names
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def _c_layout(struct, fields):
+    src = "#include <stdio.h>\n#include <stddef.h>\n#include \"meu.h\"\nint main(){\n"
+    src += f'printf("%zu\\n", sizeof({struct}));\n'
+    for f in fields:
+        src += f'printf("%zu\\n", offsetof({struct}, {f}));\n'
+    src += "return 0;}\n"
+    with tempfile.TemporaryDirectory() as d:
+        cfile, exe = os.path.join(d, "t.c"), os.path.join(d, "t")
+        open(cfile, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), cfile, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    return [int(x) for x in out]
+
+
+def test_struct_layouts_match_c():
+    for cls, cname in ((P.MeuParams, "meu_params"), (P.MeuDiag, "meu_diag"), (_lib.Ran2State, "meu_ran2_state")):
+        names = [f[0] for f in cls._fields_]
+        got = _c_layout(cname, names)
+        assert got[0] == C.sizeof(cls), cname
+        for n, off in zip(names, got[1:]):
+            assert getattr(cls, n).offset == off, (cname, n)
+
+
+def test_bad_arguments_fail_without_gpu():
+    L = _lib.lib()
+    assert L.meu_run(None, 1, None) == 100
+    assert L.meu_destroy(None) == 100
+    assert L.meu_get_step(None) == -1

@@ -1,0 +1,118 @@
+"""KKS model: the GPU plain-FP64 step against the CPU FP64 oracle, which
+restates Multi_MEUMAPPS.f:548-1106 and ModElastic.f.  Gate: <= 1e-10 max-abs
+on the fields over the first 100 steps."""
+import numpy as np
+import pytest
+
+from helpers import kks_case
+from meumapps_ss_b200 import params as P
+from meumapps_ss_b200.sim import Simulation
+
+TOL = 1e-10
+
+
+def _run_both(oracle, p, cons, phi, steps, chunks=1, ustate=None):
+    o = oracle.OracleSim(p)
+    o.set_fields(cons, phi, ustate)
+    g = Simulation(p)
+    g.set_fields(cons, phi, ustate)
+    per = steps // chunks
+    do, dg = [], []
+    for _ in range(chunks):
+        do.append(o.run(per))
+        dg.append(g.run(per))
+    return o, g, do, dg
+
+
+def _cat(ds, k):
+    return np.concatenate([d[k] for d in ds])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nvar,n", [(1, 16), (3, 16), (1, 24)])
+def test_kks_fields_parity_100_steps(oracle, nvar, n):
+    _, p, cons, phi = kks_case(n=n, nvar=nvar, steps=100)
+    o, g, do, dg = _run_both(oracle, p, cons, phi, 100, chunks=4)
+    co, fo, eo, uo = o.get_fields()
+    cg, fg, eg, ug = g.get_fields(ustate=True)
+    assert np.max(np.abs(cg - co)) <= TOL
+    assert np.max(np.abs(fg - fo)) <= TOL
+    assert np.max(np.abs(ug - uo)) <= TOL * max(1.0, np.max(np.abs(uo)))
+    assert np.max(np.abs(eg - eo)) <= 1e-9 * np.max(np.abs(eo))
+    assert np.array_equal(_cat(do, "el_iters"), _cat(dg, "el_iters"))
+    for k in ("fint", "fw", "fch", "elen", "etot"):
+        a, b = _cat(do, k), _cat(dg, k)
+        assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-300)) < 1e-9, k
+    for k in ("cmin", "cmax", "phimax", "solid_now", "glob_min", "glob_max", "phi_max", "solid"):
+        assert np.max(np.abs(_cat(do, k) - _cat(dg, k))) <= TOL, k
+    assert np.max(np.abs(_cat(do, "cavg") - _cat(dg, "cavg"))) <= 1e-13
+    assert g.step == o.step == p.step + 100
+
+
+@pytest.mark.gpu
+def test_kks_two_solutes_parity(oracle):
+    _, p, cons, phi = kks_case(n=16, nvar=1, steps=30, numel_in=3)
+    assert p.numel == 2
+    o, g, _, _ = _run_both(oracle, p, cons, phi, 30)
+    co, fo, _, _ = o.get_fields()
+    cg, fg, _, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(fg - fo)) <= TOL
+
+
+@pytest.mark.gpu
+def test_kks_noise_and_restart_state(oracle):
+    _, p, cons, phi = kks_case(n=16, nvar=3, steps=20)
+    p.noise_step = p.step + 4
+    from meumapps_ss_b200._lib import Ran2
+    rng = Ran2(-17)
+    o = oracle.OracleSim(p)
+    o.set_fields(cons, phi)
+    g = Simulation(p)
+    g.set_fields(cons, phi)
+    for s in range(8):
+        incr = np.array([rng.langevin(1e-3) for _ in range(phi.size)]).reshape(phi.shape[1:] + (3,))
+        incr = np.moveaxis(incr, -1, 0)
+        o.add_noise(incr)
+        g.add_noise(incr)
+        o.run(1)
+        g.run(1)
+    _, fo, _, uo = o.get_fields()
+    _, fg, _, ug = g.get_fields(ustate=True)
+    assert np.max(np.abs(fg - fo)) <= TOL
+    # restart through the data_save state (u, grad u): both continue identically
+    c1, f1, _, _ = o.get_fields()
+    p2 = p.copy()
+    p2.step = o.step
+    o2 = oracle.OracleSim(p2)
+    o2.set_fields(c1, f1, uo)
+    g2 = Simulation(p2)
+    g2.set_fields(c1, f1, ug)
+    o2.run(5)
+    g2.run(5)
+    assert np.max(np.abs(g2.get_fields()[1] - o2.get_fields()[1])) <= TOL
+
+
+@pytest.mark.gpu
+def test_kks_mass_conservation_and_clip():
+    _, p, cons, phi = kks_case(n=16, nvar=3, steps=50)
+    with Simulation(p) as g:
+        g.set_fields(cons, phi)
+        d = g.run(50)
+        c, f, _, _ = g.get_fields()
+    assert np.max(np.abs(d["cavg"][:, 0] - cons.mean())) < 1e-13
+    assert f.min() >= 0.0 and f.max() <= 1.0
+
+
+@pytest.mark.gpu
+def test_kks_rejects_fp32_and_bad_sizes():
+    from meumapps_ss_b200._lib import MeuError
+    _, p, _, _ = kks_case(n=16)
+    q = p.copy()
+    q.precision = P.PREC_F32
+    with pytest.raises(MeuError) as e:
+        Simulation(q)
+    assert e.value.code == 103
+    q = p.copy()
+    q.nx = 10
+    with pytest.raises(MeuError):
+        Simulation(q)

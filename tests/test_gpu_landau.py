@@ -1,0 +1,107 @@
+"""Landau decks: GPU plain FP64 against the CPU FP64 oracle (<= 1e-10 max-abs),
+and the FP32 bulk path against the GPU FP64 path (stated relative L2 bounds)."""
+import numpy as np
+import pytest
+
+from helpers import active_landau, py_uniform
+from meumapps_ss_b200 import configs as CF
+from meumapps_ss_b200 import params as P
+from meumapps_ss_b200.sim import Simulation
+
+TOL = 1e-10
+
+
+def _pair(oracle, p, c, e, steps, chunks=1):
+    o = oracle.OracleSim(p)
+    o.set_fields(c, e)
+    g = Simulation(p)
+    g.set_fields(c, e)
+    do, dg = [], []
+    for _ in range(chunks):
+        do.append(o.run(steps // chunks))
+        dg.append(g.run(steps // chunks))
+    cat = lambda ds, k: np.concatenate([d[k] for d in ds])
+    return o, g, do, dg, cat
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nvar,elastic,coupling", [(1, P.ELAST_HOMOG, P.EIG_ETA2), (3, P.ELAST_HOMOG, P.EIG_ETA2),
+                                                   (2, P.ELAST_NONE, P.EIG_ETA2), (1, P.ELAST_HOMOG, P.EIG_H)])
+def test_landau_active_parity(oracle, nvar, elastic, coupling):
+    p, c, e = active_landau(n=16, nvar=nvar, elastic=elastic, coupling=coupling)
+    o, g, do, dg, cat = _pair(oracle, p, c, e, 100, chunks=2)
+    co, eo, _, _ = o.get_fields()
+    cg, eg, _, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL
+    assert np.max(np.abs(eg - eo)) <= TOL
+    assert np.max(np.abs(eo - e)) > 1e-2  # the deck really evolves
+    for k in ("fint", "fch", "elen", "etot", "cmin", "cmax", "phimax", "solid_now"):
+        a, b = cat(do, k), cat(dg, k)
+        assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-30)) < 1e-9, k
+    assert np.max(np.abs(cat(dg, "cavg")[:, 0] - c.mean())) < 1e-14
+
+
+@pytest.mark.gpu
+def test_landau_hetero_parity(oracle):
+    p, c, e = active_landau(n=16, nvar=2, elastic=P.ELAST_HETERO, coupling=P.EIG_H, ppt_scale=1.5, el_tol=1e-8)
+    o, g, do, dg, cat = _pair(oracle, p, c, e, 40, chunks=2)
+    assert np.array_equal(cat(do, "el_iters"), cat(dg, "el_iters"))
+    co, eo, elo, _ = o.get_fields()
+    cg, eg, elg, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(eg - eo)) <= TOL
+    assert np.max(np.abs(elg - elo)) <= 1e-9 * np.max(np.abs(elo))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_landau_configs_small_parity(oracle, k):
+    w = CF.landau_config(k, n=16, precision=P.PREC_F64)
+    c, e = py_uniform(16, 16, 16, w.params.nvar, w.seed, w.c0, w.c_amp, w.eta_amp)
+    o, g, do, dg, cat = _pair(oracle, w.params, c, e, 30)
+    co, eo, _, _ = o.get_fields()
+    cg, eg, _, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(eg - eo)) <= TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nvar", [1, 3])
+def test_fp32_bulk_vs_fp64(nvar):
+    p64, c, e = active_landau(n=32, nvar=nvar, elastic=P.ELAST_HOMOG)
+    p32 = p64.copy()
+    p32.precision = P.PREC_F32
+    out = {}
+    for name, p in (("f64", p64), ("f32", p32)):
+        with Simulation(p) as g:
+            g.set_fields(c, e)
+            d = g.run(200)
+            out[name] = (g.get_fields(), d)
+    (c64, e64, _, _), d64 = out["f64"]
+    (c32, e32, _, _), d32 = out["f32"]
+    rc = np.linalg.norm(c32 - c64) / np.linalg.norm(c64)
+    re = np.linalg.norm(e32 - e64) / np.linalg.norm(e64)
+    assert rc < 1e-5 and re < 1e-4, (rc, re)
+    # FP64 k = 0 mode and reductions keep the mean concentration exact
+    assert np.max(np.abs(d32["cavg"][:, 0] - c.mean())) < 1e-7
+
+
+@pytest.mark.gpu
+def test_single_mode_decay_exact():
+    """Linear operator known answer: with a zero local free energy one Fourier
+    mode of eta decays by exactly 1/(1 + dt L kappa k^2) per step and one mode
+    of c by 1/(1 + dt M kappa_c k^4)."""
+    n = 32
+    p = CF.landau_params(n, 1, [[0, 0, 0]], elastic=P.ELAST_NONE, A=0.0, B=0.0, Cq=0.0, D=0.0, dt=0.05,
+                         kappa_eta=1.3, kappa_c=0.7, M=0.9, L=1.1)
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    k = 2 * np.pi * np.sqrt(2.0 ** 2 + 3.0 ** 2) / n
+    mode = np.cos(2 * np.pi * (2 * x + 3 * y) / n)
+    c = 0.3 + 0.01 * mode
+    e = 0.02 * mode
+    with Simulation(p) as g:
+        g.set_fields(c[None], e[None])
+        g.run(10)
+        cg, eg, _, _ = g.get_fields()
+    fe = (1.0 / (1.0 + 0.05 * 1.1 * 1.3 * k * k)) ** 10
+    fc = (1.0 / (1.0 + 0.05 * 0.9 * 0.7 * k ** 4)) ** 10
+    assert np.max(np.abs(eg[0] - 0.02 * fe * mode)) < 1e-14
+    assert np.max(np.abs(cg[0] - (0.3 + 0.01 * fc * mode))) < 1e-14
