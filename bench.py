@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the MEUMAPPS-SS time step on B200.
+
+Workload (default): Landau deck 1 -- 128^3 grid, one conserved c and three
+tetragonal variants eta_1..3, homogeneous cubic elasticity through the Green
+operator, dt = 0.005, FP32 bulk arithmetic (FP64 for Omega(k), the k = 0 mode
+and every reduction).  A "step" is one time step of that grid.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank advances its own
+independent replica (the single-grid step has no data-parallel exchange), so
+scaling is weak and the only collectives are the timing barrier/max.
+
+--impl reference times the CPU FP64 restatement of the reference step
+(oracle/, "port": the Fortran/MPI/P3DFFT reference cannot be built in this
+image) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s: FP32-bulk vs FP64 plain at stated err; adjoint/forward cost"
+UNIT = "Mcell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--n", type=int, default=0, help="override the grid edge (tests only)")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the warm-up and timed FP32 steps (for ncu launch lists and captures)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.lines = []
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+# ------------------------------------------------------------ CPU side
+def oracle_throughput(params, c, e, steps: int, threads: int):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(threads)
+    s = O.OracleSim(params)
+    s.set_fields(c, e)
+    t0 = time.perf_counter()
+    s.run(steps)
+    dt = time.perf_counter() - t0
+    s.close()
+    n3 = params.nx * params.ny * params.nz
+    return n3 * steps / dt / 1e6, dt
+
+
+def cpu_sample(cfg: int, n_override: int, budget_s: float, min_steps: int, threads: int):
+    """Oracle time steps on the deck's grid (or a smaller grid of the same deck
+    when one step at full size does not fit the budget)."""
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200 import _lib
+    w0 = CF.landau_config(cfg, n=n_override or None, precision=P.PREC_F64)
+    sizes = [w0.params.nx] + [s for s in (96, 64, 48, 32, 16) if s < w0.params.nx]
+    for n in sizes:
+        w = CF.landau_config(cfg, n=n, precision=P.PREC_F64)
+        p = w.params
+        c, e = _lib.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed, w.c0, w.c_amp, w.eta_amp)
+        _, t1 = oracle_throughput(p, c, e, 1, threads)
+        if t1 * min_steps <= budget_s or n == sizes[-1]:
+            steps = max(min_steps, int(budget_s / max(t1, 1e-6)))
+            steps = max(1, min(steps, 100000))
+            return w, p, c, e, steps, t1
+    raise RuntimeError("unreachable")
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    K, W = args.steps, args.warmup
+    budget = 150.0
+    # choose the sample grid so that W + K oracle steps take about `budget` seconds
+    w, p, c, e, _, t1 = cpu_sample(args.config, args.n, budget, K + W, threads)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(threads)
+    s = O.OracleSim(p)
+    s.set_fields(c, e)
+    s.run(W)
+    t0 = time.perf_counter()
+    s.run(K)
+    dt = time.perf_counter() - t0
+    n3 = p.nx * p.ny * p.nz
+    val = n3 * K / dt / 1e6
+    sample = (f"{K} time steps of the {w.name} deck on a {p.nx}^3 grid (FP64 oracle port, {threads} threads; "
+              f"the Fortran/MPI/P3DFFT reference cannot be built in this image)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": K,
+        "warmup": W, "ms_per_step": dt / K * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": f"synthetic (ran_2 uniform noise, seed {w.seed})",
+        "config": {"workload": w.name, "grid": [p.nx, p.ny, p.nz], "variants": p.nvar, "parallelism": "host threads"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU side
+def read_traffic(kernel: str):
+    """dram read+write bytes per launch of `kernel` from the committed ncu
+    summary (profiles/*.md line 'traffic_bytes_per_launch[<kernel>]: <bytes> at <grid>')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith(".md"):
+            continue
+        for ln in open(os.path.join(d, f)):
+            key = f"traffic_bytes_per_launch[{kernel}]:"
+            if ln.strip().startswith(key):
+                try:
+                    return float(ln.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200.sim import Simulation
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    K, W = args.steps, max(3, args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = CF.landau_config(args.config, n=args.n or None, precision=P.PREC_F32)
+    p32 = w.params
+    nx, ny, nz, V, E = p32.nx, p32.ny, p32.nz, p32.nvar, p32.numel
+    n3 = nx * ny * nz
+    seed = w.seed - rank
+    c0, e0 = _lib.init_uniform(nx, ny, nz, V, seed, w.c0, w.c_amp, w.eta_amp)
+    stream = torch.cuda.Stream(device=dev)
+
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    sim = Simulation(p32)
+    footprint = free0 - torch.cuda.mem_get_info(dev)[0]
+    sim.set_stream(stream.cuda_stream)
+    sim.set_fields(c0, e0)
+    sim.run(W, diag=True)
+
+    # ---------------- timed region: K FP32 steps with the fort.98 diagnostics
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    l0 = sim.launch_count
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        diag = sim.run(K, diag=True)
+        ev1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    launches = sim.launch_count - l0
+    clocks = sampler.stop()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * n3 * K / (ms / 1e3) / 1e6
+    if args.profile:
+        sim.close()
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"profile_run": w.name, "steps": K, "warmup": W, "ms_per_step": ms / K}), flush=True)
+        return 0
+    c32, e32, _, _ = sim.get_fields()
+
+    # ---------------- FP64 plain path, same deck and initial fields
+    p64 = p32.copy()
+    p64.precision = P.PREC_F64
+    sim64 = Simulation(p64)
+    sim64.set_stream(stream.cuda_stream)
+    sim64.set_fields(c0, e0)
+    sim64.run(W, diag=True)
+    K64 = min(K, 500)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    sim64.run(K64, diag=True)
+    b.record(stream)
+    stream.synchronize()
+    ms64 = max_over_ranks(a.elapsed_time(b))
+    value64 = world * n3 * K64 / (ms64 / 1e3) / 1e6
+    if K > K64:
+        sim64.run(K - K64, diag=False)
+    c64, e64, _, _ = sim64.get_fields()
+    sim64.close()
+    err_c = float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64))
+    err_e = float(np.linalg.norm(e32 - e64) / max(np.linalg.norm(e64), 1e-300))
+
+    # ---------------- per-kernel CUDA-event timing (roofline of the dominant kernel)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        pk = json.load(open(peaks_path))
+        peak, peak_src = float(pk["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    sim.timing(True)
+    kt = min(K, 100)
+    sim.run(kt, diag=True)
+    rep = sim.timing_report()
+    sim.timing(False)
+    tot = sum(v["ms"] for v in rep.values())
+    dom = max(rep, key=lambda k: rep[k]["ms"])
+    dr = rep[dom]
+    dom_ms = dr["ms"] / dr["launches"]
+    achieved = dr["bytes"] / dr["launches"] / (dom_ms / 1e3) / 1e9
+    traffic = read_traffic(dom)
+    step_bytes = sum(v["bytes"] for v in rep.values()) / kt
+    kernels = {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / v["launches"],
+                   "share": v["ms"] / tot, "GB/s": v["bytes"] / v["ms"] / 1e6} for k, v in
+               sorted(rep.items(), key=lambda kv: -kv[1]["ms"])}
+
+    # ---------------- end to end through the C-ABI with pinned host buffers
+    L = _lib.lib()
+    hc = torch.empty(E * n3, dtype=torch.float64).pin_memory()
+    hp = torch.empty(V * n3, dtype=torch.float64).pin_memory()
+    hc.copy_(torch.from_numpy(P.to_fortran(c32)))
+    hp.copy_(torch.from_numpy(P.to_fortran(e32)))
+    dp = C.POINTER(C.c_double)
+    pc = C.cast(hc.data_ptr(), dp)
+    pp = C.cast(hp.data_ptr(), dp)
+    rows = (P.MeuDiag * 1)()
+    ke = min(K, 100)
+    for _ in range(2):
+        L.meu_set_fields(sim.h, pc, pp, None)
+        L.meu_run(sim.h, 1, rows)
+        L.meu_get_fields(sim.h, pc, pp, None, None)
+    barrier()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(ke):
+        st1 = L.meu_set_fields(sim.h, pc, pp, None)
+        st2 = L.meu_run(sim.h, 1, rows)
+        st3 = L.meu_get_fields(sim.h, pc, pp, None, None)
+        if st1 or st2 or st3:
+            raise RuntimeError(f"C-ABI status {st1} {st2} {st3}")
+    b.record(stream)
+    stream.synchronize()
+    ms_e2e = max_over_ranks(a.elapsed_time(b))
+    e2e = world * n3 * ke / (ms_e2e / 1e3) / 1e6
+    # window form: upload once, K steps with diagnostics, download once
+    torch.cuda.synchronize()
+    a.record(stream)
+    L.meu_set_fields(sim.h, pc, pp, None)
+    rowsK = (P.MeuDiag * K)()
+    L.meu_run(sim.h, K, rowsK)
+    L.meu_get_fields(sim.h, pc, pp, None, None)
+    b.record(stream)
+    stream.synchronize()
+    ms_win = max_over_ranks(a.elapsed_time(b))
+    e2e_win = world * n3 * K / (ms_win / 1e3) / 1e6
+    sim.close()
+
+    # ---------------- CPU baseline (rank 0, N = 1): the oracle port on host cores
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        wc, pc64, cc, ec, steps, _ = cpu_sample(args.config, args.n, 20.0, 1, threads)
+        v, dt = oracle_throughput(pc64, cc, ec, steps, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{steps} FP64 time steps of {wc.name} on a {pc64.nx}^3 grid ({dt:.1f} s, {threads} threads)"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    l2_mb = 126
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": f"synthetic (ran_2 uniform noise c0={w.c0}+-{w.c_amp}, eta+-{w.eta_amp}, seed {w.seed})",
+        "config": {"workload": w.name, "grid": [nx, ny, nz], "variants": V, "free_energy": "landau",
+                   "elasticity": "homogeneous cubic 250/150/100, Green operator", "dt": p32.dt,
+                   "precision": "FP32 bulk; FP64 Omega(k), k=0 mode, reductions",
+                   "l2": f"device working set {footprint / 2**20:.0f} MiB > {l2_mb} MB L2, no flush",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64_plain": {"value": value64, "unit": UNIT, "steps": K64, "ms_per_step": ms64 / K64,
+                       "fp32_speedup": value / value64},
+        "err_vs_fp64": {"c_rel_l2": err_c, "eta_rel_l2": err_e, "after_steps": W + K},
+        "adjoint_forward_cost": None,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dr["bytes"] / dr["launches"],
+                     "kernel_ms_per_launch": dom_ms,
+                     "step_algorithmic_bytes": step_bytes,
+                     "step_frac": step_bytes / (ms / K / 1e3) / 1e9 / peak},
+        "kernels": kernels,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": (E + V) * n3 * 8,
+                "d2h_bytes_per_step": (E + V) * n3 * 8 + C.sizeof(P.MeuDiag), "steps": ke,
+                "form": "per step: meu_set_fields + meu_run(1) + meu_get_fields, pinned host buffers"},
+        "e2e_window": {"value": e2e_win, "unit": UNIT, "steps": K,
+                       "form": "meu_set_fields once, meu_run(K) with diagnostics, meu_get_fields once"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

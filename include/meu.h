@@ -179,6 +179,23 @@ void meu_init_uniform(meu_ran2_state* s, int32_t nx, int32_t ny, int32_t nz, int
 
 /* Diagnostics. --------------------------------------------------------- */
 
+/* Launch the handle's work on a caller-owned CUDA stream (cudaStream_t passed
+ * as void*; NULL returns to the handle's own stream).  The stream must outlive
+ * its use by the handle. */
+int meu_set_stream(meu_handle* h, void* cuda_stream);
+
+/* Per-kernel CUDA-event timing: enable = 1 clears and starts it, 0 stops it. */
+int meu_timing(meu_handle* h, int32_t enable);
+
+/* Per-kernel timing table: up to max rows of (name[32], launches, total ms,
+ * algorithmic bytes = compulsory reads + writes summed over the launches).
+ * Returns the number of kernel names (or -status). */
+int32_t meu_timing_report(meu_handle* h, int32_t max, char* names, int64_t* counts, double* total_ms,
+                          double* bytes);
+
+/* Number of kernels this handle has launched since creation. */
+int64_t meu_launch_count(const meu_handle* h);
+
 /* One f_trans / inv_trans pair (ModFunc.f:15-40) of a real (Nx,Ny,Nz) field on
  * the GPU, for transform tests: spec_out receives the scaled half spectrum
  * [z][y][kx] as interleaved re,im doubles (Nz*Ny*(Nx/2+1) complex), back_out

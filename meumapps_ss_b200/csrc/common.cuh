@@ -57,6 +57,14 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 16) {
   return (unsigned)g;
 }
 
+// Observer of kernel launches (launch counting and per-kernel event timing).
+// bytes = algorithmic bytes the launch must move (compulsory reads + writes).
+struct LaunchHook {
+  virtual ~LaunchHook() {}
+  virtual void begin(const char* name, double bytes, cudaStream_t st) = 0;
+  virtual void end(cudaStream_t st) = 0;
+};
+
 // Up to MAXF field pointers passed by value to batched kernels.
 constexpr int MAXF = 32;
 template <typename T> struct PtrList {

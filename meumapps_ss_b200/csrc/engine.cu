@@ -27,6 +27,23 @@ __global__ void k_finalize(const double* __restrict__ partials, int nb, const in
   block_reduce_store(acc, op, out + q);
 }
 
+// per-component sums of an AoS chunk (block partials; component e at out[e*RED_BLOCKS + b])
+__global__ void __launch_bounds__(RED_THREADS) k_aos_colsum(const double* __restrict__ src, int ncomp, int64_t nv,
+                                                            double* out) {
+  for (int e = 0; e < ncomp; ++e) {
+    double acc = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x)
+      acc += src[i * ncomp + e];
+    block_reduce_store(acc, 0, out + (int64_t)e * RED_BLOCKS + blockIdx.x);
+  }
+}
+__global__ void k_accumulate(const double* __restrict__ r, double* acc, int n) {
+  if (threadIdx.x < n) acc[threadIdx.x] += r[threadIdx.x];
+}
+__global__ void k_set_cmean(DevConst* K, const double* __restrict__ acc, int n, double inv_n3) {
+  if (threadIdx.x < n) K->c_mean[threadIdx.x] = acc[threadIdx.x] * inv_n3;
+}
+
 // AoS (component fastest, double) <-> SoA (R)
 template <typename R>
 __global__ void k_aos_to_soa(const double* __restrict__ src, R* __restrict__ dst, int ncomp, int64_t v0, int64_t nv,
@@ -91,14 +108,96 @@ __global__ void k_u_spectra(const DevConst* __restrict__ Kp, const cplx<R>* __re
 }
 
 // ==========================================================================
+// Launch counter and per-kernel CUDA-event timing (off unless requested).
+class Profiler : public LaunchHook {
+ public:
+  int64_t launches = 0;
+  bool on = false;
+  struct Stat { int64_t n = 0; double ms = 0, bytes = 0; };
+  std::vector<std::string> names;
+  std::vector<Stat> stats;
+  ~Profiler() override {
+    for (auto& q : pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  void begin(const char* n, double b, cudaStream_t st) override {
+    ++launches;
+    if (!on) return;
+    cur_id = id_of(n);
+    cur_bytes = b;
+    cur_a = get();
+    MEU_CUDA(cudaEventRecord(cur_a, st));
+  }
+  void end(cudaStream_t st) override {
+    if (!on) return;
+    cudaEvent_t e = get();
+    MEU_CUDA(cudaEventRecord(e, st));
+    pend.push_back({cur_id, cur_bytes, cur_a, e});
+  }
+  void resolve() {
+    for (auto& q : pend) {
+      MEU_CUDA(cudaEventSynchronize(q.b));
+      float ms = 0;
+      MEU_CUDA(cudaEventElapsedTime(&ms, q.a, q.b));
+      stats[q.id].n += 1;
+      stats[q.id].ms += ms;
+      stats[q.id].bytes += q.bytes;
+      pool.push_back(q.a);
+      pool.push_back(q.b);
+    }
+    pend.clear();
+  }
+  void reset() {
+    resolve();
+    names.clear();
+    stats.clear();
+  }
+
+ private:
+  struct Pend { int id; double bytes; cudaEvent_t a, b; };
+  std::vector<Pend> pend;
+  std::vector<cudaEvent_t> pool;
+  int cur_id = 0;
+  double cur_bytes = 0;
+  cudaEvent_t cur_a = nullptr;
+  int id_of(const char* n) {
+    for (size_t i = 0; i < names.size(); ++i)
+      if (names[i] == n) return (int)i;
+    names.push_back(n);
+    stats.push_back(Stat());
+    return (int)names.size() - 1;
+  }
+  cudaEvent_t get() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      MEU_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+};
+
+#define KLAUNCH(name, bytes, ...)  \
+  do {                             \
+    prof.begin(name, bytes, st);   \
+    __VA_ARGS__;                   \
+    MEU_CHECK_LAUNCH();            \
+    prof.end(st);                  \
+  } while (0)
+
+// ==========================================================================
 struct EngineBase {
   virtual ~EngineBase() {}
   virtual void set_fields(const double* cons, const double* phi, const double* ustate) = 0;
   virtual void add_noise(const double* incr) = 0;
   virtual void run(int nsteps, meu_diag* diag) = 0;
   virtual void get_fields(double* cons, double* phi, double* el_en, double* ustate) = 0;
+  virtual void set_stream(cudaStream_t s) = 0;
   int64_t step = 0;
   std::string err;
+  Profiler prof;
 };
 
 template <typename R>
@@ -112,13 +211,14 @@ class Engine : public EngineBase {
   void add_noise(const double* incr) override;
   void run(int nsteps, meu_diag* diag) override;
   void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
+  void set_stream(cudaStream_t s) override { st = s ? s : own_st; }
 
  private:
   meu_params P;
   DevConst hK;
   DevConst* dK = nullptr;
   std::unique_ptr<FFT3> fft;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr, own_st = nullptr;
   int V, E;
   int64_t n3, nk;
   // device buffers
@@ -181,6 +281,13 @@ class Engine : public EngineBase {
   void kks_step(meu_diag* d);
   void landau_step(meu_diag* d);
   void end_step(meu_diag* d, int clip);
+  void flush_hist(meu_diag* diag);
+  static constexpr int HIST_MAX = 4096;
+  double* hist = nullptr;  // per-step reductions [HIST_MAX][Q_STEP_COUNT]
+  double* cmean_acc = nullptr;
+  int hist_n = 0;
+  std::vector<int64_t> hist_step = std::vector<int64_t>(HIST_MAX);
+  std::vector<int> hist_iters = std::vector<int>(HIST_MAX);
 };
 
 template <typename R>
@@ -198,8 +305,10 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   for (int n = 0; n < p.numph; ++n) sum += p.nvar_ph[n];
   if (V + 1 - sum != 0) throw CudaError("variant numbers (initerr 1)", MEU_ERR_BADARG);
   step = p.step;
-  MEU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  MEU_CUDA(cudaStreamCreateWithFlags(&own_st, cudaStreamNonBlocking));
+  st = own_st;
   fft.reset(new FFT3(p.nx, p.ny, p.nz, sizeof(R) == 8));
+  fft->hook = &prof;
   n3 = fft->n3();
   nk = fft->nk();
   // ---- device constants
@@ -293,6 +402,8 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   sp = dalloc<C>((int64_t)NS * nk);
   partials = dalloc<double>((int64_t)Q_TOTAL * RED_BLOCKS);
   results = dalloc<double>(Q_TOTAL);
+  hist = dalloc<double>((int64_t)HIST_MAX * Q_STEP_COUNT);
+  cmean_acc = dalloc<double>(MEU_MAX_EL);
   d_ops = dalloc<int>(Q_TOTAL);
   d_err = dalloc<int>(1);
   dK = dalloc<DevConst>(1);
@@ -319,11 +430,13 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
 template <typename R>
 Engine<R>::~Engine() {
   if (st) cudaStreamSynchronize(st);
+  if (own_st) cudaStreamSynchronize(own_st);
+  prof.reset();
   for (void* q : allocs) cudaFree(q);
   if (h_results) cudaFreeHost(h_results);
   if (h_err) cudaFreeHost(h_err);
   fft.reset();
-  if (st) cudaStreamDestroy(st);
+  if (own_st) cudaStreamDestroy(own_st);
 }
 
 template <typename R>
@@ -339,8 +452,7 @@ void Engine<R>::check_err() {
 
 template <typename R>
 void Engine<R>::finalize(int q0, int nq) {
-  k_finalize<<<nq, 256, 0, st>>>(partials + (int64_t)q0 * RED_BLOCKS, RED_BLOCKS, d_ops + q0, results + q0);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("finalize", 8.0 * nq * RED_BLOCKS, k_finalize<<<nq, 256, 0, st>>>(partials + (int64_t)q0 * RED_BLOCKS, RED_BLOCKS, d_ops + q0, results + q0));
 }
 
 // ---- host-side AoS conversion in chunks through the staging buffer
@@ -351,21 +463,27 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
       const int64_t nv = std::min(chunk, n3 - v0);
       MEU_CUDA(cudaMemcpyAsync(stage, src + v0 * ncomp, sizeof(double) * nv * ncomp, cudaMemcpyHostToDevice, st));
-      k_aos_to_soa<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(stage, dst, ncomp, v0, nv, n3, add);
-      MEU_CHECK_LAUNCH();
+      KLAUNCH("aos_to_soa", (double)nv * ncomp * (8 + sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(stage, dst, ncomp, v0, nv, n3, add));
     }
   };
-  if (cons) up(cons, c, E, 0);
-  if (phi_in) up(phi_in, phi, V, 0);
-  // conserved mean per solute (k = 0 mode), FP64
   if (cons) {
-    for (int e = 0; e < E; ++e) {
-      long double s = 0;
-      for (int64_t i = 0; i < n3; ++i) s += cons[i * E + e];
-      hK.c_mean[e] = (double)(s / (long double)n3);
+    // upload + conserved FP64 mean of each solute (the k = 0 mode), summed from
+    // the double input in a fixed order: per chunk, block partials -> finalize -> accumulate
+    MEU_CUDA(cudaMemsetAsync(cmean_acc, 0, sizeof(double) * MEU_MAX_EL, st));
+    const int64_t chunk = std::max<int64_t>(stage_elems / E, 1);
+    for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+      const int64_t nv = std::min(chunk, n3 - v0);
+      MEU_CUDA(cudaMemcpyAsync(stage, cons + v0 * E, sizeof(double) * nv * E, cudaMemcpyHostToDevice, st));
+      KLAUNCH("aos_to_soa", (double)nv * E * (8 + sizeof(R)),
+              k_aos_to_soa<R><<<grid_for(nv * E, 256), 256, 0, st>>>(stage, c, E, v0, nv, n3, 0));
+      KLAUNCH("aos_colsum", (double)nv * E * 8,
+              k_aos_colsum<<<RED_BLOCKS, RED_THREADS, 0, st>>>(stage, E, nv, partials + (int64_t)Q_CSUM0 * RED_BLOCKS));
+      finalize(Q_CSUM0, E);
+      KLAUNCH("accumulate", 16.0 * E, k_accumulate<<<1, 32, 0, st>>>(results + Q_CSUM0, cmean_acc, E));
     }
-    MEU_CUDA(cudaMemcpyAsync(dK, &hK, sizeof(DevConst), cudaMemcpyHostToDevice, st));
+    KLAUNCH("set_cmean", 16.0 * E, k_set_cmean<<<1, 32, 0, st>>>(dK, cmean_acc, E, 1.0 / (double)n3));
   }
+  if (phi_in) up(phi_in, phi, V, 0);
   if (strain) {
     if (ustate) {
       // u (3 x n3) -> u^ ; grads (9 x n3) -> engineering strain
@@ -374,8 +492,7 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
         for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
           const int64_t nv = std::min(chunk, n3 - v0);
           MEU_CUDA(cudaMemcpyAsync(stage, ustate + i * n3 + v0, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
-          k_convert_in<R><<<grid_for(nv, 256), 256, 0, st>>>(stage, wr + v0, nv);
-          MEU_CHECK_LAUNCH();
+          KLAUNCH("convert_in", (double)nv * (8 + sizeof(R)), k_convert_in<R><<<grid_for(nv, 256), 256, 0, st>>>(stage, wr + v0, nv));
         }
         PtrList<const R> a{};
         PtrList<C> b{};
@@ -390,8 +507,7 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
         for (int g = 0; g < 9; ++g)
           MEU_CUDA(cudaMemcpyAsync(stage + (int64_t)g * nv, ustate + (int64_t)(3 + g) * n3 + v0, sizeof(double) * nv,
                                    cudaMemcpyHostToDevice, st));
-        k_grads_to_strain<R><<<grid_for(nv, 256), 256, 0, st>>>(stage, strain + v0, nv, n3);
-        MEU_CHECK_LAUNCH();
+        KLAUNCH("grads_to_strain", (double)nv * (9 * 8 + 6 * sizeof(R)), k_grads_to_strain<R><<<grid_for(nv, 256), 256, 0, st>>>(stage, strain + v0, nv, n3));
       }
       el_ready = true;
     } else {
@@ -410,8 +526,7 @@ void Engine<R>::add_noise(const double* incr) {
   for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
     const int64_t nv = std::min(chunk, n3 - v0);
     MEU_CUDA(cudaMemcpyAsync(stage, incr + v0 * V, sizeof(double) * nv * V, cudaMemcpyHostToDevice, st));
-    k_aos_to_soa<R><<<grid_for(nv * V, 256), 256, 0, st>>>(stage, noise, V, v0, nv, n3, 1);
-    MEU_CHECK_LAUNCH();
+    KLAUNCH("aos_to_soa", (double)nv * V * (8 + 2 * sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * V, 256), 256, 0, st>>>(stage, noise, V, v0, nv, n3, 1));
   }
   MEU_CUDA(cudaStreamSynchronize(st));
 }
@@ -422,8 +537,7 @@ void Engine<R>::get_fields(double* cons, double* phi_out, double* el_out, double
     const int64_t chunk = std::max<int64_t>(stage_elems / ncomp, 1);
     for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
       const int64_t nv = std::min(chunk, n3 - v0);
-      k_soa_to_aos<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(src, stage, ncomp, v0, nv, n3);
-      MEU_CHECK_LAUNCH();
+      KLAUNCH("soa_to_aos", (double)nv * ncomp * (8 + sizeof(R)), k_soa_to_aos<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(src, stage, ncomp, v0, nv, n3));
       MEU_CUDA(cudaMemcpyAsync(dst + v0 * ncomp, stage, sizeof(double) * nv * ncomp, cudaMemcpyDeviceToHost, st));
     }
   };
@@ -432,8 +546,7 @@ void Engine<R>::get_fields(double* cons, double* phi_out, double* el_out, double
   if (el_out) down(el_en, el_out, 1);
   if (ustate) {
     if (uk) {
-      k_u_spectra<R><<<gridk(), 256, 0, st>>>(dK, uk, specs(0, 12));
-      MEU_CHECK_LAUNCH();
+      KLAUNCH("u_spectra", 15.0 * nk * sizeof(C), k_u_spectra<R><<<gridk(), 256, 0, st>>>(dK, uk, specs(0, 12)));
       for (int f = 0; f < 12; ++f) {
         PtrList<C> a{};
         PtrList<R> b{};
@@ -462,8 +575,7 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
     fwd_list(in, 0);
-    k_el_zeroth<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, uk, specs(V, 6), d_err);
-    MEU_CHECK_LAUNCH();
+    KLAUNCH("el_zeroth", (double)(V + 9) * nk * sizeof(C), k_el_zeroth<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, uk, specs(V, 6), d_err));
     std::vector<R*> out;
     for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
     inv_list(V, out);
@@ -478,13 +590,11 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
       niter += 1;
       total += 1;
       if (total > 100000) throw CudaError("elastic iteration runaway", MEU_ERR_NOT_CONVERGED);
-      k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err);
-      MEU_CHECK_LAUNCH();
+      KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
       std::vector<const R*> in;
       for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
       fwd_list(in, 0);
-      k_el_k<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 6), uk, partials, d_err);
-      MEU_CHECK_LAUNCH();
+      KLAUNCH("el_k", 18.0 * nk * sizeof(C), k_el_k<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 6), uk, partials, d_err));
       std::vector<R*> out;
       for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
       inv_list(0, out);
@@ -520,10 +630,9 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
     }
   }
   last_iters = total;
-  k_elener<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+  KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
-                                                  partials, d_err);
-  MEU_CHECK_LAUNCH();
+                                                  partials, d_err));
 }
 
 // ------------------------------------------------------------------- KKS step
@@ -536,16 +645,14 @@ void Engine<R>::kks_step(meu_diag* d) {
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
     fwd_list(in, 0);
-    k_kks_grad<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), specs(V, 4 * V), V);
-    MEU_CHECK_LAUNCH();
+    KLAUNCH("kks_grad", (double)5 * V * nk * sizeof(C), k_kks_grad<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), specs(V, 4 * V), V));
     std::vector<R*> out;
     for (int f = 0; f < 4 * V; ++f) out.push_back(field(wr, f));
     inv_list(V, out);
   }
   // local driving force (:619-845)
-  k_kks_point<<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, (const double*)phi, (const double*)c, (const double*)wr,
-                                                  (double*)pphi, (double*)fd, (double*)fc, partials, d_err);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("kks_point", (double)(7 * V + 4 * E) * n3 * sizeof(R), k_kks_point<<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, (const double*)phi, (const double*)c, (const double*)wr,
+                                                  (double*)pphi, (double*)fd, (double*)fc, partials, d_err));
   // elasticity (:851-880)
   last_iters = 0;
   if (step >= P.elastep0 && P.elastic != MEU_ELAST_NONE) {
@@ -556,19 +663,16 @@ void Engine<R>::kks_step(meu_diag* d) {
   // diffusion (:910-949)
   for (int e = 0; e < E; ++e) {
     fwd({field(c, e), field(fc, 3 * e), field(fc, 3 * e + 1), field(fc, 3 * e + 2)}, 0);
-    k_kks_ch<R><<<gridk(), 256, 0, st>>>(dK, spec(0), spec(1), spec(2), spec(3), P.dt * P.cmobs[e]);
-    MEU_CHECK_LAUNCH();
+    KLAUNCH("kks_ch", 5.0 * nk * sizeof(C), k_kks_ch<R><<<gridk(), 256, 0, st>>>(dK, spec(0), spec(1), spec(2), spec(3), P.dt * P.cmobs[e]));
     inv_list(0, {field(c, e)});
   }
   // TDGL (:955-1001)
-  k_tdgl_pre<R><<<grid_for((int64_t)V * n3, 256), 256, 0, st>>>(phi, fd, noise, wr, (int64_t)V * n3, P.dt * P.b_mob, P.dt);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("tdgl_pre", 4.0 * V * n3 * sizeof(R), k_tdgl_pre<R><<<grid_for((int64_t)V * n3, 256), 256, 0, st>>>(phi, fd, noise, wr, (int64_t)V * n3, P.dt * P.b_mob, P.dt));
   {
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(wr, v));
     fwd_list(in, 0);
-    k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob);
-    MEU_CHECK_LAUNCH();
+    KLAUNCH("tdgl", 2.0 * V * nk * sizeof(C), k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob));
     std::vector<R*> out;
     for (int v = 0; v < V; ++v) out.push_back(field(phi, v));
     inv_list(0, out);
@@ -584,8 +688,7 @@ void Engine<R>::landau_step(meu_diag* d) {
   const bool homog = elast && P.elastic == MEU_ELAST_HOMOG;
   const bool het = elast && P.elastic == MEU_ELAST_HETERO;
   R* mu = field(wr, 0);
-  k_lan_a<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, pphi, mu, partials);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("lan_a", (double)(2 * V + 2) * n3 * sizeof(R), k_lan_a<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, pphi, mu, partials));
   // [theta_v, mu, c, eta_v]
   {
     std::vector<const R*> in;
@@ -595,8 +698,7 @@ void Engine<R>::landau_step(meu_diag* d) {
     for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
     fwd_list(in, 0);
   }
-  k_lan_k1<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 2 * V + 2), V, homog ? 1 : 0, P.diag_energy, partials, d_err);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("lan_k1", (double)(homog ? 3 * V + 3 : 2 * V + 3) * nk * sizeof(C), k_lan_k1<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 2 * V + 2), V, homog ? 1 : 0, P.diag_energy, partials, d_err));
   R* phel = field(wr, 1);  // V fields: strain interaction (homog) or el_grad (hetero)
   {
     std::vector<R*> out;
@@ -617,14 +719,12 @@ void Engine<R>::landau_step(meu_diag* d) {
   } else if (!homog) {
     MEU_CUDA(cudaMemsetAsync(el_en, 0, sizeof(R) * n3, st));
   }
-  k_lan_b<R><<<gridr(), 256, 0, st>>>(dK, c, phi, elast ? phel : nullptr, homog ? 1 : 0, pphi);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("lan_b", (double)(3 * V + 1) * n3 * sizeof(R), k_lan_b<R><<<gridr(), 256, 0, st>>>(dK, c, phi, elast ? phel : nullptr, homog ? 1 : 0, pphi));
   {
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
     fwd_list(in, 0);
-    k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob);
-    MEU_CHECK_LAUNCH();
+    KLAUNCH("tdgl", 2.0 * V * nk * sizeof(C), k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob));
     std::vector<R*> out;
     for (int v = 0; v < V; ++v) out.push_back(field(phi, v));
     inv_list(0, out);
@@ -635,56 +735,76 @@ void Engine<R>::landau_step(meu_diag* d) {
 
 template <typename R>
 void Engine<R>::end_step(meu_diag* d, int clip) {
-  k_stats<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, clip, partials);
-  MEU_CHECK_LAUNCH();
+  KLAUNCH("stats", (double)(E + V * (clip ? 2 : 1)) * n3 * sizeof(R),
+          k_stats<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, clip, partials));
   finalize(0, Q_STEP_COUNT);
-  MEU_CUDA(cudaMemcpyAsync(h_results, results, sizeof(double) * Q_STEP_COUNT, cudaMemcpyDeviceToHost, st));
-  if (d) {
-    check_err();
-    const double* r = h_results;
-    const double sn3 = (double)n3;
-    d->step = step;
-    d->el_iters = last_iters;
-    d->status = 0;
-    const bool lan = P.model == MEU_MODEL_LANDAU;
-    d->fint = lan ? r[Q_FINT] * sn3 : r[Q_FINT];
-    d->fw = r[Q_FW];
-    d->fch = r[Q_FCH];
-    d->elen = (lan && P.elastic == MEU_ELAST_HOMOG) ? r[Q_ELEN] * sn3 : r[Q_ELEN];
-    d->etot = d->fint + d->fch + d->elen + d->fw;
-    d->glob_min = prev_min;
-    d->glob_max = prev_max;
-    d->phi_max = prev_phimax;
-    d->solid = prev_solid / sn3;
-    d->cmin = r[Q_CMIN];
-    d->cmax = r[Q_CMAX];
-    d->phimax = r[Q_PHIMAX];
-    d->solid_now = r[Q_SOLID] / sn3;
-    for (int e = 0; e < MEU_MAX_EL; ++e) d->cavg[e] = e < E ? r[Q_CSUM0 + e] / sn3 : 0.0;
+  // keep this step's reductions on the device; they are read once per meu_run
+  MEU_CUDA(cudaMemcpyAsync(hist + (int64_t)hist_n * Q_STEP_COUNT, results, sizeof(double) * Q_STEP_COUNT,
+                           cudaMemcpyDeviceToDevice, st));
+  hist_step[hist_n] = step;
+  hist_iters[hist_n] = last_iters;
+  hist_n += 1;
+  (void)d;
+  step += 1;
+}
+
+// Turn the device history of reductions into fort.98 / fort.99 rows.
+template <typename R>
+void Engine<R>::flush_hist(meu_diag* diag) {
+  if (hist_n == 0) return;
+  std::vector<double> h((size_t)hist_n * Q_STEP_COUNT);
+  MEU_CUDA(cudaMemcpyAsync(h.data(), hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+  MEU_CUDA(cudaStreamSynchronize(st));
+  const double sn3 = (double)n3;
+  const bool lan = P.model == MEU_MODEL_LANDAU;
+  for (int i = 0; i < hist_n; ++i) {
+    const double* r = h.data() + (size_t)i * Q_STEP_COUNT;
+    if (diag) {
+      meu_diag* d = diag + i;
+      d->step = hist_step[i];
+      d->el_iters = hist_iters[i];
+      d->status = 0;
+      d->fint = lan ? r[Q_FINT] * sn3 : r[Q_FINT];
+      d->fw = r[Q_FW];
+      d->fch = r[Q_FCH];
+      d->elen = (lan && P.elastic == MEU_ELAST_HOMOG) ? r[Q_ELEN] * sn3 : r[Q_ELEN];
+      d->etot = d->fint + d->fch + d->elen + d->fw;
+      d->glob_min = prev_min;
+      d->glob_max = prev_max;
+      d->phi_max = prev_phimax;
+      d->solid = prev_solid / sn3;
+      d->cmin = r[Q_CMIN];
+      d->cmax = r[Q_CMAX];
+      d->phimax = r[Q_PHIMAX];
+      d->solid_now = r[Q_SOLID] / sn3;
+      for (int e = 0; e < MEU_MAX_EL; ++e) d->cavg[e] = e < E ? r[Q_CSUM0 + e] / sn3 : 0.0;
+    }
     prev_min = r[Q_CMIN];
     prev_max = r[Q_CMAX];
     prev_phimax = r[Q_PHIMAX];
     prev_solid = r[Q_SOLID];
-    if (!std::isfinite(d->etot) || !std::isfinite(d->cavg[0]))
-      throw CudaError("non-finite field values", MEU_ERR_NOT_FINITE);
+    const double et = r[Q_FINT] + r[Q_FCH] + r[Q_ELEN] + r[Q_FW];
+    if (!std::isfinite(et) || !std::isfinite(r[Q_CSUM0]) || !std::isfinite(r[Q_SOLID])) {
+      hist_n = 0;
+      throw CudaError("non-finite field values at step " + std::to_string(hist_step[i]), MEU_ERR_NOT_FINITE);
+    }
   }
-  step += 1;
+  hist_n = 0;
 }
 
 template <typename R>
 void Engine<R>::run(int nsteps, meu_diag* diag) {
-  for (int i = 0; i < nsteps; ++i) {
-    meu_diag* d = diag ? diag + i : nullptr;
-    if (P.model == MEU_MODEL_KKS) kks_step(d);
-    else landau_step(d);
-  }
-  check_err();
-  if (!diag && nsteps > 0) {
-    const double* r = h_results;
-    prev_min = r[Q_CMIN];
-    prev_max = r[Q_CMAX];
-    prev_phimax = r[Q_PHIMAX];
-    prev_solid = r[Q_SOLID];
+  int done = 0;
+  hist_n = 0;
+  while (done < nsteps) {
+    const int chunk = std::min(nsteps - done, HIST_MAX);
+    for (int i = 0; i < chunk; ++i) {
+      if (P.model == MEU_MODEL_KKS) kks_step(nullptr);
+      else landau_step(nullptr);
+    }
+    check_err();
+    flush_hist(diag ? diag + done : nullptr);
+    done += chunk;
   }
 }
 
@@ -771,6 +891,45 @@ const char* meu_last_error(const meu_handle* h) {
   if (!h) return g_create_err.c_str();
   return h->err.c_str();
 }
+
+int meu_set_stream(meu_handle* h, void* cuda_stream) {
+  if (!h) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->set_stream((cudaStream_t)cuda_stream));
+  return MEU_OK;
+}
+
+int meu_timing(meu_handle* h, int32_t enable) {
+  if (!h) return MEU_ERR_BADARG;
+  MEU_TRY(h, {
+    h->eng->prof.reset();
+    h->eng->prof.on = enable != 0;
+  });
+  return MEU_OK;
+}
+
+int32_t meu_timing_report(meu_handle* h, int32_t max, char* names, int64_t* counts, double* total_ms, double* bytes) {
+  if (!h || max < 0) return -MEU_ERR_BADARG;
+  try {
+    meu::Profiler& pr = h->eng->prof;
+    pr.resolve();
+    const int n = (int)pr.names.size();
+    for (int i = 0; i < n && i < max; ++i) {
+      if (names) {
+        memset(names + 32 * i, 0, 32);
+        strncpy(names + 32 * i, pr.names[i].c_str(), 31);
+      }
+      if (counts) counts[i] = pr.stats[i].n;
+      if (total_ms) total_ms[i] = pr.stats[i].ms;
+      if (bytes) bytes[i] = pr.stats[i].bytes;
+    }
+    return n;
+  } catch (const meu::CudaError& e) {
+    h->err = e.what();
+    return -e.code;
+  }
+}
+
+int64_t meu_launch_count(const meu_handle* h) { return h ? h->eng->prof.launches : -1; }
 
 int meu_destroy(meu_handle* h) {
   if (!h) return MEU_ERR_BADARG;

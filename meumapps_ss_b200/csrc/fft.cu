@@ -262,6 +262,17 @@ static inline int col_tile(int L, bool fp64) {
   return 16;
 }
 
+struct HookScope {
+  LaunchHook* h;
+  cudaStream_t st;
+  HookScope(LaunchHook* h_, const char* n, double b, cudaStream_t s) : h(h_), st(s) {
+    if (h) h->begin(n, b, st);
+  }
+  ~HookScope() {
+    if (h) h->end(st);
+  }
+};
+
 template <typename R>
 void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const {
   using C = cplx<R>;
@@ -271,7 +282,8 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
   size_t sm = (size_t)rpb * odd_pitch(Lx) * sizeof(C);
   set_smem<R>((const void*)k_rows_r2c<R>, sm);
   dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
-  k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw);
+  { HookScope hs_(hook, "fft_x_r2c", (double)nf * (n3() * sizeof(R) + nk() * sizeof(C)), st);
+  k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
   // y columns: outer = z, inner = nxh
   {
@@ -279,7 +291,8 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     size_t s2 = (size_t)ny * tm * sizeof(C);
     set_smem<R>((const void*)k_cols<R, true>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
-    k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1);
+    { HookScope hs_(hook, "fft_y_fwd", 2.0 * nf * nk() * sizeof(C), st);
+  k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
   // z columns: outer = 1, inner = ny*nxh
@@ -289,7 +302,8 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     set_smem<R>((const void*)k_cols<R, true>, s3);
     int inner = ny * nxh;
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
-    k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, (R)(1.0 / ((double)nx * ny * nz)));
+    { HookScope hs_(hook, "fft_z_fwd", 2.0 * nf * nk() * sizeof(C), st);
+  k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, (R)(1.0 / ((double)nx * ny * nz))); }
     MEU_CHECK_LAUNCH();
   }
 }
@@ -303,7 +317,8 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     set_smem<R>((const void*)k_cols<R, false>, s3);
     int inner = ny * nxh;
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
-    k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1);
+    { HookScope hs_(hook, "fft_z_inv", 2.0 * nf * nk() * sizeof(C), st);
+  k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1); }
     MEU_CHECK_LAUNCH();
   }
   {
@@ -311,7 +326,8 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     size_t s2 = (size_t)ny * tm * sizeof(C);
     set_smem<R>((const void*)k_cols<R, false>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
-    k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1);
+    { HookScope hs_(hook, "fft_y_inv", 2.0 * nf * nk() * sizeof(C), st);
+  k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
   const int Lx = px.L;
@@ -322,7 +338,8 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
   PtrList<const C> cin;
   for (int f = 0; f < MAXF; ++f) cin.p[f] = in.p[f];
   dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
-  k_rows_c2r<R><<<g, 256, sm, st>>>(cin, out, nx, nrows, px, (const C*)post_tw);
+  { HookScope hs_(hook, "fft_x_c2r", (double)nf * (n3() * sizeof(R) + nk() * sizeof(C)), st);
+  k_rows_c2r<R><<<g, 256, sm, st>>>(cin, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
 }
 

@@ -179,6 +179,7 @@ class FFT3 {
   void inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
 
   LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
+  LaunchHook* hook = nullptr;
   const void* post_tw;  // cplx<R>[nx/2+1]: exp(-2 pi i k / nx)
   bool fp64;
 

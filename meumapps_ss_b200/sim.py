@@ -89,6 +89,32 @@ class Simulation:
             return None
         return P.diag_to_dict(list(rows)[:nsteps])
 
+    # -- instrumentation --
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(lib().meu_set_stream(self.h, C.c_void_p(int(stream_ptr)) if stream_ptr else None))
+
+    def timing(self, enable: bool) -> None:
+        self._check(lib().meu_timing(self.h, 1 if enable else 0))
+
+    def timing_report(self) -> Dict[str, Dict[str, float]]:
+        mx = 64
+        names = C.create_string_buffer(32 * mx)
+        cnt = (C.c_int64 * mx)()
+        ms = (C.c_double * mx)()
+        by = (C.c_double * mx)()
+        n = lib().meu_timing_report(self.h, mx, names, cnt, ms, by)
+        if n < 0:
+            raise MeuError(-n, lib().meu_last_error(self.h).decode())
+        out = {}
+        for i in range(min(n, mx)):
+            nm = names.raw[32 * i:32 * i + 32].split(b"\0")[0].decode()
+            out[nm] = {"launches": int(cnt[i]), "ms": float(ms[i]), "bytes": float(by[i])}
+        return out
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().meu_launch_count(self.h))
+
     @property
     def step(self) -> int:
         return int(lib().meu_get_step(self.h))
