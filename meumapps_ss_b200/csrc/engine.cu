@@ -45,24 +45,26 @@ __global__ void k_set_cmean(DevConst* K, const double* __restrict__ acc, int n, 
 }
 
 // AoS (component fastest, double) <-> SoA (R)
+// offs: NULL or per-component offsets subtracted on the way in (added on the way out)
 template <typename R>
 __global__ void k_aos_to_soa(const double* __restrict__ src, R* __restrict__ dst, int ncomp, int64_t v0, int64_t nv,
-                             int64_t n3, int add) {
+                             int64_t n3, int add, const double* offs) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv * ncomp; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t vox = i / ncomp;
     const int c = (int)(i - vox * ncomp);
     R* d = dst + (int64_t)c * n3 + v0 + vox;
-    if (add) *d = (R)((double)*d + src[i]);
-    else *d = (R)src[i];
+    const double v = offs ? src[i] - offs[c] : src[i];
+    if (add) *d = (R)((double)*d + v);
+    else *d = (R)v;
   }
 }
 template <typename R>
 __global__ void k_soa_to_aos(const R* __restrict__ src, double* __restrict__ dst, int ncomp, int64_t v0, int64_t nv,
-                             int64_t n3) {
+                             int64_t n3, const double* offs) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv * ncomp; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t vox = i / ncomp;
     const int c = (int)(i - vox * ncomp);
-    dst[i] = (double)src[(int64_t)c * n3 + v0 + vox];
+    dst[i] = (double)src[(int64_t)c * n3 + v0 + vox] + (offs ? offs[c] : 0.0);
   }
 }
 template <typename R>
@@ -327,6 +329,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     }
   }
   hK.zdim = p.numph * p.numel;
+  hK.c_shift = (p.model == MEU_MODEL_LANDAU) ? 1 : 0;
   if (p.model == MEU_MODEL_KKS) {
     const int numel = p.numel, numph = p.numph, zdim = hK.zdim;
     for (int e = 1; e <= numel; ++e) {
@@ -463,7 +466,7 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
       const int64_t nv = std::min(chunk, n3 - v0);
       MEU_CUDA(cudaMemcpyAsync(stage, src + v0 * ncomp, sizeof(double) * nv * ncomp, cudaMemcpyHostToDevice, st));
-      KLAUNCH("aos_to_soa", (double)nv * ncomp * (8 + sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(stage, dst, ncomp, v0, nv, n3, add));
+      KLAUNCH("aos_to_soa", (double)nv * ncomp * (8 + sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(stage, dst, ncomp, v0, nv, n3, add, nullptr));
     }
   };
   if (cons) {
@@ -471,17 +474,24 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     // the double input in a fixed order: per chunk, block partials -> finalize -> accumulate
     MEU_CUDA(cudaMemsetAsync(cmean_acc, 0, sizeof(double) * MEU_MAX_EL, st));
     const int64_t chunk = std::max<int64_t>(stage_elems / E, 1);
+    const bool one_chunk = chunk >= n3;
     for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
       const int64_t nv = std::min(chunk, n3 - v0);
       MEU_CUDA(cudaMemcpyAsync(stage, cons + v0 * E, sizeof(double) * nv * E, cudaMemcpyHostToDevice, st));
-      KLAUNCH("aos_to_soa", (double)nv * E * (8 + sizeof(R)),
-              k_aos_to_soa<R><<<grid_for(nv * E, 256), 256, 0, st>>>(stage, c, E, v0, nv, n3, 0));
       KLAUNCH("aos_colsum", (double)nv * E * 8,
               k_aos_colsum<<<RED_BLOCKS, RED_THREADS, 0, st>>>(stage, E, nv, partials + (int64_t)Q_CSUM0 * RED_BLOCKS));
       finalize(Q_CSUM0, E);
       KLAUNCH("accumulate", 16.0 * E, k_accumulate<<<1, 32, 0, st>>>(results + Q_CSUM0, cmean_acc, E));
     }
     KLAUNCH("set_cmean", 16.0 * E, k_set_cmean<<<1, 32, 0, st>>>(dK, cmean_acc, E, 1.0 / (double)n3));
+    const double* offs = hK.c_shift ? dK->c_mean : nullptr;
+    for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
+      const int64_t nv = std::min(chunk, n3 - v0);
+      if (!one_chunk)
+        MEU_CUDA(cudaMemcpyAsync(stage, cons + v0 * E, sizeof(double) * nv * E, cudaMemcpyHostToDevice, st));
+      KLAUNCH("aos_to_soa", (double)nv * E * (8 + sizeof(R)),
+              k_aos_to_soa<R><<<grid_for(nv * E, 256), 256, 0, st>>>(stage, c, E, v0, nv, n3, 0, offs));
+    }
   }
   if (phi_in) up(phi_in, phi, V, 0);
   if (strain) {
@@ -526,22 +536,22 @@ void Engine<R>::add_noise(const double* incr) {
   for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
     const int64_t nv = std::min(chunk, n3 - v0);
     MEU_CUDA(cudaMemcpyAsync(stage, incr + v0 * V, sizeof(double) * nv * V, cudaMemcpyHostToDevice, st));
-    KLAUNCH("aos_to_soa", (double)nv * V * (8 + 2 * sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * V, 256), 256, 0, st>>>(stage, noise, V, v0, nv, n3, 1));
+    KLAUNCH("aos_to_soa", (double)nv * V * (8 + 2 * sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * V, 256), 256, 0, st>>>(stage, noise, V, v0, nv, n3, 1, nullptr));
   }
   MEU_CUDA(cudaStreamSynchronize(st));
 }
 
 template <typename R>
 void Engine<R>::get_fields(double* cons, double* phi_out, double* el_out, double* ustate) {
-  auto down = [&](const R* src, double* dst, int ncomp) {
+  auto down = [&](const R* src, double* dst, int ncomp, const double* offs = nullptr) {
     const int64_t chunk = std::max<int64_t>(stage_elems / ncomp, 1);
     for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
       const int64_t nv = std::min(chunk, n3 - v0);
-      KLAUNCH("soa_to_aos", (double)nv * ncomp * (8 + sizeof(R)), k_soa_to_aos<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(src, stage, ncomp, v0, nv, n3));
+      KLAUNCH("soa_to_aos", (double)nv * ncomp * (8 + sizeof(R)), k_soa_to_aos<R><<<grid_for(nv * ncomp, 256), 256, 0, st>>>(src, stage, ncomp, v0, nv, n3, offs));
       MEU_CUDA(cudaMemcpyAsync(dst + v0 * ncomp, stage, sizeof(double) * nv * ncomp, cudaMemcpyDeviceToHost, st));
     }
   };
-  if (cons) down(c, cons, E);
+  if (cons) down(c, cons, E, hK.c_shift ? dK->c_mean : nullptr);
   if (phi_out) down(phi, phi_out, V);
   if (el_out) down(el_en, el_out, 1);
   if (ustate) {

@@ -32,7 +32,11 @@ struct DevConst {
   double ebar_eng[6];                  // e_mean with engineering shear
   double c0m[36];                      // C0 = CEla(:,:,2) (column-major)
   int use_var[MEU_MAX_VAR];            // elener: variant contributes (transsum > 1e-9)
-  double c_mean[MEU_MAX_EL];           // conserved mean of each solute (k = 0 mode)
+  double c_mean[MEU_MAX_EL];           // conserved mean of each solute (k = 0 mode), FP64
+  // 1: the stored concentration is the fluctuation c - c_mean (Landau decks).  The
+  // mean is exactly conserved, so it is kept in FP64 and the bulk FP32 field and
+  // its transforms only carry the fluctuation.
+  int c_shift;
 };
 
 // ------------------------------------------------------------ reductions

@@ -455,8 +455,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_a(const DevConst* __restric
   const int V = p.nvar;
   const int hcp = p.eig_coupling == MEU_EIG_H;
   double fch = 0;
+  const double cbar = K.c_shift ? K.c_mean[0] : 0.0;
+  // mu is transformed only to be multiplied by k^2: its constant part A (cbar - c1) is dropped
+  const double mu0 = K.c_shift ? p.lan_a * (cbar - p.lan_c1) : 0.0;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
-    const double cv = (double)c[id];
+    const double cv = cbar + (double)c[id];
     double s2 = 0, s4 = 0, s6 = 0;
     for (int v = 0; v < V; ++v) {
       const double e = (double)eta[v * n3 + id], e2 = e * e;
@@ -467,7 +470,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_a(const DevConst* __restric
     const double cross = s2 * s2 - s4;
     fch += 0.5 * p.lan_a * (cv - p.lan_c1) * (cv - p.lan_c1) + 0.5 * p.lan_b * (p.lan_c2 - cv) * s2 - 0.25 * p.lan_c * s4 +
            p.lan_d / 6.0 * s6 + p.cross_w * cross;
-    mu[id] = (R)(p.lan_a * (cv - p.lan_c1) - 0.5 * p.lan_b * s2);
+    mu[id] = (R)((p.lan_a * (cv - p.lan_c1) - mu0) - 0.5 * p.lan_b * s2);
   }
   block_reduce_store(fch, 0, partials + Q_FCH * RED_BLOCKS + blockIdx.x);
 }
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_k1(const DevConst* __restri
     // Cahn-Hilliard
     const double k2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
     double nr, ni;
-    if (id == 0) { nr = K.c_mean[0]; ni = 0.0; }
+    if (id == 0) { nr = K.c_shift ? 0.0 : K.c_mean[0]; ni = 0.0; }
     else {
       const double den = 1.0 + dm * p.kappa_c * k2 * k2;
       nr = (cr - dm * k2 * mr) / den;
@@ -600,8 +603,9 @@ __global__ void __launch_bounds__(256) k_lan_b(const DevConst* __restrict__ Kp, 
   const int V = p.nvar;
   const int hcp = p.eig_coupling == MEU_EIG_H;
   const double dtl = p.dt * p.b_mob;
+  const double cbar = K.c_shift ? K.c_mean[0] : 0.0;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
-    const double cv = (double)c[id];
+    const double cv = cbar + (double)c[id];
     double e[MEU_MAX_VAR], th[MEU_MAX_VAR], s2 = 0;
     for (int v = 0; v < V; ++v) {
       e[v] = (double)eta[v * n3 + id];
@@ -640,7 +644,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_stats(const DevConst* __restric
   double cmin = 1.0, cmax = 0.0, pmax = 0.0, solid = 0.0, cs[MEU_MAX_EL] = {0, 0, 0};
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
     for (int e = 0; e < E; ++e) {
-      const double v = (double)c[(int64_t)e * n3 + id];
+      const double v = (K.c_shift ? K.c_mean[e] : 0.0) + (double)c[(int64_t)e * n3 + id];
       cmin = fmin(cmin, v);
       cmax = fmax(cmax, v);
       cs[e] += v;
