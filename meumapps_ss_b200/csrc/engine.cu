@@ -13,35 +13,58 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "landau_fused.cuh"
 #include "step_kernels.cuh"
 
 namespace meu {
 
-__global__ void k_finalize(const double* __restrict__ partials, int nb, const int* __restrict__ ops, double* out) {
+// Fixed-order finalisation: block q reduces partials[q*PSTRIDE .. + nb[q]) with ops[q].
+__global__ void k_finalize(const double* __restrict__ partials, NbList nb, const int* __restrict__ ops, double* out) {
   const int q = blockIdx.x, op = ops[q];
   double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-    const double v = partials[(int64_t)q * nb + i];
+  for (int i = threadIdx.x; i < nb.nb[q]; i += blockDim.x) {
+    const double v = partials[(int64_t)q * PSTRIDE + i];
     acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
   }
   block_reduce_store(acc, op, out + q);
 }
 
-// per-component sums of an AoS chunk (block partials; component e at out[e*RED_BLOCKS + b])
+// per-component sums of an AoS chunk (block partials; component e at out[e*PSTRIDE + b])
 __global__ void __launch_bounds__(RED_THREADS) k_aos_colsum(const double* __restrict__ src, int ncomp, int64_t nv,
                                                             double* out) {
   for (int e = 0; e < ncomp; ++e) {
     double acc = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x)
       acc += src[i * ncomp + e];
-    block_reduce_store(acc, 0, out + (int64_t)e * RED_BLOCKS + blockIdx.x);
+    block_reduce_store(acc, 0, out + (int64_t)e * PSTRIDE + blockIdx.x);
   }
 }
 __global__ void k_accumulate(const double* __restrict__ r, double* acc, int n) {
   if (threadIdx.x < n) acc[threadIdx.x] += r[threadIdx.x];
 }
-__global__ void k_set_cmean(DevConst* K, const double* __restrict__ acc, int n, double inv_n3) {
+__global__ void k_set_cmean(DevConst* K, LanFusedConst* F, const double* __restrict__ acc, int n, double inv_n3) {
   if (threadIdx.x < n) K->c_mean[threadIdx.x] = acc[threadIdx.x] * inv_n3;
+  if (F && threadIdx.x == 0) F->cbar = acc[0] * inv_n3;
+}
+// gradient energy of eta (Parseval on natural-order spectra), block partials
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_grad_energy(const DevConst* __restrict__ Kp, PtrList<cplx<R>> sp, int V,
+                                                             double* out) {
+  const DevConst& K = *Kp;
+  double acc = 0;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    double f = 0;
+    for (int v = 0; v < V; ++v) {
+      const double re = (double)sp.p[v][id].x, im = (double)sp.p[v][id].y;
+      f += kkappak_b(K.p.grad_coeff[v], b) * (re * re + im * im);
+    }
+    acc += 0.5 * hweight(K, kx) * f;
+  }
+  block_reduce_store(acc, 0, out + blockIdx.x);
 }
 
 // AoS (component fastest, double) <-> SoA (R)
@@ -219,6 +242,8 @@ class Engine : public EngineBase {
   meu_params P;
   DevConst hK;
   DevConst* dK = nullptr;
+  LanFusedConst* dF = nullptr;  // constants of the fused Landau step (when it applies)
+  bool fused = false;
   std::unique_ptr<FFT3> fft;
   cudaStream_t st = nullptr, own_st = nullptr;
   int V, E;
@@ -237,6 +262,9 @@ class Engine : public EngineBase {
   std::vector<void*> allocs;
   // reference quirk state: values written on the next fort.98 line
   double prev_min = 1.0, prev_max = 0.0, prev_phimax = 0.0, prev_solid = 0.0;
+  // gradient energy of eta at the start of the next step, when a step computes it
+  // from its result (fused Landau path); 0 when each step computes its own
+  double fint_carry = 0.0;
   bool el_ready = false;  // u^ / strain hold a valid elastic state
   int last_iters = 0;
 
@@ -278,10 +306,11 @@ class Engine : public EngineBase {
     return l;
   }
   void check_err();
-  void finalize(int q0, int nq);
+  void finalize(int q0, int nq, double* out = nullptr, const int* nbs = nullptr);
   void elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only);
   void kks_step(meu_diag* d);
   void landau_step(meu_diag* d);
+  void landau_step_fused();
   void end_step(meu_diag* d, int clip);
   void flush_hist(meu_diag* diag);
   static constexpr int HIST_MAX = 4096;
@@ -403,7 +432,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   NWR = std::max(NWR, 1);
   wr = dalloc<R>((int64_t)NWR * n3);
   sp = dalloc<C>((int64_t)NS * nk);
-  partials = dalloc<double>((int64_t)Q_TOTAL * RED_BLOCKS);
+  partials = dalloc<double>((int64_t)Q_TOTAL * PSTRIDE);
   results = dalloc<double>(Q_TOTAL);
   hist = dalloc<double>((int64_t)HIST_MAX * Q_STEP_COUNT);
   cmean_acc = dalloc<double>(MEU_MAX_EL);
@@ -419,6 +448,35 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   ops[Q_PHIMAX] = 1;
   MEU_CUDA(cudaMemcpy(d_ops, ops, sizeof(ops), cudaMemcpyHostToDevice));
   MEU_CUDA(cudaMemcpy(dK, &hK, sizeof(DevConst), cudaMemcpyHostToDevice));
+  fused = lan_fused_supported(p);
+  if (fused) {
+    LanFusedConst F;
+    memset(&F, 0, sizeof(F));
+    // Q_il = -sum_{j,k} C0(voigt(i,j), voigt(k,l)) K_kj, K_kk = a_k^2, K_kj = b_k b_j (k != j)
+    const int mi[6] = {1, 2, 3, 2, 1, 1}, ml[6] = {1, 2, 3, 3, 3, 2};
+    auto kidx = [](int k, int j) { return k == j ? k - 1 : (k + j == 5 ? 3 : (k + j == 4 ? 4 : 5)); };
+    for (int m = 0; m < 6; ++m)
+      for (int j = 1; j <= 3; ++j)
+        for (int k = 1; k <= 3; ++k)
+          F.qcoef[m][kidx(k, j)] -= p.cela[1][(vg(mi[m], j) - 1) + (vg(k, ml[m]) - 1) * 6];
+    for (int v = 0; v < V; ++v) {
+      for (int m = 0; m < 6; ++m) {
+        F.sig0[v][m] = hK.sig0[v][m];
+        F.eps_eng[v][m] = hK.eps_eng[v][m];
+      }
+      for (int i = 0; i < 9; ++i) F.g[v][i] = p.grad_coeff[v][i];
+      for (int q = 0; q < V; ++q) F.A[v][q] = hK.A[v][q];
+      F.sig0_ebar[v] = hK.sig0_ebar[v];
+    }
+    for (int i = 0; i < 36; ++i) F.c0m[i] = p.cela[1][i];
+    for (int m = 0; m < 6; ++m) F.ebar_eng[m] = hK.ebar_eng[m];
+    F.lan_a = p.lan_a; F.lan_b = p.lan_b; F.lan_c = p.lan_c; F.lan_d = p.lan_d;
+    F.lan_c1 = p.lan_c1; F.lan_c2 = p.lan_c2; F.cross_w = p.cross_w; F.kappa_c = p.kappa_c;
+    F.dm = p.dt * p.cmobs[0];
+    F.dtl = p.dt * p.b_mob;
+    dF = dalloc<LanFusedConst>(1);
+    MEU_CUDA(cudaMemcpy(dF, &F, sizeof(F), cudaMemcpyHostToDevice));
+  }
   MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
   MEU_CUDA(cudaMemset(c, 0, sizeof(R) * E * n3));
   MEU_CUDA(cudaMemset(phi, 0, sizeof(R) * V * n3));
@@ -454,8 +512,11 @@ void Engine<R>::check_err() {
 }
 
 template <typename R>
-void Engine<R>::finalize(int q0, int nq) {
-  KLAUNCH("finalize", 8.0 * nq * RED_BLOCKS, k_finalize<<<nq, 256, 0, st>>>(partials + (int64_t)q0 * RED_BLOCKS, RED_BLOCKS, d_ops + q0, results + q0));
+void Engine<R>::finalize(int q0, int nq, double* out, const int* nbs) {
+  NbList nb;
+  for (int q = 0; q < nq; ++q) nb.nb[q] = nbs ? nbs[q] : RED_BLOCKS;
+  KLAUNCH("finalize", 8.0 * nq * RED_BLOCKS,
+          k_finalize<<<nq, 256, 0, st>>>(partials + (int64_t)q0 * PSTRIDE, nb, d_ops + q0, out ? out : results + q0));
 }
 
 // ---- host-side AoS conversion in chunks through the staging buffer
@@ -479,11 +540,11 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
       const int64_t nv = std::min(chunk, n3 - v0);
       MEU_CUDA(cudaMemcpyAsync(stage, cons + v0 * E, sizeof(double) * nv * E, cudaMemcpyHostToDevice, st));
       KLAUNCH("aos_colsum", (double)nv * E * 8,
-              k_aos_colsum<<<RED_BLOCKS, RED_THREADS, 0, st>>>(stage, E, nv, partials + (int64_t)Q_CSUM0 * RED_BLOCKS));
+              k_aos_colsum<<<RED_BLOCKS, RED_THREADS, 0, st>>>(stage, E, nv, partials + (int64_t)Q_CSUM0 * PSTRIDE));
       finalize(Q_CSUM0, E);
       KLAUNCH("accumulate", 16.0 * E, k_accumulate<<<1, 32, 0, st>>>(results + Q_CSUM0, cmean_acc, E));
     }
-    KLAUNCH("set_cmean", 16.0 * E, k_set_cmean<<<1, 32, 0, st>>>(dK, cmean_acc, E, 1.0 / (double)n3));
+    KLAUNCH("set_cmean", 16.0 * E, k_set_cmean<<<1, 32, 0, st>>>(dK, dF, cmean_acc, E, 1.0 / (double)n3));
     const double* offs = hK.c_shift ? dK->c_mean : nullptr;
     for (int64_t v0 = 0; v0 < n3; v0 += chunk) {
       const int64_t nv = std::min(chunk, n3 - v0);
@@ -494,6 +555,22 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     }
   }
   if (phi_in) up(phi_in, phi, V, 0);
+  if (phi_in) {
+    fint_carry = 0.0;
+    if (fused && P.diag_energy) {
+      // gradient energy of the uploaded eta: the fused step reports each step's
+      // start-of-step value from the transform of the previous step's result
+      std::vector<const R*> in;
+      for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
+      fwd_list(in, 0);
+      KLAUNCH("grad_energy", (double)V * nk * sizeof(C),
+              k_grad_energy<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, V), V, partials + (int64_t)Q_FINT2 * PSTRIDE));
+      finalize(Q_FINT2, 1);
+      MEU_CUDA(cudaMemcpyAsync(h_results + Q_FINT2, results + Q_FINT2, sizeof(double), cudaMemcpyDeviceToHost, st));
+      MEU_CUDA(cudaStreamSynchronize(st));
+      fint_carry = h_results[Q_FINT2] * (double)n3;
+    }
+  }
   if (strain) {
     if (ustate) {
       // u (3 x n3) -> u^ ; grads (9 x n3) -> engineering strain
@@ -648,7 +725,7 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
 // ------------------------------------------------------------------- KKS step
 template <typename R>
 void Engine<R>::kks_step(meu_diag* d) {
-  MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * RED_BLOCKS, st));
+  MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * PSTRIDE, st));
   if (!(step <= P.noise_step)) MEU_CUDA(cudaMemsetAsync(noise, 0, sizeof(R) * V * n3, st));
   // spectral gradients (:575-615)
   {
@@ -692,8 +769,41 @@ void Engine<R>::kks_step(meu_diag* d) {
 
 // ---------------------------------------------------------------- Landau step
 template <typename R>
+void Engine<R>::landau_step_fused() {
+  const bool elast = P.elastic != MEU_ELAST_NONE && step >= P.elastep0;
+  LanFusedArgs<R> a;
+  a.F = dF;
+  a.eta = phi;
+  a.c = c;
+  a.c2 = c2;
+  a.M = sp;
+  a.partials = partials;
+  a.pstride = PSTRIDE;
+  a.err = d_err;
+  a.homog = elast ? 1 : 0;
+  a.energy = P.diag_energy;
+  a.twx = (const C*)fft->px.tw;
+  a.twy = (const C*)fft->py.tw;
+  a.twz = (const C*)fft->pz.tw;
+  a.post = (const C*)fft->post_tw;
+  int nb[Q_TOTAL];
+  if (!lan_fused_step<R>(P.nx, V, a, st, &prof, nb)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+  std::swap(c, c2);
+  last_iters = 0;
+  finalize(0, Q_STEP_COUNT, hist + (int64_t)hist_n * Q_STEP_COUNT, nb);
+  hist_step[hist_n] = step;
+  hist_iters[hist_n] = 0;
+  hist_n += 1;
+  step += 1;
+}
+
+template <typename R>
 void Engine<R>::landau_step(meu_diag* d) {
-  MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * RED_BLOCKS, st));
+  if (fused) {
+    landau_step_fused();
+    return;
+  }
+  MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * PSTRIDE, st));
   const bool elast = P.elastic != MEU_ELAST_NONE && step >= P.elastep0;
   const bool homog = elast && P.elastic == MEU_ELAST_HOMOG;
   const bool het = elast && P.elastic == MEU_ELAST_HETERO;
@@ -747,10 +857,8 @@ template <typename R>
 void Engine<R>::end_step(meu_diag* d, int clip) {
   KLAUNCH("stats", (double)(E + V * (clip ? 2 : 1)) * n3 * sizeof(R),
           k_stats<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, clip, partials));
-  finalize(0, Q_STEP_COUNT);
-  // keep this step's reductions on the device; they are read once per meu_run
-  MEU_CUDA(cudaMemcpyAsync(hist + (int64_t)hist_n * Q_STEP_COUNT, results, sizeof(double) * Q_STEP_COUNT,
-                           cudaMemcpyDeviceToDevice, st));
+  // this step's reductions go straight into the device history, read once per meu_run
+  finalize(0, Q_STEP_COUNT, hist + (int64_t)hist_n * Q_STEP_COUNT);
   hist_step[hist_n] = step;
   hist_iters[hist_n] = last_iters;
   hist_n += 1;
@@ -774,7 +882,7 @@ void Engine<R>::flush_hist(meu_diag* diag) {
       d->step = hist_step[i];
       d->el_iters = hist_iters[i];
       d->status = 0;
-      d->fint = lan ? r[Q_FINT] * sn3 : r[Q_FINT];
+      d->fint = (lan ? r[Q_FINT] * sn3 : r[Q_FINT]) + fint_carry;
       d->fw = r[Q_FW];
       d->fch = r[Q_FCH];
       d->elen = (lan && P.elastic == MEU_ELAST_HOMOG) ? r[Q_ELEN] * sn3 : r[Q_ELEN];
@@ -793,6 +901,7 @@ void Engine<R>::flush_hist(meu_diag* diag) {
     prev_max = r[Q_CMAX];
     prev_phimax = r[Q_PHIMAX];
     prev_solid = r[Q_SOLID];
+    fint_carry = r[Q_FINT2] * sn3;
     const double et = r[Q_FINT] + r[Q_FCH] + r[Q_ELEN] + r[Q_FW];
     if (!std::isfinite(et) || !std::isfinite(r[Q_CSUM0]) || !std::isfinite(r[Q_SOLID])) {
       hist_n = 0;

@@ -1,0 +1,232 @@
+// fused.cuh -- compile-time shared-memory FFT building blocks for the fused
+// step kernels (grids with Nx = Ny = Nz = N, N in {32, 48, 64, 96, 128}).
+//
+// Every transform length, radix plan, line count and stride is a template
+// constant, so all index arithmetic folds to shifts and constant multiplies.
+//
+// Spectral layout of the fused path ("M-form"): a plane z of a field holds
+// [p_y][c] with c in [0, N/2] (N/2+1 columns) where
+//   c < N/2   holds kx = rev_x(c)   (digit-reversed order of the half-length x transform)
+//   c = N/2   holds kx = N/2        (Nyquist)
+//   p_y       holds ky = rev_y(p_y) (digit-reversed order of the y transform)
+// The z-kernels transform columns in place and keep kz in digit-reversed order
+// between their forward and inverse passes.  Nothing outside the fused step
+// sees this layout.
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace meu {
+namespace fz {
+
+struct RPlan {
+  int ns;
+  int r[8];
+};
+// radix plan: 8s first, then 4, 2, 3s (product = L)
+__host__ __device__ constexpr RPlan rplan(int L) {
+  RPlan p{0, {1, 1, 1, 1, 1, 1, 1, 1}};
+  int n = L;
+  while (n % 8 == 0 && n > 8) { p.r[p.ns++] = 8; n /= 8; }
+  if (n % 8 == 0) { p.r[p.ns++] = 8; n /= 8; }
+  if (n % 4 == 0) { p.r[p.ns++] = 4; n /= 4; }
+  if (n % 2 == 0) { p.r[p.ns++] = 2; n /= 2; }
+  while (n % 3 == 0) { p.r[p.ns++] = 3; n /= 3; }
+  return p;
+}
+__host__ __device__ constexpr int span_of(int L, int s) {
+  int sp = L;
+  for (int i = 0; i < s; ++i) sp /= rplan(L).r[i];
+  return sp;
+}
+
+// position after DIF -> frequency index
+template <int L>
+__device__ __forceinline__ int rev(int p) {
+  constexpr RPlan pl = rplan(L);
+  int k = 0, mul = 1, span = L;
+#pragma unroll
+  for (int s = 0; s < pl.ns; ++s) {
+    span /= pl.r[s];
+    const int q = (p / span) % pl.r[s];
+    k += q * mul;
+    mul *= pl.r[s];
+  }
+  return k;
+}
+// frequency index -> position after DIF
+template <int L>
+__device__ __forceinline__ int pos(int k) {
+  constexpr RPlan pl = rplan(L);
+  int p = 0, span = L;
+#pragma unroll
+  for (int s = 0; s < pl.ns; ++s) {
+    span /= pl.r[s];
+    p += (k % pl.r[s]) * span;
+    k /= pl.r[s];
+  }
+  return p;
+}
+
+// One DIF stage over NL lines (element e of line l at buf[l*LS + e*ES]).
+template <typename C, int L, int S, int NL, int LS, int ES, int NT>
+__device__ __forceinline__ void dif_stage_s(C* buf, const C* __restrict__ tw) {
+  constexpr int R = rplan(L).r[S];
+  constexpr int SPAN = span_of(L, S);
+  constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
+#pragma unroll 2
+  for (int t = threadIdx.x; t < NBF; t += NT) {
+    const int line = t % NL, u = t / NL, j = u % M, b = u / M;
+    C* base = buf + line * LS + (b * SPAN + j) * ES;
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = base[r * M * ES];
+    Dft<R, -1, C>::run(x);
+    if (M > 1) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) x[q] = cmul(x[q], tw[j * q * TWS]);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) base[q * M * ES] = x[q];
+  }
+}
+template <typename C, int L, int S, int NL, int LS, int ES, int NT>
+__device__ __forceinline__ void dit_stage_s(C* buf, const C* __restrict__ tw) {
+  constexpr int R = rplan(L).r[S];
+  constexpr int SPAN = span_of(L, S);
+  constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
+#pragma unroll 2
+  for (int t = threadIdx.x; t < NBF; t += NT) {
+    const int line = t % NL, u = t / NL, j = u % M, b = u / M;
+    C* base = buf + line * LS + (b * SPAN + j) * ES;
+    C x[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) x[q] = base[q * M * ES];
+    if (M > 1) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) x[q] = cmulc(x[q], tw[j * q * TWS]);
+    }
+    Dft<R, 1, C>::run(x);
+#pragma unroll
+    for (int r = 0; r < R; ++r) base[r * M * ES] = x[r];
+  }
+}
+
+// Forward DIF over all stages (natural -> digit reversed); syncs after each stage.
+template <typename C, int L, int NL, int LS, int ES, int NT, int S = 0>
+__device__ __forceinline__ void dif(C* buf, const C* tw) {
+  if constexpr (S < rplan(L).ns) {
+    dif_stage_s<C, L, S, NL, LS, ES, NT>(buf, tw);
+    __syncthreads();
+    dif<C, L, NL, LS, ES, NT, S + 1>(buf, tw);
+  }
+}
+// Inverse DIT over all stages (digit reversed -> natural), unscaled.
+template <typename C, int L, int NL, int LS, int ES, int NT, int S = rplan(L).ns - 1>
+__device__ __forceinline__ void dit(C* buf, const C* tw) {
+  if constexpr (S >= 0) {
+    dit_stage_s<C, L, S, NL, LS, ES, NT>(buf, tw);
+    __syncthreads();
+    dit<C, L, NL, LS, ES, NT, S - 1>(buf, tw);
+  }
+}
+
+// ----------------------------------------------------------- plane (x + y)
+// Shared-memory image of one z-plane: NY rows of PITCH = N/2+1 complex.
+template <typename R, int N, int NT>
+struct Plane {
+  using C = cplx<R>;
+  static constexpr int LX = N / 2, NXH = LX + 1, PITCH = NXH, NY = N;
+  static constexpr int ELEMS = NY * PITCH;
+  // twiddles: twx[LX], twy[NY], post[NXH]
+  static constexpr int TW_ELEMS = LX + NY + NXH;
+  static constexpr size_t smem_bytes() { return sizeof(C) * (size_t)(ELEMS + TW_ELEMS); }
+
+  static __device__ __forceinline__ void load_tw(C* tws, const C* __restrict__ gx, const C* __restrict__ gy,
+                                                 const C* __restrict__ gpost) {
+    for (int i = threadIdx.x; i < LX; i += NT) tws[i] = gx[i];
+    for (int i = threadIdx.x; i < NY; i += NT) tws[LX + i] = gy[i];
+    for (int i = threadIdx.x; i < NXH; i += NT) tws[LX + NY + i] = gpost[i];
+  }
+
+  // buf rows hold (x[2n], x[2n+1]) at n in [0, LX): R2C along x, FFT along y.
+  static __device__ __forceinline__ void forward(C* buf, const C* tws) {
+    const C* twx = tws;
+    const C* twy = tws + LX;
+    const C* post = tws + LX + NY;
+    dif<C, LX, NY, PITCH, 1, NT>(buf, twx);
+    // split in place, in digit-reversed column order (Nyquist into column LX)
+    constexpr int NP = LX / 2 + 1;
+    for (int i = threadIdx.x; i < NY * NP; i += NT) {
+      const int row = i % NY, k = i / NY;
+      C* rb = buf + row * PITCH;
+      const int pk = pos<LX>(k % LX), pm = pos<LX>((LX - k) % LX);
+      const C zk = rb[pk], zm = rb[pm];
+      C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
+      C o = cscale(csub(zk, cconj(zm)), (R)0.5);
+      o = mk(o.y, -o.x);
+      const C xk = cadd(e, cmul(post[k], o));
+      if (k == 0) {
+        // X[0] = E + O, X[LX] = E - O
+        rb[0] = xk;
+        rb[LX] = csub(e, o);
+      } else {
+        rb[pk] = xk;
+        if (k != LX - k) {
+          C e2 = cscale(cadd(zm, cconj(zk)), (R)0.5);
+          C o2 = cscale(csub(zm, cconj(zk)), (R)0.5);
+          o2 = mk(o2.y, -o2.x);
+          rb[pm] = cadd(e2, cmul(post[LX - k], o2));
+        }
+      }
+    }
+    __syncthreads();
+    dif<C, NY, NXH, 1, PITCH, NT>(buf, twy);
+  }
+
+  // inverse of forward(): M-form plane -> rows of (x[2n], x[2n+1]), unscaled.
+  static __device__ __forceinline__ void inverse(C* buf, const C* tws) {
+    const C* twx = tws;
+    const C* twy = tws + LX;
+    const C* post = tws + LX + NY;
+    dit<C, NY, NXH, 1, PITCH, NT>(buf, twy);
+    constexpr int NP = LX / 2 + 1;
+    for (int i = threadIdx.x; i < NY * NP; i += NT) {
+      const int row = i % NY, k = i / NY;
+      C* rb = buf + row * PITCH;
+      const int pk = (k == 0) ? 0 : pos<LX>(k);
+      const int pm = (k == 0) ? LX : pos<LX>(LX - k);
+      C xk = rb[pk], xm = rb[pm];
+      if (k == 0) { xk.y = 0; xm.y = 0; }
+      {
+        const C ex = cadd(xk, cconj(xm));
+        const C ox = cmulc(csub(xk, cconj(xm)), post[k]);
+        rb[pk] = cadd(ex, mk(-ox.y, ox.x));
+      }
+      if (k != 0 && k != LX - k) {
+        const C ex = cadd(xm, cconj(xk));
+        const C ox = cmulc(csub(xm, cconj(xk)), post[LX - k]);
+        rb[pm] = cadd(ex, mk(-ox.y, ox.x));
+      }
+    }
+    __syncthreads();
+    dit<C, LX, NY, PITCH, 1, NT>(buf, twx);
+  }
+
+  // M-form plane <-> shared memory (rows of NXH complex, contiguous in both)
+  static __device__ __forceinline__ void load_m(C* buf, const C* __restrict__ src) {
+    for (int i = threadIdx.x; i < ELEMS; i += NT) buf[i] = src[i];
+  }
+  static __device__ __forceinline__ void store_m(const C* buf, C* __restrict__ dst) {
+    for (int i = threadIdx.x; i < ELEMS; i += NT) dst[i] = buf[i];
+  }
+};
+
+// kx of M-form column c
+template <int N>
+__device__ __forceinline__ int kx_of_col(int c) {
+  return c == N / 2 ? N / 2 : rev<N / 2>(c);
+}
+
+}  // namespace fz
+}  // namespace meu

@@ -39,6 +39,20 @@ struct DevConst {
   int c_shift;
 };
 
+enum RedQ : int {
+  Q_FCH = 0, Q_FW, Q_FINT, Q_ELEN, Q_CMIN, Q_CMAX, Q_PHIMAX, Q_SOLID, Q_CSUM0,
+  // gradient energy of the fields a step produces (the next step's start-of-step value)
+  Q_FINT2 = Q_CSUM0 + MEU_MAX_EL,
+  Q_STEP_COUNT,
+  // elastic convergence sums, separate finalisation
+  Q_ERR0 = Q_STEP_COUNT, Q_TOTAL = Q_ERR0 + 6
+};
+// row length of the partials array: quantity q of block b at partials[q * PSTRIDE + b]
+constexpr int PSTRIDE = 2048;
+struct NbList {
+  int nb[Q_TOTAL];
+};
+
 // ------------------------------------------------------------ reductions
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -71,8 +85,6 @@ __device__ __forceinline__ void block_reduce_store(double v, int op, double* out
   }
 }
 
-// Fixed-order finalisation: block q reduces partials[q*nb .. q*nb+nb) with ops[q].
-__global__ void k_finalize(const double* __restrict__ partials, int nb, const int* __restrict__ ops, double* out);
 
 // --------------------------------------------------------------- k helpers
 __device__ __forceinline__ void kdecode(const DevConst& K, int64_t id, int& kx, int& ky, int& kz) {

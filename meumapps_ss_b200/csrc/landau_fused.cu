@@ -1,0 +1,484 @@
+// landau_fused.cu -- kernels and dispatch of the fused Landau step (see
+// landau_fused.cuh for the data flow).
+#include <vector>
+
+#include "landau_fused.cuh"
+
+namespace meu {
+
+namespace {
+constexpr int NT = 256;
+constexpr double TWO_PI = 6.283185307179586476925286766559;
+
+template <int N>
+__device__ __forceinline__ void kvec_n(int kx, int ky, int kz, double a[3], double b[3]) {
+  const int m[3] = {kx, ky, kz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int mm = (m[d] <= N / 2) ? m[d] : m[d] - N;
+    a[d] = (double)mm * (TWO_PI / (double)N);
+    b[d] = (2 * m[d] == N) ? 0.0 : a[d];
+  }
+}
+
+template <typename R> constexpr int col_tile() { return sizeof(R) == 4 ? 16 : 8; }
+
+}  // namespace
+
+// ------------------------------------------------------------------ PF
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V) {
+  using P = fz::Plane<R, N, NT>;
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x, f = blockIdx.y;
+  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  const LanFusedConst& F = *a.F;
+  const R* ez = a.eta + z * PL;
+  const R* cz = a.c + z * PL;
+  double fch = 0;
+  for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const int64_t off = (int64_t)y * N;
+    C v;
+    if (f < V) {
+      const C e = ((const C*)(ez + f * N3 + off))[n];
+      v = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
+    } else {
+      v = ((const C*)(cz + off))[n];
+      if (a.energy) {
+        double s2[2] = {0, 0}, s4[2] = {0, 0}, s6[2] = {0, 0};
+        for (int q = 0; q < V; ++q) {
+          const C e = ((const C*)(ez + q * N3 + off))[n];
+          const double e0 = (double)e.x * (double)e.x, e1 = (double)e.y * (double)e.y;
+          s2[0] += e0; s4[0] += e0 * e0; s6[0] += e0 * e0 * e0;
+          s2[1] += e1; s4[1] += e1 * e1; s6[1] += e1 * e1 * e1;
+        }
+        const double cv[2] = {F.cbar + (double)v.x, F.cbar + (double)v.y};
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          fch += 0.5 * F.lan_a * (cv[h] - F.lan_c1) * (cv[h] - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv[h]) * s2[h] -
+                 0.25 * F.lan_c * s4[h] + F.lan_d / 6.0 * s6[h] + F.cross_w * (s2[h] * s2[h] - s4[h]);
+      }
+    }
+    buf[y * P::PITCH + n] = v;
+  }
+  __syncthreads();
+  P::forward(buf, tws);
+  P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+  if (f == V) block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + z);
+}
+
+// ------------------------------------------------------------------ Z1
+template <typename R, int N, int V>
+__global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
+  using C = cplx<R>;
+  constexpr int TM = col_tile<R>(), NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;  // [N][NF][TM]
+  C* tw = buf + N * LN;
+  __shared__ LanFusedConst F;
+  for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
+  for (int i = threadIdx.x; i < N; i += NT) tw[i] = a.twz[i];
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
+    buf[i] = a.M[f * NK + zz * PL + m0 + c];
+  }
+  __syncthreads();
+  fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  double fint = 0, elen = 0;
+  for (int i = threadIdx.x; i < N * TM; i += NT) {
+    const int p = i / TM, c = i - p * TM;
+    const int64_t m = m0 + c;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N>(cx), ky = fz::rev<N>(py), kz = fz::rev<N>(p);
+    double av[3], b[3];
+    kvec_n<N>(kx, ky, kz, av, b);
+    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    C* e = buf + p * LN + c;
+    double tr[V], ti[V], str = 0, sti = 0;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      tr[v] = (double)e[v * TM].x * s;
+      ti[v] = (double)e[v * TM].y * s;
+      str += tr[v];
+      sti += ti[v];
+    }
+    const double cr = (double)e[V * TM].x * s, ci = (double)e[V * TM].y * s;
+    const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+    if (a.energy) fint += 0.5 * w * F.kappa_c * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci);
+    // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
+    double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+    if (a.homog && !k0) {
+      double Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * F.sig0[v][q]; Si[q] += ti[v] * F.sig0[v][q]; }
+      // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
+      const double t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
+      const double t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
+      const double t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
+      const double Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
+      const double Kv[6] = {av[0] * av[0], av[1] * av[1], av[2] * av[2], b[1] * b[2], b[0] * b[2], b[0] * b[1]};
+      double Qs[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        double acc = 0;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
+        Qs[q] = acc;
+      }
+      // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
+      const double qa = Qs[0], qb = Qs[1], qc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+      const double i00 = qb * qc - qf * qf, i01 = qe * qf - qc * qd, i02 = qd * qf - qb * qe;
+      const double i11 = qa * qc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+      const double det = qa * i00 + qd * i01 + qe * i02;
+      if (det == 0.0) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
+      const double rd = 1.0 / det;
+      const double Qi[3][3] = {{i00 * rd, i01 * rd, i02 * rd}, {i01 * rd, i11 * rd, i12 * rd}, {i02 * rd, i12 * rd, i22 * rd}};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
+        ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      double pr = 0, pi = 0;
+      if (a.homog && !k0) {
+        const double* sg = F.sig0[v];
+        const double sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
+        const double sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
+        const double sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
+        const double dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
+        const double di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
+        pr = -di;
+        pi = dr;
+      }
+      e[v * TM] = mk((R)pr, (R)pi);
+    }
+    if (a.homog && a.energy) {
+      // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
+      const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+      double er[6], ei[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const int ii = I1[q], jj = J1[q];
+        double gr, gi;
+        if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
+        else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
+#pragma unroll
+        for (int v = 0; v < V; ++v) { gr -= tr[v] * F.eps_eng[v][q]; gi -= ti[v] * F.eps_eng[v][q]; }
+        if (k0) gr += F.ebar_eng[q];
+        er[q] = gr;
+        ei[q] = gi;
+      }
+      double qq = 0;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        double cr2 = 0, ci2 = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) { cr2 += F.c0m[r + j * 6] * er[j]; ci2 += F.c0m[r + j * 6] * ei[j]; }
+        qq += er[r] * cr2 + ei[r] * ci2;
+      }
+      elen += 0.5 * w * qq;
+    }
+    // ---- Cahn-Hilliard on the fluctuation: mu^ = A dc^ - B/2 sum theta^
+    double nr = 0, ni = 0;
+    if (!k0) {
+      const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+      const double mr = F.lan_a * cr - 0.5 * F.lan_b * str, mi = F.lan_a * ci - 0.5 * F.lan_b * sti;
+      const double den = 1.0 + F.dm * F.kappa_c * k2 * k2;
+      nr = (cr - F.dm * k2 * mr) / den;
+      ni = (ci - F.dm * k2 * mi) / den;
+    }
+    e[V * TM] = mk((R)nr, (R)ni);
+  }
+  __syncthreads();
+  fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
+    a.M[f * NK + zz * PL + m0 + c] = buf[i];
+  }
+  block_reduce_store(fint, 0, a.partials + LQ_FINT * a.pstride + blockIdx.x);
+  block_reduce_store(elen, 0, a.partials + LQ_ELEN * a.pstride + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ PB
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
+  using P = fz::Plane<R, N, NT>;
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x, f = blockIdx.y;
+  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
+  P::load_m(buf, mp);
+  __syncthreads();
+  P::inverse(buf, tws);
+  if (f == V) {
+    R* c2z = a.c2 + z * PL;
+    for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+      const int y = i / P::LX, n = i - y * P::LX;
+      ((C*)(c2z + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
+    }
+    return;
+  }
+  const LanFusedConst& F = *a.F;
+  const R* ez = a.eta + z * PL;
+  const R* cz = a.c + z * PL;
+  for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const int64_t off = (int64_t)y * N;
+    double e[2][4], s2[2] = {0, 0};
+    for (int q = 0; q < V; ++q) {
+      const C ev = ((const C*)(ez + q * N3 + off))[n];
+      e[0][q] = ev.x;
+      e[1][q] = ev.y;
+      s2[0] += (double)ev.x * ev.x;
+      s2[1] += (double)ev.y * ev.y;
+    }
+    const C dcv = ((const C*)(cz + off))[n];
+    const C ph = buf[y * P::PITCH + n];
+    const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
+    const double phv[2] = {(double)ph.x, (double)ph.y};
+    double out[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const double ev = e[h][f], e2 = ev * ev;
+      double g = F.lan_b * (F.lan_c2 - cv[h]) * ev - F.lan_c * e2 * ev + F.lan_d * e2 * e2 * ev +
+                 4.0 * F.cross_w * ev * (s2[h] - e2);
+      if (a.homog) {
+        double sacc = F.sig0_ebar[f] + phv[h];
+        for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
+        g += -2.0 * ev * sacc;
+      }
+      out[h] = ev - F.dtl * g;
+    }
+    buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
+  }
+  __syncthreads();
+  P::forward(buf, tws);
+  P::store_m(buf, mp);
+}
+
+// ------------------------------------------------------------------ Z2
+template <typename R, int N, int V>
+__global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
+  using C = cplx<R>;
+  constexpr int TM = col_tile<R>(), NXH = N / 2 + 1, LN = V * TM;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tw = buf + N * LN;
+  __shared__ double g[V][9];
+  __shared__ double dtl;
+  for (int i = threadIdx.x; i < V * 9; i += NT) g[i / 9][i % 9] = a.F->g[i / 9][i % 9];
+  if (threadIdx.x == 0) dtl = a.F->dtl;
+  for (int i = threadIdx.x; i < N; i += NT) tw[i] = a.twz[i];
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
+    buf[i] = a.M[f * NK + zz * PL + m0 + c];
+  }
+  __syncthreads();
+  fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  double fint = 0;
+  for (int i = threadIdx.x; i < N * TM; i += NT) {
+    const int p = i / TM, c = i - p * TM;
+    const int64_t m = m0 + c;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N>(cx), ky = fz::rev<N>(py), kz = fz::rev<N>(p);
+    double av[3], b[3];
+    kvec_n<N>(kx, ky, kz, av, b);
+    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    C* e = buf + p * LN + c;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double* gv = g[v];
+      const double kk = gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] +
+                        (gv[3] + gv[1]) * b[0] * b[1] + (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+      const double sc = s / (1.0 + dtl * kk);
+      const double er = (double)e[v * TM].x * sc, ei = (double)e[v * TM].y * sc;
+      e[v * TM] = mk((R)er, (R)ei);
+      if (a.energy) {
+        const double kb = gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
+                          (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+        fint += 0.5 * w * kb * (er * er + ei * ei);
+      }
+    }
+  }
+  __syncthreads();
+  fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
+    a.M[f * NK + zz * PL + m0 + c] = buf[i];
+  }
+  block_reduce_store(fint, 0, a.partials + Q_FINT2 * a.pstride + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ PI
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) k_lf_pi(LanFusedArgs<R> a, int V) {
+  using P = fz::Plane<R, N, NT>;
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x, f = blockIdx.y;
+  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  P::load_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+  __syncthreads();
+  P::inverse(buf, tws);
+  R* ez = a.eta + f * N3 + z * PL;
+  double emax = 0.0, s2 = 0.0, cmin = 1.0, cmax = 0.0, csum = 0.0;
+  const double cbar = a.F->cbar;
+  const R* c2z = a.c2 + z * PL;
+  for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const C v = buf[y * P::PITCH + n];
+    ((C*)(ez + (int64_t)y * N))[n] = v;
+    emax = fmax(emax, fmax((double)v.x, (double)v.y));
+    s2 += (double)v.x * v.x + (double)v.y * v.y;
+    if (f == 0) {
+      const C cv = ((const C*)(c2z + (int64_t)y * N))[n];
+      const double c0 = cbar + (double)cv.x, c1 = cbar + (double)cv.y;
+      cmin = fmin(cmin, fmin(c0, c1));
+      cmax = fmax(cmax, fmax(c0, c1));
+      csum += c0 + c1;
+    }
+  }
+  const int blk = z * V + f;
+  block_reduce_store(emax, 1, a.partials + LQ_PHIMAX * a.pstride + blk);
+  block_reduce_store(s2, 0, a.partials + LQ_SOLID * a.pstride + blk);
+  block_reduce_store(cmin, 2, a.partials + LQ_CMIN * a.pstride + blk);
+  block_reduce_store(cmax, 1, a.partials + LQ_CMAX * a.pstride + blk);
+  block_reduce_store(csum, 0, a.partials + LQ_CSUM * a.pstride + blk);
+}
+
+// ------------------------------------------------------------------ dispatch
+namespace {
+struct Scope {
+  LaunchHook* h;
+  cudaStream_t st;
+  Scope(LaunchHook* h_, const char* n, double b, cudaStream_t s) : h(h_), st(s) {
+    if (h) h->begin(n, b, st);
+  }
+  ~Scope() {
+    if (h) h->end(st);
+  }
+};
+
+template <typename K>
+void ensure_smem(K fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static thread_local std::vector<const void*> done;
+  for (const void* f : done)
+    if (f == (const void*)fn) return;
+  int dev = 0, optin = 0;
+  MEU_CUDA(cudaGetDevice(&dev));
+  MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  MEU_CUDA(cudaFuncGetAttributes(&fa, (const void*)fn));
+  const int lim = optin - (int)fa.sharedSizeBytes;
+  if ((int)bytes > lim) throw CudaError("fused tile exceeds shared memory", MEU_ERR_UNSUPPORTED);
+  MEU_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  done.push_back((const void*)fn);
+}
+
+template <typename R, int N, int V>
+void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
+  using P = fz::Plane<R, N, NT>;
+  using C = cplx<R>;
+  constexpr int TM = col_tile<R>();
+  constexpr int NXH = N / 2 + 1;
+  const int tiles = N * NXH / TM;
+  const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
+  const size_t sp = P::smem_bytes();
+  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N);
+  const size_t s2 = sizeof(C) * ((size_t)N * V * TM + N);
+  ensure_smem(k_lf_pf<R, N>, sp);
+  ensure_smem(k_lf_pb<R, N>, sp);
+  ensure_smem(k_lf_pi<R, N>, sp);
+  ensure_smem(k_lf_z1<R, N, V>, s1);
+  ensure_smem(k_lf_z2<R, N, V>, s2);
+  {
+    Scope s(hook, "lf_plane_fwd", (double)(V + 1) * nk * sizeof(C) + (2.0 * V + 1) * n3 * sizeof(R), st);
+    k_lf_pf<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_z_green_ch", 2.0 * (V + 1) * nk * sizeof(C), st);
+    k_lf_z1<R, N, V><<<tiles, NT, s1, st>>>(a);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V + 1) * nk * sizeof(C) + (2.0 * V + 2) * n3 * sizeof(R), st);
+    k_lf_pb<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_z_tdgl", 2.0 * V * nk * sizeof(C), st);
+    k_lf_z2<R, N, V><<<tiles, NT, s2, st>>>(a);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_plane_inv_stats", (double)V * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pi<R, N><<<dim3(N, V), NT, sp, st>>>(a, V);
+    MEU_CHECK_LAUNCH();
+  }
+  for (int q = 0; q < Q_TOTAL; ++q) nb[q] = 0;
+  nb[Q_FCH] = N;
+  nb[Q_FINT] = tiles;
+  nb[Q_ELEN] = tiles;
+  nb[Q_FINT2] = tiles;
+  nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * V;
+}
+
+template <typename R, int N>
+bool dispatch_v(int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
+  switch (V) {
+    case 1: run_step<R, N, 1>(a, st, hook, nb); return true;
+    case 2: run_step<R, N, 2>(a, st, hook, nb); return true;
+    case 3: run_step<R, N, 3>(a, st, hook, nb); return true;
+    case 4: run_step<R, N, 4>(a, st, hook, nb); return true;
+    default: return false;
+  }
+}
+}  // namespace
+
+bool lan_fused_supported(const meu_params& p) {
+  const int n = p.nx;
+  const bool size_ok = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128) && p.ny == n && p.nz == n;
+  return size_ok && p.model == MEU_MODEL_LANDAU && p.nvar >= 1 && p.nvar <= 4 && p.numel == 1 &&
+         p.eig_coupling == MEU_EIG_ETA2 && (p.elastic == MEU_ELAST_NONE || p.elastic == MEU_ELAST_HOMOG);
+}
+
+template <typename R>
+bool lan_fused_step(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
+  switch (N) {
+    case 32: return dispatch_v<R, 32>(V, a, st, hook, nb);
+    case 48: return dispatch_v<R, 48>(V, a, st, hook, nb);
+    case 64: return dispatch_v<R, 64>(V, a, st, hook, nb);
+    case 96: return dispatch_v<R, 96>(V, a, st, hook, nb);
+    case 128: return dispatch_v<R, 128>(V, a, st, hook, nb);
+    default: return false;
+  }
+}
+
+template bool lan_fused_step<float>(int, int, const LanFusedArgs<float>&, cudaStream_t, LaunchHook*, int*);
+template bool lan_fused_step<double>(int, int, const LanFusedArgs<double>&, cudaStream_t, LaunchHook*, int*);
+
+}  // namespace meu

@@ -6,13 +6,6 @@
 
 namespace meu {
 
-enum RedQ : int {
-  Q_FCH = 0, Q_FW, Q_FINT, Q_ELEN, Q_CMIN, Q_CMAX, Q_PHIMAX, Q_SOLID, Q_CSUM0,
-  Q_STEP_COUNT = Q_CSUM0 + MEU_MAX_EL,
-  // elastic convergence sums, separate finalisation
-  Q_ERR0 = Q_STEP_COUNT, Q_TOTAL = Q_ERR0 + 6
-};
-
 __device__ __forceinline__ void set_err(int* err, int code) {
   if (code) atomicMax(err, code);
 }
@@ -146,9 +139,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
       fdiff[jv * n3 + id] = fgrad[jv] - term11 / (double)nt;
     }
   }
-  block_reduce_store(fch, 0, partials + Q_FCH * RED_BLOCKS + blockIdx.x);
-  block_reduce_store(fw, 0, partials + Q_FW * RED_BLOCKS + blockIdx.x);
-  block_reduce_store(fint, 0, partials + Q_FINT * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(fch, 0, partials + Q_FCH * PSTRIDE + blockIdx.x);
+  block_reduce_store(fw, 0, partials + Q_FW * PSTRIDE + blockIdx.x);
+  block_reduce_store(fint, 0, partials + Q_FINT * PSTRIDE + blockIdx.x);
 }
 
 // ------------------------------------------------------ elastic: zeroth order
@@ -307,7 +300,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict
     }
   }
 #pragma unroll
-  for (int q = 0; q < 6; ++q) block_reduce_store(e[q], 0, partials + (Q_ERR0 + q) * RED_BLOCKS + blockIdx.x);
+  for (int q = 0; q < 6; ++q) block_reduce_store(e[q], 0, partials + (Q_ERR0 + q) * PSTRIDE + blockIdx.x);
 }
 
 // -------------------------------------------------------------- elener
@@ -388,7 +381,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
     el_en[id] = (R)en;
     esum += en;
   }
-  block_reduce_store(esum, 0, partials + Q_ELEN * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(esum, 0, partials + Q_ELEN * PSTRIDE + blockIdx.x);
 }
 
 // --------------------------------------------------- KKS: diffusion update
@@ -472,7 +465,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_a(const DevConst* __restric
            p.lan_d / 6.0 * s6 + p.cross_w * cross;
     mu[id] = (R)((p.lan_a * (cv - p.lan_c1) - mu0) - 0.5 * p.lan_b * s2);
   }
-  block_reduce_store(fch, 0, partials + Q_FCH * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(fch, 0, partials + Q_FCH * PSTRIDE + blockIdx.x);
 }
 
 // Landau k-space kernel: gradient energy (Parseval), homogeneous Green
@@ -587,8 +580,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_k1(const DevConst* __restri
     }
     sp.p[V + 1][id] = mk((R)nr, (R)ni);
   }
-  block_reduce_store(fint, 0, partials + Q_FINT * RED_BLOCKS + blockIdx.x);
-  if (homog) block_reduce_store(elen, 0, partials + Q_ELEN * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(fint, 0, partials + Q_FINT * PSTRIDE + blockIdx.x);
+  if (homog) block_reduce_store(elen, 0, partials + Q_ELEN * PSTRIDE + blockIdx.x);
 }
 
 // Landau TDGL right-hand side w_v = eta_v - dt L (df/deta_v + el_grad_v)
@@ -662,11 +655,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_stats(const DevConst* __restric
       pmax = fmax(pmax, f);
     }
   }
-  block_reduce_store(cmin, 2, partials + Q_CMIN * RED_BLOCKS + blockIdx.x);
-  block_reduce_store(cmax, 1, partials + Q_CMAX * RED_BLOCKS + blockIdx.x);
-  block_reduce_store(pmax, 1, partials + Q_PHIMAX * RED_BLOCKS + blockIdx.x);
-  block_reduce_store(solid, 0, partials + Q_SOLID * RED_BLOCKS + blockIdx.x);
-  for (int e = 0; e < MEU_MAX_EL; ++e) block_reduce_store(cs[e], 0, partials + (Q_CSUM0 + e) * RED_BLOCKS + blockIdx.x);
+  block_reduce_store(cmin, 2, partials + Q_CMIN * PSTRIDE + blockIdx.x);
+  block_reduce_store(cmax, 1, partials + Q_CMAX * PSTRIDE + blockIdx.x);
+  block_reduce_store(pmax, 1, partials + Q_PHIMAX * PSTRIDE + blockIdx.x);
+  block_reduce_store(solid, 0, partials + Q_SOLID * PSTRIDE + blockIdx.x);
+  for (int e = 0; e < MEU_MAX_EL; ++e) block_reduce_store(cs[e], 0, partials + (Q_CSUM0 + e) * PSTRIDE + blockIdx.x);
 }
 
 }  // namespace meu
