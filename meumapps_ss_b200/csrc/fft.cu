@@ -63,29 +63,33 @@ FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_) : nx(nx_), ny(ny_), nz(nz_), n
   const int Lx = nx / 2;
   auto rvx = rev_table(Lx, rx), rvy = rev_table(ny, ry), rvz = rev_table(nz, rz);
   const size_t csz = fp64 ? sizeof(double2) : sizeof(float2);
-  // layout: twx[Lx] twy[ny] twz[nz] post[nxh] | revx revy revz
-  size_t ntw = (size_t)Lx + ny + nz + nxh;
+  const int K = fp64 ? 1 : 2;  // float tables hold hi then lo
+  // layout: twx[Lx*K] twy[ny*K] twz[nz*K] post[nxh*K] | revx revy revz
+  size_t ntw = ((size_t)Lx + ny + nz + nxh) * K;
   size_t bytes_tw = ntw * csz;
   size_t bytes = bytes_tw + sizeof(int) * ((size_t)Lx + ny + nz) + 256;
   std::vector<unsigned char> host(bytes, 0);
-  auto put = [&](size_t idx, long double c, long double s) {
-    if (fp64) {
-      double2 v = make_double2((double)c, (double)s);
-      memcpy(host.data() + idx * csz, &v, csz);
-    } else {
-      float2 v = make_float2((float)(double)c, (float)(double)s);
-      memcpy(host.data() + idx * csz, &v, csz);
+  auto put_table = [&](size_t base, int n_entries, int L) {
+    for (int n = 0; n < n_entries; ++n) {
+      long double c, s;
+      twiddle(n, L, c, s);
+      if (fp64) {
+        double2 v = make_double2((double)c, (double)s);
+        memcpy(host.data() + (base + n) * csz, &v, csz);
+      } else {
+        const float ch = (float)(double)c, sh = (float)(double)s;
+        float2 hi = make_float2(ch, sh);
+        float2 lo = make_float2((float)(double)(c - (long double)ch), (float)(double)(s - (long double)sh));
+        memcpy(host.data() + (base + n) * csz, &hi, csz);
+        memcpy(host.data() + (base + n_entries + n) * csz, &lo, csz);
+      }
     }
   };
-  size_t off = 0;
-  long double c, s;
-  for (int n = 0; n < Lx; ++n) { twiddle(n, Lx, c, s); put(off + n, c, s); }
-  off += Lx;
-  for (int n = 0; n < ny; ++n) { twiddle(n, ny, c, s); put(off + n, c, s); }
-  off += ny;
-  for (int n = 0; n < nz; ++n) { twiddle(n, nz, c, s); put(off + n, c, s); }
-  off += nz;
-  for (int n = 0; n < nxh; ++n) { twiddle(n, nx, c, s); put(off + n, c, s); }
+  const size_t ox = 0, oy = (size_t)Lx * K, oz = oy + (size_t)ny * K, op = oz + (size_t)nz * K;
+  put_table(ox, Lx, Lx);
+  put_table(oy, ny, ny);
+  put_table(oz, nz, nz);
+  put_table(op, nxh, nx);
   int* ri = (int*)(host.data() + bytes_tw);
   memcpy(ri, rvx.data(), sizeof(int) * Lx);
   memcpy(ri + Lx, rvy.data(), sizeof(int) * ny);
@@ -101,10 +105,10 @@ FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_) : nx(nx_), ny(ny_), nz(nz_), n
     p.tw = tw;
     p.rev = rev;
   };
-  fill(px, Lx, rx, d, dr);
-  fill(py, ny, ry, d + (size_t)Lx * csz, dr + Lx);
-  fill(pz, nz, rz, d + (size_t)(Lx + ny) * csz, dr + Lx + ny);
-  post_tw = d + (size_t)(Lx + ny + nz) * csz;
+  fill(px, Lx, rx, d + ox * csz, dr);
+  fill(py, ny, ry, d + oy * csz, dr + Lx);
+  fill(pz, nz, rz, d + oz * csz, dr + Lx + ny);
+  post_tw = d + op * csz;
 }
 
 FFT3::~FFT3() {
@@ -152,13 +156,13 @@ __global__ void __launch_bounds__(256) k_rows_r2c(PtrList<const R> in, PtrList<c
       C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
       C o = cscale(csub(zk, cconj(zm)), (R)0.5);
       o = mk(o.y, -o.x);
-      drow[k] = cadd(e, cmul(post[k], o));
+      drow[k] = cadd(e, Tw<C>::mul(o, post, k, nxh));
     }
     if (k != L - k) {
       C e = cscale(cadd(zm, cconj(zk)), (R)0.5);
       C o = cscale(csub(zm, cconj(zk)), (R)0.5);
       o = mk(o.y, -o.x);
-      drow[L - k] = cadd(e, cmul(post[L - k], o));
+      drow[L - k] = cadd(e, Tw<C>::mul(o, post, L - k, nxh));
     }
   }
 }
@@ -188,12 +192,12 @@ __global__ void __launch_bounds__(256) k_rows_c2r(PtrList<const cplx<R>> in, Ptr
     // Z[k] = (X[k] + conj X[L-k]) + i (X[k] - conj X[L-k]) W^-k
     {
       C ex = cadd(xk, cconj(xm));
-      C ox = cmulc(csub(xk, cconj(xm)), post[k]);
+      C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, nxh);
       buf[r * pitch + posk[k % L]] = cadd(ex, mk(-ox.y, ox.x));
     }
     if (k != 0 && k != L - k) {
       C ex = cadd(xm, cconj(xk));
-      C ox = cmulc(csub(xm, cconj(xk)), post[L - k]);
+      C ox = Tw<C>::mulc(csub(xm, cconj(xk)), post, L - k, nxh);
       buf[r * pitch + posk[L - k]] = cadd(ex, mk(-ox.y, ox.x));
     }
   }

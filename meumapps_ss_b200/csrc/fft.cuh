@@ -20,8 +20,35 @@ struct LinePlan {
   int L;       // transform length
   int ns;      // number of stages
   int r[12];   // radix of each DIF stage (product = L)
-  const void* tw;   // cplx<R>[L], tw[n] = exp(-2 pi i n / L)
+  const void* tw;   // cplx<R>[L * Tw::K], tw[n] = exp(-2 pi i n / L) (float: hi then lo)
   const int* rev;   // rev[p] = frequency index held at position p after DIF
+};
+
+// ------------------------------------------------------ compensated twiddles
+// FP32 transforms carry every twiddle as an unevaluated sum hi + lo of two
+// floats (hi = W rounded to float, lo = W - hi rounded to float) and multiply
+// x*hi + x*lo.  A forward/inverse pair then equals the identity up to random
+// rounding instead of a fixed bias |W_hi|^2 != 1 that every time step would
+// re-apply.  A twiddle table of length L stores hi at [0, L) and lo at [L, 2L)
+// for float; double tables have no lo part.
+template <typename C> struct Tw;
+template <> struct Tw<double2> {
+  static constexpr int K = 1;
+  static __device__ __forceinline__ double2 mul(double2 x, const double2* t, int i, int) { return cmul(x, t[i]); }
+  static __device__ __forceinline__ double2 mulc(double2 x, const double2* t, int i, int) { return cmulc(x, t[i]); }
+  static __device__ __forceinline__ double2 scale(double2 x, double hi, double) { return cscale(x, hi); }
+};
+template <> struct Tw<float2> {
+  static constexpr int K = 2;
+  static __device__ __forceinline__ float2 mul(float2 x, const float2* t, int i, int L) {
+    return cadd(cmul(x, t[i]), cmul(x, t[i + L]));
+  }
+  static __device__ __forceinline__ float2 mulc(float2 x, const float2* t, int i, int L) {
+    return cadd(cmulc(x, t[i]), cmulc(x, t[i + L]));
+  }
+  static __device__ __forceinline__ float2 scale(float2 x, double hi, double lo) {
+    return cadd(cscale(x, (float)hi), cscale(x, (float)lo));
+  }
 };
 
 // ---------------------------------------------------------------- butterflies
@@ -48,9 +75,12 @@ template <int S, typename C> struct Dft<4, S, C> {
 template <int S, typename C> struct Dft<3, S, C> {
   static __device__ __forceinline__ void run(C* x) {
     using R = decltype(x[0].x);
-    const R h = (R)0.5, s3 = (R)0.86602540378443864676372317075293618;
+    const R h = (R)0.5;
+    // sqrt(3)/2 as hi + lo (lo = 0 for double)
+    const double s3h = sizeof(R) == 4 ? (double)0.8660254f : 0.86602540378443864676;
+    const double s3l = sizeof(R) == 4 ? 0.86602540378443864676 - (double)0.8660254f : 0.0;
     C t = cadd(x[1], x[2]);
-    C u = cmul_is<S>(cscale(csub(x[1], x[2]), s3));
+    C u = cmul_is<S>(Tw<C>::scale(csub(x[1], x[2]), s3h, s3l));
     C m = csub(x[0], cscale(t, h));
     x[0] = cadd(x[0], t);
     x[1] = cadd(m, u);
@@ -60,7 +90,9 @@ template <int S, typename C> struct Dft<3, S, C> {
 template <int S, typename C> struct Dft<8, S, C> {
   static __device__ __forceinline__ void run(C* x) {
     using R = decltype(x[0].x);
-    const R r2 = (R)0.70710678118654752440084436210484904;
+    // sqrt(2)/2 as hi + lo (lo = 0 for double)
+    const double r2h = sizeof(R) == 4 ? (double)0.70710677f : 0.70710678118654752440;
+    const double r2l = sizeof(R) == 4 ? 0.70710678118654752440 - (double)0.70710677f : 0.0;
     C a[4], b[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
@@ -68,9 +100,9 @@ template <int S, typename C> struct Dft<8, S, C> {
       b[r] = csub(x[r], x[r + 4]);
     }
     // b_r *= W8^r, W8 = exp(S 2 pi i / 8)
-    b[1] = cscale(cadd(b[1], cmul_is<S>(b[1])), r2);
+    b[1] = Tw<C>::scale(cadd(b[1], cmul_is<S>(b[1])), r2h, r2l);
     b[2] = cmul_is<S>(b[2]);
-    b[3] = cscale(csub(cmul_is<S>(b[3]), b[3]), r2);
+    b[3] = Tw<C>::scale(csub(cmul_is<S>(b[3]), b[3]), r2h, r2l);
     Dft<4, S, C>::run(a);
     Dft<4, S, C>::run(b);
 #pragma unroll
@@ -94,7 +126,7 @@ __device__ __forceinline__ void dif_stage(C* buf, int span, int L, int nlines, i
     for (int r = 0; r < R; ++r) x[r] = base[r * m * es];
     Dft<R, -1, C>::run(x);
 #pragma unroll
-    for (int q = 1; q < R; ++q) x[q] = cmul(x[q], tw[j * q * tws]);
+    for (int q = 1; q < R; ++q) x[q] = Tw<C>::mul(x[q], tw, j * q * tws, L);
 #pragma unroll
     for (int q = 0; q < R; ++q) base[q * m * es] = x[q];
   }
@@ -110,7 +142,7 @@ __device__ __forceinline__ void dit_stage(C* buf, int span, int L, int nlines, i
 #pragma unroll
     for (int q = 0; q < R; ++q) x[q] = base[q * m * es];
 #pragma unroll
-    for (int q = 1; q < R; ++q) x[q] = cmulc(x[q], tw[j * q * tws]);
+    for (int q = 1; q < R; ++q) x[q] = Tw<C>::mulc(x[q], tw, j * q * tws, L);
     Dft<R, 1, C>::run(x);
 #pragma unroll
     for (int r = 0; r < R; ++r) base[r * m * es] = x[r];
@@ -180,7 +212,7 @@ class FFT3 {
 
   LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
   LaunchHook* hook = nullptr;
-  const void* post_tw;  // cplx<R>[nx/2+1]: exp(-2 pi i k / nx)
+  const void* post_tw;  // cplx<R>[(nx/2+1) * Tw::K]: exp(-2 pi i k / nx) (float: hi then lo)
   bool fp64;
 
  private:

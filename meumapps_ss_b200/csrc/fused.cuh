@@ -84,7 +84,7 @@ __device__ __forceinline__ void dif_stage_s(C* buf, const C* __restrict__ tw) {
     Dft<R, -1, C>::run(x);
     if (M > 1) {
 #pragma unroll
-      for (int q = 1; q < R; ++q) x[q] = cmul(x[q], tw[j * q * TWS]);
+      for (int q = 1; q < R; ++q) x[q] = Tw<C>::mul(x[q], tw, j * q * TWS, L);
     }
 #pragma unroll
     for (int q = 0; q < R; ++q) base[q * M * ES] = x[q];
@@ -104,7 +104,7 @@ __device__ __forceinline__ void dit_stage_s(C* buf, const C* __restrict__ tw) {
     for (int q = 0; q < R; ++q) x[q] = base[q * M * ES];
     if (M > 1) {
 #pragma unroll
-      for (int q = 1; q < R; ++q) x[q] = cmulc(x[q], tw[j * q * TWS]);
+      for (int q = 1; q < R; ++q) x[q] = Tw<C>::mulc(x[q], tw, j * q * TWS, L);
     }
     Dft<R, 1, C>::run(x);
 #pragma unroll
@@ -138,22 +138,23 @@ struct Plane {
   using C = cplx<R>;
   static constexpr int LX = N / 2, NXH = LX + 1, PITCH = NXH, NY = N;
   static constexpr int ELEMS = NY * PITCH;
-  // twiddles: twx[LX], twy[NY], post[NXH]
-  static constexpr int TW_ELEMS = LX + NY + NXH;
+  // twiddles (hi then lo for float): twx[LX*K], twy[NY*K], post[NXH*K]
+  static constexpr int K = Tw<C>::K;
+  static constexpr int TW_ELEMS = (LX + NY + NXH) * K;
   static constexpr size_t smem_bytes() { return sizeof(C) * (size_t)(ELEMS + TW_ELEMS); }
 
   static __device__ __forceinline__ void load_tw(C* tws, const C* __restrict__ gx, const C* __restrict__ gy,
                                                  const C* __restrict__ gpost) {
-    for (int i = threadIdx.x; i < LX; i += NT) tws[i] = gx[i];
-    for (int i = threadIdx.x; i < NY; i += NT) tws[LX + i] = gy[i];
-    for (int i = threadIdx.x; i < NXH; i += NT) tws[LX + NY + i] = gpost[i];
+    for (int i = threadIdx.x; i < LX * K; i += NT) tws[i] = gx[i];
+    for (int i = threadIdx.x; i < NY * K; i += NT) tws[LX * K + i] = gy[i];
+    for (int i = threadIdx.x; i < NXH * K; i += NT) tws[(LX + NY) * K + i] = gpost[i];
   }
 
   // buf rows hold (x[2n], x[2n+1]) at n in [0, LX): R2C along x, FFT along y.
   static __device__ __forceinline__ void forward(C* buf, const C* tws) {
     const C* twx = tws;
-    const C* twy = tws + LX;
-    const C* post = tws + LX + NY;
+    const C* twy = tws + LX * K;
+    const C* post = tws + (LX + NY) * K;
     dif<C, LX, NY, PITCH, 1, NT>(buf, twx);
     // split in place, in digit-reversed column order (Nyquist into column LX)
     constexpr int NP = LX / 2 + 1;
@@ -165,7 +166,7 @@ struct Plane {
       C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
       C o = cscale(csub(zk, cconj(zm)), (R)0.5);
       o = mk(o.y, -o.x);
-      const C xk = cadd(e, cmul(post[k], o));
+      const C xk = cadd(e, Tw<C>::mul(o, post, k, NXH));
       if (k == 0) {
         // X[0] = E + O, X[LX] = E - O
         rb[0] = xk;
@@ -176,7 +177,7 @@ struct Plane {
           C e2 = cscale(cadd(zm, cconj(zk)), (R)0.5);
           C o2 = cscale(csub(zm, cconj(zk)), (R)0.5);
           o2 = mk(o2.y, -o2.x);
-          rb[pm] = cadd(e2, cmul(post[LX - k], o2));
+          rb[pm] = cadd(e2, Tw<C>::mul(o2, post, LX - k, NXH));
         }
       }
     }
@@ -187,8 +188,8 @@ struct Plane {
   // inverse of forward(): M-form plane -> rows of (x[2n], x[2n+1]), unscaled.
   static __device__ __forceinline__ void inverse(C* buf, const C* tws) {
     const C* twx = tws;
-    const C* twy = tws + LX;
-    const C* post = tws + LX + NY;
+    const C* twy = tws + LX * K;
+    const C* post = tws + (LX + NY) * K;
     dit<C, NY, NXH, 1, PITCH, NT>(buf, twy);
     constexpr int NP = LX / 2 + 1;
     for (int i = threadIdx.x; i < NY * NP; i += NT) {
@@ -200,12 +201,12 @@ struct Plane {
       if (k == 0) { xk.y = 0; xm.y = 0; }
       {
         const C ex = cadd(xk, cconj(xm));
-        const C ox = cmulc(csub(xk, cconj(xm)), post[k]);
+        const C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, NXH);
         rb[pk] = cadd(ex, mk(-ox.y, ox.x));
       }
       if (k != 0 && k != LX - k) {
         const C ex = cadd(xm, cconj(xk));
-        const C ox = cmulc(csub(xm, cconj(xk)), post[LX - k]);
+        const C ox = Tw<C>::mulc(csub(xm, cconj(xk)), post, LX - k, NXH);
         rb[pm] = cadd(ex, mk(-ox.y, ox.x));
       }
     }

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
   C* tw = buf + N * LN;
   __shared__ LanFusedConst F;
   for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
-  for (int i = threadIdx.x; i < N; i += NT) tw[i] = a.twz[i];
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   for (int i = threadIdx.x; i < N * LN; i += NT) {
     const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
   __shared__ double dtl;
   for (int i = threadIdx.x; i < V * 9; i += NT) g[i / 9][i % 9] = a.F->g[i / 9][i % 9];
   if (threadIdx.x == 0) dtl = a.F->dtl;
-  for (int i = threadIdx.x; i < N; i += NT) tw[i] = a.twz[i];
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   for (int i = threadIdx.x; i < N * LN; i += NT) {
     const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
@@ -407,8 +407,8 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
   const int tiles = N * NXH / TM;
   const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
   const size_t sp = P::smem_bytes();
-  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N);
-  const size_t s2 = sizeof(C) * ((size_t)N * V * TM + N);
+  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
+  const size_t s2 = sizeof(C) * ((size_t)N * V * TM + N * Tw<C>::K);
   ensure_smem(k_lf_pf<R, N>, sp);
   ensure_smem(k_lf_pb<R, N>, sp);
   ensure_smem(k_lf_pi<R, N>, sp);
