@@ -262,9 +262,6 @@ class Engine : public EngineBase {
   std::vector<void*> allocs;
   // reference quirk state: values written on the next fort.98 line
   double prev_min = 1.0, prev_max = 0.0, prev_phimax = 0.0, prev_solid = 0.0;
-  // gradient energy of eta at the start of the next step, when a step computes it
-  // from its result (fused Landau path); 0 when each step computes its own
-  double fint_carry = 0.0;
   bool el_ready = false;  // u^ / strain hold a valid elastic state
   int last_iters = 0;
 
@@ -311,6 +308,8 @@ class Engine : public EngineBase {
   void kks_step(meu_diag* d);
   void landau_step(meu_diag* d);
   void landau_step_fused();
+  LanFusedArgs<R> fused_args() const;
+  C *keta = nullptr, *kc = nullptr;  // spectral state of the fused Landau step
   void end_step(meu_diag* d, int clip);
   void flush_hist(meu_diag* diag);
   static constexpr int HIST_MAX = 4096;
@@ -476,6 +475,8 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     F.dtl = p.dt * p.b_mob;
     dF = dalloc<LanFusedConst>(1);
     MEU_CUDA(cudaMemcpy(dF, &F, sizeof(F), cudaMemcpyHostToDevice));
+    keta = dalloc<C>((int64_t)V * nk);
+    kc = dalloc<C>(nk);
   }
   MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
   MEU_CUDA(cudaMemset(c, 0, sizeof(R) * E * n3));
@@ -555,21 +556,10 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     }
   }
   if (phi_in) up(phi_in, phi, V, 0);
-  if (phi_in) {
-    fint_carry = 0.0;
-    if (fused && P.diag_energy) {
-      // gradient energy of the uploaded eta: the fused step reports each step's
-      // start-of-step value from the transform of the previous step's result
-      std::vector<const R*> in;
-      for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
-      fwd_list(in, 0);
-      KLAUNCH("grad_energy", (double)V * nk * sizeof(C),
-              k_grad_energy<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, V), V, partials + (int64_t)Q_FINT2 * PSTRIDE));
-      finalize(Q_FINT2, 1);
-      MEU_CUDA(cudaMemcpyAsync(h_results + Q_FINT2, results + Q_FINT2, sizeof(double), cudaMemcpyDeviceToHost, st));
-      MEU_CUDA(cudaStreamSynchronize(st));
-      fint_carry = h_results[Q_FINT2] * (double)n3;
-    }
+  if (fused && (cons || phi_in)) {
+    // spectral state of the fused step from the uploaded real fields
+    const LanFusedArgs<R> a = fused_args();
+    if (!lan_fused_init<R>(P.nx, V, a, st, &prof)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
   }
   if (strain) {
     if (ustate) {
@@ -769,23 +759,30 @@ void Engine<R>::kks_step(meu_diag* d) {
 
 // ---------------------------------------------------------------- Landau step
 template <typename R>
-void Engine<R>::landau_step_fused() {
-  const bool elast = P.elastic != MEU_ELAST_NONE && step >= P.elastep0;
+LanFusedArgs<R> Engine<R>::fused_args() const {
   LanFusedArgs<R> a;
   a.F = dF;
   a.eta = phi;
   a.c = c;
   a.c2 = c2;
   a.M = sp;
+  a.Keta = keta;
+  a.Kc = kc;
   a.partials = partials;
   a.pstride = PSTRIDE;
   a.err = d_err;
-  a.homog = elast ? 1 : 0;
+  a.homog = (P.elastic != MEU_ELAST_NONE && step >= P.elastep0) ? 1 : 0;
   a.energy = P.diag_energy;
   a.twx = (const C*)fft->px.tw;
   a.twy = (const C*)fft->py.tw;
   a.twz = (const C*)fft->pz.tw;
   a.post = (const C*)fft->post_tw;
+  return a;
+}
+
+template <typename R>
+void Engine<R>::landau_step_fused() {
+  const LanFusedArgs<R> a = fused_args();
   int nb[Q_TOTAL];
   if (!lan_fused_step<R>(P.nx, V, a, st, &prof, nb)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
   std::swap(c, c2);
@@ -882,7 +879,7 @@ void Engine<R>::flush_hist(meu_diag* diag) {
       d->step = hist_step[i];
       d->el_iters = hist_iters[i];
       d->status = 0;
-      d->fint = (lan ? r[Q_FINT] * sn3 : r[Q_FINT]) + fint_carry;
+      d->fint = lan ? (r[Q_FINT] + r[Q_FINT2]) * sn3 : r[Q_FINT];
       d->fw = r[Q_FW];
       d->fch = r[Q_FCH];
       d->elen = (lan && P.elastic == MEU_ELAST_HOMOG) ? r[Q_ELEN] * sn3 : r[Q_ELEN];
@@ -901,7 +898,6 @@ void Engine<R>::flush_hist(meu_diag* diag) {
     prev_max = r[Q_CMAX];
     prev_phimax = r[Q_PHIMAX];
     prev_solid = r[Q_SOLID];
-    fint_carry = r[Q_FINT2] * sn3;
     const double et = r[Q_FINT] + r[Q_FCH] + r[Q_ELEN] + r[Q_FW];
     if (!std::isfinite(et) || !std::isfinite(r[Q_CSUM0]) || !std::isfinite(r[Q_SOLID])) {
       hist_n = 0;

@@ -26,8 +26,10 @@ template <typename R> constexpr int col_tile() { return sizeof(R) == 4 ? 16 : 8;
 }  // namespace
 
 // ------------------------------------------------------------------ PF
+// raw = 0: fields theta_v (f < V); block f == V only accumulates the bulk energy.
+// raw = 1: fields eta_v (f < V) and dc (f == V), for the spectral state.
 template <typename R, int N>
-__global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V) {
+__global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V, int raw) {
   using P = fz::Plane<R, N, NT>;
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -46,7 +48,9 @@ __global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V) {
     C v;
     if (f < V) {
       const C e = ((const C*)(ez + f * N3 + off))[n];
-      v = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
+      v = raw ? e : mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
+    } else if (raw) {
+      v = ((const C*)(cz + off))[n];
     } else {
       v = ((const C*)(cz + off))[n];
       if (a.energy) {
@@ -66,10 +70,42 @@ __global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V) {
     }
     buf[y * P::PITCH + n] = v;
   }
+  if (f == V && !raw) {
+    block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + z);
+    return;
+  }
   __syncthreads();
   P::forward(buf, tws);
   P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
-  if (f == V) block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + z);
+}
+
+// ------------------------------------------------------------------ Z0
+// set-up: z FFT of eta_v (f < V) and dc (f == V) into the spectral state
+template <typename R, int N, int V>
+__global__ void __launch_bounds__(NT) k_lf_z0(LanFusedArgs<R> a) {
+  using C = cplx<R>;
+  constexpr int TM = col_tile<R>(), NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tw = buf + N * LN;
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
+    buf[i] = a.M[f * NK + zz * PL + m0 + c];
+  }
+  __syncthreads();
+  fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int p = i / LN, r = i - p * LN, f = r / TM, c = r - f * TM;
+    const C v = buf[i];
+    C o = mk((R)((double)v.x * s), (R)((double)v.y * s));
+    if (f == V && p == 0 && m0 + c == 0) o = mk((R)0, (R)0);  // dc has no k = 0 mode
+    C* dst = (f < V) ? a.Keta + f * NK : a.Kc;
+    dst[p * PL + m0 + c] = o;
+  }
 }
 
 // ------------------------------------------------------------------ Z1
@@ -79,18 +115,18 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
   constexpr int TM = col_tile<R>(), NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;  // [N][NF][TM]
+  C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
   C* tw = buf + N * LN;
   __shared__ LanFusedConst F;
   for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
-  for (int i = threadIdx.x; i < N * LN; i += NT) {
-    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
-    buf[i] = a.M[f * NK + zz * PL + m0 + c];
+  for (int i = threadIdx.x; i < N * V * TM; i += NT) {
+    const int zz = i / (V * TM), r = i - zz * (V * TM), f = r / TM, c = r - f * TM;
+    buf[zz * LN + r] = a.M[f * NK + zz * PL + m0 + c];
   }
   __syncthreads();
-  fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
+  fz::dif<C, N, V * TM, 1, LN, NT>(buf, tw);
   const double s = 1.0 / ((double)N * N * N);
   double fint = 0, elen = 0;
   for (int i = threadIdx.x; i < N * TM; i += NT) {
@@ -110,7 +146,9 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
       str += tr[v];
       sti += ti[v];
     }
-    const double cr = (double)e[V * TM].x * s, ci = (double)e[V * TM].y * s;
+    C* kc = a.Kc + p * PL + m;
+    const C cs = *kc;
+    const double cr = (double)cs.x, ci = (double)cs.y;
     const bool k0 = (kx == 0 && ky == 0 && kz == 0);
     if (a.energy) fint += 0.5 * w * F.kappa_c * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci);
     // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
@@ -190,7 +228,7 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
       }
       elen += 0.5 * w * qq;
     }
-    // ---- Cahn-Hilliard on the fluctuation: mu^ = A dc^ - B/2 sum theta^
+    // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
     double nr = 0, ni = 0;
     if (!k0) {
       const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
@@ -199,7 +237,9 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
       nr = (cr - F.dm * k2 * mr) / den;
       ni = (ci - F.dm * k2 * mi) / den;
     }
-    e[V * TM] = mk((R)nr, (R)ni);
+    const C cn = mk((R)nr, (R)ni);
+    *kc = cn;
+    e[V * TM] = cn;
   }
   __syncthreads();
   fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
@@ -263,7 +303,7 @@ __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
         for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
         g += -2.0 * ev * sacc;
       }
-      out[h] = ev - F.dtl * g;
+      out[h] = g;
     }
     buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
   }
@@ -307,16 +347,22 @@ __global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const double* gv = g[v];
-      const double kk = gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] +
-                        (gv[3] + gv[1]) * b[0] * b[1] + (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-      const double sc = s / (1.0 + dtl * kk);
-      const double er = (double)e[v * TM].x * sc, ei = (double)e[v * TM].y * sc;
-      e[v * TM] = mk((R)er, (R)ei);
+      C* ks = a.Keta + v * NK + p * PL + m;
+      const C st = *ks;
+      const double hr = (double)st.x, hi = (double)st.y;
       if (a.energy) {
         const double kb = gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
                           (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-        fint += 0.5 * w * kb * (er * er + ei * ei);
+        fint += 0.5 * w * kb * (hr * hr + hi * hi);
       }
+      const double kk = gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] +
+                        (gv[3] + gv[1]) * b[0] * b[1] + (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+      const double rden = 1.0 / (1.0 + dtl * kk);
+      const double nr = (hr - dtl * s * (double)e[v * TM].x) * rden;
+      const double ni = (hi - dtl * s * (double)e[v * TM].y) * rden;
+      const C o = mk((R)nr, (R)ni);
+      *ks = o;
+      e[v * TM] = o;
     }
   }
   __syncthreads();
@@ -415,12 +461,12 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
   ensure_smem(k_lf_z1<R, N, V>, s1);
   ensure_smem(k_lf_z2<R, N, V>, s2);
   {
-    Scope s(hook, "lf_plane_fwd", (double)(V + 1) * nk * sizeof(C) + (2.0 * V + 1) * n3 * sizeof(R), st);
-    k_lf_pf<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V);
+    Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pf<R, N><<<dim3(N, a.energy ? V + 1 : V), NT, sp, st>>>(a, V, 0);
     MEU_CHECK_LAUNCH();
   }
   {
-    Scope s(hook, "lf_z_green_ch", 2.0 * (V + 1) * nk * sizeof(C), st);
+    Scope s(hook, "lf_z_green_ch", (2.0 * V + 3) * nk * sizeof(C), st);
     k_lf_z1<R, N, V><<<tiles, NT, s1, st>>>(a);
     MEU_CHECK_LAUNCH();
   }
@@ -430,7 +476,7 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
     MEU_CHECK_LAUNCH();
   }
   {
-    Scope s(hook, "lf_z_tdgl", 2.0 * V * nk * sizeof(C), st);
+    Scope s(hook, "lf_z_tdgl", 4.0 * V * nk * sizeof(C), st);
     k_lf_z2<R, N, V><<<tiles, NT, s2, st>>>(a);
     MEU_CHECK_LAUNCH();
   }
@@ -440,11 +486,46 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
     MEU_CHECK_LAUNCH();
   }
   for (int q = 0; q < Q_TOTAL; ++q) nb[q] = 0;
-  nb[Q_FCH] = N;
+  nb[Q_FCH] = a.energy ? N : 0;
   nb[Q_FINT] = tiles;
   nb[Q_ELEN] = tiles;
   nb[Q_FINT2] = tiles;
   nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * V;
+}
+
+template <typename R, int N, int V>
+void run_init(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
+  using P = fz::Plane<R, N, NT>;
+  using C = cplx<R>;
+  constexpr int TM = col_tile<R>();
+  constexpr int NXH = N / 2 + 1;
+  const int tiles = N * NXH / TM;
+  const size_t sp = P::smem_bytes();
+  const size_t s0 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
+  ensure_smem(k_lf_pf<R, N>, sp);
+  ensure_smem(k_lf_z0<R, N, V>, s0);
+  const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
+  {
+    Scope s(hook, "lf_plane_fwd_state", (V + 1.0) * (nk * sizeof(C) + n3 * sizeof(R)), st);
+    k_lf_pf<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V, 1);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_z_state", 2.0 * (V + 1) * nk * sizeof(C), st);
+    k_lf_z0<R, N, V><<<tiles, NT, s0, st>>>(a);
+    MEU_CHECK_LAUNCH();
+  }
+}
+
+template <typename R, int N>
+bool dispatch_init(int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
+  switch (V) {
+    case 1: run_init<R, N, 1>(a, st, hook); return true;
+    case 2: run_init<R, N, 2>(a, st, hook); return true;
+    case 3: run_init<R, N, 3>(a, st, hook); return true;
+    case 4: run_init<R, N, 4>(a, st, hook); return true;
+    default: return false;
+  }
 }
 
 template <typename R, int N>
@@ -478,6 +559,19 @@ bool lan_fused_step(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, Lau
   }
 }
 
+template <typename R>
+bool lan_fused_init(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
+  switch (N) {
+    case 32: return dispatch_init<R, 32>(V, a, st, hook);
+    case 48: return dispatch_init<R, 48>(V, a, st, hook);
+    case 64: return dispatch_init<R, 64>(V, a, st, hook);
+    case 96: return dispatch_init<R, 96>(V, a, st, hook);
+    case 128: return dispatch_init<R, 128>(V, a, st, hook);
+    default: return false;
+  }
+}
+template bool lan_fused_init<float>(int, int, const LanFusedArgs<float>&, cudaStream_t, LaunchHook*);
+template bool lan_fused_init<double>(int, int, const LanFusedArgs<double>&, cudaStream_t, LaunchHook*);
 template bool lan_fused_step<float>(int, int, const LanFusedArgs<float>&, cudaStream_t, LaunchHook*, int*);
 template bool lan_fused_step<double>(int, int, const LanFusedArgs<double>&, cudaStream_t, LaunchHook*, int*);
 

@@ -1,17 +1,25 @@
 // landau_fused.cuh -- the fused Landau time step (cubic grids N in
 // {32, 48, 64, 96, 128}, 1..4 variants, theta = eta^2 coupling, homogeneous
-// elasticity or none).  Five launches per step:
+// elasticity or none).
 //
-//   PF  plane:  theta_v = eta_v^2 and the fluctuation dc -> x R2C + y FFT   (+ bulk energy)
-//   Z1  column: z FFT -> Green operator phi_v, Cahn-Hilliard update of dc -> z iFFT
-//              (mu^ = A dc^ - B/2 sum theta^_v, so mu needs no transform of its own)
-//   PB  plane:  y iFFT + x C2R of phi_v -> w_v = eta_v - dt L (df/deta_v + el_grad_v)
-//              -> x R2C + y FFT;  plane of dc_new -> real
-//   Z2  column: z FFT -> w^_v / (1 + dt L k.kappa.k) -> z iFFT             (+ gradient energy of eta_new)
+// The state of the step is spectral: eta^_v and the fluctuation dc^ are kept
+// in device memory in the column kernels' layout ([kz position][column]) and
+// every step only adds its increment to them.  The real-space eta and dc are
+// re-derived each step for the nonlinear terms and the output.  (Re-transforming
+// the real fields every step instead makes an FP32 forward/inverse pair act on
+// slowly varying data each step, whose rounding errors then add up coherently.)
+// Five launches per step:
+//
+//   PF  plane:  theta_v = eta_v^2 -> x R2C + y FFT                         (+ bulk energy)
+//   Z1  column: z FFT of theta -> Green operator phi_v; Cahn-Hilliard update of
+//              the dc^ state (mu^ = A dc^ - B/2 sum theta^_v) -> z iFFT of phi_v, dc_new
+//   PB  plane:  y iFFT + x C2R of phi_v -> g_v = df/deta_v + el_grad_v -> x R2C + y FFT;
+//              plane of dc_new -> real
+//   Z2  column: z FFT of g -> eta^ state <- (eta^ - dt L g^) / (1 + dt L k.kappa.k) -> z iFFT
 //   PI  plane:  y iFFT + x C2R of eta_new -> real eta (+ end-of-step statistics)
 //
-// The reduction partials of each kernel are indexed by its block; the engine
-// finalises them once per step.
+// Set-up (after new fields are uploaded): PF in raw mode transforms eta_v and dc,
+// Z0 finishes the z transform into the spectral state.
 #pragma once
 #include "fused.cuh"
 #include "kernels.cuh"
@@ -38,6 +46,8 @@ struct LanFusedArgs {
   R* c;       // dc (start of step)
   R* c2;      // dc (end of step)
   cplx<R>* M; // V+1 M-form spectra
+  cplx<R>* Keta;  // spectral state eta^_v (V spectra, normalised, column-kernel layout)
+  cplx<R>* Kc;    // spectral state dc^ (normalised, column-kernel layout)
   double* partials;
   int pstride;
   int* err;
@@ -56,6 +66,9 @@ enum LanQ : int {
 // host launch entry (landau_fused.cu): returns false if (N, V) has no instantiation
 template <typename R>
 bool lan_fused_step(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb_out);
+// spectral state from the real fields eta and dc (after an upload)
+template <typename R>
+bool lan_fused_init(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook);
 bool lan_fused_supported(const meu_params& p);
 
 }  // namespace meu

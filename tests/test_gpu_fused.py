@@ -71,3 +71,27 @@ def test_fused_fp32_vs_fp64_128():
     re = np.linalg.norm(e32 - e64) / np.linalg.norm(e64)
     assert rc < 1e-5 and re < 1e-5, (rc, re)
     assert np.max(np.abs(d32["etot"] - d64["etot"]) / np.abs(d64["etot"])) < 1e-5
+
+
+@pytest.mark.gpu
+def test_config1_fp32_error_after_1000_steps():
+    """Accuracy gate of the mixed-precision step: Landau deck 1 (128^3, 3
+    variants, seed -7) after 1000 steps, FP32 bulk against the GPU's plain FP64
+    path: relative L2 error <= 1e-5 in c and in eta."""
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200 import configs as CF
+    w = CF.landau_config(1, precision=P.PREC_F64)
+    c, e = _lib.init_uniform(128, 128, 128, 3, w.seed, w.c0, w.c_amp, w.eta_amp)
+    out = {}
+    for prec in (P.PREC_F64, P.PREC_F32):
+        p = w.params.copy()
+        p.precision = prec
+        with Simulation(p) as g:
+            g.set_fields(c, e)
+            g.run(1000, diag=False)
+            out[prec] = g.get_fields()
+    c64, e64, _, _ = out[P.PREC_F64]
+    c32, e32, _, _ = out[P.PREC_F32]
+    rc = np.linalg.norm(c32 - c64) / np.linalg.norm(c64)
+    re = np.linalg.norm(e32 - e64) / np.linalg.norm(e64)
+    assert rc <= 1e-5 and re <= 1e-5, (rc, re)
