@@ -1,0 +1,122 @@
+! meu_iface.f90 -- ISO_C_BINDING interface of include/meu.h for the MEUMAPPS-SS
+! Fortran driver (Multi_MEUMAPPS.f).  The driver keeps its set-up (Input.txt,
+! ModGparams, ModInitials, ran_2) and its data_save writer; the body of its
+! time loop (Multi_MEUMAPPS.f:548-1106) becomes one call of meu_run.
+!
+! Not compiled in the build image (it has no Fortran compiler); compile with
+! any Fortran 2003 compiler:  gfortran -c meu_iface.f90
+module meu_iface
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: MEU_MAX_VAR = 16, MEU_MAX_PH = 4, MEU_MAX_EL = 3
+  integer(c_int), parameter :: MEU_MAX_GP = 2 * MEU_MAX_EL + 1
+  integer(c_int), parameter :: MEU_MODEL_KKS = 0, MEU_MODEL_LANDAU = 1
+  integer(c_int), parameter :: MEU_PREC_F64 = 0, MEU_PREC_F32 = 1
+  integer(c_int), parameter :: MEU_ELAST_NONE = 0, MEU_ELAST_HOMOG = 1, MEU_ELAST_HETERO = 2
+
+  ! mirror of struct meu_params (field order and kinds as in meu.h)
+  type, bind(C) :: meu_params
+    integer(c_int64_t) :: step, elastep0, noise_step
+    integer(c_int32_t) :: nx, ny, nz, model, precision, nvar, numel, numph
+    integer(c_int32_t) :: nvar_ph(MEU_MAX_PH)
+    integer(c_int32_t) :: elastic, eig_coupling, el_min_iter, el_max_iter, clip_phi, diag_energy, reserved0
+    real(c_double) :: dt, b_mob
+    real(c_double) :: cmobs(MEU_MAX_EL)
+    real(c_double) :: el_tol
+    real(c_double) :: e_mean(6)
+    real(c_double) :: grad_coeff(9, MEU_MAX_VAR)   ! grad_coeff(:,:,v) flattened column-major
+    real(c_double) :: trans_ppt(6, MEU_MAX_VAR)
+    real(c_double) :: cela(36, MEU_MAX_PH)         ! CEla(:,:,n) flattened column-major
+    real(c_double) :: sela(36, MEU_MAX_PH)
+    real(c_double) :: gparams(MEU_MAX_GP, MEU_MAX_PH)
+    real(c_double) :: wellph(MEU_MAX_PH)
+    real(c_double) :: lan_a, lan_b, lan_c, lan_d, lan_c1, lan_c2, kappa_c, cross_w
+  end type meu_params
+
+  ! mirror of struct meu_diag: one fort.98 / fort.99 line
+  type, bind(C) :: meu_diag
+    integer(c_int64_t) :: step
+    integer(c_int32_t) :: el_iters, status
+    real(c_double) :: fint, fw, fch, elen, etot
+    real(c_double) :: glob_min, glob_max, phi_max, solid
+    real(c_double) :: cmin, cmax, phimax, solid_now
+    real(c_double) :: cavg(MEU_MAX_EL)
+  end type meu_diag
+
+  interface
+    integer(c_int) function meu_create(params, handle) bind(C, name="meu_create")
+      import :: c_int, c_ptr, meu_params
+      type(meu_params), intent(in) :: params
+      type(c_ptr), intent(out) :: handle
+    end function
+    integer(c_int) function meu_set_fields(h, cons, phi, u_state) bind(C, name="meu_set_fields")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, cons, phi, u_state
+    end function
+    integer(c_int) function meu_add_noise(h, incr) bind(C, name="meu_add_noise")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, incr
+    end function
+    integer(c_int) function meu_run(h, nsteps, diag) bind(C, name="meu_run")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: nsteps
+      type(c_ptr), value :: diag
+    end function
+    integer(c_int) function meu_get_fields(h, cons, phi, el_en, u_state) bind(C, name="meu_get_fields")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, cons, phi, el_en, u_state
+    end function
+    integer(c_int64_t) function meu_get_step(h) bind(C, name="meu_get_step")
+      import :: c_int64_t, c_ptr
+      type(c_ptr), value :: h
+    end function
+    type(c_ptr) function meu_last_error(h) bind(C, name="meu_last_error")
+      import :: c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function meu_destroy(h) bind(C, name="meu_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+  end interface
+
+contains
+
+  ! Copy the ModGparams state (after the set-up of Multi_MEUMAPPS.f:153-417) into
+  ! a meu_params block.  Arguments are the module variables of ModGparams.
+  subroutine meu_fill_params(p, Nx, Ny, Nz, vartot, numel, numph, Nvar, step, elastep0, noise_step, &
+                             t_step, b_mob, Cmobs, e_mean, grad_coeff, trans_ppt, CEla, SEla, Gparams, Wellph)
+    type(meu_params), intent(out) :: p
+    integer, intent(in) :: Nx, Ny, Nz, vartot, numel, numph, Nvar(numph), step, elastep0, noise_step
+    real(8), intent(in) :: t_step, b_mob, Cmobs(numel), e_mean(6)
+    real(8), intent(in) :: grad_coeff(3, 3, vartot), trans_ppt(6, vartot), CEla(6, 6, numph), SEla(6, 6, numph)
+    real(8), intent(in) :: Gparams(2 * numel + 1, numph), Wellph(numph)
+    integer :: v, n
+    p%step = step; p%elastep0 = elastep0; p%noise_step = noise_step
+    p%nx = Nx; p%ny = Ny; p%nz = Nz
+    p%model = MEU_MODEL_KKS; p%precision = MEU_PREC_F64
+    p%nvar = vartot; p%numel = numel; p%numph = numph
+    p%nvar_ph = 0; p%nvar_ph(1:numph) = Nvar
+    p%elastic = MEU_ELAST_HETERO; p%eig_coupling = 0
+    p%el_min_iter = 4; p%el_max_iter = 10; p%clip_phi = 1; p%diag_energy = 1; p%reserved0 = 0
+    p%dt = t_step; p%b_mob = b_mob
+    p%cmobs = 0; p%cmobs(1:numel) = Cmobs
+    p%el_tol = 1.0d-7
+    p%e_mean = e_mean
+    p%grad_coeff = 0; p%trans_ppt = 0; p%cela = 0; p%sela = 0; p%gparams = 0; p%wellph = 0
+    do v = 1, vartot
+      p%grad_coeff(:, v) = reshape(grad_coeff(:, :, v), (/9/))
+      p%trans_ppt(:, v) = trans_ppt(:, v)
+    end do
+    do n = 1, numph
+      p%cela(:, n) = reshape(CEla(:, :, n), (/36/))
+      p%sela(:, n) = reshape(SEla(:, :, n), (/36/))
+      p%gparams(1:2 * numel + 1, n) = Gparams(:, n)
+      p%wellph(n) = Wellph(n)
+    end do
+    p%lan_a = 0; p%lan_b = 0; p%lan_c = 0; p%lan_d = 0; p%lan_c1 = 0; p%lan_c2 = 0; p%kappa_c = 0; p%cross_w = 0
+  end subroutine meu_fill_params
+
+end module meu_iface

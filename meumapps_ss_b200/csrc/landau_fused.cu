@@ -471,7 +471,7 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
     MEU_CHECK_LAUNCH();
   }
   {
-    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V + 1) * nk * sizeof(C) + (2.0 * V + 2) * n3 * sizeof(R), st);
+    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V + 1) * nk * sizeof(C) + (V + 2.0) * n3 * sizeof(R), st);
     k_lf_pb<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V);
     MEU_CHECK_LAUNCH();
   }
