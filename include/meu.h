@@ -203,6 +203,27 @@ int64_t meu_launch_count(const meu_handle* h);
 int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t precision, const double* in, double* spec_out,
                       double* back_out);
 
+/* Allocation-free variant of meu_fft_roundtrip.  It has no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: a driver whose device
+ * memory belongs to its OpenACC / managed-memory runtime, a framework whose
+ * allocator has already reserved the GPU, or code that must not add the device
+ * synchronisation of cudaMalloc/cudaFree.  in_dev, spec_dev and back_dev are
+ * device-accessible arrays of the caller (device or managed memory): in_dev
+ * holds Nx*Ny*Nz doubles, spec_dev receives 2*Nz*Ny*(Nx/2+1) doubles (the scaled
+ * half spectrum, re,im interleaved), back_dev the unscaled inverse (Nx*Ny*Nz
+ * doubles).  The library's own working memory is a fixed static device array of
+ * about 3.3 MB that every GPU loading the library keeps until exit, so the grid
+ * may hold at most MEU_NOALLOC_MAX_POINTS points; larger grids return
+ * MEU_ERR_UNSUPPORTED (message in meu_last_error(NULL)).  The first call on a
+ * device looks up that array's device address; make that first call before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents (nothing in it needs to start at zero): calls that overlap on the GPU
+ * -- from several host threads at once -- race.  Runs on the default stream and
+ * is synchronous on return. */
+#define MEU_NOALLOC_MAX_POINTS 262144 /* 64^3 */
+int meu_fft_roundtrip_noalloc(int32_t nx, int32_t ny, int32_t nz, int32_t precision, const double* in_dev,
+                              double* spec_dev, double* back_dev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,7 @@ def lib():
     L.meu_langevin.restype = C.c_double
     L.meu_init_uniform.argtypes = [C.POINTER(Ran2State), i32, i32, i32, i32, C.c_double, C.c_double, C.c_double, dp, dp]
     L.meu_fft_roundtrip.argtypes = [i32, i32, i32, i32, dp, dp, dp]
+    L.meu_fft_roundtrip_noalloc.argtypes = [i32, i32, i32, i32, vp, vp, vp]
     L.meu_set_stream.argtypes = [vp, vp]
     L.meu_timing.argtypes = [vp, i32]
     L.meu_timing_report.argtypes = [vp, i32, C.c_char_p, C.POINTER(i64), dp, dp]

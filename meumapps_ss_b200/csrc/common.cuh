@@ -57,6 +57,9 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 16) {
   return (unsigned)g;
 }
 
+// Message returned by meu_last_error(NULL) for calls that have no handle.
+void set_thread_error(const std::string& msg);
+
 // Observer of kernel launches (launch counting and per-kernel event timing).
 // bytes = algorithmic bytes the launch must move (compulsory reads + writes).
 struct LaunchHook {

@@ -950,9 +950,13 @@ static int fail(meu_handle* h, int code, const std::string& msg) {
     return fail(h, MEU_ERR_CUDA, e.what());                           \
   }
 
-extern "C" {
-
 static thread_local std::string g_create_err;
+namespace meu {
+// message returned by meu_last_error(NULL) for calls that have no handle
+void set_thread_error(const std::string& msg) { g_create_err = msg; }
+}  // namespace meu
+
+extern "C" {
 
 int meu_create(const meu_params* params, meu_handle** out) {
   if (!params || !out) return MEU_ERR_BADARG;

@@ -56,7 +56,14 @@ static void twiddle(int n, int L, long double& c, long double& s) {
   s = sinl(a);
 }
 
-FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_) : nx(nx_), ny(ny_), nz(nz_), nxh(nx_ / 2 + 1), fp64(fp64_) {
+size_t FFT3::table_bytes(int nx, int ny, int nz, bool fp64) {
+  const size_t csz = fp64 ? sizeof(double2) : sizeof(float2);
+  const int K = fp64 ? 1 : 2;
+  return ((size_t)nx / 2 + ny + nz + nx / 2 + 1) * K * csz + sizeof(int) * ((size_t)nx / 2 + ny + nz) + 256;
+}
+
+FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_, void* table_mem, size_t table_cap)
+    : nx(nx_), ny(ny_), nz(nz_), nxh(nx_ / 2 + 1), fp64(fp64_) {
   std::vector<int> rx, ry, rz;
   if (!(nx % 2 == 0 && factor_23(nx / 2, rx) && factor_23(ny, ry) && factor_23(nz, rz)))
     throw CudaError("grid sizes must be 2^a 3^b (Nx even)", 100);
@@ -94,7 +101,14 @@ FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_) : nx(nx_), ny(ny_), nz(nz_), n
   memcpy(ri, rvx.data(), sizeof(int) * Lx);
   memcpy(ri + Lx, rvy.data(), sizeof(int) * ny);
   memcpy(ri + Lx + ny, rvz.data(), sizeof(int) * nz);
-  MEU_CUDA(cudaMalloc(&dev_mem, bytes));
+  if (table_mem) {
+    if (bytes > table_cap) throw CudaError("transform tables exceed the provided memory", 103);
+    dev_mem = table_mem;
+    owns_mem = false;
+  } else {
+    MEU_CUDA(cudaMalloc(&dev_mem, bytes));
+    owns_mem = true;
+  }
   MEU_CUDA(cudaMemcpy(dev_mem, host.data(), bytes, cudaMemcpyHostToDevice));
   unsigned char* d = (unsigned char*)dev_mem;
   const int* dr = (const int*)(d + bytes_tw);
@@ -112,7 +126,7 @@ FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_) : nx(nx_), ny(ny_), nz(nz_), n
 }
 
 FFT3::~FFT3() {
-  if (dev_mem) cudaFree(dev_mem);
+  if (dev_mem && owns_mem) cudaFree(dev_mem);
 }
 
 // ------------------------------------------------------------------ kernels

@@ -193,7 +193,11 @@ struct FFTPlan3;  // defined in fft.cu
 // Plan of a 3-D real transform of one grid (twiddle tables live on the device).
 class FFT3 {
  public:
-  FFT3(int nx, int ny, int nz, bool fp64);
+  // table_mem == NULL: the plan allocates its twiddle/digit tables with
+  // cudaMalloc.  Otherwise the tables are copied into table_mem (device memory
+  // of table_cap bytes owned by the caller) and the plan allocates nothing.
+  FFT3(int nx, int ny, int nz, bool fp64, void* table_mem = nullptr, size_t table_cap = 0);
+  static size_t table_bytes(int nx, int ny, int nz, bool fp64);
   ~FFT3();
   FFT3(const FFT3&) = delete;
   FFT3& operator=(const FFT3&) = delete;
@@ -217,6 +221,7 @@ class FFT3 {
 
  private:
   void* dev_mem = nullptr;
+  bool owns_mem = false;
 };
 
 bool fft_size_ok(int n, bool is_x);
