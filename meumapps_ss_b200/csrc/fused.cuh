@@ -23,13 +23,18 @@ struct RPlan {
   int ns;
   int r[8];
 };
-// radix plan: 8s first, then 4, 2, 3s (product = L)
+// radix plan (product = L): radix 8 while the remainder does not end in a
+// single factor 2 (128 = 8*4*4, not 8*8*2), then 4s, at most one 2, then 3s
+__host__ __device__ constexpr int twos(int n) {
+  int k = 0;
+  while (n > 0 && n % 2 == 0) { n /= 2; ++k; }
+  return k;
+}
 __host__ __device__ constexpr RPlan rplan(int L) {
   RPlan p{0, {1, 1, 1, 1, 1, 1, 1, 1}};
   int n = L;
-  while (n % 8 == 0 && n > 8) { p.r[p.ns++] = 8; n /= 8; }
-  if (n % 8 == 0) { p.r[p.ns++] = 8; n /= 8; }
-  if (n % 4 == 0) { p.r[p.ns++] = 4; n /= 4; }
+  while (n % 8 == 0 && twos(n / 8) != 1) { p.r[p.ns++] = 8; n /= 8; }
+  while (n % 4 == 0) { p.r[p.ns++] = 4; n /= 4; }
   if (n % 2 == 0) { p.r[p.ns++] = 2; n /= 2; }
   while (n % 3 == 0) { p.r[p.ns++] = 3; n /= 3; }
   return p;
@@ -74,7 +79,7 @@ __device__ __forceinline__ void dif_stage_s(C* buf, const C* __restrict__ tw) {
   constexpr int R = rplan(L).r[S];
   constexpr int SPAN = span_of(L, S);
   constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
-#pragma unroll 2
+#pragma unroll 1
   for (int t = threadIdx.x; t < NBF; t += NT) {
     const int line = t % NL, u = t / NL, j = u % M, b = u / M;
     C* base = buf + line * LS + (b * SPAN + j) * ES;
@@ -95,7 +100,7 @@ __device__ __forceinline__ void dit_stage_s(C* buf, const C* __restrict__ tw) {
   constexpr int R = rplan(L).r[S];
   constexpr int SPAN = span_of(L, S);
   constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
-#pragma unroll 2
+#pragma unroll 1
   for (int t = threadIdx.x; t < NBF; t += NT) {
     const int line = t % NL, u = t / NL, j = u % M, b = u / M;
     C* base = buf + line * LS + (b * SPAN + j) * ES;
@@ -131,6 +136,43 @@ __device__ __forceinline__ void dit(C* buf, const C* tw) {
   }
 }
 
+// ------------------------------------------------------- asynchronous copies
+// cp.async (global -> shared without staging through registers): every thread
+// issues all of its copies before any wait, so a tile's loads are in flight together.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// copy one complex element (8 B for float2, 16 B for double2)
+template <typename C>
+__device__ __forceinline__ void cp_async_c(C* smem, const C* gmem) {
+  if constexpr (sizeof(C) == 16) cp_async16(smem, gmem);
+  else cp_async8(smem, gmem);
+}
+// copy n complex elements (n even, both ends 16-byte aligned) with 16-byte copies
+template <typename C, int NT>
+__device__ __forceinline__ void cp_async_span(C* smem, const C* gmem, int n) {
+  constexpr int PER = 16 / sizeof(C);
+  for (int i = threadIdx.x; i < n / PER; i += NT) cp_async16(smem + i * PER, gmem + i * PER);
+}
+// 16-byte vector store of n complex (n even, 16-byte aligned)
+template <typename C, int NT>
+__device__ __forceinline__ void store_span(C* gmem, const C* smem, int n) {
+  constexpr int PER = 16 / sizeof(C);
+  for (int i = threadIdx.x; i < n / PER; i += NT) *(float4*)(gmem + i * PER) = *(const float4*)(smem + i * PER);
+}
+
 // ----------------------------------------------------------- plane (x + y)
 // Shared-memory image of one z-plane: NY rows of PITCH = N/2+1 complex.
 template <typename R, int N, int NT>
@@ -158,6 +200,7 @@ struct Plane {
     dif<C, LX, NY, PITCH, 1, NT>(buf, twx);
     // split in place, in digit-reversed column order (Nyquist into column LX)
     constexpr int NP = LX / 2 + 1;
+#pragma unroll 1
     for (int i = threadIdx.x; i < NY * NP; i += NT) {
       const int row = i % NY, k = i / NY;
       C* rb = buf + row * PITCH;
@@ -192,6 +235,7 @@ struct Plane {
     const C* post = tws + (LX + NY) * K;
     dit<C, NY, NXH, 1, PITCH, NT>(buf, twy);
     constexpr int NP = LX / 2 + 1;
+#pragma unroll 1
     for (int i = threadIdx.x; i < NY * NP; i += NT) {
       const int row = i % NY, k = i / NY;
       C* rb = buf + row * PITCH;
@@ -214,12 +258,20 @@ struct Plane {
     dit<C, LX, NY, PITCH, 1, NT>(buf, twx);
   }
 
-  // M-form plane <-> shared memory (rows of NXH complex, contiguous in both)
+  // M-form plane <-> shared memory (rows of NXH complex, contiguous in both).
+  // load_m only issues the copies; the caller waits (cp_async_wait_all + sync).
   static __device__ __forceinline__ void load_m(C* buf, const C* __restrict__ src) {
-    for (int i = threadIdx.x; i < ELEMS; i += NT) buf[i] = src[i];
+    cp_async_span<C, NT>(buf, src, ELEMS);
   }
   static __device__ __forceinline__ void store_m(const C* buf, C* __restrict__ dst) {
-    for (int i = threadIdx.x; i < ELEMS; i += NT) dst[i] = buf[i];
+    store_span<C, NT>(dst, buf, ELEMS);
+  }
+  // real plane (NY rows of N reals) into rows of (x[2n], x[2n+1]); issue only
+  static __device__ __forceinline__ void load_real(C* buf, const R* __restrict__ src) {
+    for (int i = threadIdx.x; i < NY * LX; i += NT) {
+      const int y = i / LX, n = i - y * LX;
+      cp_async_c(buf + y * PITCH + n, (const C*)(src + (int64_t)y * N) + n);
+    }
   }
 };
 

@@ -23,10 +23,34 @@ __device__ __forceinline__ void kvec_n(int kx, int ky, int kz, double a[3], doub
 
 template <typename R> constexpr int col_tile() { return sizeof(R) == 4 ? 16 : 8; }
 
+// Column tile of nf fields: smem [z][slot][TM] with LN complex per z row, global
+// M-form (or state) field f at G + f*NK, row z at + z*PL, columns m0 .. m0+TM.
+// tile_load only issues cp.async copies; the caller waits.
+template <typename C, int N, int TM>
+__device__ __forceinline__ void tile_load(C* buf, int LN, int slot0, const C* G, int64_t NK, int64_t PL, int64_t m0,
+                                          int nf) {
+  constexpr int PER = 16 / sizeof(C);
+  const int per_row = nf * TM / PER;
+  for (int i = threadIdx.x; i < N * per_row; i += NT) {
+    const int zz = i / per_row, r = (i - zz * per_row) * PER, f = r / TM, c = r - f * TM;
+    fz::cp_async16(buf + zz * LN + (slot0 + f) * TM + c, G + f * NK + zz * PL + m0 + c);
+  }
+}
+template <typename C, int N, int TM>
+__device__ __forceinline__ void tile_store(const C* buf, int LN, int slot0, C* G, int64_t NK, int64_t PL, int64_t m0,
+                                           int nf) {
+  constexpr int PER = 16 / sizeof(C);
+  const int per_row = nf * TM / PER;
+  for (int i = threadIdx.x; i < N * per_row; i += NT) {
+    const int zz = i / per_row, r = (i - zz * per_row) * PER, f = r / TM, c = r - f * TM;
+    *(float4*)(G + f * NK + zz * PL + m0 + c) = *(const float4*)(buf + zz * LN + (slot0 + f) * TM + c);
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ PF
-// raw = 0: fields theta_v (f < V); block f == V only accumulates the bulk energy.
+// raw = 0: fields theta_v (f < V).
 // raw = 1: fields eta_v (f < V) and dc (f == V), for the spectral state.
 template <typename R, int N>
 __global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V, int raw) {
@@ -37,44 +61,22 @@ __global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V, int raw)
   C* tws = buf + P::ELEMS;
   const int z = blockIdx.x, f = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  P::load_tw(tws, a.twx, a.twy, a.post);
   const LanFusedConst& F = *a.F;
   const R* ez = a.eta + z * PL;
   const R* cz = a.c + z * PL;
-  double fch = 0;
-  for (int i = threadIdx.x; i < N * P::LX; i += NT) {
-    const int y = i / P::LX, n = i - y * P::LX;
-    const int64_t off = (int64_t)y * N;
-    C v;
-    if (f < V) {
-      const C e = ((const C*)(ez + f * N3 + off))[n];
-      v = raw ? e : mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
-    } else if (raw) {
-      v = ((const C*)(cz + off))[n];
-    } else {
-      v = ((const C*)(cz + off))[n];
-      if (a.energy) {
-        double s2[2] = {0, 0}, s4[2] = {0, 0}, s6[2] = {0, 0};
-        for (int q = 0; q < V; ++q) {
-          const C e = ((const C*)(ez + q * N3 + off))[n];
-          const double e0 = (double)e.x * (double)e.x, e1 = (double)e.y * (double)e.y;
-          s2[0] += e0; s4[0] += e0 * e0; s6[0] += e0 * e0 * e0;
-          s2[1] += e1; s4[1] += e1 * e1; s6[1] += e1 * e1 * e1;
-        }
-        const double cv[2] = {F.cbar + (double)v.x, F.cbar + (double)v.y};
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-          fch += 0.5 * F.lan_a * (cv[h] - F.lan_c1) * (cv[h] - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv[h]) * s2[h] -
-                 0.25 * F.lan_c * s4[h] + F.lan_d / 6.0 * s6[h] + F.cross_w * (s2[h] * s2[h] - s4[h]);
-      }
-    }
-    buf[y * P::PITCH + n] = v;
-  }
-  if (f == V && !raw) {
-    block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + z);
-    return;
-  }
+  P::load_real(buf, f < V ? ez + f * N3 : cz);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_all();
   __syncthreads();
+  if (f < V && !raw) {
+    // theta_v = eta_v^2 in place
+    for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+      const int y = i / P::LX, n = i - y * P::LX;
+      const C e = buf[y * P::PITCH + n];
+      buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
+    }
+    __syncthreads();
+  }
   P::forward(buf, tws);
   P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
 }
@@ -89,12 +91,10 @@ __global__ void __launch_bounds__(NT) k_lf_z0(LanFusedArgs<R> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tw = buf + N * LN;
-  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
-  for (int i = threadIdx.x; i < N * LN; i += NT) {
-    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
-    buf[i] = a.M[f * NK + zz * PL + m0 + c];
-  }
+  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  fz::cp_async_wait_all();
   __syncthreads();
   fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
   const double s = 1.0 / ((double)N * N * N);
@@ -116,15 +116,15 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
-  C* tw = buf + N * LN;
+  C* ks = buf + N * LN;  // dc^ state tile [N][TM]
+  C* tw = ks + N * TM;
   __shared__ LanFusedConst F;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
+  tile_load<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
   for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  for (int i = threadIdx.x; i < N * V * TM; i += NT) {
-    const int zz = i / (V * TM), r = i - zz * (V * TM), f = r / TM, c = r - f * TM;
-    buf[zz * LN + r] = a.M[f * NK + zz * PL + m0 + c];
-  }
+  fz::cp_async_wait_all();
   __syncthreads();
   fz::dif<C, N, V * TM, 1, LN, NT>(buf, tw);
   const double s = 1.0 / ((double)N * N * N);
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
       str += tr[v];
       sti += ti[v];
     }
-    C* kc = a.Kc + p * PL + m;
+    C* kc = ks + p * TM + c;
     const C cs = *kc;
     const double cr = (double)cs.x, ci = (double)cs.y;
     const bool k0 = (kx == 0 && ky == 0 && kz == 0);
@@ -242,72 +242,131 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
     e[V * TM] = cn;
   }
   __syncthreads();
+  tile_store<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
   fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
-  for (int i = threadIdx.x; i < N * LN; i += NT) {
-    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
-    a.M[f * NK + zz * PL + m0 + c] = buf[i];
-  }
+  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
   block_reduce_store(fint, 0, a.partials + LQ_FINT * a.pstride + blockIdx.x);
   block_reduce_store(elen, 0, a.partials + LQ_ELEN * a.pstride + blockIdx.x);
 }
 
 // ------------------------------------------------------------------ PB
+// Pointwise inputs (eta_0..V-1 and dc of this plane) stream through a two-deep
+// cp.async pipeline of PB_CH-row chunks; the first two chunks load during the
+// inverse transform.  Block f < V: g_v -> forward transform.  Block f == V:
+// dc_new -> real, and the bulk free energy of the start-of-step fields.
+constexpr int PB_CH = 8;
+
+template <typename R, int N>
+constexpr size_t pb_smem(int V) {
+  return fz::Plane<R, N, NT>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
+}
+
 template <typename R, int N>
 __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
   using P = fz::Plane<R, N, NT>;
   using C = cplx<R>;
+  constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
-  const int z = blockIdx.x, f = blockIdx.y;
+  R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR]
+  // field index fastest: the V+1 blocks of one plane, which read the same eta and
+  // dc planes, are resident together and share those reads through L2
+  const int f = blockIdx.x, z = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  P::load_tw(tws, a.twx, a.twy, a.post);
+  const int NFI = V + 1;
+  auto issue = [&](int k) {
+    R* dst = stg + (k & 1) * NFI * CHR;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < NFI * (CHR / PER); i += NT) {
+      const int q = i / (CHR / PER), r = (i - q * (CHR / PER)) * PER;
+      const R* src = (q < V ? a.eta + q * N3 : a.c) + z * PL + (int64_t)k * CHR + r;
+      fz::cp_async16(dst + q * CHR + r, src);
+    }
+    fz::cp_async_commit();
+  };
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_m(buf, mp);
+  fz::cp_async_commit();
+  const bool pointwise = (f < V) || a.energy;
+  if (pointwise) {
+    issue(0);
+    issue(1);
+  }
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  if (pointwise) fz::cp_async_wait_group<2>();
+  else fz::cp_async_wait_group<0>();
   __syncthreads();
   P::inverse(buf, tws);
+  const LanFusedConst& F = *a.F;
   if (f == V) {
     R* c2z = a.c2 + z * PL;
+#pragma unroll 1
     for (int i = threadIdx.x; i < N * P::LX; i += NT) {
       const int y = i / P::LX, n = i - y * P::LX;
       ((C*)(c2z + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
     }
+  }
+  double fch = 0;
+  if (pointwise) {
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+      if (k + 1 < NCH) fz::cp_async_wait_group<1>();
+      else fz::cp_async_wait_group<0>();
+      __syncthreads();
+      const R* sb = stg + (k & 1) * NFI * CHR;
+#pragma unroll 1
+      for (int i = threadIdx.x; i < CH * P::LX; i += NT) {
+        const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
+        double e[2][4], s2[2] = {0, 0};
+        for (int q = 0; q < V; ++q) {
+          const C ev = ((const C*)(sb + q * CHR + yl * N))[n];
+          e[0][q] = ev.x;
+          e[1][q] = ev.y;
+          s2[0] += e[0][q] * e[0][q];
+          s2[1] += e[1][q] * e[1][q];
+        }
+        const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
+        const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
+        if (f < V) {
+          const C ph = buf[y * P::PITCH + n];
+          const double phv[2] = {(double)ph.x, (double)ph.y};
+          double out[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const double ev = e[h][f], e2 = ev * ev;
+            double g = F.lan_b * (F.lan_c2 - cv[h]) * ev - F.lan_c * e2 * ev + F.lan_d * e2 * e2 * ev +
+                       4.0 * F.cross_w * ev * (s2[h] - e2);
+            if (a.homog) {
+              double sacc = F.sig0_ebar[f] + phv[h];
+              for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
+              g += -2.0 * ev * sacc;
+            }
+            out[h] = g;
+          }
+          buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
+        } else {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            double s4 = 0, s6 = 0;
+            for (int q = 0; q < V; ++q) {
+              const double e2 = e[h][q] * e[h][q];
+              s4 += e2 * e2;
+              s6 += e2 * e2 * e2;
+            }
+            fch += 0.5 * F.lan_a * (cv[h] - F.lan_c1) * (cv[h] - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv[h]) * s2[h] -
+                   0.25 * F.lan_c * s4 + F.lan_d / 6.0 * s6 + F.cross_w * (s2[h] * s2[h] - s4);
+          }
+        }
+      }
+      __syncthreads();
+      if (k + 2 < NCH) issue(k + 2);
+    }
+  }
+  if (f == V) {
+    if (a.energy) block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + z);
     return;
   }
-  const LanFusedConst& F = *a.F;
-  const R* ez = a.eta + z * PL;
-  const R* cz = a.c + z * PL;
-  for (int i = threadIdx.x; i < N * P::LX; i += NT) {
-    const int y = i / P::LX, n = i - y * P::LX;
-    const int64_t off = (int64_t)y * N;
-    double e[2][4], s2[2] = {0, 0};
-    for (int q = 0; q < V; ++q) {
-      const C ev = ((const C*)(ez + q * N3 + off))[n];
-      e[0][q] = ev.x;
-      e[1][q] = ev.y;
-      s2[0] += (double)ev.x * ev.x;
-      s2[1] += (double)ev.y * ev.y;
-    }
-    const C dcv = ((const C*)(cz + off))[n];
-    const C ph = buf[y * P::PITCH + n];
-    const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
-    const double phv[2] = {(double)ph.x, (double)ph.y};
-    double out[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const double ev = e[h][f], e2 = ev * ev;
-      double g = F.lan_b * (F.lan_c2 - cv[h]) * ev - F.lan_c * e2 * ev + F.lan_d * e2 * e2 * ev +
-                 4.0 * F.cross_w * ev * (s2[h] - e2);
-      if (a.homog) {
-        double sacc = F.sig0_ebar[f] + phv[h];
-        for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
-        g += -2.0 * ev * sacc;
-      }
-      out[h] = g;
-    }
-    buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
-  }
-  __syncthreads();
   P::forward(buf, tws);
   P::store_m(buf, mp);
 }
@@ -320,17 +379,17 @@ __global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
-  C* tw = buf + N * LN;
+  C* ks = buf + N * LN;  // eta^ state tiles [N][V][TM]
+  C* tw = ks + N * LN;
   __shared__ double g[V][9];
   __shared__ double dtl;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
+  tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
   for (int i = threadIdx.x; i < V * 9; i += NT) g[i / 9][i % 9] = a.F->g[i / 9][i % 9];
   if (threadIdx.x == 0) dtl = a.F->dtl;
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  for (int i = threadIdx.x; i < N * LN; i += NT) {
-    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
-    buf[i] = a.M[f * NK + zz * PL + m0 + c];
-  }
+  fz::cp_async_wait_all();
   __syncthreads();
   fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
   const double s = 1.0 / ((double)N * N * N);
@@ -347,8 +406,8 @@ __global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const double* gv = g[v];
-      C* ks = a.Keta + v * NK + p * PL + m;
-      const C st = *ks;
+      C* kst = ks + p * LN + v * TM + c;
+      const C st = *kst;
       const double hr = (double)st.x, hi = (double)st.y;
       if (a.energy) {
         const double kb = gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
@@ -361,16 +420,14 @@ __global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
       const double nr = (hr - dtl * s * (double)e[v * TM].x) * rden;
       const double ni = (hi - dtl * s * (double)e[v * TM].y) * rden;
       const C o = mk((R)nr, (R)ni);
-      *ks = o;
+      *kst = o;
       e[v * TM] = o;
     }
   }
   __syncthreads();
+  tile_store<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
   fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
-  for (int i = threadIdx.x; i < N * LN; i += NT) {
-    const int zz = i / LN, r = i - zz * LN, f = r / TM, c = r - f * TM;
-    a.M[f * NK + zz * PL + m0 + c] = buf[i];
-  }
+  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
   block_reduce_store(fint, 0, a.partials + Q_FINT2 * a.pstride + blockIdx.x);
 }
 
@@ -384,8 +441,9 @@ __global__ void __launch_bounds__(NT) k_lf_pi(LanFusedArgs<R> a, int V) {
   C* tws = buf + P::ELEMS;
   const int z = blockIdx.x, f = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  P::load_tw(tws, a.twx, a.twy, a.post);
   P::load_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_all();
   __syncthreads();
   P::inverse(buf, tws);
   R* ez = a.eta + f * N3 + z * PL;
@@ -453,16 +511,17 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
   const int tiles = N * NXH / TM;
   const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
   const size_t sp = P::smem_bytes();
-  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
-  const size_t s2 = sizeof(C) * ((size_t)N * V * TM + N * Tw<C>::K);
+  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + (size_t)N * TM + N * Tw<C>::K);
+  const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
+  const size_t spb = pb_smem<R, N>(V);
   ensure_smem(k_lf_pf<R, N>, sp);
-  ensure_smem(k_lf_pb<R, N>, sp);
+  ensure_smem(k_lf_pb<R, N>, spb);
   ensure_smem(k_lf_pi<R, N>, sp);
   ensure_smem(k_lf_z1<R, N, V>, s1);
   ensure_smem(k_lf_z2<R, N, V>, s2);
   {
-    Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pf<R, N><<<dim3(N, a.energy ? V + 1 : V), NT, sp, st>>>(a, V, 0);
+    Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
+    k_lf_pf<R, N><<<dim3(N, V), NT, sp, st>>>(a, V, 0);
     MEU_CHECK_LAUNCH();
   }
   {
@@ -472,7 +531,7 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
   }
   {
     Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V + 1) * nk * sizeof(C) + (V + 2.0) * n3 * sizeof(R), st);
-    k_lf_pb<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V);
+    k_lf_pb<R, N><<<dim3(V + 1, N), NT, spb, st>>>(a, V);
     MEU_CHECK_LAUNCH();
   }
   {
