@@ -1,5 +1,6 @@
 // landau_fused.cu -- kernels and dispatch of the fused Landau step (see
 // landau_fused.cuh for the data flow).
+#include <type_traits>
 #include <vector>
 
 #include "landau_fused.cuh"
@@ -7,7 +8,9 @@
 namespace meu {
 
 namespace {
-constexpr int NT = 256;
+constexpr int NT = 256;   // column kernels
+constexpr int NTP = 512;  // plane kernels
+constexpr int FCH_BLOCKS = 592;
 constexpr double TWO_PI = 6.283185307179586476925286766559;
 
 template <int N>
@@ -53,8 +56,8 @@ __device__ __forceinline__ void tile_store(const C* buf, int LN, int slot0, C* G
 // raw = 0: fields theta_v (f < V).
 // raw = 1: fields eta_v (f < V) and dc (f == V), for the spectral state.
 template <typename R, int N>
-__global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V, int raw) {
-  using P = fz::Plane<R, N, NT>;
+__global__ void __launch_bounds__(NTP) k_lf_pf(LanFusedArgs<R> a, int V, int raw) {
+  using P = fz::Plane<R, N, NTP>;
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
@@ -70,7 +73,7 @@ __global__ void __launch_bounds__(NT) k_lf_pf(LanFusedArgs<R> a, int V, int raw)
   __syncthreads();
   if (f < V && !raw) {
     // theta_v = eta_v^2 in place
-    for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
       const int y = i / P::LX, n = i - y * P::LX;
       const C e = buf[y * P::PITCH + n];
       buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
@@ -252,18 +255,17 @@ __global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
 // ------------------------------------------------------------------ PB
 // Pointwise inputs (eta_0..V-1 and dc of this plane) stream through a two-deep
 // cp.async pipeline of PB_CH-row chunks; the first two chunks load during the
-// inverse transform.  Block f < V: g_v -> forward transform.  Block f == V:
-// dc_new -> real, and the bulk free energy of the start-of-step fields.
+// inverse transform.  Block (f, z): g_f of plane z -> forward transform.
 constexpr int PB_CH = 8;
 
 template <typename R, int N>
 constexpr size_t pb_smem(int V) {
-  return fz::Plane<R, N, NT>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
+  return fz::Plane<R, N, NTP>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
 }
 
 template <typename R, int N>
-__global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
-  using P = fz::Plane<R, N, NT>;
+__global__ void __launch_bounds__(NTP) k_lf_pb(LanFusedArgs<R> a, int V) {
+  using P = fz::Plane<R, N, NTP>;
   using C = cplx<R>;
   constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
   auto issue = [&](int k) {
     R* dst = stg + (k & 1) * NFI * CHR;
 #pragma unroll 1
-    for (int i = threadIdx.x; i < NFI * (CHR / PER); i += NT) {
+    for (int i = threadIdx.x; i < NFI * (CHR / PER); i += NTP) {
       const int q = i / (CHR / PER), r = (i - q * (CHR / PER)) * PER;
       const R* src = (q < V ? a.eta + q * N3 : a.c) + z * PL + (int64_t)k * CHR + r;
       fz::cp_async16(dst + q * CHR + r, src);
@@ -288,27 +290,14 @@ __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_m(buf, mp);
   fz::cp_async_commit();
-  const bool pointwise = (f < V) || a.energy;
-  if (pointwise) {
-    issue(0);
-    issue(1);
-  }
+  issue(0);
+  issue(1);
   P::load_tw(tws, a.twx, a.twy, a.post);
-  if (pointwise) fz::cp_async_wait_group<2>();
-  else fz::cp_async_wait_group<0>();
+  fz::cp_async_wait_group<2>();
   __syncthreads();
   P::inverse(buf, tws);
   const LanFusedConst& F = *a.F;
-  if (f == V) {
-    R* c2z = a.c2 + z * PL;
-#pragma unroll 1
-    for (int i = threadIdx.x; i < N * P::LX; i += NT) {
-      const int y = i / P::LX, n = i - y * P::LX;
-      ((C*)(c2z + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
-    }
-  }
-  double fch = 0;
-  if (pointwise) {
+  {
 #pragma unroll 1
     for (int k = 0; k < NCH; ++k) {
       if (k + 1 < NCH) fz::cp_async_wait_group<1>();
@@ -316,7 +305,7 @@ __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
       __syncthreads();
       const R* sb = stg + (k & 1) * NFI * CHR;
 #pragma unroll 1
-      for (int i = threadIdx.x; i < CH * P::LX; i += NT) {
+      for (int i = threadIdx.x; i < CH * P::LX; i += NTP) {
         const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
         double e[2][4], s2[2] = {0, 0};
         for (int q = 0; q < V; ++q) {
@@ -328,7 +317,7 @@ __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
         }
         const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
         const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
-        if (f < V) {
+        {
           const C ph = buf[y * P::PITCH + n];
           const double phv[2] = {(double)ph.x, (double)ph.y};
           double out[2];
@@ -345,27 +334,11 @@ __global__ void __launch_bounds__(NT) k_lf_pb(LanFusedArgs<R> a, int V) {
             out[h] = g;
           }
           buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
-        } else {
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            double s4 = 0, s6 = 0;
-            for (int q = 0; q < V; ++q) {
-              const double e2 = e[h][q] * e[h][q];
-              s4 += e2 * e2;
-              s6 += e2 * e2 * e2;
-            }
-            fch += 0.5 * F.lan_a * (cv[h] - F.lan_c1) * (cv[h] - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv[h]) * s2[h] -
-                   0.25 * F.lan_c * s4 + F.lan_d / 6.0 * s6 + F.cross_w * (s2[h] * s2[h] - s4);
-          }
         }
       }
       __syncthreads();
       if (k + 2 < NCH) issue(k + 2);
     }
-  }
-  if (f == V) {
-    if (a.energy) block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + z);
-    return;
   }
   P::forward(buf, tws);
   P::store_m(buf, mp);
@@ -432,9 +405,11 @@ __global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
 }
 
 // ------------------------------------------------------------------ PI
+// Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
+// -> real (into c2), concentration statistics.
 template <typename R, int N>
-__global__ void __launch_bounds__(NT) k_lf_pi(LanFusedArgs<R> a, int V) {
-  using P = fz::Plane<R, N, NT>;
+__global__ void __launch_bounds__(NTP) k_lf_pi(LanFusedArgs<R> a, int V) {
+  using P = fz::Plane<R, N, NTP>;
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
@@ -446,30 +421,71 @@ __global__ void __launch_bounds__(NT) k_lf_pi(LanFusedArgs<R> a, int V) {
   fz::cp_async_wait_all();
   __syncthreads();
   P::inverse(buf, tws);
-  R* ez = a.eta + f * N3 + z * PL;
+  R* dst = (f < V) ? a.eta + f * N3 + z * PL : a.c2 + z * PL;
   double emax = 0.0, s2 = 0.0, cmin = 1.0, cmax = 0.0, csum = 0.0;
   const double cbar = a.F->cbar;
-  const R* c2z = a.c2 + z * PL;
-  for (int i = threadIdx.x; i < N * P::LX; i += NT) {
+#pragma unroll 1
+  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
     const int y = i / P::LX, n = i - y * P::LX;
     const C v = buf[y * P::PITCH + n];
-    ((C*)(ez + (int64_t)y * N))[n] = v;
-    emax = fmax(emax, fmax((double)v.x, (double)v.y));
-    s2 += (double)v.x * v.x + (double)v.y * v.y;
-    if (f == 0) {
-      const C cv = ((const C*)(c2z + (int64_t)y * N))[n];
-      const double c0 = cbar + (double)cv.x, c1 = cbar + (double)cv.y;
+    ((C*)(dst + (int64_t)y * N))[n] = v;
+    if (f < V) {
+      emax = fmax(emax, fmax((double)v.x, (double)v.y));
+      s2 += (double)v.x * v.x + (double)v.y * v.y;
+    } else {
+      const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
       cmin = fmin(cmin, fmin(c0, c1));
       cmax = fmax(cmax, fmax(c0, c1));
       csum += c0 + c1;
     }
   }
-  const int blk = z * V + f;
+  const int blk = z * (V + 1) + f;
   block_reduce_store(emax, 1, a.partials + LQ_PHIMAX * a.pstride + blk);
   block_reduce_store(s2, 0, a.partials + LQ_SOLID * a.pstride + blk);
   block_reduce_store(cmin, 2, a.partials + LQ_CMIN * a.pstride + blk);
   block_reduce_store(cmax, 1, a.partials + LQ_CMAX * a.pstride + blk);
   block_reduce_store(csum, 0, a.partials + LQ_CSUM * a.pstride + blk);
+}
+
+// ------------------------------------------------------------------ FCH
+// bulk free energy of the start-of-step fields (all eta and dc), streamed with
+// 16-byte loads over the whole grid
+template <typename R>
+__global__ void __launch_bounds__(256) k_lf_fch(LanFusedArgs<R> a, int V, int64_t n3) {
+  using V4 = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
+  constexpr int PER = 16 / sizeof(R);
+  const LanFusedConst& F = *a.F;
+  double fch = 0;
+  const int64_t nv = n3 / PER;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+    R e[4][PER], d[PER];
+    {
+      const V4 t = ((const V4*)a.c)[i];
+      const R* tp = (const R*)&t;
+#pragma unroll
+      for (int h = 0; h < PER; ++h) d[h] = tp[h];
+    }
+    for (int q = 0; q < V; ++q) {
+      const V4 t = ((const V4*)(a.eta + q * n3))[i];
+      const R* tp = (const R*)&t;
+#pragma unroll
+      for (int h = 0; h < PER; ++h) e[q][h] = tp[h];
+    }
+#pragma unroll
+    for (int h = 0; h < PER; ++h) {
+      double s2 = 0, s4 = 0, s6 = 0;
+      for (int q = 0; q < V; ++q) {
+        const double e2 = (double)e[q][h] * (double)e[q][h];
+        s2 += e2;
+        s4 += e2 * e2;
+        s6 += e2 * e2 * e2;
+      }
+      const double cv = F.cbar + (double)d[h];
+      fch += 0.5 * F.lan_a * (cv - F.lan_c1) * (cv - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv) * s2 - 0.25 * F.lan_c * s4 +
+             F.lan_d / 6.0 * s6 + F.cross_w * (s2 * s2 - s4);
+    }
+  }
+  block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + blockIdx.x);
 }
 
 // ------------------------------------------------------------------ dispatch
@@ -504,7 +520,7 @@ void ensure_smem(K fn, size_t bytes) {
 
 template <typename R, int N, int V>
 void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
-  using P = fz::Plane<R, N, NT>;
+  using P = fz::Plane<R, N, NTP>;
   using C = cplx<R>;
   constexpr int TM = col_tile<R>();
   constexpr int NXH = N / 2 + 1;
@@ -521,7 +537,12 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
   ensure_smem(k_lf_z2<R, N, V>, s2);
   {
     Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
-    k_lf_pf<R, N><<<dim3(N, V), NT, sp, st>>>(a, V, 0);
+    k_lf_pf<R, N><<<dim3(N, V), NTP, sp, st>>>(a, V, 0);
+    MEU_CHECK_LAUNCH();
+  }
+  if (a.energy) {
+    Scope s(hook, "lf_bulk_energy", (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_fch<R><<<FCH_BLOCKS, 256, 0, st>>>(a, V, (int64_t)N * N * N);
     MEU_CHECK_LAUNCH();
   }
   {
@@ -530,8 +551,8 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
     MEU_CHECK_LAUNCH();
   }
   {
-    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V + 1) * nk * sizeof(C) + (V + 2.0) * n3 * sizeof(R), st);
-    k_lf_pb<R, N><<<dim3(V + 1, N), NT, spb, st>>>(a, V);
+    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pb<R, N><<<dim3(V, N), NTP, spb, st>>>(a, V);
     MEU_CHECK_LAUNCH();
   }
   {
@@ -540,21 +561,21 @@ void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* 
     MEU_CHECK_LAUNCH();
   }
   {
-    Scope s(hook, "lf_plane_inv_stats", (double)V * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pi<R, N><<<dim3(N, V), NT, sp, st>>>(a, V);
+    Scope s(hook, "lf_plane_inv_stats", (V + 1.0) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pi<R, N><<<dim3(N, V + 1), NTP, sp, st>>>(a, V);
     MEU_CHECK_LAUNCH();
   }
   for (int q = 0; q < Q_TOTAL; ++q) nb[q] = 0;
-  nb[Q_FCH] = a.energy ? N : 0;
+  nb[Q_FCH] = a.energy ? FCH_BLOCKS : 0;
   nb[Q_FINT] = tiles;
   nb[Q_ELEN] = tiles;
   nb[Q_FINT2] = tiles;
-  nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * V;
+  nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * (V + 1);
 }
 
 template <typename R, int N, int V>
 void run_init(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
-  using P = fz::Plane<R, N, NT>;
+  using P = fz::Plane<R, N, NTP>;
   using C = cplx<R>;
   constexpr int TM = col_tile<R>();
   constexpr int NXH = N / 2 + 1;
@@ -566,7 +587,7 @@ void run_init(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
   const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
   {
     Scope s(hook, "lf_plane_fwd_state", (V + 1.0) * (nk * sizeof(C) + n3 * sizeof(R)), st);
-    k_lf_pf<R, N><<<dim3(N, V + 1), NT, sp, st>>>(a, V, 1);
+    k_lf_pf<R, N><<<dim3(N, V + 1), NTP, sp, st>>>(a, V, 1);
     MEU_CHECK_LAUNCH();
   }
   {
