@@ -116,22 +116,31 @@ def oracle_throughput(params, c, e, steps: int, threads: int):
 
 
 def cpu_sample(cfg: int, n_override: int, budget_s: float, min_steps: int, threads: int):
-    """Oracle time steps on the deck's grid (or a smaller grid of the same deck
-    when one step at full size does not fit the budget)."""
+    """Oracle time steps on the deck's grid, or on a smaller grid of the same deck
+    when min_steps steps at full size do not fit the budget.  The size is chosen
+    from one calibration step at 32^3 scaled by N^3 log N."""
+    import math
     from meumapps_ss_b200 import configs as CF
     from meumapps_ss_b200 import params as P
     from meumapps_ss_b200 import _lib
-    w0 = CF.landau_config(cfg, n=n_override or None, precision=P.PREC_F64)
-    sizes = [w0.params.nx] + [s for s in (96, 64, 48, 32, 16) if s < w0.params.nx]
-    for n in sizes:
+
+    def deck(n):
         w = CF.landau_config(cfg, n=n, precision=P.PREC_F64)
         p = w.params
         c, e = _lib.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed, w.c0, w.c_amp, w.eta_amp)
-        _, t1 = oracle_throughput(p, c, e, 1, threads)
+        return w, p, c, e
+
+    w0, p0, c0, e0 = deck(32)
+    _, t32 = oracle_throughput(p0, c0, e0, 2, threads)
+    t32 /= 2.0
+    nmax = n_override or CF.landau_config(cfg, precision=P.PREC_F64).params.nx
+    sizes = [nmax] + [s for s in (256, 128, 96, 64, 48, 32) if s < nmax]
+    for n in sizes:
+        t1 = t32 * (n / 32.0) ** 3 * math.log(n) / math.log(32)
         if t1 * min_steps <= budget_s or n == sizes[-1]:
+            w, p, c, e = deck(n)
             steps = max(min_steps, int(budget_s / max(t1, 1e-6)))
-            steps = max(1, min(steps, 100000))
-            return w, p, c, e, steps, t1
+            return w, p, c, e, max(1, min(steps, 100000)), t1
     raise RuntimeError("unreachable")
 
 
@@ -319,7 +328,7 @@ def run_ours(args):
     pc = C.cast(hc.data_ptr(), dp)
     pp = C.cast(hp.data_ptr(), dp)
     rows = (P.MeuDiag * 1)()
-    ke = min(K, 100)
+    ke = min(K, 100) if n3 * (E + V) * 8 <= (1 << 28) else min(K, 3)
     for _ in range(2):
         L.meu_set_fields(sim.h, pc, pp, None)
         L.meu_run(sim.h, 1, rows)

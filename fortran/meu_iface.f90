@@ -20,7 +20,7 @@ module meu_iface
     integer(c_int64_t) :: step, elastep0, noise_step
     integer(c_int32_t) :: nx, ny, nz, model, precision, nvar, numel, numph
     integer(c_int32_t) :: nvar_ph(MEU_MAX_PH)
-    integer(c_int32_t) :: elastic, eig_coupling, el_min_iter, el_max_iter, clip_phi, diag_energy, reserved0
+    integer(c_int32_t) :: elastic, eig_coupling, el_min_iter, el_max_iter, clip_phi, diag_energy, flags
     real(c_double) :: dt, b_mob
     real(c_double) :: cmobs(MEU_MAX_EL)
     real(c_double) :: el_tol
@@ -100,7 +100,7 @@ contains
     p%nvar = vartot; p%numel = numel; p%numph = numph
     p%nvar_ph = 0; p%nvar_ph(1:numph) = Nvar
     p%elastic = MEU_ELAST_HETERO; p%eig_coupling = 0
-    p%el_min_iter = 4; p%el_max_iter = 10; p%clip_phi = 1; p%diag_energy = 1; p%reserved0 = 0
+    p%el_min_iter = 4; p%el_max_iter = 10; p%clip_phi = 1; p%diag_energy = 1; p%flags = 0
     p%dt = t_step; p%b_mob = b_mob
     p%cmobs = 0; p%cmobs(1:numel) = Cmobs
     p%el_tol = 1.0d-7

@@ -46,6 +46,9 @@ extern "C" {
 #define MEU_ELAST_HOMOG 1  /* Landau only: homogeneous moduli, Green operator */
 #define MEU_ELAST_HETERO 2 /* eldis fixed-point iteration (KKS always uses it) */
 
+/* flags */
+#define MEU_FLAG_GENERIC 1 /* use the generic kernels even where the fused Landau step applies */
+
 /* Landau eigenstrain coupling theta(eta) */
 #define MEU_EIG_ETA2 0 /* theta = eta^2 */
 #define MEU_EIG_H 1    /* theta = eta^3 (6 eta^2 - 15 eta + 10) */
@@ -93,7 +96,7 @@ typedef struct meu_params {
   int32_t el_max_iter;  /* 10 in the reference (ModElastic.f:462) */
   int32_t clip_phi;     /* 1: clip phi to [0,1] after each step (:1034-1035) */
   int32_t diag_energy;  /* 1: compute the fort.98 energies every step */
-  int32_t reserved0;
+  int32_t flags;        /* MEU_FLAG_* */
   double dt;            /* t_step */
   double b_mob;         /* L */
   double cmobs[MEU_MAX_EL]; /* Cmobs = diff_coeff/del_N**2 (M for Landau) */

@@ -67,6 +67,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_grad_energy(const DevConst* __r
   block_reduce_store(acc, 0, out + blockIdx.x);
 }
 
+// the fluctuation spectrum has no k = 0 mode
+template <typename R>
+__global__ void k_zero_k0(cplx<R>* kc) {
+  if (threadIdx.x == 0) kc[0] = mk((R)0, (R)0);
+}
+
 // AoS (component fastest, double) <-> SoA (R)
 // offs: NULL or per-component offsets subtracted on the way in (added on the way out)
 template <typename R>
@@ -447,7 +453,14 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   ops[Q_PHIMAX] = 1;
   MEU_CUDA(cudaMemcpy(d_ops, ops, sizeof(ops), cudaMemcpyHostToDevice));
   MEU_CUDA(cudaMemcpy(dK, &hK, sizeof(DevConst), cudaMemcpyHostToDevice));
-  fused = lan_fused_supported(p);
+  if (p.model == MEU_MODEL_LANDAU) {
+    // spectral state eta^ and dc^ of the Landau step (layout of the path in use)
+    keta = dalloc<C>((int64_t)V * nk);
+    kc = dalloc<C>(nk);
+    MEU_CUDA(cudaMemset(keta, 0, sizeof(C) * V * nk));
+    MEU_CUDA(cudaMemset(kc, 0, sizeof(C) * nk));
+  }
+  fused = lan_fused_supported(p) && !(p.flags & MEU_FLAG_GENERIC);
   if (fused) {
     LanFusedConst F;
     memset(&F, 0, sizeof(F));
@@ -475,8 +488,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     F.dtl = p.dt * p.b_mob;
     dF = dalloc<LanFusedConst>(1);
     MEU_CUDA(cudaMemcpy(dF, &F, sizeof(F), cudaMemcpyHostToDevice));
-    keta = dalloc<C>((int64_t)V * nk);
-    kc = dalloc<C>(nk);
+
   }
   MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
   MEU_CUDA(cudaMemset(c, 0, sizeof(R) * E * n3));
@@ -556,10 +568,23 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     }
   }
   if (phi_in) up(phi_in, phi, V, 0);
-  if (fused && (cons || phi_in)) {
-    // spectral state of the fused step from the uploaded real fields
-    const LanFusedArgs<R> a = fused_args();
-    if (!lan_fused_init<R>(P.nx, V, a, st, &prof)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+  if (P.model == MEU_MODEL_LANDAU && (cons || phi_in)) {
+    // spectral state of the step from the uploaded real fields
+    if (fused) {
+      const LanFusedArgs<R> a = fused_args();
+      if (!lan_fused_init<R>(P.nx, V, a, st, &prof)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+    } else {
+      PtrList<const R> a{};
+      PtrList<C> b{};
+      a.p[0] = c;
+      b.p[0] = kc;
+      for (int v = 0; v < V; ++v) {
+        a.p[1 + v] = field(phi, v);
+        b.p[1 + v] = keta + (int64_t)v * nk;
+      }
+      fft->forward<R>(a, b, 1 + V, st);
+      KLAUNCH("zero_k0", 16.0, k_zero_k0<R><<<1, 32, 0, st>>>(kc));
+    }
   }
   if (strain) {
     if (ustate) {
@@ -800,33 +825,32 @@ void Engine<R>::landau_step(meu_diag* d) {
     landau_step_fused();
     return;
   }
+  // generic path: eta^ and dc^ are spectral state (keta, kc); the real fields
+  // are re-derived each step for the nonlinear terms
   MEU_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * Q_TOTAL * PSTRIDE, st));
   const bool elast = P.elastic != MEU_ELAST_NONE && step >= P.elastep0;
   const bool homog = elast && P.elastic == MEU_ELAST_HOMOG;
   const bool het = elast && P.elastic == MEU_ELAST_HETERO;
   R* mu = field(wr, 0);
   KLAUNCH("lan_a", (double)(2 * V + 2) * n3 * sizeof(R), k_lan_a<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, c, phi, pphi, mu, partials));
-  // [theta_v, mu, c, eta_v]
   {
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
     in.push_back(mu);
-    in.push_back(c);
-    for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
     fwd_list(in, 0);
   }
-  KLAUNCH("lan_k1", (double)(homog ? 3 * V + 3 : 2 * V + 3) * nk * sizeof(C), k_lan_k1<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 2 * V + 2), V, homog ? 1 : 0, P.diag_energy, partials, d_err));
+  KLAUNCH("lan_k1", (double)(homog ? 3 * V + 4 : 2 * V + 4) * nk * sizeof(C),
+          k_lan_k1<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, V + 1), V, kc, keta, homog ? 1 : 0,
+                                                          P.diag_energy, partials, d_err));
   R* phel = field(wr, 1);  // V fields: strain interaction (homog) or el_grad (hetero)
   {
     std::vector<R*> out;
     if (homog) {
       for (int v = 0; v < V; ++v) out.push_back(field(phel, v));
       out.push_back(c2);
-      // spectra 0..V-1 then V+1: move c^ next to them
-      MEU_CUDA(cudaMemcpyAsync(spec(V), spec(V + 1), sizeof(C) * nk, cudaMemcpyDeviceToDevice, st));
       inv_list(0, out);
     } else {
-      inv_list(V + 1, {c2});
+      inv_list(V, {c2});
     }
   }
   last_iters = 0;
@@ -841,7 +865,7 @@ void Engine<R>::landau_step(meu_diag* d) {
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(pphi, v));
     fwd_list(in, 0);
-    KLAUNCH("tdgl", 2.0 * V * nk * sizeof(C), k_tdgl<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, P.dt * P.b_mob));
+    KLAUNCH("tdgl", 4.0 * V * nk * sizeof(C), k_tdgl_state<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), V, keta, P.dt * P.b_mob));
     std::vector<R*> out;
     for (int v = 0; v < V; ++v) out.push_back(field(phi, v));
     inv_list(0, out);

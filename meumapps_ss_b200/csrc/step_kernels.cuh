@@ -436,6 +436,29 @@ __global__ void __launch_bounds__(256) k_tdgl(const DevConst* __restrict__ Kp, P
   }
 }
 
+// TDGL update of the spectral state: eta^ <- (eta^ - dt L g^) / (1 + dt L k.kappa.k);
+// the new spectrum is also written to sp (the inverse transform consumes it).
+template <typename R>
+__global__ void __launch_bounds__(256) k_tdgl_state(const DevConst* __restrict__ Kp, PtrList<cplx<R>> sp, int V,
+                                                    cplx<R>* __restrict__ keta, double dtl) {
+  const DevConst& K = *Kp;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    kdecode(K, id, kx, ky, kz);
+    double a[3], b[3];
+    kvec(K, kx, ky, kz, a, b);
+    for (int v = 0; v < V; ++v) {
+      const double den = 1.0 + dtl * kkappak(K.p.grad_coeff[v], a, b);
+      double gr, gi, hr, hi;
+      ld2(sp.p[v][id], gr, gi);
+      ld2(keta[(int64_t)v * K.nk + id], hr, hi);
+      const cplx<R> o = mk((R)((hr - dtl * gr) / den), (R)((hi - dtl * gi) / den));
+      keta[(int64_t)v * K.nk + id] = o;
+      sp.p[v][id] = o;
+    }
+  }
+}
+
 // -------------------------------------------------------------- Landau
 // theta_v, mu_c and the bulk free energy
 template <typename R>
@@ -471,11 +494,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_a(const DevConst* __restric
 // Landau k-space kernel: gradient energy (Parseval), homogeneous Green
 // operator phi^_p = sum_q (sig0_p b).Omega.(sig0_q b) theta^_q with
 // Omega = -Q^-1 (the reference's Q, ModElastic.f:119-158), its exact elastic
-// energy, and the Cahn-Hilliard update
-//   c^ <- (c^ - dt M k^2 mu^) / (1 + dt M kappa_c k^4),  c^(0) = conserved mean.
-// sp: [theta_0..V-1, mu, c, eta_0..V-1]
+// energy, and the Cahn-Hilliard update of the spectral state
+//   dc^ <- (dc^ - dt M k^2 mu^) / (1 + dt M kappa_c k^4),  dc^(0) = 0.
+// sp: [theta_0..V-1, mu] on entry; [phi_0..V-1 (homog), dc_new] on exit.
+// kc: dc^ state (read, updated); keta: eta^ state (read for the energy).
 template <typename R>
 __global__ void __launch_bounds__(RED_THREADS) k_lan_k1(const DevConst* __restrict__ Kp, PtrList<cplx<R>> sp, int V,
+                                                        cplx<R>* __restrict__ kc, const cplx<R>* __restrict__ keta,
                                                         int homog, int energy, double* partials, int* err) {
   const DevConst& K = *Kp;
   const meu_params& p = K.p;
@@ -489,14 +514,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_k1(const DevConst* __restri
     kvec(K, kx, ky, kz, a, b);
     const double w = hweight(K, kx);
     double cr, ci, mr, mi;
-    ld2(sp.p[V + 1][id], cr, ci);
+    ld2(kc[id], cr, ci);
     ld2(sp.p[V][id], mr, mi);
     if (energy) {
       const double bb = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
       double f = p.kappa_c * bb * (cr * cr + ci * ci);
       for (int v = 0; v < V; ++v) {
         double er, ei;
-        ld2(sp.p[V + 2 + v][id], er, ei);
+        ld2(keta[(int64_t)v * nk + id], er, ei);
         f += kkappak_b(p.grad_coeff[v], b) * (er * er + ei * ei);
       }
       fint += 0.5 * w * f;
@@ -569,22 +594,23 @@ __global__ void __launch_bounds__(RED_THREADS) k_lan_k1(const DevConst* __restri
         elen += 0.5 * w * q;
       }
     }
-    // Cahn-Hilliard
+    // Cahn-Hilliard on the spectral state of the fluctuation
     const double k2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
-    double nr, ni;
-    if (id == 0) { nr = K.c_shift ? 0.0 : K.c_mean[0]; ni = 0.0; }
-    else {
+    double nr = 0.0, ni = 0.0;
+    if (id != 0) {
       const double den = 1.0 + dm * p.kappa_c * k2 * k2;
       nr = (cr - dm * k2 * mr) / den;
       ni = (ci - dm * k2 * mi) / den;
     }
-    sp.p[V + 1][id] = mk((R)nr, (R)ni);
+    const cplx<R> o = mk((R)nr, (R)ni);
+    kc[id] = o;
+    sp.p[V][id] = o;
   }
   block_reduce_store(fint, 0, partials + Q_FINT * PSTRIDE + blockIdx.x);
   if (homog) block_reduce_store(elen, 0, partials + Q_ELEN * PSTRIDE + blockIdx.x);
 }
 
-// Landau TDGL right-hand side w_v = eta_v - dt L (df/deta_v + el_grad_v)
+// Landau TDGL driving force g_v = df/deta_v + el_grad_v
 // homog: el_grad_v = -theta'_v (sig0_v:e_mean + phi_v - sum_q A_vq theta_q); else el from elener.
 template <typename R>
 __global__ void __launch_bounds__(256) k_lan_b(const DevConst* __restrict__ Kp, const R* __restrict__ c,
@@ -595,7 +621,6 @@ __global__ void __launch_bounds__(256) k_lan_b(const DevConst* __restrict__ Kp, 
   const int64_t n3 = K.n3;
   const int V = p.nvar;
   const int hcp = p.eig_coupling == MEU_EIG_H;
-  const double dtl = p.dt * p.b_mob;
   const double cbar = K.c_shift ? K.c_mean[0] : 0.0;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
     const double cv = cbar + (double)c[id];
@@ -620,7 +645,7 @@ __global__ void __launch_bounds__(256) k_lan_b(const DevConst* __restrict__ Kp, 
           g += (double)el[v * n3 + id];
         }
       }
-      w[v * n3 + id] = (R)(ev - dtl * g);
+      w[v * n3 + id] = (R)g;
     }
   }
 }

@@ -32,6 +32,7 @@ ELAST_HOMOG = 1
 ELAST_HETERO = 2
 EIG_ETA2 = 0
 EIG_H = 1
+FLAG_GENERIC = 1
 
 
 class MeuParams(C.Structure):
@@ -52,7 +53,7 @@ class MeuParams(C.Structure):
         ("el_max_iter", C.c_int32),
         ("clip_phi", C.c_int32),
         ("diag_energy", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("flags", C.c_int32),
         ("dt", C.c_double),
         ("b_mob", C.c_double),
         ("cmobs", C.c_double * MAX_EL),

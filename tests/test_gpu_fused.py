@@ -95,3 +95,46 @@ def test_config1_fp32_error_after_1000_steps():
     rc = np.linalg.norm(c32 - c64) / np.linalg.norm(c64)
     re = np.linalg.norm(e32 - e64) / np.linalg.norm(e64)
     assert rc <= 1e-5 and re <= 1e-5, (rc, re)
+
+
+@pytest.mark.gpu
+def test_generic_path_matches_fused_and_oracle(oracle):
+    """The generic kernels (spectral state in natural order) and the fused
+    kernels compute the same step: both agree with the oracle to 1e-10."""
+    p, c, e = active_landau(n=32, nvar=2, elastic=P.ELAST_HOMOG)
+    q = p.copy()
+    q.flags = P.FLAG_GENERIC
+    o = oracle.OracleSim(p)
+    o.set_fields(c, e)
+    o.run(30)
+    co, eo, _, _ = o.get_fields()
+    for params in (p, q):
+        with Simulation(params) as g:
+            g.set_fields(c, e)
+            g.timing(True)
+            g.run(30)
+            names = set(g.timing_report())
+            cg, eg, _, _ = g.get_fields()
+        assert ("lf_z_green_ch" in names) == (params.flags == 0)
+        assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(eg - eo)) <= TOL
+
+
+@pytest.mark.gpu
+def test_generic_path_fp32_error_after_1000_steps():
+    """Accuracy of the generic FP32 path with spectral state (config-1 deck)."""
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200 import configs as CF
+    w = CF.landau_config(1, precision=P.PREC_F64)
+    c, e = _lib.init_uniform(128, 128, 128, 3, w.seed, w.c0, w.c_amp, w.eta_amp)
+    out = {}
+    for prec in (P.PREC_F64, P.PREC_F32):
+        p = w.params.copy()
+        p.precision = prec
+        p.flags = P.FLAG_GENERIC
+        with Simulation(p) as g:
+            g.set_fields(c, e)
+            g.run(1000, diag=False)
+            out[prec] = g.get_fields()
+    rc = np.linalg.norm(out[P.PREC_F32][0] - out[P.PREC_F64][0]) / np.linalg.norm(out[P.PREC_F64][0])
+    re = np.linalg.norm(out[P.PREC_F32][1] - out[P.PREC_F64][1]) / np.linalg.norm(out[P.PREC_F64][1])
+    assert rc <= 1e-5 and re <= 1e-5, (rc, re)
