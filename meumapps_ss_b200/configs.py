@@ -149,7 +149,7 @@ def landau_config(k: int, n: Optional[int] = None, precision: int = P.PREC_F32) 
     """
     if k == 0:
         n = n or 64
-        p = landau_params(n, 1, [[0.01, 0.01, 0.01]], dt=0.01, precision=P.PREC_F64)
+        p = landau_params(n, 1, [[0.01, 0.01, 0.01]], dt=0.01, precision=precision)
         return Workload("landau-cfg0-64^3-1var-homog", p, 1000, -1, 0.15, 0.01, 0.001)
     if k == 1:
         n = n or 128

@@ -377,6 +377,29 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     }
   }
   for (int i = 0; i < 36; ++i) hK.c0m[i] = p.cela[1][i];
+  // proportional compliances: S_n = alpha_n S_1 for every phase (and a non-zero matrix)
+  {
+    bool prop = p.cela[0][0] > 0;
+    hK.alpha[0] = 1.0;
+    for (int n = 1; n < p.numph && prop; ++n) {
+      const double al = p.sela[n][0] / p.sela[0][0];
+      for (int i = 0; i < 36; ++i) {
+        const double d = p.sela[n][i] - al * p.sela[0][i];
+        if (std::fabs(d) > 1e-12 * (std::fabs(p.sela[n][i]) + std::fabs(al * p.sela[0][i])) + 1e-300) prop = false;
+      }
+      hK.alpha[n] = al;
+    }
+    // C_1 must be the inverse of S_1 for C = C_1 / s to hold
+    if (prop) {
+      for (int i = 0; i < 6 && prop; ++i)
+        for (int j = 0; j < 6; ++j) {
+          double acc = 0;
+          for (int k = 0; k < 6; ++k) acc += p.cela[0][i + k * 6] * p.sela[0][k + j * 6];
+          if (std::fabs(acc - (i == j ? 1.0 : 0.0)) > 1e-10) { prop = false; break; }
+        }
+    }
+    hK.prop_moduli = prop ? 1 : 0;
+  }
   auto vg = [](int i, int j) { return i == j ? i : 9 - i - j; };
   for (int v = 0; v < V; ++v) {
     const int n = hK.var_phase[v];

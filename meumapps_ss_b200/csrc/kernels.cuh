@@ -32,6 +32,10 @@ struct DevConst {
   double ebar_eng[6];                  // e_mean with engineering shear
   double c0m[36];                      // C0 = CEla(:,:,2) (column-major)
   int use_var[MEU_MAX_VAR];            // elener: variant contributes (transsum > 1e-9)
+  // prop_moduli: every phase's compliance is alpha[n] * SEla(:,:,1), so the mixed
+  // stiffness (sum_v P_v S_n(v) + w S_1)^-1 is CEla(:,:,1) / (sum_v alpha P_v + w)
+  int prop_moduli;
+  double alpha[MEU_MAX_PH];
   double c_mean[MEU_MAX_EL];           // conserved mean of each solute (k = 0 mode), FP64
   // 1: the stored concentration is the fluctuation c - c_mean (Landau decks).  The
   // mean is exactly conserved, so it is kept in FP64 and the bulk FP32 field and
@@ -191,6 +195,60 @@ __device__ int invert_small(double* a, int n, int flag) {
   const double rcond = 1.0 / (anorm * inorm);
   if (!(rcond > 1e-16)) return flag;
   return 0;
+}
+
+// 6x6 inverse by Gauss-Jordan without pivoting, fully unrolled so the matrix
+// stays in registers (the compliance mixes inverted per voxel are symmetric
+// positive definite).  Returns false when a pivot is not safely positive; the
+// caller then falls back to invert_small (partial pivoting).
+__device__ __forceinline__ bool invert6_spd(double* a) {
+  double amax = 0;
+#pragma unroll
+  for (int i = 0; i < 36; ++i) amax = fmax(amax, fabs(a[i]));
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double pv = a[k + k * 6];
+    ok = ok && (pv > 1e-13 * amax);
+    const double d = 1.0 / pv;
+    a[k + k * 6] = 1.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) a[k + j * 6] *= d;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      if (i == k) continue;
+      const double f = a[i + k * 6];
+      a[i + k * 6] = 0.0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) a[i + j * 6] -= f * a[k + j * 6];
+    }
+  }
+  return ok;
+}
+
+// Inverse of a per-voxel 6x6 mix with the reference's singularity test
+// (ModFunc.f:44-72): fast unrolled path, pivoting fallback.
+__device__ __forceinline__ int invert6(double* a, int flag) {
+  double b[36];
+#pragma unroll
+  for (int i = 0; i < 36; ++i) b[i] = a[i];
+  if (invert6_spd(b)) {
+    double anorm = 0, inorm = 0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      double sa = 0, si = 0;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) { sa += fabs(a[i + j * 6]); si += fabs(b[i + j * 6]); }
+      anorm = fmax(anorm, sa);
+      inorm = fmax(inorm, si);
+    }
+    if (1.0 / (anorm * inorm) > 1e-16) {
+#pragma unroll
+      for (int i = 0; i < 36; ++i) a[i] = b[i];
+      return 0;
+    }
+  }
+  return invert_small<6>(a, 6, flag);
 }
 
 // 3x3 inverse in closed form (adjugate), column-major; returns 0 or flag.

@@ -211,25 +211,40 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
   const int V = p.nvar;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
     double Cm[36], e0[6] = {0, 0, 0, 0, 0, 0}, psum = 0;
-#pragma unroll
-    for (int i = 0; i < 36; ++i) Cm[i] = 0;
-    for (int n = 2; n <= p.numph; ++n)
-      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
-        const double pv = (double)pphi[v * n3 + id];
-        psum += pv;
-#pragma unroll
-        for (int i = 0; i < 36; ++i) Cm[i] += pv * p.sela[n - 1][i];
-      }
     for (int v = 0; v < V; ++v) {
       const double pv = (double)pphi[v * n3 + id];
 #pragma unroll
       for (int m = 0; m < 6; ++m) e0[m] += pv * K.eps_eng[v][m];
     }
-    if (psum < 1.0) {
+    if (K.prop_moduli) {
+      double sc = 0;
+      for (int n = 2; n <= p.numph; ++n)
+        for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+          const double pv = (double)pphi[v * n3 + id];
+          psum += pv;
+          sc += K.alpha[n - 1] * pv;
+        }
+      if (psum < 1.0) sc += 1.0 - psum;
+      if (!(sc != 0.0)) set_err(err, MEU_ERR_C_SINGULAR);
+      const double r = 1.0 / sc;
 #pragma unroll
-      for (int i = 0; i < 36; ++i) Cm[i] += (1.0 - psum) * p.sela[0][i];
+      for (int i = 0; i < 36; ++i) Cm[i] = p.cela[0][i] * r;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 36; ++i) Cm[i] = 0;
+      for (int n = 2; n <= p.numph; ++n)
+        for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+          const double pv = (double)pphi[v * n3 + id];
+          psum += pv;
+#pragma unroll
+          for (int i = 0; i < 36; ++i) Cm[i] += pv * p.sela[n - 1][i];
+        }
+      if (psum < 1.0) {
+#pragma unroll
+        for (int i = 0; i < 36; ++i) Cm[i] += (1.0 - psum) * p.sela[0][i];
+      }
+      set_err(err, invert6(Cm, MEU_ERR_C_SINGULAR));
     }
-    set_err(err, invert_small<6>(Cm, 6, MEU_ERR_C_SINGULAR));
     double gam[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) gam[m] = (double)strain[(int64_t)m * n3 + id] + K.ebar_eng[m];
@@ -331,14 +346,24 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
       eps[m] = (m < 3) ? (p.e_mean[m] + gm - te[m]) : (2.0 * p.e_mean[m] + gm - 2.0 * te[m]);
     }
     double Cm[36];
+    if (K.prop_moduli) {
+      double sc = 1.0 - psum;
+      for (int n = 2; n <= p.numph; ++n)
+        for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) sc += K.alpha[n - 1] * P[v];
+      if (!(sc != 0.0)) set_err(err, MEU_ERR_C_ELENER_SINGULAR);
+      const double r = 1.0 / sc;
 #pragma unroll
-    for (int i = 0; i < 36; ++i) Cm[i] = (1.0 - psum) * p.sela[0][i];
-    for (int n = 2; n <= p.numph; ++n)
-      for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+      for (int i = 0; i < 36; ++i) Cm[i] = p.cela[0][i] * r;
+    } else {
 #pragma unroll
-        for (int i = 0; i < 36; ++i) Cm[i] += P[v] * p.sela[n - 1][i];
-      }
-    set_err(err, invert_small<6>(Cm, 6, MEU_ERR_C_ELENER_SINGULAR));
+      for (int i = 0; i < 36; ++i) Cm[i] = (1.0 - psum) * p.sela[0][i];
+      for (int n = 2; n <= p.numph; ++n)
+        for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
+#pragma unroll
+          for (int i = 0; i < 36; ++i) Cm[i] += P[v] * p.sela[n - 1][i];
+        }
+      set_err(err, invert6(Cm, MEU_ERR_C_ELENER_SINGULAR));
+    }
     double sig[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
@@ -361,14 +386,18 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
       for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
         if (!K.use_var[v]) continue;
         double elp = 0;
+        if (K.prop_moduli) {
+          elp = K.alpha[n - 1] * elmat;
+        } else {
 #pragma unroll
-        for (int i = 0; i < 6; ++i) {
-          double ep = 0;
+          for (int i = 0; i < 6; ++i) {
+            double ep = 0;
 #pragma unroll
-          for (int j = 0; j < 6; ++j) ep += p.sela[n - 1][i + j * 6] * sig[j];
-          elp += sig[i] * ep;
+            for (int j = 0; j < 6; ++j) ep += p.sela[n - 1][i + j * 6] * sig[j];
+            elp += sig[i] * ep;
+          }
+          elp *= 0.5;
         }
-        elp *= 0.5;
         en += elp * P[v];
         const double* t = p.trans_ppt[v];
         const double g = sig[0] * t[0] + sig[1] * t[1] + sig[2] * t[2] + 2.0 * (sig[3] * t[3] + sig[4] * t[4] + sig[5] * t[5]);

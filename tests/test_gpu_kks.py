@@ -116,3 +116,16 @@ def test_kks_rejects_fp32_and_bad_sizes():
     q.nx = 10
     with pytest.raises(MeuError):
         Simulation(q)
+
+
+@pytest.mark.gpu
+def test_kks_equal_moduli_parity(oracle):
+    # matrix and precipitate share one stiffness: the per-voxel compliance mix
+    # reduces to a scalar multiple of the matrix's (the scalar-mix path)
+    _, p, cons, phi = kks_case(n=16, nvar=3, steps=40, hetero=False)
+    o, g, do, dg = _run_both(oracle, p, cons, phi, 40)
+    co, fo, eo, _ = o.get_fields()
+    cg, fg, eg, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(fg - fo)) <= TOL
+    assert np.max(np.abs(eg - eo)) <= 1e-9 * np.max(np.abs(eo))
+    assert np.array_equal(_cat(do, "el_iters"), _cat(dg, "el_iters"))
