@@ -5,6 +5,9 @@ Workload (default): Landau deck 1 -- 128^3 grid, one conserved c and three
 tetragonal variants eta_1..3, homogeneous cubic elasticity through the Green
 operator, dt = 0.005, FP32 bulk arithmetic (FP64 for Omega(k), the k = 0 mode
 and every reduction).  A "step" is one time step of that grid.
+--config 0 / 2 select the 64^3 single-variant and the 512^3 heterogeneous decks;
+--config 3 the batched ensemble of 96 single-variant runs on 32^3..128^3 grids
+(a "step" advances every member once; cells = the members' grid points).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -359,6 +362,12 @@ def run_ours(args):
     e2e_win = world * n3 * K / (ms_win / 1e3) / 1e6
     sim.close()
 
+    # ---------------- adjoint of deck 4 (gradient call against the forward), rank 0
+    adj = None
+    if rank == 0 and not args.n:
+        adj = measure_adjoint(stream, fd=False)
+        adj.pop("kernels_ms", None)
+
     # ---------------- CPU baseline (rank 0, N = 1): the oracle port on host cores
     cpu = None
     if rank == 0 and world == 1:
@@ -386,7 +395,8 @@ def run_ours(args):
         "fp64_plain": {"value": value64, "unit": UNIT, "steps": K64, "ms_per_step": ms64 / K64,
                        "fp32_speedup": value / value64},
         "err_vs_fp64": {"c_rel_l2": err_c, "eta_rel_l2": err_e, "after_steps": W + K},
-        "adjoint_forward_cost": None,
+        "adjoint_forward_cost": None if adj is None else adj["gradient_over_forward"],
+        "adjoint": adj,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes_per_launch": dr["bytes"] / dr["launches"],
@@ -407,8 +417,387 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------- adjoint (deck 4)
+def measure_adjoint(stream, n: int = 128, steps: int = 200, fd: bool = True):
+    """Gradient of the calibration loss of deck 4 through meu_adjoint: its time
+    against the plain forward of the same steps, the FP32 gradient against the
+    FP64 one, and central differences (h = 1e-4) of the FP64 loss."""
+    import numpy as np
+    import torch
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200.sim import Simulation
+
+    K = CF.ADJOINT_CHECKPOINT_EVERY
+    w = CF.adjoint_config(n, P.PREC_F64, **CF.ADJOINT_TARGET)
+    p = w.params
+    c0, e0 = _lib.init_uniform(p.nx, p.ny, p.nz, 1, w.seed, w.c0, w.c_amp, w.eta_amp)
+    t = Simulation(p)
+    t.set_stream(stream.cuda_stream)
+    t.set_fields(c0, e0)
+    t.run(steps, diag=False)
+    ct, et, _, _ = t.get_fields()
+    t.close()
+
+    def loss_fwd(prec, **kw):
+        s = Simulation(CF.adjoint_config(n, prec, **kw).params)
+        s.set_stream(stream.cuda_stream)
+        s.set_fields(c0, e0)
+        s.run(steps, diag=False)
+        c, e, _, _ = s.get_fields()
+        s.close()
+        return 0.5 / n ** 3 * (np.sum((e - et) ** 2) + np.sum((c - ct) ** 2))
+
+    def grad(prec):
+        s = Simulation(CF.adjoint_config(n, prec, **CF.ADJOINT_START).params)
+        s.set_stream(stream.cuda_stream)
+        s.set_fields(c0, e0)
+        J, g, ge = s.adjoint(steps, K, ct, et)
+        st = CF.ADJOINT_START
+        out = {"kappa": g["beta_eta"] / st["kappa"] + g["kappa_c"], "L": g["L"], "M": g["M"],
+               "eps0": g["alpha"] / st["eps0"]}
+        return J, out, ge, s
+
+    J32, g32, ge32, s32 = grad(P.PREC_F32)
+    J64, g64, ge64, s64 = grad(P.PREC_F64)
+    s64.close()
+    # timing: the gradient call and the plain forward of the same steps, FP32, same handle
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    s32.set_fields(c0, e0)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        s32.set_fields(c0, e0)
+        s32.adjoint(steps, K, ct, et, want_field=True)
+    b.record(stream)
+    stream.synchronize()
+    t_grad = a.elapsed_time(b) / reps
+    s32.set_fields(c0, e0)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        s32.set_fields(c0, e0)
+        s32.run(steps, diag=True)
+    b.record(stream)
+    stream.synchronize()
+    t_fwd = a.elapsed_time(b) / reps
+    s32.timing(True)
+    s32.set_fields(c0, e0)
+    s32.adjoint(steps, K, ct, et)
+    rep = s32.timing_report()
+    s32.timing(False)
+    s32.close()
+    out = {"workload": w.name.replace("-adjoint-", "-adjoint-calibration-"), "steps": steps, "checkpoint_every": K,
+           "loss_fp32": J32, "loss_fp64": J64, "gradient_fp32": g32, "gradient_fp64": g64,
+           "fp32_vs_fp64_rel": {k: abs(g32[k] - g64[k]) / max(abs(g64[k]), 1e-300) for k in g64},
+           "eta0_grad_fp32_vs_fp64_rel_l2": float(np.linalg.norm(ge32 - ge64) / np.linalg.norm(ge64)),
+           "ms_gradient": t_grad, "ms_forward": t_fwd,
+           "gradient_over_forward": t_grad / t_fwd,
+           "reverse_over_forward": (t_grad - t_fwd) / t_fwd,
+           "kernels_ms": {k: v["ms"] for k, v in sorted(rep.items(), key=lambda kv: -kv[1]["ms"])}}
+    if fd:
+        h = 1e-4
+        rel = {}
+        for k in ("kappa", "L", "M", "eps0"):
+            up, dn = dict(CF.ADJOINT_START), dict(CF.ADJOINT_START)
+            up[k] += h
+            dn[k] -= h
+            fdv = (loss_fwd(P.PREC_F64, **up) - loss_fwd(P.PREC_F64, **dn)) / (2 * h)
+            rel[k] = {"fd": fdv, "adjoint_fp64": g64[k], "rel": abs(g64[k] - fdv) / max(abs(fdv), 1e-300)}
+        out["central_fd_h1e-4"] = rel
+    return out
+
+
+def run_adjoint_bench(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    r = measure_adjoint(stream, n=args.n or 128, steps=200)
+    clocks = sampler.stop()
+    if rank != 0:
+        return 0
+    n = args.n or 128
+    cells = n ** 3 * r["steps"]
+    line = {
+        "metric": METRIC, "value": cells / (r["ms_gradient"] / 1e3) / 1e6, "unit": UNIT, "n_gpus": 1,
+        "steps": r["steps"], "warmup": 1, "ms_per_step": r["ms_gradient"] / r["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (ran_2 uniform noise, seed -1)",
+        "config": {"workload": r["workload"], "grid": [n, n, n], "variants": 1,
+                   "value_is": "cell-steps of the gradient call (forward with checkpoints + reverse sweep) per second"},
+        "adjoint_forward_cost": r["gradient_over_forward"], "adjoint": r, "clocks": clocks,
+        "gpu_launches": None, "e2e": None, "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------- ensemble (deck 3)
+ENS_MEMBERS = 96
+
+
+def ensemble_fields(w, rank: int = 0):
+    from meumapps_ss_b200 import _lib
+    p = w.params
+    return _lib.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed - 1000 * rank, w.c0, w.c_amp, w.eta_amp)
+
+
+def ensemble_cpu_sample(budget_s: float, threads: int):
+    """Oracle steps over members of the ensemble deck taken in order (each member's
+    own grid), about budget_s seconds in all; returns (cells*steps, seconds, text)."""
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    ws = CF.ensemble_config(ENS_MEMBERS, precision=P.PREC_F64)
+    cells, secs, used = 0, 0.0, []
+    for w in ws:
+        c, e = ensemble_fields(w)
+        _, dt1 = oracle_throughput(w.params, c, e, 1, threads)
+        steps = max(1, min(50, int((budget_s - secs) / max(dt1, 1e-6) * 0.5)))
+        v, dt = oracle_throughput(w.params, c, e, steps, threads)
+        n3 = w.params.nx ** 3
+        cells += n3 * (steps + 1)
+        secs += dt + dt1
+        used.append(f"{w.params.nx}^3x{steps + 1}")
+        if secs >= budget_s:
+            break
+    return cells, secs, f"FP64 oracle steps of the first {len(used)} ensemble members ({', '.join(used)}), {threads} threads"
+
+
+def run_ensemble(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200.sim import Ensemble
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    K, W = args.steps, max(3, args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ws = CF.ensemble_config(ENS_MEMBERS, precision=P.PREC_F32)
+    cells = sum(w.params.nx ** 3 for w in ws)
+    fields = [ensemble_fields(w, rank) for w in ws]
+    stream = torch.cuda.Stream(device=dev)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    ens = Ensemble([w.params for w in ws], autotune=True)
+    footprint = free0 - torch.cuda.mem_get_info(dev)[0]
+    ens.set_stream(stream.cuda_stream)
+    scheds = {}
+    for i, w in enumerate(ws):
+        ens.set_fields(i, *fields[i])
+        scheds[w.params.nx] = ens.schedule(i)[:3]
+    ens.run(W, diag=True)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ens.launch_count
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        ens.run(K, diag=True)
+        ev1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    launches = ens.launch_count - l0
+    clocks = sampler.stop()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * cells * K / (ms / 1e3) / 1e6
+    if args.profile:
+        ens.close()
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"profile_run": "ensemble", "steps": K, "warmup": W, "ms_per_step": ms / K}), flush=True)
+        return 0
+    out32 = [ens.get_fields(i)[:2] for i in range(len(ws))]
+
+    # FP64 plain ensemble: same members and fields
+    ws64 = CF.ensemble_config(ENS_MEMBERS, precision=P.PREC_F64)
+    e64 = Ensemble([w.params for w in ws64])
+    e64.set_stream(stream.cuda_stream)
+    for i in range(len(ws64)):
+        e64.set_fields(i, *fields[i])
+    e64.run(W, diag=True)
+    K64 = min(K, 500)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    e64.run(K64, diag=True)
+    b.record(stream)
+    stream.synchronize()
+    ms64 = max_over_ranks(a.elapsed_time(b))
+    value64 = world * cells * K64 / (ms64 / 1e3) / 1e6
+    if K > K64:
+        e64.run(K - K64, diag=False)
+    err_c, err_e = 0.0, 0.0
+    for i in range(len(ws)):
+        c64, f64, _ = e64.get_fields(i)
+        c32, f32 = out32[i]
+        err_c = max(err_c, float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64)))
+        err_e = max(err_e, float(np.linalg.norm(f32 - f64) / max(np.linalg.norm(f64), 1e-300)))
+    e64.close()
+
+    # per-kernel timing (all buckets together)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    ens.timing(True)
+    kt = min(K, 50)
+    ens.run(kt, diag=True)
+    rep = ens.timing_report()
+    ens.timing(False)
+    tot = sum(v["ms"] for v in rep.values())
+    dom = max(rep, key=lambda k: rep[k]["ms"])
+    dr = rep[dom]
+    dom_ms = dr["ms"] / dr["launches"]
+    achieved = dr["bytes"] / dr["launches"] / (dom_ms / 1e3) / 1e9
+    step_bytes = sum(v["bytes"] for v in rep.values()) / kt
+    kernels = {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / v["launches"], "share": v["ms"] / tot,
+                   "GB/s": v["bytes"] / v["ms"] / 1e6} for k, v in sorted(rep.items(), key=lambda kv: -kv[1]["ms"])}
+
+    # end to end through the C-ABI: every member's fields in and out each step, pinned host buffers
+    L = _lib.lib()
+    host = []
+    for i, w in enumerate(ws):
+        n3 = w.params.nx ** 3
+        hc = torch.empty(n3, dtype=torch.float64).pin_memory()
+        hp = torch.empty(n3, dtype=torch.float64).pin_memory()
+        hc.copy_(torch.from_numpy(P.to_fortran(out32[i][0])))
+        hp.copy_(torch.from_numpy(P.to_fortran(out32[i][1])))
+        host.append((hc, hp))
+    dp = C.POINTER(C.c_double)
+    ptrs = [(C.cast(hc.data_ptr(), dp), C.cast(hp.data_ptr(), dp)) for hc, hp in host]
+    rows = (P.MeuDiag * len(ws))()
+
+    def e2e_step():
+        for i, (pc, pp) in enumerate(ptrs):
+            if L.meu_ensemble_set_fields(ens.h, i, pc, pp):
+                raise RuntimeError(L.meu_ensemble_last_error(ens.h).decode())
+        if L.meu_ensemble_run(ens.h, 1, rows):
+            raise RuntimeError(L.meu_ensemble_last_error(ens.h).decode())
+        for i, (pc, pp) in enumerate(ptrs):
+            if L.meu_ensemble_get_fields(ens.h, i, pc, pp, None):
+                raise RuntimeError(L.meu_ensemble_last_error(ens.h).decode())
+
+    e2e_step()
+    ke = min(K, 5)
+    barrier()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(ke):
+        e2e_step()
+    b.record(stream)
+    stream.synchronize()
+    ms_e2e = max_over_ranks(a.elapsed_time(b))
+    e2e = world * cells * ke / (ms_e2e / 1e3) / 1e6
+    ens.close()
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        cc, secs, txt = ensemble_cpu_sample(20.0, threads)
+        cpu = {"value": cc / secs / 1e6, "unit": UNIT, "cores": threads, "kind": "port", "sample": txt}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    sizes = {}
+    for w in ws:
+        sizes[w.params.nx] = sizes.get(w.params.nx, 0) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (ran_2 uniform noise per member, seeds -1..-96; member parameters drawn with ran_2 seed -3)",
+        "config": {"workload": f"landau-ensemble-{len(ws)}x1var", "members": len(ws),
+                   "grids": {f"{n}^3": k for n, k in sorted(sizes.items())}, "cells_per_step": cells,
+                   "schedules": {f"{n}^3": list(s) for n, s in sorted(scheds.items())},
+                   "launch": "one batched launch per kernel and size bucket, buckets on parallel streams, "
+                             "8-step CUDA graph replays",
+                   "l2": f"device working set {footprint / 2**20:.0f} MiB > 126 MB L2, no flush",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64_plain": {"value": value64, "unit": UNIT, "steps": K64, "ms_per_step": ms64 / K64,
+                       "fp32_speedup": value / value64},
+        "err_vs_fp64": {"c_rel_l2_max_member": err_c, "eta_rel_l2_max_member": err_e, "after_steps": W + K},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": read_traffic(dom + "@ensemble"),
+                     "algorithmic_bytes_per_launch": dr["bytes"] / dr["launches"], "kernel_ms_per_launch": dom_ms,
+                     "step_algorithmic_bytes": step_bytes, "step_frac": step_bytes / (ms / K / 1e3) / 1e9 / peak},
+        "kernels": kernels,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * cells * 8,
+                "d2h_bytes_per_step": 2 * cells * 8 + C.sizeof(P.MeuDiag) * len(ws), "steps": ke,
+                "form": "per step: meu_ensemble_set_fields of every member + meu_ensemble_run(1) + "
+                        "meu_ensemble_get_fields of every member, pinned host buffers"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_ensemble(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    K, W = args.steps, args.warmup
+    # each "step" of the sample: oracle steps over ensemble members, about 150 s in all
+    cc, secs, txt = ensemble_cpu_sample(150.0, threads)
+    val = cc / secs / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": K,
+        "warmup": W, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (ran_2 uniform noise per member)",
+        "config": {"workload": f"landau-ensemble-{ENS_MEMBERS}x1var", "parallelism": "host threads"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": txt},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.config == 4:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}), flush=True)
+            return 0
+        return run_adjoint_bench(args)
+    if args.config == 3:
+        return run_reference_ensemble(args) if args.impl == "reference" else run_ensemble(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

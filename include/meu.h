@@ -47,7 +47,8 @@ extern "C" {
 #define MEU_ELAST_HETERO 2 /* eldis fixed-point iteration (KKS always uses it) */
 
 /* flags */
-#define MEU_FLAG_GENERIC 1 /* use the generic kernels even where the fused Landau step applies */
+#define MEU_FLAG_GENERIC 1  /* use the generic kernels even where the fused Landau step applies */
+#define MEU_FLAG_AUTOTUNE 2 /* fused Landau step: time the schedule variants in meu_create and keep the fastest */
 
 /* Landau eigenstrain coupling theta(eta) */
 #define MEU_EIG_ETA2 0 /* theta = eta^2 */
@@ -160,6 +161,68 @@ int64_t meu_get_step(const meu_handle* h);
 const char* meu_last_error(const meu_handle* h);
 
 int meu_destroy(meu_handle* h);
+
+/* Schedule of a fused Landau handle: out3 = radix plan variant (0: radix 8
+ * first, 1: radix 4 first), threads of the plane kernels, complex columns per
+ * column-kernel block.  MEU_ERR_UNSUPPORTED for handles on the generic path. */
+int meu_schedule(meu_handle* h, int32_t* out3);
+/* Choose the schedule (same three values) of a fused Landau handle before its
+ * first meu_set_fields; MEU_ERR_UNSUPPORTED if the grid and precision have no
+ * such variant (the variants: radix plan 0 or 1, 512 or 256 plane threads,
+ * column tile 16 or 8 in FP32, 8 or 4 in FP64 where the tiles fit). */
+int meu_set_schedule(meu_handle* h, const int32_t* in3);
+
+/* Adjoint. ---------------------------------------------------------------
+ * Loss and gradient of the Landau step for calibration.  From the handle's
+ * current fields (eta_0, c_0) the call runs nsteps steps (the handle ends at
+ * the final state, step counter advanced) and returns
+ *   loss = 1/(2 Nx Ny Nz) sum_x [ (eta_T - eta*)^2 + (c_T - c*)^2 ]
+ * with its derivatives computed by the hand-written adjoint of the step
+ * (checkpoints of the state every checkpoint_every steps, recomputation of
+ * each segment in the reverse sweep):
+ *   dparams[0] = dJ/dbeta   (grad_coeff of eta scaled by beta, at beta = 1)
+ *   dparams[1] = dJ/dkappa_c
+ *   dparams[2] = dJ/db_mob  (L)
+ *   dparams[3] = dJ/dcmobs[0] (M)
+ *   dparams[4] = dJ/dalpha  (every eigenstrain scaled by alpha, at alpha = 1)
+ *   dphi0      = dJ/deta_0 (layout as phi; may be NULL)
+ * cons_target and phi_target hold c* and eta* (layouts as meu_set_fields).
+ * Fused Landau handles with one order parameter on the default schedule only
+ * (MEU_ERR_UNSUPPORTED otherwise).  The reference has no adjoint. */
+int meu_adjoint(meu_handle* h, int32_t nsteps, int32_t checkpoint_every, const double* cons_target,
+                const double* phi_target, double* loss, double* dparams, double* dphi0);
+
+/* Ensembles. -------------------------------------------------------------
+ * Many independent fused Landau simulations ("members", each a meu_params
+ * deck on a cubic grid N in {32,48,64,96,128}, 1-4 variants, eta^2 coupling,
+ * homogeneous or no elasticity, one shared precision and start step) advanced
+ * together: members of equal (N, nvar, diag_energy) share every kernel launch
+ * of a step, the size buckets run concurrently, and runs of whole-ensemble
+ * steps replay one CUDA graph.  This batching has no counterpart in the
+ * reference, which runs one simulation per MPI job; each member's step is the
+ * single-handle step (same results as meu_run on its own handle). */
+typedef struct meu_ensemble meu_ensemble;
+
+/* flags for meu_ensemble_create */
+#define MEU_ENS_AUTOTUNE 1 /* time the schedule variants of each bucket before any field is set */
+
+int meu_ensemble_create(int32_t n_members, const meu_params* params, int32_t flags, meu_ensemble** out);
+/* fields of one member, layouts as meu_set_fields (no u_state: no heterogeneous elasticity) */
+int meu_ensemble_set_fields(meu_ensemble* e, int32_t member, const double* cons, const double* phi);
+/* nsteps steps of every member; diag: NULL or n_members * nsteps rows, member-major */
+int meu_ensemble_run(meu_ensemble* e, int32_t nsteps, meu_diag* diag);
+int meu_ensemble_get_fields(meu_ensemble* e, int32_t member, double* cons, double* phi, double* el_en);
+int64_t meu_ensemble_get_step(const meu_ensemble* e);
+/* out4 = the member's bucket schedule as meu_schedule, then its bucket index */
+int meu_ensemble_schedule(meu_ensemble* e, int32_t member, int32_t* out4);
+int meu_ensemble_set_stream(meu_ensemble* e, void* cuda_stream);
+int meu_ensemble_timing(meu_ensemble* e, int32_t enable);
+int32_t meu_ensemble_timing_report(meu_ensemble* e, int32_t max, char* names, int64_t* counts, double* total_ms,
+                                   double* bytes);
+int64_t meu_ensemble_launch_count(const meu_ensemble* e);
+/* message of the last failing call (e = NULL: of the last failed meu_ensemble_create) */
+const char* meu_ensemble_last_error(const meu_ensemble* e);
+int meu_ensemble_destroy(meu_ensemble* e);
 
 /* Host-side helpers (no GPU work). ------------------------------------- */
 

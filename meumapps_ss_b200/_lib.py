@@ -71,6 +71,25 @@ def lib():
     L.meu_timing_report.restype = i32
     L.meu_launch_count.argtypes = [vp]
     L.meu_launch_count.restype = i64
+    L.meu_schedule.argtypes = [vp, C.POINTER(i32)]
+    L.meu_set_schedule.argtypes = [vp, C.POINTER(i32)]
+    L.meu_adjoint.argtypes = [vp, i32, i32, dp, dp, dp, dp, dp]
+    L.meu_ensemble_create.argtypes = [i32, C.POINTER(P.MeuParams), i32, C.POINTER(vp)]
+    L.meu_ensemble_set_fields.argtypes = [vp, i32, dp, dp]
+    L.meu_ensemble_run.argtypes = [vp, i32, C.POINTER(P.MeuDiag)]
+    L.meu_ensemble_get_fields.argtypes = [vp, i32, dp, dp, dp]
+    L.meu_ensemble_get_step.argtypes = [vp]
+    L.meu_ensemble_get_step.restype = i64
+    L.meu_ensemble_schedule.argtypes = [vp, i32, C.POINTER(i32)]
+    L.meu_ensemble_set_stream.argtypes = [vp, vp]
+    L.meu_ensemble_timing.argtypes = [vp, i32]
+    L.meu_ensemble_timing_report.argtypes = [vp, i32, C.c_char_p, C.POINTER(i64), dp, dp]
+    L.meu_ensemble_timing_report.restype = i32
+    L.meu_ensemble_launch_count.argtypes = [vp]
+    L.meu_ensemble_launch_count.restype = i64
+    L.meu_ensemble_last_error.argtypes = [vp]
+    L.meu_ensemble_last_error.restype = C.c_char_p
+    L.meu_ensemble_destroy.argtypes = [vp]
     _LIB = L
     return L
 

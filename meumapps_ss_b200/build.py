@@ -43,8 +43,33 @@ def up_to_date() -> bool:
     return os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime()
 
 
+def _includes(path: str, seen=None) -> set:
+    """The file and every local header it includes (#include "..."), recursively."""
+    seen = set() if seen is None else seen
+    path = os.path.abspath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for line in f:
+            t = line.strip()
+            if t.startswith("#include \""):
+                inc = t.split('"')[1]
+                _includes(os.path.join(os.path.dirname(path), inc), seen)
+    return seen
+
+
+def _obj_fresh(src: str, obj: str) -> bool:
+    if not os.path.exists(obj):
+        return False
+    deps = _includes(src) | {os.path.abspath(__file__)}
+    return os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps)
+
+
 def _compile(src: str, extra) -> str:
     obj = os.path.join(BUILD, os.path.basename(src).replace(".cu", ".o"))
+    if not extra and _obj_fresh(src, obj):
+        return obj
     cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -59,8 +84,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+    # the per-size fused-kernel units take longest: start them first
+    srcs = sorted(sources(), key=lambda f: (not os.path.basename(f).startswith("lf_inst"), f))
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, extra), sources()))
+        objs = list(ex.map(lambda s: _compile(s, extra), srcs))
     tmp = LIB + ".tmp"
     cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -5,6 +5,7 @@
   reference ships no example input, so these decks are synthetic: a binary
   alloy (one solute), one matrix and one precipitate phase with 1 or 3
   variants, heterogeneous cubic moduli and a spherical nucleus.
+* ``ensemble_config`` draws the members of the batched ensemble (configuration 3).
 * ``landau_params`` / ``landau_config`` build the Landau decks (one conserved
   concentration c, p non-conserved order parameters eta).  Their free energy
   is not in the reference; it uses the reference's spectral skeleton and
@@ -163,6 +164,45 @@ def landau_config(k: int, n: Optional[int] = None, precision: int = P.PREC_F32) 
                           precision=precision)
         return Workload("landau-cfg2-512^3-4var-hetero", p, 500, -11, 0.2, 0.01, 0.005)
     raise ValueError(k)
+
+
+def adjoint_config(n: int = 128, precision: int = P.PREC_F32, kappa: float = 1.0, L: float = 1.0, M: float = 1.0,
+                   eps0: float = 0.01) -> Workload:
+    """Configuration 4: the configuration-0 deck (one eta and c, homogeneous cubic
+    elasticity, dilatational eps0 eta^2 I, dt 0.01, c = 0.15 +- 0.01,
+    eta +- 0.001, seed -1) on an n^3 grid for 200 steps with gradient
+    parameters kappa (kappa_c = kappa_eta), L, M and eps0.  The calibration
+    target is the FP64 forward at kappa 1.2, L 0.8, M 1.1, eps0 0.012."""
+    p = landau_params(n, 1, [[eps0, eps0, eps0]], dt=0.01, precision=precision, kappa_c=kappa, kappa_eta=kappa,
+                      M=M, L=L)
+    return Workload(f"landau-adjoint-{n}^3-1var", p, 200, -1, 0.15, 0.01, 0.001)
+
+
+ADJOINT_TARGET = dict(kappa=1.2, L=0.8, M=1.1, eps0=0.012)
+ADJOINT_START = dict(kappa=1.0, L=1.0, M=1.0, eps0=0.01)
+ADJOINT_CHECKPOINT_EVERY = 20
+
+
+ENSEMBLE_SIZES = (32, 48, 64, 96, 128)
+
+
+def ensemble_config(count: int = 96, precision: int = P.PREC_F32, sizes: Sequence[int] = ENSEMBLE_SIZES,
+                    draw_seed: int = -3) -> List[Workload]:
+    """Configuration 3: ``count`` independent single-variant runs of the
+    configuration-0 deck.  Member m (seed -(m+1)) draws, with ran_2 seeded by
+    ``draw_seed``, its grid uniformly from ``sizes`` and B ~ U(0.5, 1.5),
+    eps0 ~ U(0.005, 0.02) (dilatational eps0 eta^2 I), c0 ~ U(0.1, 0.3); c noise
+    +-0.01, eta noise +-0.001, dt 0.01, 2000 steps."""
+    r = P.Ran2(draw_seed)
+    out = []
+    for m in range(count):
+        n = sizes[min(int(r() * len(sizes)), len(sizes) - 1)]
+        b = 0.5 + r()
+        e0 = 0.005 + 0.015 * r()
+        c0 = 0.1 + 0.2 * r()
+        p = landau_params(n, 1, [[e0, e0, e0]], dt=0.01, precision=precision, B=b)
+        out.append(Workload(f"landau-ens-{m}-{n}^3", p, 2000, -(m + 1), c0, 0.01, 0.001))
+    return out
 
 
 def uniform_fields(w: Workload) -> Tuple[np.ndarray, np.ndarray]:

@@ -1,0 +1,230 @@
+// adjoint_kernels.cuh -- kernels of the adjoint step (see adjoint.cuh).
+#pragma once
+#include "adjoint.cuh"
+
+namespace meu {
+namespace adj {
+
+using lf::NT;
+constexpr int NTP = 512;
+constexpr int PV = 0;
+
+// g(k) = -(sig0 b)^T Omega (sig0 b) for one variant (same Q as the forward Green operator)
+__device__ __forceinline__ double green_scalar(const LanFusedConst& F, const double av[3], const double b[3]) {
+  const double* sg = F.sig0[0];
+  const double t0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
+  const double t1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
+  const double t2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
+  const double Kv[6] = {av[0] * av[0], av[1] * av[1], av[2] * av[2], b[1] * b[2], b[0] * b[2], b[0] * b[1]};
+  double Qs[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double acc = 0;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
+    Qs[q] = acc;
+  }
+  const double qa = Qs[0], qb = Qs[1], qc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+  const double i00 = qb * qc - qf * qf, i01 = qe * qf - qc * qd, i02 = qd * qf - qb * qe;
+  const double i11 = qa * qc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+  const double det = qa * i00 + qd * i01 + qe * i02;
+  const double quad = t0 * (i00 * t0 + i01 * t1 + i02 * t2) + t1 * (i01 * t0 + i11 * t1 + i12 * t2) +
+                      t2 * (i02 * t0 + i12 * t1 + i22 * t2);
+  return det != 0.0 ? -quad / det : 0.0;
+}
+
+// k.kappa_eta.k as in the forward eta update
+__device__ __forceinline__ double kk_eta(const double* gv, const double av[3], const double b[3]) {
+  return gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] + (gv[3] + gv[1]) * b[0] * b[1] +
+         (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+}
+
+// ------------------------------------------------------------------ EA
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) k_ad_ea(AdjArgs<R> a) {
+  using C = cplx<R>;
+  constexpr int TM = lf::col_tile_default<R>(), NXH = N / 2 + 1;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;  // [N][TM]
+  C* tw = buf + N * TM;
+  __shared__ LanFusedConst F;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  lf::tile_load<C, N, TM>(buf, TM, 0, a.from_seed ? a.lam_seed : a.M, NK, PL, m0, 1);
+  for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  fz::cp_async_wait_all();
+  __syncthreads();
+  if (!a.from_seed) fz::dif<C, N, TM, 1, TM, NT, PV>(buf, tw);
+  const double s = a.from_seed ? 1.0 : 1.0 / ((double)N * N * N);
+  double X = 0, Y = 0, Z = 0;
+  for (int i = threadIdx.x; i < N * TM; i += NT) {
+    const int p = i / TM, c = i - p * TM;
+    const int64_t m = m0 + c, id = p * PL + m;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+    double av[3], b[3];
+    lf::kvec_n<N>(kx, ky, kz, av, b);
+    const double wk = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+    const double lr = (double)buf[i].x * s, li = (double)buf[i].y * s;
+    const double kk = kk_eta(F.g[0], av, b);
+    const double H = 1.0 / (1.0 + F.dtl * kk);
+    const C e1 = a.eta_k1[id];
+    X += wk * kk * H * (lr * (double)e1.x + li * (double)e1.y);
+    if (!k0) {
+      const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+      const double P = 1.0 / (1.0 + F.dm * F.kappa_c * k2 * k2);
+      const C n1 = a.nu[id], c1 = a.c_k1[id], c0 = a.c_k0[id], t0 = a.theta_k0[id];
+      const double nr = (double)n1.x, ni = (double)n1.y;
+      Y += wk * k2 * k2 * P * (nr * (double)c1.x + ni * (double)c1.y);
+      const double mr = F.lan_a * (double)c0.x - 0.5 * F.lan_b * (double)t0.x;
+      const double mi = F.lan_a * (double)c0.y - 0.5 * F.lan_b * (double)t0.y;
+      Z += wk * P * k2 * (nr * mr + ni * mi);
+    }
+    buf[i] = mk((R)(H * lr), (R)(H * li));
+  }
+  __syncthreads();
+  fz::dit<C, N, TM, 1, TM, NT, PV>(buf, tw);
+  lf::tile_store<C, N, TM>(buf, TM, 0, a.M, NK, PL, m0, 1);
+  block_reduce_store(X, 0, a.partials + AQ_X * PSTRIDE + blockIdx.x);
+  block_reduce_store(Y, 0, a.partials + AQ_Y * PSTRIDE + blockIdx.x);
+  block_reduce_store(Z, 0, a.partials + AQ_Z * PSTRIDE + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ B
+template <typename R, int N>
+__global__ void __launch_bounds__(NTP) k_ad_b(AdjArgs<R> a) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x;
+  constexpr int64_t PL = (int64_t)N * N;
+  C* mp = a.M + z * (int64_t)N * P::NXH;
+  P::load_m(buf, mp);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_all();
+  __syncthreads();
+  P::inverse(buf, tws);
+  const LanFusedConst& F = *a.F;
+  const double dtl = F.dtl, cbar = F.cbar, s0 = F.sig0_ebar[0], A11 = F.A[0][0];
+  double wg = 0, ea = 0;
+  const int64_t off = z * PL;
+#pragma unroll 1
+  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const int64_t g = off + (int64_t)y * N + 2 * n;
+    const C wv = buf[y * P::PITCH + n];
+    const C ev = *(const C*)(a.eta + g), cv = *(const C*)(a.c + g), pv = *(const C*)(a.phi + g);
+    const double w2[2] = {(double)wv.x, (double)wv.y}, e2v[2] = {(double)ev.x, (double)ev.y};
+    const double c2v[2] = {cbar + (double)cv.x, cbar + (double)cv.y}, p2v[2] = {(double)pv.x, (double)pv.y};
+    double ao[2], ho[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const double e = e2v[h], e2 = e * e, cc = c2v[h], ph = p2v[h], w = w2[h];
+      double G = F.lan_b * (F.lan_c2 - cc) * e - F.lan_c * e2 * e + F.lan_d * e2 * e2 * e;
+      double dG = F.lan_b * (F.lan_c2 - cc) - 3.0 * F.lan_c * e2 + 5.0 * F.lan_d * e2 * e2;
+      if (a.homog) {
+        G += -2.0 * e * (s0 + ph - A11 * e2);
+        dG += -2.0 * (s0 + ph) + 6.0 * A11 * e2;
+        ea += -dtl * w * (-2.0 * e * (s0 + 2.0 * ph - 2.0 * A11 * e2));
+      }
+      wg += w * G;
+      ao[h] = w * (1.0 - dtl * dG);
+      ho[h] = dtl * e * w;
+    }
+    *(C*)(a.aw + g) = mk((R)ao[0], (R)ao[1]);
+    buf[y * P::PITCH + n] = mk((R)ho[0], (R)ho[1]);
+  }
+  __syncthreads();
+  P::forward(buf, tws);
+  P::store_m(buf, mp);
+  block_reduce_store(wg, 0, a.partials + AQ_WG * PSTRIDE + z);
+  block_reduce_store(ea, 0, a.partials + AQ_EA * PSTRIDE + z);
+}
+
+// ------------------------------------------------------------------ C
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) k_ad_c(AdjArgs<R> a) {
+  using C = cplx<R>;
+  constexpr int TM = lf::col_tile_default<R>(), NXH = N / 2 + 1;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tw = buf + N * TM;
+  __shared__ LanFusedConst F;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  lf::tile_load<C, N, TM>(buf, TM, 0, a.M, NK, PL, m0, 1);
+  for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  fz::cp_async_wait_all();
+  __syncthreads();
+  fz::dif<C, N, TM, 1, TM, NT, PV>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  for (int i = threadIdx.x; i < N * TM; i += NT) {
+    const int p = i / TM, c = i - p * TM;
+    const int64_t m = m0 + c, id = p * PL + m;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+    double av[3], b[3];
+    lf::kvec_n<N>(kx, ky, kz, av, b);
+    const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+    const double hr = (double)buf[i].x * s, hi = (double)buf[i].y * s;
+    const C n1 = a.nu[id];
+    double rr = 0, ri = 0, nr = F.lan_b * hr, ni = F.lan_b * hi;
+    if (!k0) {
+      const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+      const double P = 1.0 / (1.0 + F.dm * F.kappa_c * k2 * k2);
+      const double P1 = P * (1.0 - F.dm * F.lan_a * k2), P2 = P * F.dm * k2 * 0.5 * F.lan_b;
+      const double g = a.homog ? green_scalar(F, av, b) : 0.0;
+      rr = 2.0 * g * hr + P2 * (double)n1.x;
+      ri = 2.0 * g * hi + P2 * (double)n1.y;
+      nr += P1 * (double)n1.x;
+      ni += P1 * (double)n1.y;
+    }
+    a.nu[id] = mk((R)nr, (R)ni);
+    buf[i] = mk((R)rr, (R)ri);
+  }
+  __syncthreads();
+  fz::dit<C, N, TM, 1, TM, NT, PV>(buf, tw);
+  lf::tile_store<C, N, TM>(buf, TM, 0, a.M, NK, PL, m0, 1);
+}
+
+// ------------------------------------------------------------------ D
+template <typename R, int N>
+__global__ void __launch_bounds__(NTP) k_ad_d(AdjArgs<R> a) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x;
+  constexpr int64_t PL = (int64_t)N * N;
+  C* mp = a.M + z * (int64_t)N * P::NXH;
+  P::load_m(buf, mp);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_all();
+  __syncthreads();
+  P::inverse(buf, tws);
+  const int64_t off = z * PL;
+#pragma unroll 1
+  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const int64_t g = off + (int64_t)y * N + 2 * n;
+    const C rv = buf[y * P::PITCH + n];
+    const C av = *(const C*)(a.aw + g), ev = *(const C*)(a.eta + g);
+    const C lam = mk((R)((double)av.x + 2.0 * (double)ev.x * (double)rv.x),
+                     (R)((double)av.y + 2.0 * (double)ev.y * (double)rv.y));
+    if (a.lam_out) *(C*)(a.lam_out + g) = lam;
+    else buf[y * P::PITCH + n] = lam;
+  }
+  if (a.lam_out) return;
+  __syncthreads();
+  P::forward(buf, tws);
+  P::store_m(buf, mp);
+}
+
+}  // namespace adj
+}  // namespace meu

@@ -12,8 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "fft.cuh"
-#include "landau_fused.cuh"
+#include "engine.cuh"
 #include "step_kernels.cuh"
 
 namespace meu {
@@ -137,194 +136,6 @@ __global__ void k_u_spectra(const DevConst* __restrict__ Kp, const cplx<R>* __re
     }
   }
 }
-
-// ==========================================================================
-// Launch counter and per-kernel CUDA-event timing (off unless requested).
-class Profiler : public LaunchHook {
- public:
-  int64_t launches = 0;
-  bool on = false;
-  struct Stat { int64_t n = 0; double ms = 0, bytes = 0; };
-  std::vector<std::string> names;
-  std::vector<Stat> stats;
-  ~Profiler() override {
-    for (auto& q : pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
-    for (auto e : pool) cudaEventDestroy(e);
-  }
-  void begin(const char* n, double b, cudaStream_t st) override {
-    ++launches;
-    if (!on) return;
-    cur_id = id_of(n);
-    cur_bytes = b;
-    cur_a = get();
-    MEU_CUDA(cudaEventRecord(cur_a, st));
-  }
-  void end(cudaStream_t st) override {
-    if (!on) return;
-    cudaEvent_t e = get();
-    MEU_CUDA(cudaEventRecord(e, st));
-    pend.push_back({cur_id, cur_bytes, cur_a, e});
-  }
-  void resolve() {
-    for (auto& q : pend) {
-      MEU_CUDA(cudaEventSynchronize(q.b));
-      float ms = 0;
-      MEU_CUDA(cudaEventElapsedTime(&ms, q.a, q.b));
-      stats[q.id].n += 1;
-      stats[q.id].ms += ms;
-      stats[q.id].bytes += q.bytes;
-      pool.push_back(q.a);
-      pool.push_back(q.b);
-    }
-    pend.clear();
-  }
-  void reset() {
-    resolve();
-    names.clear();
-    stats.clear();
-  }
-
- private:
-  struct Pend { int id; double bytes; cudaEvent_t a, b; };
-  std::vector<Pend> pend;
-  std::vector<cudaEvent_t> pool;
-  int cur_id = 0;
-  double cur_bytes = 0;
-  cudaEvent_t cur_a = nullptr;
-  int id_of(const char* n) {
-    for (size_t i = 0; i < names.size(); ++i)
-      if (names[i] == n) return (int)i;
-    names.push_back(n);
-    stats.push_back(Stat());
-    return (int)names.size() - 1;
-  }
-  cudaEvent_t get() {
-    if (pool.empty()) {
-      cudaEvent_t e;
-      MEU_CUDA(cudaEventCreate(&e));
-      return e;
-    }
-    cudaEvent_t e = pool.back();
-    pool.pop_back();
-    return e;
-  }
-};
-
-#define KLAUNCH(name, bytes, ...)  \
-  do {                             \
-    prof.begin(name, bytes, st);   \
-    __VA_ARGS__;                   \
-    MEU_CHECK_LAUNCH();            \
-    prof.end(st);                  \
-  } while (0)
-
-// ==========================================================================
-struct EngineBase {
-  virtual ~EngineBase() {}
-  virtual void set_fields(const double* cons, const double* phi, const double* ustate) = 0;
-  virtual void add_noise(const double* incr) = 0;
-  virtual void run(int nsteps, meu_diag* diag) = 0;
-  virtual void get_fields(double* cons, double* phi, double* el_en, double* ustate) = 0;
-  virtual void set_stream(cudaStream_t s) = 0;
-  int64_t step = 0;
-  std::string err;
-  Profiler prof;
-};
-
-template <typename R>
-class Engine : public EngineBase {
-  using C = cplx<R>;
-
- public:
-  explicit Engine(const meu_params& p);
-  ~Engine() override;
-  void set_fields(const double* cons, const double* phi, const double* ustate) override;
-  void add_noise(const double* incr) override;
-  void run(int nsteps, meu_diag* diag) override;
-  void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
-  void set_stream(cudaStream_t s) override { st = s ? s : own_st; }
-
- private:
-  meu_params P;
-  DevConst hK;
-  DevConst* dK = nullptr;
-  LanFusedConst* dF = nullptr;  // constants of the fused Landau step (when it applies)
-  bool fused = false;
-  std::unique_ptr<FFT3> fft;
-  cudaStream_t st = nullptr, own_st = nullptr;
-  int V, E;
-  int64_t n3, nk;
-  // device buffers
-  R *c = nullptr, *c2 = nullptr, *phi = nullptr, *noise = nullptr, *pphi = nullptr, *wr = nullptr, *fd = nullptr,
-    *fc = nullptr, *el_en = nullptr, *strain = nullptr, *xs = nullptr;
-  C *sp = nullptr, *uk = nullptr;
-  int NS = 0, NWR = 0;
-  double *partials = nullptr, *results = nullptr, *h_results = nullptr;
-  int* d_ops = nullptr;
-  int* d_err = nullptr;
-  int* h_err = nullptr;
-  double* stage = nullptr;  // AoS staging (double)
-  int64_t stage_elems = 0;
-  std::vector<void*> allocs;
-  // reference quirk state: values written on the next fort.98 line
-  double prev_min = 1.0, prev_max = 0.0, prev_phimax = 0.0, prev_solid = 0.0;
-  bool el_ready = false;  // u^ / strain hold a valid elastic state
-  int last_iters = 0;
-
-  template <typename T> T* dalloc(int64_t n) {
-    void* ptr = nullptr;
-    MEU_CUDA(cudaMalloc(&ptr, (size_t)std::max<int64_t>(n, 1) * sizeof(T)));
-    allocs.push_back(ptr);
-    return (T*)ptr;
-  }
-  R* field(R* base, int f) const { return base + (int64_t)f * n3; }
-  C* spec(int f) const { return sp + (int64_t)f * nk; }
-  unsigned gridk() const { return grid_for(nk, 256); }
-  unsigned gridr() const { return grid_for(n3, 256); }
-
-  void fwd(std::initializer_list<const R*> in, int s0) {
-    PtrList<const R> a{};
-    PtrList<C> b{};
-    int n = 0;
-    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
-    fft->forward<R>(a, b, n, st);
-  }
-  void fwd_list(const std::vector<const R*>& in, int s0) {
-    PtrList<const R> a{};
-    PtrList<C> b{};
-    int n = 0;
-    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
-    fft->forward<R>(a, b, n, st);
-  }
-  void inv_list(int s0, const std::vector<R*>& out) {
-    PtrList<C> a{};
-    PtrList<R> b{};
-    int n = 0;
-    for (R* q : out) { a.p[n] = spec(s0 + n); b.p[n] = q; ++n; }
-    fft->inverse<R>(a, b, n, st);
-  }
-  PtrList<C> specs(int s0, int n) const {
-    PtrList<C> l{};
-    for (int i = 0; i < n; ++i) l.p[i] = spec(s0 + i);
-    return l;
-  }
-  void check_err();
-  void finalize(int q0, int nq, double* out = nullptr, const int* nbs = nullptr);
-  void elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only);
-  void kks_step(meu_diag* d);
-  void landau_step(meu_diag* d);
-  void landau_step_fused();
-  LanFusedArgs<R> fused_args() const;
-  C *keta = nullptr, *kc = nullptr;  // spectral state of the fused Landau step
-  void end_step(meu_diag* d, int clip);
-  void flush_hist(meu_diag* diag);
-  static constexpr int HIST_MAX = 4096;
-  double* hist = nullptr;  // per-step reductions [HIST_MAX][Q_STEP_COUNT]
-  double* cmean_acc = nullptr;
-  int hist_n = 0;
-  std::vector<int64_t> hist_step = std::vector<int64_t>(HIST_MAX);
-  std::vector<int> hist_iters = std::vector<int>(HIST_MAX);
-};
 
 template <typename R>
 Engine<R>::Engine(const meu_params& p) : P(p) {
@@ -511,6 +322,10 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     F.dtl = p.dt * p.b_mob;
     dF = dalloc<LanFusedConst>(1);
     MEU_CUDA(cudaMemcpy(dF, &F, sizeof(F), cudaMemcpyHostToDevice));
+    dA = dalloc<LanFusedArgs<R>>(1);
+    d_row = dalloc<int>(2);
+    d_ticket = d_row + 1;
+    MEU_CUDA(cudaMemset(d_row, 0, 2 * sizeof(int)));
 
   }
   MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
@@ -522,12 +337,51 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   if (uk) MEU_CUDA(cudaMemset(uk, 0, sizeof(C) * 3 * nk));
   stage_elems = std::min<int64_t>(n3 * std::max(std::max(V, E), 1), (int64_t)32 << 20);
   stage = dalloc<double>(stage_elems);
+  if (fused) {
+    MEU_CUDA(cudaMemset(sp, 0, sizeof(C) * (size_t)NS * nk));
+    if (p.flags & MEU_FLAG_AUTOTUNE) {
+      sync_args();
+      sched = lan_autotune<R>(p.nx, V, dA, 1, p.diag_energy != 0, d_ops, st, nullptr);
+      reset_fused_state();
+    }
+  }
+}
+
+template <typename R>
+void Engine<R>::set_schedule(const int32_t* in3) {
+  if (!fused) throw CudaError("the handle runs the generic path (no schedule)", MEU_ERR_UNSUPPORTED);
+  if (fields_set) throw CudaError("set the schedule before the first meu_set_fields", MEU_ERR_BADARG);
+  for (const LanSched& c : lan_sched_candidates(P.nx, sizeof(R) == 8)) {
+    if (c.pv == in3[0] && c.ntp == in3[1] && c.tm == in3[2]) {
+      sched = c;
+      if (gexec) cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+      fused_warm = false;
+      return;
+    }
+  }
+  throw CudaError("no such schedule for this grid and precision", MEU_ERR_UNSUPPORTED);
+}
+
+// zero fields, spectral state and history after the autotuner ran steps on them
+template <typename R>
+void Engine<R>::reset_fused_state() {
+  MEU_CUDA(cudaMemsetAsync(c, 0, sizeof(R) * E * n3, st));
+  MEU_CUDA(cudaMemsetAsync(phi, 0, sizeof(R) * V * n3, st));
+  MEU_CUDA(cudaMemsetAsync(sp, 0, sizeof(C) * (size_t)NS * nk, st));
+  MEU_CUDA(cudaMemsetAsync(keta, 0, sizeof(C) * V * nk, st));
+  MEU_CUDA(cudaMemsetAsync(kc, 0, sizeof(C) * nk, st));
+  MEU_CUDA(cudaMemsetAsync(hist, 0, sizeof(double) * HIST_MAX * Q_STEP_COUNT, st));
+  MEU_CUDA(cudaMemsetAsync(d_row, 0, 2 * sizeof(int), st));
+  MEU_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+  MEU_CUDA(cudaStreamSynchronize(st));
 }
 
 template <typename R>
 Engine<R>::~Engine() {
   if (st) cudaStreamSynchronize(st);
   if (own_st) cudaStreamSynchronize(own_st);
+  if (gexec) cudaGraphExecDestroy(gexec);
   prof.reset();
   for (void* q : allocs) cudaFree(q);
   if (h_results) cudaFreeHost(h_results);
@@ -591,11 +445,13 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     }
   }
   if (phi_in) up(phi_in, phi, V, 0);
+  if (cons || phi_in) fields_set = true;
   if (P.model == MEU_MODEL_LANDAU && (cons || phi_in)) {
     // spectral state of the step from the uploaded real fields
     if (fused) {
-      const LanFusedArgs<R> a = fused_args();
-      if (!lan_fused_init<R>(P.nx, V, a, st, &prof)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+      sync_args();
+      if (!lan_fused_init<R>(P.nx, V, sched, dA, 1, st, &prof))
+        throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
     } else {
       PtrList<const R> a{};
       PtrList<C> b{};
@@ -809,15 +665,14 @@ void Engine<R>::kks_step(meu_diag* d) {
 template <typename R>
 LanFusedArgs<R> Engine<R>::fused_args() const {
   LanFusedArgs<R> a;
+  memset(&a, 0, sizeof(a));
   a.F = dF;
   a.eta = phi;
   a.c = c;
-  a.c2 = c2;
   a.M = sp;
   a.Keta = keta;
   a.Kc = kc;
   a.partials = partials;
-  a.pstride = PSTRIDE;
   a.err = d_err;
   a.homog = (P.elastic != MEU_ELAST_NONE && step >= P.elastep0) ? 1 : 0;
   a.energy = P.diag_energy;
@@ -825,21 +680,91 @@ LanFusedArgs<R> Engine<R>::fused_args() const {
   a.twy = (const C*)fft->py.tw;
   a.twz = (const C*)fft->pz.tw;
   a.post = (const C*)fft->post_tw;
+  a.hist = hist;
+  a.hist_row = d_row;
+  a.ticket = d_ticket;
+  a.hist_rows = HIST_MAX;
+  a.eta_next = phi;
+  a.c_next = c;
+  a.Keta_out = keta;
+  a.Kc_out = kc;
   return a;
 }
 
 template <typename R>
-void Engine<R>::landau_step_fused() {
+void Engine<R>::sync_args() {
   const LanFusedArgs<R> a = fused_args();
-  int nb[Q_TOTAL];
-  if (!lan_fused_step<R>(P.nx, V, a, st, &prof, nb)) throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
-  std::swap(c, c2);
+  if (hA_valid && memcmp(&a, &hA, sizeof(a)) == 0) return;
+  hA = a;
+  hA_valid = true;
+  // pageable source: the call returns once hA has been staged, so hA may change afterwards
+  MEU_CUDA(cudaMemcpyAsync(dA, &hA, sizeof(hA), cudaMemcpyHostToDevice, st));
+}
+
+template <typename R>
+void Engine<R>::fused_step_launches() {
+  if (!lan_fused_step<R>(P.nx, V, sched, dA, 1, P.diag_energy != 0, st, &prof, fnb))
+    throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+  lan_fused_finalize<R>(dA, 1, fnb, d_ops, st, &prof);
+}
+
+template <typename R>
+void Engine<R>::landau_step_fused() { fused_steps(1); }
+
+// n fused steps into history rows hist_n .. hist_n + n - 1 (d_row == hist_n on entry).
+// Runs of GRAPH_STEPS steps with one elastic state (homog flag) replay a CUDA
+// graph when the per-kernel timer is off and the stream can be captured.
+template <typename R>
+void Engine<R>::fused_steps(int n) {
+  int done = 0;
+  while (done < n) {
+    sync_args();
+    const bool homog_now = hA.homog != 0;
+    const bool homog_later = P.elastic != MEU_ELAST_NONE && step + GRAPH_STEPS - 1 >= P.elastep0;
+    const bool graphable =
+        fused_warm && !prof.on && st != nullptr && n - done >= GRAPH_STEPS && homog_now == homog_later;
+    if (graphable) {
+      if (!gexec) {
+        const int64_t l0 = prof.launches;
+        cudaGraph_t g = nullptr;
+        MEU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int i = 0; i < GRAPH_STEPS; ++i) fused_step_launches();
+        } catch (...) {
+          cudaStreamEndCapture(st, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        MEU_CUDA(cudaStreamEndCapture(st, &g));
+        const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+          gexec = nullptr;
+          throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), MEU_ERR_CUDA);
+        }
+        graph_launches = prof.launches - l0;
+        prof.launches = l0;  // captured, not run
+      }
+      MEU_CUDA(cudaGraphLaunch(gexec, st));
+      prof.launches += graph_launches;
+      for (int i = 0; i < GRAPH_STEPS; ++i) {
+        hist_step[hist_n] = step;
+        hist_iters[hist_n] = 0;
+        hist_n += 1;
+        step += 1;
+      }
+      done += GRAPH_STEPS;
+    } else {
+      fused_step_launches();
+      fused_warm = true;  // kernel attributes are set; capture is possible from here
+      hist_step[hist_n] = step;
+      hist_iters[hist_n] = 0;
+      hist_n += 1;
+      step += 1;
+      done += 1;
+    }
+  }
   last_iters = 0;
-  finalize(0, Q_STEP_COUNT, hist + (int64_t)hist_n * Q_STEP_COUNT, nb);
-  hist_step[hist_n] = step;
-  hist_iters[hist_n] = 0;
-  hist_n += 1;
-  step += 1;
 }
 
 template <typename R>
@@ -960,9 +885,14 @@ void Engine<R>::run(int nsteps, meu_diag* diag) {
   hist_n = 0;
   while (done < nsteps) {
     const int chunk = std::min(nsteps - done, HIST_MAX);
-    for (int i = 0; i < chunk; ++i) {
-      if (P.model == MEU_MODEL_KKS) kks_step(nullptr);
-      else landau_step(nullptr);
+    if (fused) {
+      MEU_CUDA(cudaMemsetAsync(d_row, 0, 2 * sizeof(int), st));
+      fused_steps(chunk);
+    } else {
+      for (int i = 0; i < chunk; ++i) {
+        if (P.model == MEU_MODEL_KKS) kks_step(nullptr);
+        else landau_step(nullptr);
+      }
     }
     check_err();
     flush_hist(diag ? diag + done : nullptr);
@@ -1096,6 +1026,25 @@ int32_t meu_timing_report(meu_handle* h, int32_t max, char* names, int64_t* coun
 }
 
 int64_t meu_launch_count(const meu_handle* h) { return h ? h->eng->prof.launches : -1; }
+
+int meu_adjoint(meu_handle* h, int32_t nsteps, int32_t checkpoint_every, const double* cons_target,
+                const double* phi_target, double* loss, double* dparams, double* dphi0) {
+  if (!h) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->adjoint(nsteps, checkpoint_every, cons_target, phi_target, loss, dparams, dphi0));
+  return MEU_OK;
+}
+
+int meu_set_schedule(meu_handle* h, const int32_t* in3) {
+  if (!h || !in3) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->set_schedule(in3));
+  return MEU_OK;
+}
+
+int meu_schedule(meu_handle* h, int32_t* out3) {
+  if (!h || !out3) return MEU_ERR_BADARG;
+  if (!h->eng->schedule(out3)) return fail(h, MEU_ERR_UNSUPPORTED, "the handle runs the generic path (no schedule)");
+  return MEU_OK;
+}
 
 int meu_destroy(meu_handle* h) {
   if (!h) return MEU_ERR_BADARG;

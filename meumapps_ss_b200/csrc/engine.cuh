@@ -1,0 +1,246 @@
+// engine.cuh -- the step engine class behind include/meu.h (implementation in
+// engine.cu) and its launch counter / per-kernel timer.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/meu.h"
+#include "fft.cuh"
+#include "landau_fused.cuh"
+
+namespace meu {
+
+// ==========================================================================
+// Launch counter and per-kernel CUDA-event timing (off unless requested).
+class Profiler : public LaunchHook {
+ public:
+  int64_t launches = 0;
+  bool on = false;
+  struct Stat { int64_t n = 0; double ms = 0, bytes = 0; };
+  std::vector<std::string> names;
+  std::vector<Stat> stats;
+  ~Profiler() override {
+    for (auto& q : pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  void begin(const char* n, double b, cudaStream_t st) override {
+    ++launches;
+    if (!on) return;
+    cur_id = id_of(n);
+    cur_bytes = b;
+    cur_a = get();
+    MEU_CUDA(cudaEventRecord(cur_a, st));
+  }
+  void end(cudaStream_t st) override {
+    if (!on) return;
+    cudaEvent_t e = get();
+    MEU_CUDA(cudaEventRecord(e, st));
+    pend.push_back({cur_id, cur_bytes, cur_a, e});
+  }
+  void resolve() {
+    for (auto& q : pend) {
+      MEU_CUDA(cudaEventSynchronize(q.b));
+      float ms = 0;
+      MEU_CUDA(cudaEventElapsedTime(&ms, q.a, q.b));
+      stats[q.id].n += 1;
+      stats[q.id].ms += ms;
+      stats[q.id].bytes += q.bytes;
+      pool.push_back(q.a);
+      pool.push_back(q.b);
+    }
+    pend.clear();
+  }
+  void reset() {
+    resolve();
+    names.clear();
+    stats.clear();
+  }
+
+ private:
+  struct Pend { int id; double bytes; cudaEvent_t a, b; };
+  std::vector<Pend> pend;
+  std::vector<cudaEvent_t> pool;
+  int cur_id = 0;
+  double cur_bytes = 0;
+  cudaEvent_t cur_a = nullptr;
+  int id_of(const char* n) {
+    for (size_t i = 0; i < names.size(); ++i)
+      if (names[i] == n) return (int)i;
+    names.push_back(n);
+    stats.push_back(Stat());
+    return (int)names.size() - 1;
+  }
+  cudaEvent_t get() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      MEU_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+};
+
+#define KLAUNCH(name, bytes, ...)  \
+  do {                             \
+    prof.begin(name, bytes, st);   \
+    __VA_ARGS__;                   \
+    MEU_CHECK_LAUNCH();            \
+    prof.end(st);                  \
+  } while (0)
+
+// ==========================================================================
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual void set_fields(const double* cons, const double* phi, const double* ustate) = 0;
+  virtual void add_noise(const double* incr) = 0;
+  virtual void run(int nsteps, meu_diag* diag) = 0;
+  virtual void get_fields(double* cons, double* phi, double* el_en, double* ustate) = 0;
+  virtual void set_stream(cudaStream_t s) = 0;
+  virtual bool schedule(int32_t* out3) const = 0;
+  virtual void set_schedule(const int32_t* in3) = 0;
+  // loss and gradient of the last of nsteps steps from the current fields (adjoint.cu)
+  virtual void adjoint(int nsteps, int checkpoint_every, const double* cons_tgt, const double* phi_tgt, double* loss,
+                       double* dparams, double* dphi0) = 0;
+  int64_t step = 0;
+  std::string err;
+  Profiler prof;
+};
+
+template <typename R>
+class EnsembleT;
+template <typename R>
+struct AdjBuffers;
+template <typename R>
+void adj_buffers_free(AdjBuffers<R>* b);
+
+template <typename R>
+class Engine : public EngineBase {
+  using C = cplx<R>;
+  friend class EnsembleT<R>;
+
+ public:
+  explicit Engine(const meu_params& p);
+  ~Engine() override;
+  void set_fields(const double* cons, const double* phi, const double* ustate) override;
+  void add_noise(const double* incr) override;
+  void run(int nsteps, meu_diag* diag) override;
+  void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
+  void set_stream(cudaStream_t s) override { st = s ? s : own_st; }
+  bool schedule(int32_t* out3) const override {
+    if (!fused) return false;
+    out3[0] = sched.pv;
+    out3[1] = sched.ntp;
+    out3[2] = sched.tm ? sched.tm : (sizeof(R) == 4 ? 16 : 8);
+    return true;
+  }
+  void set_schedule(const int32_t* in3) override;
+  void adjoint(int nsteps, int checkpoint_every, const double* cons_tgt, const double* phi_tgt, double* loss,
+               double* dparams, double* dphi0) override;
+
+ private:
+  meu_params P;
+  DevConst hK;
+  DevConst* dK = nullptr;
+  LanFusedConst* dF = nullptr;  // constants of the fused Landau step (when it applies)
+  bool fused = false;
+  std::unique_ptr<FFT3> fft;
+  cudaStream_t st = nullptr, own_st = nullptr;
+  int V, E;
+  int64_t n3, nk;
+  // device buffers
+  R *c = nullptr, *c2 = nullptr, *phi = nullptr, *noise = nullptr, *pphi = nullptr, *wr = nullptr, *fd = nullptr,
+    *fc = nullptr, *el_en = nullptr, *strain = nullptr, *xs = nullptr;
+  C *sp = nullptr, *uk = nullptr;
+  int NS = 0, NWR = 0;
+  double *partials = nullptr, *results = nullptr, *h_results = nullptr;
+  int* d_ops = nullptr;
+  int* d_err = nullptr;
+  int* h_err = nullptr;
+  double* stage = nullptr;  // AoS staging (double)
+  int64_t stage_elems = 0;
+  std::vector<void*> allocs;
+  // reference quirk state: values written on the next fort.98 line
+  double prev_min = 1.0, prev_max = 0.0, prev_phimax = 0.0, prev_solid = 0.0;
+  bool el_ready = false;  // u^ / strain hold a valid elastic state
+  int last_iters = 0;
+
+  template <typename T> T* dalloc(int64_t n) {
+    void* ptr = nullptr;
+    MEU_CUDA(cudaMalloc(&ptr, (size_t)std::max<int64_t>(n, 1) * sizeof(T)));
+    allocs.push_back(ptr);
+    return (T*)ptr;
+  }
+  R* field(R* base, int f) const { return base + (int64_t)f * n3; }
+  C* spec(int f) const { return sp + (int64_t)f * nk; }
+  unsigned gridk() const { return grid_for(nk, 256); }
+  unsigned gridr() const { return grid_for(n3, 256); }
+
+  void fwd(std::initializer_list<const R*> in, int s0) {
+    PtrList<const R> a{};
+    PtrList<C> b{};
+    int n = 0;
+    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
+    fft->forward<R>(a, b, n, st);
+  }
+  void fwd_list(const std::vector<const R*>& in, int s0) {
+    PtrList<const R> a{};
+    PtrList<C> b{};
+    int n = 0;
+    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
+    fft->forward<R>(a, b, n, st);
+  }
+  void inv_list(int s0, const std::vector<R*>& out) {
+    PtrList<C> a{};
+    PtrList<R> b{};
+    int n = 0;
+    for (R* q : out) { a.p[n] = spec(s0 + n); b.p[n] = q; ++n; }
+    fft->inverse<R>(a, b, n, st);
+  }
+  PtrList<C> specs(int s0, int n) const {
+    PtrList<C> l{};
+    for (int i = 0; i < n; ++i) l.p[i] = spec(s0 + i);
+    return l;
+  }
+  void check_err();
+  void finalize(int q0, int nq, double* out = nullptr, const int* nbs = nullptr);
+  void elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only);
+  void kks_step(meu_diag* d);
+  void landau_step(meu_diag* d);
+  void landau_step_fused();
+  LanFusedArgs<R> fused_args() const;
+  void sync_args();           // upload fused_args() into dA when it changed
+  void fused_steps(int n);    // n fused steps (CUDA graphs of GRAPH_STEPS steps where possible)
+  void fused_step_launches(); // launches of one fused step (stream or capture)
+  C *keta = nullptr, *kc = nullptr;  // spectral state of the Landau step
+  // fused Landau path: schedule, device argument record, history row counter
+  LanSched sched;
+  LanFusedArgs<R>* dA = nullptr;
+  LanFusedArgs<R> hA{};
+  bool hA_valid = false;
+  int* d_row = nullptr;
+  int* d_ticket = nullptr;
+  int fnb[Q_TOTAL] = {0};
+  static constexpr int GRAPH_STEPS = 8;
+  bool fused_warm = false;
+  bool fields_set = false;  // the spectral-state layout is fixed from the first upload on
+  std::unique_ptr<AdjBuffers<R>, void (*)(AdjBuffers<R>*)> adjb{nullptr, adj_buffers_free<R>};
+  void reset_fused_state();
+  cudaGraphExec_t gexec = nullptr;
+  int64_t graph_launches = 0;  // kernels in gexec
+  void end_step(meu_diag* d, int clip);
+  void flush_hist(meu_diag* diag);
+  static constexpr int HIST_MAX = 4096;
+  double* hist = nullptr;  // per-step reductions [HIST_MAX][Q_STEP_COUNT]
+  double* cmean_acc = nullptr;
+  int hist_n = 0;
+  std::vector<int64_t> hist_step = std::vector<int64_t>(HIST_MAX);
+  std::vector<int> hist_iters = std::vector<int>(HIST_MAX);
+};
+
+}  // namespace meu

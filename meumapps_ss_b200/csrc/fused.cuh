@@ -1,5 +1,6 @@
 // fused.cuh -- compile-time shared-memory FFT building blocks for the fused
 // step kernels (grids with Nx = Ny = Nz = N, N in {32, 48, 64, 96, 128}).
+// Template parameter PV selects the radix plan (rplan), NT the threads of a block.
 //
 // Every transform length, radix plan, line count and stride is a template
 // constant, so all index arithmetic folds to shifts and constant multiplies.
@@ -23,32 +24,42 @@ struct RPlan {
   int ns;
   int r[8];
 };
-// radix plan (product = L): radix 8 while the remainder does not end in a
-// single factor 2 (128 = 8*4*4, not 8*8*2), then 4s, at most one 2, then 3s
+// Radix plans (product = L), two variants for the autotuner:
+//   pv 0: radix 8 while the remainder does not end in a single factor 2
+//         (128 = 8*4*4, not 8*8*2), then 4s, at most one 2, then 3s;
+//   pv 1: radix 4 first (128 = 4*4*4*2), then at most one 2, then 3s.
 __host__ __device__ constexpr int twos(int n) {
   int k = 0;
   while (n > 0 && n % 2 == 0) { n /= 2; ++k; }
   return k;
 }
-__host__ __device__ constexpr RPlan rplan(int L) {
+__host__ __device__ constexpr RPlan rplan(int L, int pv = 0) {
   RPlan p{0, {1, 1, 1, 1, 1, 1, 1, 1}};
   int n = L;
-  while (n % 8 == 0 && twos(n / 8) != 1) { p.r[p.ns++] = 8; n /= 8; }
+  if (pv == 0)
+    while (n % 8 == 0 && twos(n / 8) != 1) { p.r[p.ns++] = 8; n /= 8; }
   while (n % 4 == 0) { p.r[p.ns++] = 4; n /= 4; }
   if (n % 2 == 0) { p.r[p.ns++] = 2; n /= 2; }
   while (n % 3 == 0) { p.r[p.ns++] = 3; n /= 3; }
   return p;
 }
-__host__ __device__ constexpr int span_of(int L, int s) {
+__host__ __device__ constexpr bool same_plan(int L, int pa, int pb) {
+  const RPlan a = rplan(L, pa), b = rplan(L, pb);
+  if (a.ns != b.ns) return false;
+  for (int i = 0; i < a.ns; ++i)
+    if (a.r[i] != b.r[i]) return false;
+  return true;
+}
+__host__ __device__ constexpr int span_of(int L, int s, int pv) {
   int sp = L;
-  for (int i = 0; i < s; ++i) sp /= rplan(L).r[i];
+  for (int i = 0; i < s; ++i) sp /= rplan(L, pv).r[i];
   return sp;
 }
 
 // position after DIF -> frequency index
-template <int L>
+template <int L, int PV>
 __device__ __forceinline__ int rev(int p) {
-  constexpr RPlan pl = rplan(L);
+  constexpr RPlan pl = rplan(L, PV);
   int k = 0, mul = 1, span = L;
 #pragma unroll
   for (int s = 0; s < pl.ns; ++s) {
@@ -60,9 +71,9 @@ __device__ __forceinline__ int rev(int p) {
   return k;
 }
 // frequency index -> position after DIF
-template <int L>
+template <int L, int PV>
 __device__ __forceinline__ int pos(int k) {
-  constexpr RPlan pl = rplan(L);
+  constexpr RPlan pl = rplan(L, PV);
   int p = 0, span = L;
 #pragma unroll
   for (int s = 0; s < pl.ns; ++s) {
@@ -74,10 +85,10 @@ __device__ __forceinline__ int pos(int k) {
 }
 
 // One DIF stage over NL lines (element e of line l at buf[l*LS + e*ES]).
-template <typename C, int L, int S, int NL, int LS, int ES, int NT>
+template <typename C, int L, int S, int NL, int LS, int ES, int NT, int PV>
 __device__ __forceinline__ void dif_stage_s(C* buf, const C* __restrict__ tw) {
-  constexpr int R = rplan(L).r[S];
-  constexpr int SPAN = span_of(L, S);
+  constexpr int R = rplan(L, PV).r[S];
+  constexpr int SPAN = span_of(L, S, PV);
   constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
 #pragma unroll 1
   for (int t = threadIdx.x; t < NBF; t += NT) {
@@ -95,10 +106,10 @@ __device__ __forceinline__ void dif_stage_s(C* buf, const C* __restrict__ tw) {
     for (int q = 0; q < R; ++q) base[q * M * ES] = x[q];
   }
 }
-template <typename C, int L, int S, int NL, int LS, int ES, int NT>
+template <typename C, int L, int S, int NL, int LS, int ES, int NT, int PV>
 __device__ __forceinline__ void dit_stage_s(C* buf, const C* __restrict__ tw) {
-  constexpr int R = rplan(L).r[S];
-  constexpr int SPAN = span_of(L, S);
+  constexpr int R = rplan(L, PV).r[S];
+  constexpr int SPAN = span_of(L, S, PV);
   constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
 #pragma unroll 1
   for (int t = threadIdx.x; t < NBF; t += NT) {
@@ -118,21 +129,21 @@ __device__ __forceinline__ void dit_stage_s(C* buf, const C* __restrict__ tw) {
 }
 
 // Forward DIF over all stages (natural -> digit reversed); syncs after each stage.
-template <typename C, int L, int NL, int LS, int ES, int NT, int S = 0>
+template <typename C, int L, int NL, int LS, int ES, int NT, int PV, int S = 0>
 __device__ __forceinline__ void dif(C* buf, const C* tw) {
-  if constexpr (S < rplan(L).ns) {
-    dif_stage_s<C, L, S, NL, LS, ES, NT>(buf, tw);
+  if constexpr (S < rplan(L, PV).ns) {
+    dif_stage_s<C, L, S, NL, LS, ES, NT, PV>(buf, tw);
     __syncthreads();
-    dif<C, L, NL, LS, ES, NT, S + 1>(buf, tw);
+    dif<C, L, NL, LS, ES, NT, PV, S + 1>(buf, tw);
   }
 }
 // Inverse DIT over all stages (digit reversed -> natural), unscaled.
-template <typename C, int L, int NL, int LS, int ES, int NT, int S = rplan(L).ns - 1>
+template <typename C, int L, int NL, int LS, int ES, int NT, int PV, int S = rplan(L, PV).ns - 1>
 __device__ __forceinline__ void dit(C* buf, const C* tw) {
   if constexpr (S >= 0) {
-    dit_stage_s<C, L, S, NL, LS, ES, NT>(buf, tw);
+    dit_stage_s<C, L, S, NL, LS, ES, NT, PV>(buf, tw);
     __syncthreads();
-    dit<C, L, NL, LS, ES, NT, S - 1>(buf, tw);
+    dit<C, L, NL, LS, ES, NT, PV, S - 1>(buf, tw);
   }
 }
 
@@ -175,7 +186,7 @@ __device__ __forceinline__ void store_span(C* gmem, const C* smem, int n) {
 
 // ----------------------------------------------------------- plane (x + y)
 // Shared-memory image of one z-plane: NY rows of PITCH = N/2+1 complex.
-template <typename R, int N, int NT>
+template <typename R, int N, int NT, int PV>
 struct Plane {
   using C = cplx<R>;
   static constexpr int LX = N / 2, NXH = LX + 1, PITCH = NXH, NY = N;
@@ -197,14 +208,14 @@ struct Plane {
     const C* twx = tws;
     const C* twy = tws + LX * K;
     const C* post = tws + (LX + NY) * K;
-    dif<C, LX, NY, PITCH, 1, NT>(buf, twx);
+    dif<C, LX, NY, PITCH, 1, NT, PV>(buf, twx);
     // split in place, in digit-reversed column order (Nyquist into column LX)
     constexpr int NP = LX / 2 + 1;
 #pragma unroll 1
     for (int i = threadIdx.x; i < NY * NP; i += NT) {
       const int row = i % NY, k = i / NY;
       C* rb = buf + row * PITCH;
-      const int pk = pos<LX>(k % LX), pm = pos<LX>((LX - k) % LX);
+      const int pk = pos<LX, PV>(k % LX), pm = pos<LX, PV>((LX - k) % LX);
       const C zk = rb[pk], zm = rb[pm];
       C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
       C o = cscale(csub(zk, cconj(zm)), (R)0.5);
@@ -225,7 +236,7 @@ struct Plane {
       }
     }
     __syncthreads();
-    dif<C, NY, NXH, 1, PITCH, NT>(buf, twy);
+    dif<C, NY, NXH, 1, PITCH, NT, PV>(buf, twy);
   }
 
   // inverse of forward(): M-form plane -> rows of (x[2n], x[2n+1]), unscaled.
@@ -233,14 +244,14 @@ struct Plane {
     const C* twx = tws;
     const C* twy = tws + LX * K;
     const C* post = tws + (LX + NY) * K;
-    dit<C, NY, NXH, 1, PITCH, NT>(buf, twy);
+    dit<C, NY, NXH, 1, PITCH, NT, PV>(buf, twy);
     constexpr int NP = LX / 2 + 1;
 #pragma unroll 1
     for (int i = threadIdx.x; i < NY * NP; i += NT) {
       const int row = i % NY, k = i / NY;
       C* rb = buf + row * PITCH;
-      const int pk = (k == 0) ? 0 : pos<LX>(k);
-      const int pm = (k == 0) ? LX : pos<LX>(LX - k);
+      const int pk = (k == 0) ? 0 : pos<LX, PV>(k);
+      const int pm = (k == 0) ? LX : pos<LX, PV>(LX - k);
       C xk = rb[pk], xm = rb[pm];
       if (k == 0) { xk.y = 0; xm.y = 0; }
       {
@@ -255,7 +266,7 @@ struct Plane {
       }
     }
     __syncthreads();
-    dit<C, LX, NY, PITCH, 1, NT>(buf, twx);
+    dit<C, LX, NY, PITCH, 1, NT, PV>(buf, twx);
   }
 
   // M-form plane <-> shared memory (rows of NXH complex, contiguous in both).
@@ -276,9 +287,9 @@ struct Plane {
 };
 
 // kx of M-form column c
-template <int N>
+template <int N, int PV>
 __device__ __forceinline__ int kx_of_col(int c) {
-  return c == N / 2 ? N / 2 : rev<N / 2>(c);
+  return c == N / 2 ? N / 2 : rev<N / 2, PV>(c);
 }
 
 }  // namespace fz

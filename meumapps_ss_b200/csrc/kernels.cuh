@@ -74,6 +74,22 @@ __device__ __forceinline__ double warp_min(double v) {
   return v;
 }
 // op: 0 sum, 1 max, 2 min.  Stores the block result to out (thread 0).
+// block reduction whose result is valid in thread 0
+__device__ __forceinline__ double block_reduce_value(double v, int op) {
+  __shared__ double shv[32];
+  v = op == 0 ? warp_sum(v) : op == 1 ? warp_max(v) : warp_min(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) shv[w] = v;
+  __syncthreads();
+  double x = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
+  if (w == 0) {
+    x = lane < nw ? shv[lane] : x;
+    x = op == 0 ? warp_sum(x) : op == 1 ? warp_max(x) : warp_min(x);
+  }
+  return x;
+}
+
 __device__ __forceinline__ void block_reduce_store(double v, int op, double* out) {
   __shared__ double sh[32];
   v = op == 0 ? warp_sum(v) : op == 1 ? warp_max(v) : warp_min(v);

@@ -1,621 +1,41 @@
-// landau_fused.cu -- kernels and dispatch of the fused Landau step (see
-// landau_fused.cuh for the data flow).
-#include <type_traits>
-#include <vector>
+// landau_fused.cu -- size dispatch, per-step finalisation and schedule
+// autotuning of the fused Landau step (kernels: landau_fused_kernels.cuh,
+// instantiated per (precision, N) in lf_inst_*.cu).
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
 
 #include "landau_fused.cuh"
 
 namespace meu {
 
 namespace {
-constexpr int NT = 256;   // column kernels
-constexpr int NTP = 512;  // plane kernels
-constexpr int FCH_BLOCKS = 592;
-constexpr double TWO_PI = 6.283185307179586476925286766559;
-
-template <int N>
-__device__ __forceinline__ void kvec_n(int kx, int ky, int kz, double a[3], double b[3]) {
-  const int m[3] = {kx, ky, kz};
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int mm = (m[d] <= N / 2) ? m[d] : m[d] - N;
-    a[d] = (double)mm * (TWO_PI / (double)N);
-    b[d] = (2 * m[d] == N) ? 0.0 : a[d];
-  }
-}
-
-template <typename R> constexpr int col_tile() { return sizeof(R) == 4 ? 16 : 8; }
-
-// Column tile of nf fields: smem [z][slot][TM] with LN complex per z row, global
-// M-form (or state) field f at G + f*NK, row z at + z*PL, columns m0 .. m0+TM.
-// tile_load only issues cp.async copies; the caller waits.
-template <typename C, int N, int TM>
-__device__ __forceinline__ void tile_load(C* buf, int LN, int slot0, const C* G, int64_t NK, int64_t PL, int64_t m0,
-                                          int nf) {
-  constexpr int PER = 16 / sizeof(C);
-  const int per_row = nf * TM / PER;
-  for (int i = threadIdx.x; i < N * per_row; i += NT) {
-    const int zz = i / per_row, r = (i - zz * per_row) * PER, f = r / TM, c = r - f * TM;
-    fz::cp_async16(buf + zz * LN + (slot0 + f) * TM + c, G + f * NK + zz * PL + m0 + c);
-  }
-}
-template <typename C, int N, int TM>
-__device__ __forceinline__ void tile_store(const C* buf, int LN, int slot0, C* G, int64_t NK, int64_t PL, int64_t m0,
-                                           int nf) {
-  constexpr int PER = 16 / sizeof(C);
-  const int per_row = nf * TM / PER;
-  for (int i = threadIdx.x; i < N * per_row; i += NT) {
-    const int zz = i / per_row, r = (i - zz * per_row) * PER, f = r / TM, c = r - f * TM;
-    *(float4*)(G + f * NK + zz * PL + m0 + c) = *(const float4*)(buf + zz * LN + (slot0 + f) * TM + c);
-  }
-}
-
-}  // namespace
-
-// ------------------------------------------------------------------ PF
-// raw = 0: fields theta_v (f < V).
-// raw = 1: fields eta_v (f < V) and dc (f == V), for the spectral state.
-template <typename R, int N>
-__global__ void __launch_bounds__(NTP) k_lf_pf(LanFusedArgs<R> a, int V, int raw) {
-  using P = fz::Plane<R, N, NTP>;
-  using C = cplx<R>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;
-  C* tws = buf + P::ELEMS;
-  const int z = blockIdx.x, f = blockIdx.y;
-  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  const LanFusedConst& F = *a.F;
-  const R* ez = a.eta + z * PL;
-  const R* cz = a.c + z * PL;
-  P::load_real(buf, f < V ? ez + f * N3 : cz);
-  P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_all();
-  __syncthreads();
-  if (f < V && !raw) {
-    // theta_v = eta_v^2 in place
-    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-      const int y = i / P::LX, n = i - y * P::LX;
-      const C e = buf[y * P::PITCH + n];
-      buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
-    }
-    __syncthreads();
-  }
-  P::forward(buf, tws);
-  P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
-}
-
-// ------------------------------------------------------------------ Z0
-// set-up: z FFT of eta_v (f < V) and dc (f == V) into the spectral state
-template <typename R, int N, int V>
-__global__ void __launch_bounds__(NT) k_lf_z0(LanFusedArgs<R> a) {
-  using C = cplx<R>;
-  constexpr int TM = col_tile<R>(), NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
-  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;
-  C* tw = buf + N * LN;
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
-  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  fz::cp_async_wait_all();
-  __syncthreads();
-  fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
-  const double s = 1.0 / ((double)N * N * N);
-  for (int i = threadIdx.x; i < N * LN; i += NT) {
-    const int p = i / LN, r = i - p * LN, f = r / TM, c = r - f * TM;
-    const C v = buf[i];
-    C o = mk((R)((double)v.x * s), (R)((double)v.y * s));
-    if (f == V && p == 0 && m0 + c == 0) o = mk((R)0, (R)0);  // dc has no k = 0 mode
-    C* dst = (f < V) ? a.Keta + f * NK : a.Kc;
-    dst[p * PL + m0 + c] = o;
-  }
-}
-
-// ------------------------------------------------------------------ Z1
-template <typename R, int N, int V>
-__global__ void __launch_bounds__(NT) k_lf_z1(LanFusedArgs<R> a) {
-  using C = cplx<R>;
-  constexpr int TM = col_tile<R>(), NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
-  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
-  C* ks = buf + N * LN;  // dc^ state tile [N][TM]
-  C* tw = ks + N * TM;
-  __shared__ LanFusedConst F;
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
-  tile_load<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
-  for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
-  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  fz::cp_async_wait_all();
-  __syncthreads();
-  fz::dif<C, N, V * TM, 1, LN, NT>(buf, tw);
-  const double s = 1.0 / ((double)N * N * N);
-  double fint = 0, elen = 0;
-  for (int i = threadIdx.x; i < N * TM; i += NT) {
-    const int p = i / TM, c = i - p * TM;
-    const int64_t m = m0 + c;
-    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
-    const int kx = fz::kx_of_col<N>(cx), ky = fz::rev<N>(py), kz = fz::rev<N>(p);
-    double av[3], b[3];
-    kvec_n<N>(kx, ky, kz, av, b);
-    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
-    C* e = buf + p * LN + c;
-    double tr[V], ti[V], str = 0, sti = 0;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      tr[v] = (double)e[v * TM].x * s;
-      ti[v] = (double)e[v * TM].y * s;
-      str += tr[v];
-      sti += ti[v];
-    }
-    C* kc = ks + p * TM + c;
-    const C cs = *kc;
-    const double cr = (double)cs.x, ci = (double)cs.y;
-    const bool k0 = (kx == 0 && ky == 0 && kz == 0);
-    if (a.energy) fint += 0.5 * w * F.kappa_c * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci);
-    // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
-    double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
-    if (a.homog && !k0) {
-      double Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-      for (int v = 0; v < V; ++v)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * F.sig0[v][q]; Si[q] += ti[v] * F.sig0[v][q]; }
-      // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
-      const double t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
-      const double t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
-      const double t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
-      const double Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
-      const double Kv[6] = {av[0] * av[0], av[1] * av[1], av[2] * av[2], b[1] * b[2], b[0] * b[2], b[0] * b[1]};
-      double Qs[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        double acc = 0;
-#pragma unroll
-        for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
-        Qs[q] = acc;
-      }
-      // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
-      const double qa = Qs[0], qb = Qs[1], qc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
-      const double i00 = qb * qc - qf * qf, i01 = qe * qf - qc * qd, i02 = qd * qf - qb * qe;
-      const double i11 = qa * qc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
-      const double det = qa * i00 + qd * i01 + qe * i02;
-      if (det == 0.0) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
-      const double rd = 1.0 / det;
-      const double Qi[3][3] = {{i00 * rd, i01 * rd, i02 * rd}, {i01 * rd, i11 * rd, i12 * rd}, {i02 * rd, i12 * rd, i22 * rd}};
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
-        ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
-      }
-    }
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      double pr = 0, pi = 0;
-      if (a.homog && !k0) {
-        const double* sg = F.sig0[v];
-        const double sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
-        const double sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
-        const double sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
-        const double dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
-        const double di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
-        pr = -di;
-        pi = dr;
-      }
-      e[v * TM] = mk((R)pr, (R)pi);
-    }
-    if (a.homog && a.energy) {
-      // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
-      const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
-      double er[6], ei[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const int ii = I1[q], jj = J1[q];
-        double gr, gi;
-        if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
-        else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
-#pragma unroll
-        for (int v = 0; v < V; ++v) { gr -= tr[v] * F.eps_eng[v][q]; gi -= ti[v] * F.eps_eng[v][q]; }
-        if (k0) gr += F.ebar_eng[q];
-        er[q] = gr;
-        ei[q] = gi;
-      }
-      double qq = 0;
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        double cr2 = 0, ci2 = 0;
-#pragma unroll
-        for (int j = 0; j < 6; ++j) { cr2 += F.c0m[r + j * 6] * er[j]; ci2 += F.c0m[r + j * 6] * ei[j]; }
-        qq += er[r] * cr2 + ei[r] * ci2;
-      }
-      elen += 0.5 * w * qq;
-    }
-    // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
-    double nr = 0, ni = 0;
-    if (!k0) {
-      const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
-      const double mr = F.lan_a * cr - 0.5 * F.lan_b * str, mi = F.lan_a * ci - 0.5 * F.lan_b * sti;
-      const double den = 1.0 + F.dm * F.kappa_c * k2 * k2;
-      nr = (cr - F.dm * k2 * mr) / den;
-      ni = (ci - F.dm * k2 * mi) / den;
-    }
-    const C cn = mk((R)nr, (R)ni);
-    *kc = cn;
-    e[V * TM] = cn;
-  }
-  __syncthreads();
-  tile_store<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
-  fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
-  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
-  block_reduce_store(fint, 0, a.partials + LQ_FINT * a.pstride + blockIdx.x);
-  block_reduce_store(elen, 0, a.partials + LQ_ELEN * a.pstride + blockIdx.x);
-}
-
-// ------------------------------------------------------------------ PB
-// Pointwise inputs (eta_0..V-1 and dc of this plane) stream through a two-deep
-// cp.async pipeline of PB_CH-row chunks; the first two chunks load during the
-// inverse transform.  Block (f, z): g_f of plane z -> forward transform.
-constexpr int PB_CH = 8;
-
-template <typename R, int N>
-constexpr size_t pb_smem(int V) {
-  return fz::Plane<R, N, NTP>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
-}
-
-template <typename R, int N>
-__global__ void __launch_bounds__(NTP) k_lf_pb(LanFusedArgs<R> a, int V) {
-  using P = fz::Plane<R, N, NTP>;
-  using C = cplx<R>;
-  constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;
-  C* tws = buf + P::ELEMS;
-  R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR]
-  // field index fastest: the V+1 blocks of one plane, which read the same eta and
-  // dc planes, are resident together and share those reads through L2
-  const int f = blockIdx.x, z = blockIdx.y;
-  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  const int NFI = V + 1;
-  auto issue = [&](int k) {
-    R* dst = stg + (k & 1) * NFI * CHR;
-#pragma unroll 1
-    for (int i = threadIdx.x; i < NFI * (CHR / PER); i += NTP) {
-      const int q = i / (CHR / PER), r = (i - q * (CHR / PER)) * PER;
-      const R* src = (q < V ? a.eta + q * N3 : a.c) + z * PL + (int64_t)k * CHR + r;
-      fz::cp_async16(dst + q * CHR + r, src);
-    }
-    fz::cp_async_commit();
-  };
-  C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
-  P::load_m(buf, mp);
-  fz::cp_async_commit();
-  issue(0);
-  issue(1);
-  P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_group<2>();
-  __syncthreads();
-  P::inverse(buf, tws);
-  const LanFusedConst& F = *a.F;
-  {
-#pragma unroll 1
-    for (int k = 0; k < NCH; ++k) {
-      if (k + 1 < NCH) fz::cp_async_wait_group<1>();
-      else fz::cp_async_wait_group<0>();
-      __syncthreads();
-      const R* sb = stg + (k & 1) * NFI * CHR;
-#pragma unroll 1
-      for (int i = threadIdx.x; i < CH * P::LX; i += NTP) {
-        const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
-        double e[2][4], s2[2] = {0, 0};
-        for (int q = 0; q < V; ++q) {
-          const C ev = ((const C*)(sb + q * CHR + yl * N))[n];
-          e[0][q] = ev.x;
-          e[1][q] = ev.y;
-          s2[0] += e[0][q] * e[0][q];
-          s2[1] += e[1][q] * e[1][q];
-        }
-        const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
-        const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
-        {
-          const C ph = buf[y * P::PITCH + n];
-          const double phv[2] = {(double)ph.x, (double)ph.y};
-          double out[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const double ev = e[h][f], e2 = ev * ev;
-            double g = F.lan_b * (F.lan_c2 - cv[h]) * ev - F.lan_c * e2 * ev + F.lan_d * e2 * e2 * ev +
-                       4.0 * F.cross_w * ev * (s2[h] - e2);
-            if (a.homog) {
-              double sacc = F.sig0_ebar[f] + phv[h];
-              for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
-              g += -2.0 * ev * sacc;
-            }
-            out[h] = g;
-          }
-          buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
-        }
-      }
-      __syncthreads();
-      if (k + 2 < NCH) issue(k + 2);
-    }
-  }
-  P::forward(buf, tws);
-  P::store_m(buf, mp);
-}
-
-// ------------------------------------------------------------------ Z2
-template <typename R, int N, int V>
-__global__ void __launch_bounds__(NT) k_lf_z2(LanFusedArgs<R> a) {
-  using C = cplx<R>;
-  constexpr int TM = col_tile<R>(), NXH = N / 2 + 1, LN = V * TM;
-  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;
-  C* ks = buf + N * LN;  // eta^ state tiles [N][V][TM]
-  C* tw = ks + N * LN;
-  __shared__ double g[V][9];
-  __shared__ double dtl;
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
-  tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
-  for (int i = threadIdx.x; i < V * 9; i += NT) g[i / 9][i % 9] = a.F->g[i / 9][i % 9];
-  if (threadIdx.x == 0) dtl = a.F->dtl;
-  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  fz::cp_async_wait_all();
-  __syncthreads();
-  fz::dif<C, N, LN, 1, LN, NT>(buf, tw);
-  const double s = 1.0 / ((double)N * N * N);
-  double fint = 0;
-  for (int i = threadIdx.x; i < N * TM; i += NT) {
-    const int p = i / TM, c = i - p * TM;
-    const int64_t m = m0 + c;
-    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
-    const int kx = fz::kx_of_col<N>(cx), ky = fz::rev<N>(py), kz = fz::rev<N>(p);
-    double av[3], b[3];
-    kvec_n<N>(kx, ky, kz, av, b);
-    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
-    C* e = buf + p * LN + c;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const double* gv = g[v];
-      C* kst = ks + p * LN + v * TM + c;
-      const C st = *kst;
-      const double hr = (double)st.x, hi = (double)st.y;
-      if (a.energy) {
-        const double kb = gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
-                          (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-        fint += 0.5 * w * kb * (hr * hr + hi * hi);
-      }
-      const double kk = gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] +
-                        (gv[3] + gv[1]) * b[0] * b[1] + (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-      const double rden = 1.0 / (1.0 + dtl * kk);
-      const double nr = (hr - dtl * s * (double)e[v * TM].x) * rden;
-      const double ni = (hi - dtl * s * (double)e[v * TM].y) * rden;
-      const C o = mk((R)nr, (R)ni);
-      *kst = o;
-      e[v * TM] = o;
-    }
-  }
-  __syncthreads();
-  tile_store<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
-  fz::dit<C, N, LN, 1, LN, NT>(buf, tw);
-  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
-  block_reduce_store(fint, 0, a.partials + Q_FINT2 * a.pstride + blockIdx.x);
-}
-
-// ------------------------------------------------------------------ PI
-// Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
-// -> real (into c2), concentration statistics.
-template <typename R, int N>
-__global__ void __launch_bounds__(NTP) k_lf_pi(LanFusedArgs<R> a, int V) {
-  using P = fz::Plane<R, N, NTP>;
-  using C = cplx<R>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;
-  C* tws = buf + P::ELEMS;
-  const int z = blockIdx.x, f = blockIdx.y;
-  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  P::load_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
-  P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_all();
-  __syncthreads();
-  P::inverse(buf, tws);
-  R* dst = (f < V) ? a.eta + f * N3 + z * PL : a.c2 + z * PL;
-  double emax = 0.0, s2 = 0.0, cmin = 1.0, cmax = 0.0, csum = 0.0;
-  const double cbar = a.F->cbar;
-#pragma unroll 1
-  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-    const int y = i / P::LX, n = i - y * P::LX;
-    const C v = buf[y * P::PITCH + n];
-    ((C*)(dst + (int64_t)y * N))[n] = v;
-    if (f < V) {
-      emax = fmax(emax, fmax((double)v.x, (double)v.y));
-      s2 += (double)v.x * v.x + (double)v.y * v.y;
-    } else {
-      const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
-      cmin = fmin(cmin, fmin(c0, c1));
-      cmax = fmax(cmax, fmax(c0, c1));
-      csum += c0 + c1;
-    }
-  }
-  const int blk = z * (V + 1) + f;
-  block_reduce_store(emax, 1, a.partials + LQ_PHIMAX * a.pstride + blk);
-  block_reduce_store(s2, 0, a.partials + LQ_SOLID * a.pstride + blk);
-  block_reduce_store(cmin, 2, a.partials + LQ_CMIN * a.pstride + blk);
-  block_reduce_store(cmax, 1, a.partials + LQ_CMAX * a.pstride + blk);
-  block_reduce_store(csum, 0, a.partials + LQ_CSUM * a.pstride + blk);
-}
-
-// ------------------------------------------------------------------ FCH
-// bulk free energy of the start-of-step fields (all eta and dc), streamed with
-// 16-byte loads over the whole grid
+// Fixed-order reduction of member blockIdx.y's partials into its history row.
+// The last of the member's blocks advances the member's row counter, so graph
+// replays of the step need no host-side row index.
 template <typename R>
-__global__ void __launch_bounds__(256) k_lf_fch(LanFusedArgs<R> a, int V, int64_t n3) {
-  using V4 = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
-  constexpr int PER = 16 / sizeof(R);
-  const LanFusedConst& F = *a.F;
-  double fch = 0;
-  const int64_t nv = n3 / PER;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
-    R e[4][PER], d[PER];
-    {
-      const V4 t = ((const V4*)a.c)[i];
-      const R* tp = (const R*)&t;
-#pragma unroll
-      for (int h = 0; h < PER; ++h) d[h] = tp[h];
+__global__ void __launch_bounds__(256) k_lf_finalize(const LanFusedArgs<R>* __restrict__ A, NbList nb,
+                                                     const int* __restrict__ ops) {
+  const LanFusedArgs<R>& a = A[blockIdx.y];
+  const int q = blockIdx.x, op = ops[q];
+  const int row = *a.hist_row;
+  double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
+  for (int i = threadIdx.x; i < nb.nb[q]; i += blockDim.x) {
+    const double v = a.partials[(int64_t)q * PSTRIDE + i];
+    acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
+  }
+  const double x = block_reduce_value(acc, op);
+  if (threadIdx.x == 0) {
+    if (row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = x;
+    __threadfence();
+    if (atomicAdd(a.ticket, 1) == (int)gridDim.x - 1) {
+      *a.ticket = 0;
+      *a.hist_row = row + 1;
     }
-    for (int q = 0; q < V; ++q) {
-      const V4 t = ((const V4*)(a.eta + q * n3))[i];
-      const R* tp = (const R*)&t;
-#pragma unroll
-      for (int h = 0; h < PER; ++h) e[q][h] = tp[h];
-    }
-#pragma unroll
-    for (int h = 0; h < PER; ++h) {
-      double s2 = 0, s4 = 0, s6 = 0;
-      for (int q = 0; q < V; ++q) {
-        const double e2 = (double)e[q][h] * (double)e[q][h];
-        s2 += e2;
-        s4 += e2 * e2;
-        s6 += e2 * e2 * e2;
-      }
-      const double cv = F.cbar + (double)d[h];
-      fch += 0.5 * F.lan_a * (cv - F.lan_c1) * (cv - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv) * s2 - 0.25 * F.lan_c * s4 +
-             F.lan_d / 6.0 * s6 + F.cross_w * (s2 * s2 - s4);
-    }
-  }
-  block_reduce_store(fch, 0, a.partials + LQ_FCH * a.pstride + blockIdx.x);
-}
-
-// ------------------------------------------------------------------ dispatch
-namespace {
-struct Scope {
-  LaunchHook* h;
-  cudaStream_t st;
-  Scope(LaunchHook* h_, const char* n, double b, cudaStream_t s) : h(h_), st(s) {
-    if (h) h->begin(n, b, st);
-  }
-  ~Scope() {
-    if (h) h->end(st);
-  }
-};
-
-template <typename K>
-void ensure_smem(K fn, size_t bytes) {
-  if (bytes <= 48 * 1024) return;
-  static thread_local std::vector<const void*> done;
-  for (const void* f : done)
-    if (f == (const void*)fn) return;
-  int dev = 0, optin = 0;
-  MEU_CUDA(cudaGetDevice(&dev));
-  MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes fa;
-  MEU_CUDA(cudaFuncGetAttributes(&fa, (const void*)fn));
-  const int lim = optin - (int)fa.sharedSizeBytes;
-  if ((int)bytes > lim) throw CudaError("fused tile exceeds shared memory", MEU_ERR_UNSUPPORTED);
-  MEU_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  done.push_back((const void*)fn);
-}
-
-template <typename R, int N, int V>
-void run_step(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
-  using P = fz::Plane<R, N, NTP>;
-  using C = cplx<R>;
-  constexpr int TM = col_tile<R>();
-  constexpr int NXH = N / 2 + 1;
-  const int tiles = N * NXH / TM;
-  const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
-  const size_t sp = P::smem_bytes();
-  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + (size_t)N * TM + N * Tw<C>::K);
-  const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
-  const size_t spb = pb_smem<R, N>(V);
-  ensure_smem(k_lf_pf<R, N>, sp);
-  ensure_smem(k_lf_pb<R, N>, spb);
-  ensure_smem(k_lf_pi<R, N>, sp);
-  ensure_smem(k_lf_z1<R, N, V>, s1);
-  ensure_smem(k_lf_z2<R, N, V>, s2);
-  {
-    Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
-    k_lf_pf<R, N><<<dim3(N, V), NTP, sp, st>>>(a, V, 0);
-    MEU_CHECK_LAUNCH();
-  }
-  if (a.energy) {
-    Scope s(hook, "lf_bulk_energy", (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_fch<R><<<FCH_BLOCKS, 256, 0, st>>>(a, V, (int64_t)N * N * N);
-    MEU_CHECK_LAUNCH();
-  }
-  {
-    Scope s(hook, "lf_z_green_ch", (2.0 * V + 3) * nk * sizeof(C), st);
-    k_lf_z1<R, N, V><<<tiles, NT, s1, st>>>(a);
-    MEU_CHECK_LAUNCH();
-  }
-  {
-    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pb<R, N><<<dim3(V, N), NTP, spb, st>>>(a, V);
-    MEU_CHECK_LAUNCH();
-  }
-  {
-    Scope s(hook, "lf_z_tdgl", 4.0 * V * nk * sizeof(C), st);
-    k_lf_z2<R, N, V><<<tiles, NT, s2, st>>>(a);
-    MEU_CHECK_LAUNCH();
-  }
-  {
-    Scope s(hook, "lf_plane_inv_stats", (V + 1.0) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pi<R, N><<<dim3(N, V + 1), NTP, sp, st>>>(a, V);
-    MEU_CHECK_LAUNCH();
-  }
-  for (int q = 0; q < Q_TOTAL; ++q) nb[q] = 0;
-  nb[Q_FCH] = a.energy ? FCH_BLOCKS : 0;
-  nb[Q_FINT] = tiles;
-  nb[Q_ELEN] = tiles;
-  nb[Q_FINT2] = tiles;
-  nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * (V + 1);
-}
-
-template <typename R, int N, int V>
-void run_init(const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
-  using P = fz::Plane<R, N, NTP>;
-  using C = cplx<R>;
-  constexpr int TM = col_tile<R>();
-  constexpr int NXH = N / 2 + 1;
-  const int tiles = N * NXH / TM;
-  const size_t sp = P::smem_bytes();
-  const size_t s0 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
-  ensure_smem(k_lf_pf<R, N>, sp);
-  ensure_smem(k_lf_z0<R, N, V>, s0);
-  const double n3 = (double)N * N * N, nk = (double)N * N * NXH;
-  {
-    Scope s(hook, "lf_plane_fwd_state", (V + 1.0) * (nk * sizeof(C) + n3 * sizeof(R)), st);
-    k_lf_pf<R, N><<<dim3(N, V + 1), NTP, sp, st>>>(a, V, 1);
-    MEU_CHECK_LAUNCH();
-  }
-  {
-    Scope s(hook, "lf_z_state", 2.0 * (V + 1) * nk * sizeof(C), st);
-    k_lf_z0<R, N, V><<<tiles, NT, s0, st>>>(a);
-    MEU_CHECK_LAUNCH();
-  }
-}
-
-template <typename R, int N>
-bool dispatch_init(int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
-  switch (V) {
-    case 1: run_init<R, N, 1>(a, st, hook); return true;
-    case 2: run_init<R, N, 2>(a, st, hook); return true;
-    case 3: run_init<R, N, 3>(a, st, hook); return true;
-    case 4: run_init<R, N, 4>(a, st, hook); return true;
-    default: return false;
-  }
-}
-
-template <typename R, int N>
-bool dispatch_v(int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
-  switch (V) {
-    case 1: run_step<R, N, 1>(a, st, hook, nb); return true;
-    case 2: run_step<R, N, 2>(a, st, hook, nb); return true;
-    case 3: run_step<R, N, 3>(a, st, hook, nb); return true;
-    case 4: run_step<R, N, 4>(a, st, hook, nb); return true;
-    default: return false;
   }
 }
 }  // namespace
@@ -628,31 +48,152 @@ bool lan_fused_supported(const meu_params& p) {
 }
 
 template <typename R>
-bool lan_fused_step(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb) {
+bool lan_fused_step(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy,
+                    cudaStream_t st, LaunchHook* hook, int* nb) {
+  if (members < 1 || members > 65535) return false;
   switch (N) {
-    case 32: return dispatch_v<R, 32>(V, a, st, hook, nb);
-    case 48: return dispatch_v<R, 48>(V, a, st, hook, nb);
-    case 64: return dispatch_v<R, 64>(V, a, st, hook, nb);
-    case 96: return dispatch_v<R, 96>(V, a, st, hook, nb);
-    case 128: return dispatch_v<R, 128>(V, a, st, hook, nb);
+    case 32: return lf_step_n<R, 32>(V, s, dA, members, energy, st, hook, nb);
+    case 48: return lf_step_n<R, 48>(V, s, dA, members, energy, st, hook, nb);
+    case 64: return lf_step_n<R, 64>(V, s, dA, members, energy, st, hook, nb);
+    case 96: return lf_step_n<R, 96>(V, s, dA, members, energy, st, hook, nb);
+    case 128: return lf_step_n<R, 128>(V, s, dA, members, energy, st, hook, nb);
     default: return false;
   }
 }
 
 template <typename R>
-bool lan_fused_init(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook) {
+bool lan_fused_init(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st,
+                    LaunchHook* hook) {
+  if (members < 1 || members > 65535) return false;
   switch (N) {
-    case 32: return dispatch_init<R, 32>(V, a, st, hook);
-    case 48: return dispatch_init<R, 48>(V, a, st, hook);
-    case 64: return dispatch_init<R, 64>(V, a, st, hook);
-    case 96: return dispatch_init<R, 96>(V, a, st, hook);
-    case 128: return dispatch_init<R, 128>(V, a, st, hook);
+    case 32: return lf_init_n<R, 32>(V, s, dA, members, st, hook);
+    case 48: return lf_init_n<R, 48>(V, s, dA, members, st, hook);
+    case 64: return lf_init_n<R, 64>(V, s, dA, members, st, hook);
+    case 96: return lf_init_n<R, 96>(V, s, dA, members, st, hook);
+    case 128: return lf_init_n<R, 128>(V, s, dA, members, st, hook);
     default: return false;
   }
 }
-template bool lan_fused_init<float>(int, int, const LanFusedArgs<float>&, cudaStream_t, LaunchHook*);
-template bool lan_fused_init<double>(int, int, const LanFusedArgs<double>&, cudaStream_t, LaunchHook*);
-template bool lan_fused_step<float>(int, int, const LanFusedArgs<float>&, cudaStream_t, LaunchHook*, int*);
-template bool lan_fused_step<double>(int, int, const LanFusedArgs<double>&, cudaStream_t, LaunchHook*, int*);
+
+template <typename R>
+void lan_fused_finalize(const LanFusedArgs<R>* dA, int members, const int* nb, const int* ops, cudaStream_t st,
+                        LaunchHook* hook) {
+  NbList l;
+  for (int q = 0; q < Q_TOTAL; ++q) l.nb[q] = q < Q_STEP_COUNT ? nb[q] : 0;
+  double bytes = 0;
+  for (int q = 0; q < Q_STEP_COUNT; ++q) bytes += 8.0 * nb[q];
+  if (hook) hook->begin("finalize", bytes * members, st);
+  k_lf_finalize<R><<<dim3(Q_STEP_COUNT, members), 256, 0, st>>>(dA, l, ops);
+  MEU_CHECK_LAUNCH();
+  if (hook) hook->end(st);
+}
+
+std::vector<LanSched> lan_sched_candidates(int N, bool f64) {
+  std::vector<LanSched> v;
+  const int wide = f64 ? 8 : 16;
+  const int cols = N * (N / 2 + 1);
+  for (int pv = 0; pv < 2; ++pv)
+    for (int ntp : {512, 256})
+      for (int tm : {wide, wide / 2}) {
+        if (cols % tm != 0 || cols / tm > PSTRIDE) continue;
+        LanSched s;
+        s.pv = pv;
+        s.ntp = ntp;
+        s.tm = tm;
+        v.push_back(s);
+      }
+  return v;
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, LanSched> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_key(bool f64, int N, int V, int members, bool energy) {
+  std::ostringstream o;
+  o << (f64 ? "f64" : "f32") << ' ' << N << ' ' << V << ' ' << members << ' ' << (energy ? 1 : 0);
+  return o.str();
+}
+void tune_load() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = std::getenv("MEU_AUTOTUNE_CACHE");
+  if (!path || !*path) return;
+  std::ifstream f(path);
+  std::string prec;
+  int N, V, members, energy;
+  LanSched s;
+  while (f >> prec >> N >> V >> members >> energy >> s.pv >> s.ntp >> s.tm) {
+    std::string rest;
+    std::getline(f, rest);
+    g_tune[tune_key(prec == "f64", N, V, members, energy != 0)] = s;
+  }
+}
+void tune_store(const std::string& key, const LanSched& s, double ms) {
+  const char* path = std::getenv("MEU_AUTOTUNE_CACHE");
+  if (!path || !*path) return;
+  std::ofstream f(path, std::ios::app);
+  f << key << ' ' << s.pv << ' ' << s.ntp << ' ' << s.tm << ' ' << ms << '\n';
+}
+}  // namespace
+
+template <typename R>
+LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool energy, const int* d_ops,
+                      cudaStream_t st, double* best_ms) {
+  const bool f64 = sizeof(R) == 8;
+  const std::string key = tune_key(f64, N, V, members, energy);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load();
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      if (best_ms) *best_ms = -1.0;
+      return it->second;
+    }
+  }
+  constexpr int WARM = 2, TIMED = 5;
+  cudaEvent_t e0, e1;
+  MEU_CUDA(cudaEventCreate(&e0));
+  MEU_CUDA(cudaEventCreate(&e1));
+  LanSched best;
+  double best_t = 1e300;
+  int nb[Q_TOTAL];
+  for (const LanSched& s : lan_sched_candidates(N, f64)) {
+    for (int i = 0; i < WARM + TIMED; ++i) {
+      if (i == WARM) MEU_CUDA(cudaEventRecord(e0, st));
+      if (!lan_fused_step<R>(N, V, s, dA, members, energy, st, nullptr, nb)) break;
+      lan_fused_finalize<R>(dA, members, nb, d_ops, st, nullptr);
+    }
+    MEU_CUDA(cudaEventRecord(e1, st));
+    MEU_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / TIMED < best_t) {
+      best_t = ms / TIMED;
+      best = s;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_ms) *best_ms = best_t;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  tune_store(key, best, best_t);
+  return best;
+}
+
+template bool lan_fused_init<float>(int, int, const LanSched&, const LanFusedArgs<float>*, int, cudaStream_t, LaunchHook*);
+template bool lan_fused_init<double>(int, int, const LanSched&, const LanFusedArgs<double>*, int, cudaStream_t, LaunchHook*);
+template bool lan_fused_step<float>(int, int, const LanSched&, const LanFusedArgs<float>*, int, bool, cudaStream_t,
+                                    LaunchHook*, int*);
+template bool lan_fused_step<double>(int, int, const LanSched&, const LanFusedArgs<double>*, int, bool, cudaStream_t,
+                                     LaunchHook*, int*);
+template void lan_fused_finalize<float>(const LanFusedArgs<float>*, int, const int*, const int*, cudaStream_t, LaunchHook*);
+template void lan_fused_finalize<double>(const LanFusedArgs<double>*, int, const int*, const int*, cudaStream_t,
+                                         LaunchHook*);
+template LanSched lan_autotune<float>(int, int, const LanFusedArgs<float>*, int, bool, const int*, cudaStream_t, double*);
+template LanSched lan_autotune<double>(int, int, const LanFusedArgs<double>*, int, bool, const int*, cudaStream_t,
+                                       double*);
 
 }  // namespace meu

@@ -8,19 +8,24 @@
 // re-derived each step for the nonlinear terms and the output.  (Re-transforming
 // the real fields every step instead makes an FP32 forward/inverse pair act on
 // slowly varying data each step, whose rounding errors then add up coherently.)
-// Five launches per step:
+// Six launches per step (with the bulk-energy reduction) and one finalisation:
 //
 //   PF  plane:  theta_v = eta_v^2 -> x R2C + y FFT                         (+ bulk energy)
 //   Z1  column: z FFT of theta -> Green operator phi_v; Cahn-Hilliard update of
 //              the dc^ state (mu^ = A dc^ - B/2 sum theta^_v) -> z iFFT of phi_v, dc_new
-//   PB  plane:  y iFFT + x C2R of phi_v -> g_v = df/deta_v + el_grad_v -> x R2C + y FFT;
-//              plane of dc_new -> real
+//   PB  plane:  y iFFT + x C2R of phi_v -> g_v = df/deta_v + el_grad_v -> x R2C + y FFT
 //   Z2  column: z FFT of g -> eta^ state <- (eta^ - dt L g^) / (1 + dt L k.kappa.k) -> z iFFT
-//   PI  plane:  y iFFT + x C2R of eta_new -> real eta (+ end-of-step statistics)
+//   PI  plane:  y iFFT + x C2R of eta_new, dc_new -> real eta, dc in place
+//              (+ end-of-step statistics)
 //
 // Set-up (after new fields are uploaded): PF in raw mode transforms eta_v and dc,
 // Z0 finishes the z transform into the spectral state.
+//
+// The real-field inputs of the step (eta and dc) are read by PF, FCH and PB and
+// rewritten only by PI, the last launch, so both are updated in place.
 #pragma once
+#include <vector>
+
 #include "fused.cuh"
 #include "kernels.cuh"
 
@@ -39,23 +44,43 @@ struct LanFusedConst {
   double lan_a, lan_b, lan_c, lan_d, lan_c1, lan_c2, cross_w, kappa_c, dm, dtl, cbar;
 };
 
+// Device-side arguments of one simulation ("member").  Kernels read them from a
+// device array indexed by blockIdx.z, so one launch covers every member of an
+// ensemble bucket (same N, V and precision); a single simulation is a bucket of one.
 template <typename R>
 struct LanFusedArgs {
   const LanFusedConst* F;
-  R* eta;     // V real fields
-  R* c;       // dc (start of step)
-  R* c2;      // dc (end of step)
+  R* eta;     // V real fields (updated in place)
+  R* c;       // dc (updated in place)
   cplx<R>* M; // V+1 M-form spectra
   cplx<R>* Keta;  // spectral state eta^_v (V spectra, normalised, column-kernel layout)
   cplx<R>* Kc;    // spectral state dc^ (normalised, column-kernel layout)
-  double* partials;
-  int pstride;
+  double* partials;  // per-block reductions [quantity][PSTRIDE]
   int* err;
   int homog, energy;
   const cplx<R>* twx;
   const cplx<R>* twy;
   const cplx<R>* twz;
   const cplx<R>* post;
+  double* hist;   // per-step reduction rows [hist_rows][Q_STEP_COUNT]
+  int* hist_row;  // row of the current step (advanced by the finalisation)
+  int* ticket;    // completion counter of the finalisation
+  int hist_rows;
+  // where the step writes the new state (equal to eta, c, Keta, Kc for an in-place step)
+  R* eta_next;
+  R* c_next;
+  cplx<R>* Keta_out;
+  cplx<R>* Kc_out;
+  // optional records of the step for the adjoint (NULL: off): the real elastic
+  // potential phi_v (V fields) and the normalised spectra theta^_v (V spectra)
+  R* rec_phi;
+  cplx<R>* rec_theta;
+};
+
+// Schedule of the fused kernels: radix plan variant (fz::rplan), threads of the
+// plane kernels, column tile width (complex columns per column-kernel block).
+struct LanSched {
+  int pv = 0, ntp = 512, tm = 0;  // tm = 0: 16 columns (FP32) / 8 columns (FP64)
 };
 
 enum LanQ : int {
@@ -63,12 +88,37 @@ enum LanQ : int {
   LQ_SOLID = Q_SOLID, LQ_CSUM = Q_CSUM0
 };
 
-// host launch entry (landau_fused.cu): returns false if (N, V) has no instantiation
+// Host launch entries (landau_fused.cu).  dA: device array of `members`
+// argument records.  Return false if (N, V, schedule) has no instantiation.
+// lan_fused_step writes the per-block reduction counts of the step into nb.
 template <typename R>
-bool lan_fused_step(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook, int* nb_out);
+bool lan_fused_step(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy,
+                    cudaStream_t st, LaunchHook* hook, int* nb);
 // spectral state from the real fields eta and dc (after an upload)
 template <typename R>
-bool lan_fused_init(int N, int V, const LanFusedArgs<R>& a, cudaStream_t st, LaunchHook* hook);
+bool lan_fused_init(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st,
+                    LaunchHook* hook);
+// fixed-order reduction of each member's partials into its history row
+// *hist_row; the last block to finish advances *hist_row
+template <typename R>
+void lan_fused_finalize(const LanFusedArgs<R>* dA, int members, const int* nb, const int* ops, cudaStream_t st,
+                        LaunchHook* hook);
+// the schedules instantiated for (N, precision)
+std::vector<LanSched> lan_sched_candidates(int N, bool f64);
+// Times every candidate schedule on the members' buffers (a few steps each, the
+// fields must not hold a simulation yet: tuning advances them) and returns the
+// fastest.  Results are cached per (precision, N, V, members, energy) for the
+// process and, when the environment names a file in MEU_AUTOTUNE_CACHE, in that file.
+template <typename R>
+LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool energy, const int* d_ops,
+                      cudaStream_t st, double* best_ms);
 bool lan_fused_supported(const meu_params& p);
+
+// per-(R, N) entries, one translation unit each (lf_inst_*.cu)
+template <typename R, int N>
+bool lf_step_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st,
+               LaunchHook* hook, int* nb);
+template <typename R, int N>
+bool lf_init_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st, LaunchHook* hook);
 
 }  // namespace meu

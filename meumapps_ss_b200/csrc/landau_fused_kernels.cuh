@@ -1,0 +1,716 @@
+// landau_fused_kernels.cuh -- kernels of the fused Landau step (see
+// landau_fused.cuh for the data flow) and their launch sequence for one (R, N).
+// Included by the per-(R, N) translation units lf_inst_*.cu, which instantiate
+// every (V, schedule) for their grid size.
+//
+// Every kernel serves a batch of members: blockIdx.z selects the member's
+// argument record.
+#pragma once
+#include <type_traits>
+#include <vector>
+
+#include "landau_fused.cuh"
+
+namespace meu {
+namespace lf {
+
+constexpr int NT = 256;   // column kernels
+constexpr int FCH_MAX_BLOCKS = 592;
+constexpr double TWO_PI = 6.283185307179586476925286766559;
+
+template <int N>
+__device__ __forceinline__ void kvec_n(int kx, int ky, int kz, double a[3], double b[3]) {
+  const int m[3] = {kx, ky, kz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int mm = (m[d] <= N / 2) ? m[d] : m[d] - N;
+    a[d] = (double)mm * (TWO_PI / (double)N);
+    b[d] = (2 * m[d] == N) ? 0.0 : a[d];
+  }
+}
+
+template <typename R> constexpr int col_tile_default() { return sizeof(R) == 4 ? 16 : 8; }
+
+// Column tile of nf fields: smem [z][slot][TM] with LN complex per z row, global
+// M-form (or state) field f at G + f*NK, row z at + z*PL, columns m0 .. m0+TM.
+// tile_load only issues cp.async copies; the caller waits.
+template <typename C, int N, int TM>
+__device__ __forceinline__ void tile_load(C* buf, int LN, int slot0, const C* G, int64_t NK, int64_t PL, int64_t m0,
+                                          int nf) {
+  constexpr int PER = 16 / sizeof(C);
+  const int per_row = nf * TM / PER;
+  for (int i = threadIdx.x; i < N * per_row; i += NT) {
+    const int zz = i / per_row, r = (i - zz * per_row) * PER, f = r / TM, c = r - f * TM;
+    fz::cp_async16(buf + zz * LN + (slot0 + f) * TM + c, G + f * NK + zz * PL + m0 + c);
+  }
+}
+template <typename C, int N, int TM>
+__device__ __forceinline__ void tile_store(const C* buf, int LN, int slot0, C* G, int64_t NK, int64_t PL, int64_t m0,
+                                           int nf) {
+  constexpr int PER = 16 / sizeof(C);
+  const int per_row = nf * TM / PER;
+  for (int i = threadIdx.x; i < N * per_row; i += NT) {
+    const int zz = i / per_row, r = (i - zz * per_row) * PER, f = r / TM, c = r - f * TM;
+    *(float4*)(G + f * NK + zz * PL + m0 + c) = *(const float4*)(buf + zz * LN + (slot0 + f) * TM + c);
+  }
+}
+
+// ------------------------------------------------------------------ PF
+// raw = 0: fields theta_v (f < V).
+// raw = 1: fields eta_v (f < V) and dc (f == V), for the spectral state.
+template <typename R, int N, int PV, int NTP>
+__global__ void __launch_bounds__(NTP) k_lf_pf(const LanFusedArgs<R>* __restrict__ A, int V, int raw) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x, f = blockIdx.y;
+  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
+  const R* ez = a.eta + z * PL;
+  const R* cz = a.c + z * PL;
+  P::load_real(buf, f < V ? ez + f * N3 : cz);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_all();
+  __syncthreads();
+  if (f < V && !raw) {
+    // theta_v = eta_v^2 in place
+    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+      const int y = i / P::LX, n = i - y * P::LX;
+      const C e = buf[y * P::PITCH + n];
+      buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
+    }
+    __syncthreads();
+  }
+  P::forward(buf, tws);
+  P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+}
+
+// ------------------------------------------------------------------ Z0
+// set-up: z FFT of eta_v (f < V) and dc (f == V) into the spectral state
+template <typename R, int N, int V, int PV, int TM>
+__global__ void __launch_bounds__(NT) k_lf_z0(const LanFusedArgs<R>* __restrict__ A) {
+  using C = cplx<R>;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tw = buf + N * LN;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  fz::cp_async_wait_all();
+  __syncthreads();
+  fz::dif<C, N, LN, 1, LN, NT, PV>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  for (int i = threadIdx.x; i < N * LN; i += NT) {
+    const int p = i / LN, r = i - p * LN, f = r / TM, c = r - f * TM;
+    const C v = buf[i];
+    C o = mk((R)((double)v.x * s), (R)((double)v.y * s));
+    if (f == V && p == 0 && m0 + c == 0) o = mk((R)0, (R)0);  // dc has no k = 0 mode
+    C* dst = (f < V) ? a.Keta + f * NK : a.Kc;
+    dst[p * PL + m0 + c] = o;
+  }
+}
+
+// ------------------------------------------------------------------ Z1
+template <typename R, int N, int V, int PV, int TM>
+__global__ void __launch_bounds__(NT) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
+  using C = cplx<R>;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
+  C* ks = buf + N * LN;  // dc^ state tile [N][TM]
+  C* tw = ks + N * TM;
+  __shared__ LanFusedConst F;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
+  tile_load<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
+  for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  fz::cp_async_wait_all();
+  __syncthreads();
+  fz::dif<C, N, V * TM, 1, LN, NT, PV>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  double fint = 0, elen = 0;
+  for (int i = threadIdx.x; i < N * TM; i += NT) {
+    const int p = i / TM, c = i - p * TM;
+    const int64_t m = m0 + c;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+    double av[3], b[3];
+    kvec_n<N>(kx, ky, kz, av, b);
+    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    C* e = buf + p * LN + c;
+    double tr[V], ti[V], str = 0, sti = 0;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      tr[v] = (double)e[v * TM].x * s;
+      ti[v] = (double)e[v * TM].y * s;
+      str += tr[v];
+      sti += ti[v];
+    }
+    if (a.rec_theta) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) a.rec_theta[v * NK + p * PL + m] = mk((R)tr[v], (R)ti[v]);
+    }
+    C* kc = ks + p * TM + c;
+    const C cs = *kc;
+    const double cr = (double)cs.x, ci = (double)cs.y;
+    const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+    if (a.energy) fint += 0.5 * w * F.kappa_c * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci);
+    // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
+    double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+    if (a.homog && !k0) {
+      double Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * F.sig0[v][q]; Si[q] += ti[v] * F.sig0[v][q]; }
+      // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
+      const double t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
+      const double t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
+      const double t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
+      const double Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
+      const double Kv[6] = {av[0] * av[0], av[1] * av[1], av[2] * av[2], b[1] * b[2], b[0] * b[2], b[0] * b[1]};
+      double Qs[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        double acc = 0;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
+        Qs[q] = acc;
+      }
+      // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
+      const double qa = Qs[0], qb = Qs[1], qc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+      const double i00 = qb * qc - qf * qf, i01 = qe * qf - qc * qd, i02 = qd * qf - qb * qe;
+      const double i11 = qa * qc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+      const double det = qa * i00 + qd * i01 + qe * i02;
+      if (det == 0.0) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
+      const double rd = 1.0 / det;
+      const double Qi[3][3] = {{i00 * rd, i01 * rd, i02 * rd}, {i01 * rd, i11 * rd, i12 * rd}, {i02 * rd, i12 * rd, i22 * rd}};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
+        ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      double pr = 0, pi = 0;
+      if (a.homog && !k0) {
+        const double* sg = F.sig0[v];
+        const double sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
+        const double sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
+        const double sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
+        const double dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
+        const double di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
+        pr = -di;
+        pi = dr;
+      }
+      e[v * TM] = mk((R)pr, (R)pi);
+    }
+    if (a.homog && a.energy) {
+      // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
+      const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+      double er[6], ei[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const int ii = I1[q], jj = J1[q];
+        double gr, gi;
+        if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
+        else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
+#pragma unroll
+        for (int v = 0; v < V; ++v) { gr -= tr[v] * F.eps_eng[v][q]; gi -= ti[v] * F.eps_eng[v][q]; }
+        if (k0) gr += F.ebar_eng[q];
+        er[q] = gr;
+        ei[q] = gi;
+      }
+      double qq = 0;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        double cr2 = 0, ci2 = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) { cr2 += F.c0m[r + j * 6] * er[j]; ci2 += F.c0m[r + j * 6] * ei[j]; }
+        qq += er[r] * cr2 + ei[r] * ci2;
+      }
+      elen += 0.5 * w * qq;
+    }
+    // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
+    double nr = 0, ni = 0;
+    if (!k0) {
+      const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+      const double mr = F.lan_a * cr - 0.5 * F.lan_b * str, mi = F.lan_a * ci - 0.5 * F.lan_b * sti;
+      const double den = 1.0 + F.dm * F.kappa_c * k2 * k2;
+      nr = (cr - F.dm * k2 * mr) / den;
+      ni = (ci - F.dm * k2 * mi) / den;
+    }
+    const C cn = mk((R)nr, (R)ni);
+    *kc = cn;
+    e[V * TM] = cn;
+  }
+  __syncthreads();
+  tile_store<C, N, TM>(ks, TM, 0, a.Kc_out, NK, PL, m0, 1);
+  fz::dit<C, N, LN, 1, LN, NT, PV>(buf, tw);
+  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
+  block_reduce_store(fint, 0, a.partials + LQ_FINT * PSTRIDE + blockIdx.x);
+  block_reduce_store(elen, 0, a.partials + LQ_ELEN * PSTRIDE + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ PB
+// Pointwise inputs (eta_0..V-1 and dc of this plane) stream through a two-deep
+// cp.async pipeline of PB_CH-row chunks; the first two chunks load during the
+// inverse transform.  Block (f, z): g_f of plane z -> forward transform.
+constexpr int PB_CH = 8;
+
+template <typename R, int N, int PV, int NTP>
+constexpr size_t pb_smem(int V) {
+  return fz::Plane<R, N, NTP, PV>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
+}
+
+template <typename R, int N, int PV, int NTP>
+__global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict__ A, int V) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  using C = cplx<R>;
+  constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR]
+  // field index fastest: the V+1 blocks of one plane, which read the same eta and
+  // dc planes, are resident together and share those reads through L2
+  const int f = blockIdx.x, z = blockIdx.y;
+  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
+  const int NFI = V + 1;
+  auto issue = [&](int k) {
+    R* dst = stg + (k & 1) * NFI * CHR;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < NFI * (CHR / PER); i += NTP) {
+      const int q = i / (CHR / PER), r = (i - q * (CHR / PER)) * PER;
+      const R* src = (q < V ? a.eta + q * N3 : a.c) + z * PL + (int64_t)k * CHR + r;
+      fz::cp_async16(dst + q * CHR + r, src);
+    }
+    fz::cp_async_commit();
+  };
+  C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
+  P::load_m(buf, mp);
+  fz::cp_async_commit();
+  issue(0);
+  issue(1);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_group<2>();
+  __syncthreads();
+  P::inverse(buf, tws);
+  if (a.rec_phi) {
+    R* dst = a.rec_phi + f * N3 + z * PL;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+      const int y = i / P::LX, n = i - y * P::LX;
+      ((C*)(dst + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
+    }
+  }
+  const LanFusedConst& F = *a.F;
+  {
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+      if (k + 1 < NCH) fz::cp_async_wait_group<1>();
+      else fz::cp_async_wait_group<0>();
+      __syncthreads();
+      const R* sb = stg + (k & 1) * NFI * CHR;
+#pragma unroll 1
+      for (int i = threadIdx.x; i < CH * P::LX; i += NTP) {
+        const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
+        double e[2][4], s2[2] = {0, 0};
+        for (int q = 0; q < V; ++q) {
+          const C ev = ((const C*)(sb + q * CHR + yl * N))[n];
+          e[0][q] = ev.x;
+          e[1][q] = ev.y;
+          s2[0] += e[0][q] * e[0][q];
+          s2[1] += e[1][q] * e[1][q];
+        }
+        const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
+        const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
+        {
+          const C ph = buf[y * P::PITCH + n];
+          const double phv[2] = {(double)ph.x, (double)ph.y};
+          double out[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const double ev = e[h][f], e2 = ev * ev;
+            double g = F.lan_b * (F.lan_c2 - cv[h]) * ev - F.lan_c * e2 * ev + F.lan_d * e2 * e2 * ev +
+                       4.0 * F.cross_w * ev * (s2[h] - e2);
+            if (a.homog) {
+              double sacc = F.sig0_ebar[f] + phv[h];
+              for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
+              g += -2.0 * ev * sacc;
+            }
+            out[h] = g;
+          }
+          buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
+        }
+      }
+      __syncthreads();
+      if (k + 2 < NCH) issue(k + 2);
+    }
+  }
+  P::forward(buf, tws);
+  P::store_m(buf, mp);
+}
+
+// ------------------------------------------------------------------ Z2
+template <typename R, int N, int V, int PV, int TM>
+__global__ void __launch_bounds__(NT) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
+  using C = cplx<R>;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  constexpr int NXH = N / 2 + 1, LN = V * TM;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* ks = buf + N * LN;  // eta^ state tiles [N][V][TM]
+  C* tw = ks + N * LN;
+  __shared__ double g[V][9];
+  __shared__ double dtl;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
+  tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
+  for (int i = threadIdx.x; i < V * 9; i += NT) g[i / 9][i % 9] = a.F->g[i / 9][i % 9];
+  if (threadIdx.x == 0) dtl = a.F->dtl;
+  for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  fz::cp_async_wait_all();
+  __syncthreads();
+  fz::dif<C, N, LN, 1, LN, NT, PV>(buf, tw);
+  const double s = 1.0 / ((double)N * N * N);
+  double fint = 0;
+  for (int i = threadIdx.x; i < N * TM; i += NT) {
+    const int p = i / TM, c = i - p * TM;
+    const int64_t m = m0 + c;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+    double av[3], b[3];
+    kvec_n<N>(kx, ky, kz, av, b);
+    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    C* e = buf + p * LN + c;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double* gv = g[v];
+      C* kst = ks + p * LN + v * TM + c;
+      const C st = *kst;
+      const double hr = (double)st.x, hi = (double)st.y;
+      if (a.energy) {
+        const double kb = gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
+                          (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+        fint += 0.5 * w * kb * (hr * hr + hi * hi);
+      }
+      const double kk = gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] +
+                        (gv[3] + gv[1]) * b[0] * b[1] + (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+      const double rden = 1.0 / (1.0 + dtl * kk);
+      const double nr = (hr - dtl * s * (double)e[v * TM].x) * rden;
+      const double ni = (hi - dtl * s * (double)e[v * TM].y) * rden;
+      const C o = mk((R)nr, (R)ni);
+      *kst = o;
+      e[v * TM] = o;
+    }
+  }
+  __syncthreads();
+  tile_store<C, N, TM>(ks, LN, 0, a.Keta_out, NK, PL, m0, V);
+  fz::dit<C, N, LN, 1, LN, NT, PV>(buf, tw);
+  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
+  block_reduce_store(fint, 0, a.partials + Q_FINT2 * PSTRIDE + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ PI
+// Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
+// -> real, concentration statistics.
+template <typename R, int N, int PV, int NTP>
+__global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x, f = blockIdx.y;
+  constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
+  P::load_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  fz::cp_async_wait_all();
+  __syncthreads();
+  P::inverse(buf, tws);
+  R* dst = (f < V) ? a.eta_next + f * N3 + z * PL : a.c_next + z * PL;
+  double emax = 0.0, s2 = 0.0, cmin = 1.0, cmax = 0.0, csum = 0.0;
+  const double cbar = a.F->cbar;
+#pragma unroll 1
+  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const C v = buf[y * P::PITCH + n];
+    ((C*)(dst + (int64_t)y * N))[n] = v;
+    if (f < V) {
+      emax = fmax(emax, fmax((double)v.x, (double)v.y));
+      s2 += (double)v.x * v.x + (double)v.y * v.y;
+    } else {
+      const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
+      cmin = fmin(cmin, fmin(c0, c1));
+      cmax = fmax(cmax, fmax(c0, c1));
+      csum += c0 + c1;
+    }
+  }
+  const int blk = z * (V + 1) + f;
+  block_reduce_store(emax, 1, a.partials + LQ_PHIMAX * PSTRIDE + blk);
+  block_reduce_store(s2, 0, a.partials + LQ_SOLID * PSTRIDE + blk);
+  block_reduce_store(cmin, 2, a.partials + LQ_CMIN * PSTRIDE + blk);
+  block_reduce_store(cmax, 1, a.partials + LQ_CMAX * PSTRIDE + blk);
+  block_reduce_store(csum, 0, a.partials + LQ_CSUM * PSTRIDE + blk);
+}
+
+// ------------------------------------------------------------------ FCH
+// bulk free energy of the start-of-step fields (all eta and dc), streamed with
+// 16-byte loads over the whole grid
+template <typename R>
+__global__ void __launch_bounds__(256) k_lf_fch(const LanFusedArgs<R>* __restrict__ A, int V, int64_t n3) {
+  using V4 = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
+  const LanFusedArgs<R>& a = A[blockIdx.z];
+  constexpr int PER = 16 / sizeof(R);
+  const LanFusedConst& F = *a.F;
+  double fch = 0;
+  const int64_t nv = n3 / PER;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+    R e[4][PER], d[PER];
+    {
+      const V4 t = ((const V4*)a.c)[i];
+      const R* tp = (const R*)&t;
+#pragma unroll
+      for (int h = 0; h < PER; ++h) d[h] = tp[h];
+    }
+    for (int q = 0; q < V; ++q) {
+      const V4 t = ((const V4*)(a.eta + q * n3))[i];
+      const R* tp = (const R*)&t;
+#pragma unroll
+      for (int h = 0; h < PER; ++h) e[q][h] = tp[h];
+    }
+#pragma unroll
+    for (int h = 0; h < PER; ++h) {
+      double s2 = 0, s4 = 0, s6 = 0;
+      for (int q = 0; q < V; ++q) {
+        const double e2 = (double)e[q][h] * (double)e[q][h];
+        s2 += e2;
+        s4 += e2 * e2;
+        s6 += e2 * e2 * e2;
+      }
+      const double cv = F.cbar + (double)d[h];
+      fch += 0.5 * F.lan_a * (cv - F.lan_c1) * (cv - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv) * s2 - 0.25 * F.lan_c * s4 +
+             F.lan_d / 6.0 * s6 + F.cross_w * (s2 * s2 - s4);
+    }
+  }
+  block_reduce_store(fch, 0, a.partials + LQ_FCH * PSTRIDE + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ launch sequence
+struct Scope {
+  LaunchHook* h;
+  cudaStream_t st;
+  Scope(LaunchHook* h_, const char* n, double b, cudaStream_t s) : h(h_), st(s) {
+    if (h) h->begin(n, b, st);
+  }
+  ~Scope() {
+    if (h) h->end(st);
+  }
+};
+
+template <typename K>
+void ensure_smem(K fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static thread_local std::vector<const void*> done;
+  for (const void* f : done)
+    if (f == (const void*)fn) return;
+  int dev = 0, optin = 0;
+  MEU_CUDA(cudaGetDevice(&dev));
+  MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  MEU_CUDA(cudaFuncGetAttributes(&fa, (const void*)fn));
+  const int lim = optin - (int)fa.sharedSizeBytes;
+  if ((int)bytes > lim) throw CudaError("fused tile exceeds shared memory", MEU_ERR_UNSUPPORTED);
+  MEU_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  done.push_back((const void*)fn);
+}
+
+// blocks of the bulk-energy reduction for an N^3 grid
+template <typename R, int N>
+constexpr int fch_blocks() {
+  constexpr int64_t vec = (int64_t)N * N * N / (16 / sizeof(R));
+  constexpr int64_t b = (vec + 255) / 256;
+  return b < FCH_MAX_BLOCKS ? (int)b : FCH_MAX_BLOCKS;
+}
+
+template <typename R, int N, int V, int PV, int NTP, int TM>
+void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st, LaunchHook* hook, int* nb) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  using C = cplx<R>;
+  constexpr int NXH = N / 2 + 1;
+  constexpr int tiles = N * NXH / TM;
+  static_assert(N * NXH % TM == 0 && tiles <= PSTRIDE, "column tiling");
+  constexpr int FB = fch_blocks<R, N>();
+  const double mm = (double)members;
+  const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
+  const size_t sp = P::smem_bytes();
+  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + (size_t)N * TM + N * Tw<C>::K);
+  const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
+  const size_t spb = pb_smem<R, N, PV, NTP>(V);
+  ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
+  ensure_smem(k_lf_pb<R, N, PV, NTP>, spb);
+  ensure_smem(k_lf_pi<R, N, PV, NTP>, sp);
+  ensure_smem(k_lf_z1<R, N, V, PV, TM>, s1);
+  ensure_smem(k_lf_z2<R, N, V, PV, TM>, s2);
+  {
+    Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
+    k_lf_pf<R, N, PV, NTP><<<dim3(N, V, members), NTP, sp, st>>>(dA, V, 0);
+    MEU_CHECK_LAUNCH();
+  }
+  if (energy) {
+    Scope s(hook, "lf_bulk_energy", (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_fch<R><<<dim3(FB, 1, members), 256, 0, st>>>(dA, V, (int64_t)N * N * N);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_z_green_ch", (2.0 * V + 3) * nk * sizeof(C), st);
+    k_lf_z1<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s1, st>>>(dA);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pb<R, N, PV, NTP><<<dim3(V, N, members), NTP, spb, st>>>(dA, V);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_z_tdgl", 4.0 * V * nk * sizeof(C), st);
+    k_lf_z2<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s2, st>>>(dA);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_plane_inv_stats", (V + 1.0) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pi<R, N, PV, NTP><<<dim3(N, V + 1, members), NTP, sp, st>>>(dA, V);
+    MEU_CHECK_LAUNCH();
+  }
+  for (int q = 0; q < Q_TOTAL; ++q) nb[q] = 0;
+  nb[Q_FCH] = energy ? FB : 0;
+  nb[Q_FINT] = tiles;
+  nb[Q_ELEN] = tiles;
+  nb[Q_FINT2] = tiles;
+  nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * (V + 1);
+}
+
+template <typename R, int N, int V, int PV, int NTP, int TM>
+void run_init(const LanFusedArgs<R>* dA, int members, cudaStream_t st, LaunchHook* hook) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  using C = cplx<R>;
+  constexpr int NXH = N / 2 + 1;
+  constexpr int tiles = N * NXH / TM;
+  const size_t sp = P::smem_bytes();
+  const size_t s0 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
+  ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
+  ensure_smem(k_lf_z0<R, N, V, PV, TM>, s0);
+  const double mm = (double)members;
+  const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
+  {
+    Scope s(hook, "lf_plane_fwd_state", (V + 1.0) * (nk * sizeof(C) + n3 * sizeof(R)), st);
+    k_lf_pf<R, N, PV, NTP><<<dim3(N, V + 1, members), NTP, sp, st>>>(dA, V, 1);
+    MEU_CHECK_LAUNCH();
+  }
+  {
+    Scope s(hook, "lf_z_state", 2.0 * (V + 1) * nk * sizeof(C), st);
+    k_lf_z0<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s0, st>>>(dA);
+    MEU_CHECK_LAUNCH();
+  }
+}
+
+// column tile widths instantiated: T1 (default) and T0 = T1 / 2
+template <typename R> constexpr int tm_wide() { return col_tile_default<R>(); }
+template <typename R> constexpr int tm_narrow() { return col_tile_default<R>() / 2; }
+template <typename R, int N, int TM> constexpr bool tm_ok() { return (N * (N / 2 + 1)) % TM == 0 && N * (N / 2 + 1) / TM <= PSTRIDE; }
+
+// Calls f.template operator()<V, PV, NTP, TM>() for the schedule s; false when
+// s names no instantiated variant.
+template <typename R, int N, int V, typename Fn>
+bool with_sched_v(const LanSched& s, Fn&& f) {
+  const int tm = s.tm ? s.tm : tm_wide<R>();
+  auto pick_tm = [&](auto pv_c, auto ntp_c) -> bool {
+    constexpr int PV = decltype(pv_c)::value, NTP = decltype(ntp_c)::value;
+    if (tm == tm_wide<R>()) {
+      if constexpr (tm_ok<R, N, tm_wide<R>()>()) { f.template operator()<V, PV, NTP, tm_wide<R>()>(); return true; }
+    } else if (tm == tm_narrow<R>()) {
+      if constexpr (tm_ok<R, N, tm_narrow<R>()>()) { f.template operator()<V, PV, NTP, tm_narrow<R>()>(); return true; }
+    }
+    return false;
+  };
+  using I0 = std::integral_constant<int, 0>;
+  using I1 = std::integral_constant<int, 1>;
+  using T256 = std::integral_constant<int, 256>;
+  using T512 = std::integral_constant<int, 512>;
+  if (s.pv == 0 && s.ntp == 512) return pick_tm(I0{}, T512{});
+  if (s.pv == 0 && s.ntp == 256) return pick_tm(I0{}, T256{});
+  if (s.pv == 1 && s.ntp == 512) return pick_tm(I1{}, T512{});
+  if (s.pv == 1 && s.ntp == 256) return pick_tm(I1{}, T256{});
+  return false;
+}
+template <typename R, int N, typename Fn>
+bool with_sched(int V, const LanSched& s, Fn&& f) {
+  switch (V) {
+    case 1: return with_sched_v<R, N, 1>(s, f);
+    case 2: return with_sched_v<R, N, 2>(s, f);
+    case 3: return with_sched_v<R, N, 3>(s, f);
+    case 4: return with_sched_v<R, N, 4>(s, f);
+    default: return false;
+  }
+}
+
+}  // namespace lf
+
+namespace lf {
+template <typename R, int N>
+struct StepFn {
+  const LanFusedArgs<R>* dA;
+  int members;
+  bool energy;
+  cudaStream_t st;
+  LaunchHook* hook;
+  int* nb;
+  template <int V, int PV, int NTP, int TM>
+  void operator()() const {
+    run_step<R, N, V, PV, NTP, TM>(dA, members, energy, st, hook, nb);
+  }
+};
+template <typename R, int N>
+struct InitFn {
+  const LanFusedArgs<R>* dA;
+  int members;
+  cudaStream_t st;
+  LaunchHook* hook;
+  template <int V, int PV, int NTP, int TM>
+  void operator()() const {
+    run_init<R, N, V, PV, NTP, TM>(dA, members, st, hook);
+  }
+};
+}  // namespace lf
+
+template <typename R, int N>
+bool lf_step_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st,
+               LaunchHook* hook, int* nb) {
+  return lf::with_sched<R, N>(V, s, lf::StepFn<R, N>{dA, members, energy, st, hook, nb});
+}
+template <typename R, int N>
+bool lf_init_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st, LaunchHook* hook) {
+  return lf::with_sched<R, N>(V, s, lf::InitFn<R, N>{dA, members, st, hook});
+}
+
+}  // namespace meu
+
+// one translation unit per (R, N)
+#define MEU_LF_INSTANTIATE(R, N)                                                                                    \
+  template bool meu::lf_step_n<R, N>(int, const meu::LanSched&, const meu::LanFusedArgs<R>*, int, bool, cudaStream_t, \
+                                     meu::LaunchHook*, int*);                                                       \
+  template bool meu::lf_init_n<R, N>(int, const meu::LanSched&, const meu::LanFusedArgs<R>*, int, cudaStream_t,      \
+                                     meu::LaunchHook*);

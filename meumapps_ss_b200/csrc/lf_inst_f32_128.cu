@@ -1,0 +1,3 @@
+// Fused Landau step kernels for 128^3 grids in float (all variant counts and schedules).
+#include "landau_fused_kernels.cuh"
+MEU_LF_INSTANTIATE(float, 128)

@@ -33,6 +33,7 @@ ELAST_HETERO = 2
 EIG_ETA2 = 0
 EIG_H = 1
 FLAG_GENERIC = 1
+FLAG_AUTOTUNE = 2
 
 
 class MeuParams(C.Structure):

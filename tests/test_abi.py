@@ -48,3 +48,12 @@ def test_bad_arguments_fail_without_gpu():
     assert L.meu_run(None, 1, None) == 100
     assert L.meu_destroy(None) == 100
     assert L.meu_get_step(None) == -1
+
+
+def test_ensemble_bad_arguments():
+    L = _lib.lib()
+    h = C.c_void_p()
+    assert L.meu_ensemble_create(0, None, 0, C.byref(h)) == 100  # MEU_ERR_BADARG
+    assert L.meu_ensemble_run(None, 1, None) == 100  # MEU_ERR_BADARG
+    assert L.meu_ensemble_get_step(None) == -1
+    assert L.meu_set_schedule(None, None) == 100  # MEU_ERR_BADARG
