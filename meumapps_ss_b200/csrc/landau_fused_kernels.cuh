@@ -61,7 +61,7 @@ __device__ __forceinline__ void tile_store(const C* buf, int LN, int slot0, C* G
 template <typename R, int N, int PV, int NTP>
 __global__ void __launch_bounds__(NTP) k_lf_pf(const LanFusedArgs<R>* __restrict__ A, int V, int raw) {
   using P = fz::Plane<R, N, NTP, PV>;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(NTP) k_lf_pf(const LanFusedArgs<R>* __restrict
 template <typename R, int N, int V, int PV, int TM>
 __global__ void __launch_bounds__(NT) k_lf_z0(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -117,9 +117,9 @@ __global__ void __launch_bounds__(NT) k_lf_z0(const LanFusedArgs<R>* __restrict_
 
 // ------------------------------------------------------------------ Z1
 template <typename R, int N, int V, int PV, int TM>
-__global__ void __launch_bounds__(NT) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
+__global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -272,10 +272,10 @@ constexpr size_t pb_smem(int V) {
   return fz::Plane<R, N, NTP, PV>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
 }
 
-template <typename R, int N, int PV, int NTP>
-__global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict__ A, int V) {
+template <typename R, int N, int V, int PV, int NTP>
+__global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
   using P = fz::Plane<R, N, NTP, PV>;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
   constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
   // dc planes, are resident together and share those reads through L2
   const int f = blockIdx.x, z = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  const int NFI = V + 1;
+  constexpr int NFI = V + 1;
   auto issue = [&](int k) {
     R* dst = stg + (k & 1) * NFI * CHR;
 #pragma unroll 1
@@ -314,7 +314,14 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
       ((C*)(dst + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
     }
   }
+  // constants of the driving force in registers
   const LanFusedConst& F = *a.F;
+  const double cbar = F.cbar, lb = F.lan_b, lc2 = F.lan_c2, lc = F.lan_c, ld = F.lan_d, cw4 = 4.0 * F.cross_w;
+  const double s0f = F.sig0_ebar[f];
+  double Af[V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) Af[q] = F.A[f][q];
+  const bool homog = a.homog != 0;
   {
 #pragma unroll 1
     for (int k = 0; k < NCH; ++k) {
@@ -325,28 +332,31 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
 #pragma unroll 1
       for (int i = threadIdx.x; i < CH * P::LX; i += NTP) {
         const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
-        double e[2][4], s2[2] = {0, 0};
+        double e2q[2][V], s2[2] = {0, 0}, ef[2];
+#pragma unroll
         for (int q = 0; q < V; ++q) {
           const C ev = ((const C*)(sb + q * CHR + yl * N))[n];
-          e[0][q] = ev.x;
-          e[1][q] = ev.y;
-          s2[0] += e[0][q] * e[0][q];
-          s2[1] += e[1][q] * e[1][q];
+          const double x = ev.x, yv = ev.y;
+          e2q[0][q] = x * x;
+          e2q[1][q] = yv * yv;
+          s2[0] += e2q[0][q];
+          s2[1] += e2q[1][q];
+          if (q == f) { ef[0] = x; ef[1] = yv; }
         }
         const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
-        const double cv[2] = {F.cbar + (double)dcv.x, F.cbar + (double)dcv.y};
+        const double cv[2] = {cbar + (double)dcv.x, cbar + (double)dcv.y};
         {
           const C ph = buf[y * P::PITCH + n];
           const double phv[2] = {(double)ph.x, (double)ph.y};
           double out[2];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const double ev = e[h][f], e2 = ev * ev;
-            double g = F.lan_b * (F.lan_c2 - cv[h]) * ev - F.lan_c * e2 * ev + F.lan_d * e2 * e2 * ev +
-                       4.0 * F.cross_w * ev * (s2[h] - e2);
-            if (a.homog) {
-              double sacc = F.sig0_ebar[f] + phv[h];
-              for (int q = 0; q < V; ++q) sacc -= F.A[f][q] * e[h][q] * e[h][q];
+            const double ev = ef[h], e2 = ev * ev;
+            double g = lb * (lc2 - cv[h]) * ev - lc * e2 * ev + ld * e2 * e2 * ev + cw4 * ev * (s2[h] - e2);
+            if (homog) {
+              double sacc = s0f + phv[h];
+#pragma unroll
+              for (int q = 0; q < V; ++q) sacc -= Af[q] * e2q[h][q];
               g += -2.0 * ev * sacc;
             }
             out[h] = g;
@@ -364,9 +374,9 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
 
 // ------------------------------------------------------------------ Z2
 template <typename R, int N, int V, int PV, int TM>
-__global__ void __launch_bounds__(NT) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
+__global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NXH = N / 2 + 1, LN = V * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -429,7 +439,7 @@ __global__ void __launch_bounds__(NT) k_lf_z2(const LanFusedArgs<R>* __restrict_
 template <typename R, int N, int PV, int NTP>
 __global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V) {
   using P = fz::Plane<R, N, NTP, PV>;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict
 template <typename R>
 __global__ void __launch_bounds__(256) k_lf_fch(const LanFusedArgs<R>* __restrict__ A, int V, int64_t n3) {
   using V4 = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
-  const LanFusedArgs<R>& a = A[blockIdx.z];
+  const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int PER = 16 / sizeof(R);
   const LanFusedConst& F = *a.F;
   double fch = 0;
@@ -561,7 +571,7 @@ void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t 
   const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
   const size_t spb = pb_smem<R, N, PV, NTP>(V);
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
-  ensure_smem(k_lf_pb<R, N, PV, NTP>, spb);
+  ensure_smem(k_lf_pb<R, N, V, PV, NTP>, spb);
   ensure_smem(k_lf_pi<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_z1<R, N, V, PV, TM>, s1);
   ensure_smem(k_lf_z2<R, N, V, PV, TM>, s2);
@@ -582,7 +592,7 @@ void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t 
   }
   {
     Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pb<R, N, PV, NTP><<<dim3(V, N, members), NTP, spb, st>>>(dA, V);
+    k_lf_pb<R, N, V, PV, NTP><<<dim3(V, N, members), NTP, spb, st>>>(dA);
     MEU_CHECK_LAUNCH();
   }
   {
