@@ -29,6 +29,28 @@ __device__ __forceinline__ void kvec_n(int kx, int ky, int kz, double a[3], doub
   }
 }
 
+// the same k-vectors in the working precision W of the step (float for FP32 fields)
+template <int N, typename W>
+__device__ __forceinline__ void kvec_w(int kx, int ky, int kz, W a[3], W b[3]) {
+  const int m[3] = {kx, ky, kz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int mm = (m[d] <= N / 2) ? m[d] : m[d] - N;
+    a[d] = (W)mm * (W)(TWO_PI / (double)N);
+    b[d] = (2 * m[d] == N) ? (W)0 : a[d];
+  }
+}
+
+// x * r for a per-step damping factor r computed in FP64.  The factor multiplies
+// the state every step, so in FP32 it is applied as r_hi + r_lo (a rounded
+// factor would bias every mode the same way each step and the bias would compound).
+template <typename W>
+struct Damp {
+  W hi, lo;
+  __device__ __forceinline__ explicit Damp(double r) : hi((W)r), lo((W)(r - (double)(W)r)) {}
+  __device__ __forceinline__ W operator()(W x) const { return x * hi + x * lo; }
+};
+
 template <typename R> constexpr int col_tile_default() { return sizeof(R) == 4 ? 16 : 8; }
 
 // Column tile of nf fields: smem [z][slot][TM] with LN complex per z row, global
@@ -126,31 +148,47 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
   C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
   C* ks = buf + N * LN;  // dc^ state tile [N][TM]
   C* tw = ks + N * TM;
-  __shared__ LanFusedConst F;
+  // FP64 only for Omega(k) = Q^-1; every other k-space product in the field precision W
+  using W = R;
+  __shared__ double qc[6][6];
+  __shared__ W sgW[V][6], epW[V][6], c0W[36], ebW[6];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
   tile_load<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
-  for (int i = threadIdx.x; i < (int)(sizeof(LanFusedConst) / 8); i += NT) ((double*)&F)[i] = ((const double*)a.F)[i];
+  {
+    const LanFusedConst& G = *a.F;
+    for (int i = threadIdx.x; i < 36; i += NT) {
+      qc[i / 6][i % 6] = G.qcoef[i / 6][i % 6];
+      c0W[i] = (W)G.c0m[i];
+    }
+    for (int i = threadIdx.x; i < V * 6; i += NT) {
+      sgW[i / 6][i % 6] = (W)G.sig0[i / 6][i % 6];
+      epW[i / 6][i % 6] = (W)G.eps_eng[i / 6][i % 6];
+    }
+    if (threadIdx.x < 6) ebW[threadIdx.x] = (W)G.ebar_eng[threadIdx.x];
+  }
+  const double kapcd = a.F->kappa_c, dmd = a.F->dm;
+  const W kapc = (W)kapcd, lan_a = (W)a.F->lan_a, hlb = (W)(0.5 * a.F->lan_b);
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   fz::cp_async_wait_all();
   __syncthreads();
   fz::dif<C, N, V * TM, 1, LN, NT, PV>(buf, tw);
-  const double s = 1.0 / ((double)N * N * N);
+  const W s = (W)(1.0 / ((double)N * N * N));
   double fint = 0, elen = 0;
   for (int i = threadIdx.x; i < N * TM; i += NT) {
     const int p = i / TM, c = i - p * TM;
     const int64_t m = m0 + c;
     const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
     const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
-    double av[3], b[3];
-    kvec_n<N>(kx, ky, kz, av, b);
-    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    W av[3], b[3];
+    kvec_w<N, W>(kx, ky, kz, av, b);
+    const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
     C* e = buf + p * LN + c;
-    double tr[V], ti[V], str = 0, sti = 0;
+    W tr[V], ti[V], str = 0, sti = 0;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      tr[v] = (double)e[v * TM].x * s;
-      ti[v] = (double)e[v * TM].y * s;
+      tr[v] = (W)e[v * TM].x * s;
+      ti[v] = (W)e[v * TM].y * s;
       str += tr[v];
       sti += ti[v];
     }
@@ -160,39 +198,44 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     }
     C* kc = ks + p * TM + c;
     const C cs = *kc;
-    const double cr = (double)cs.x, ci = (double)cs.y;
+    const W cr = (W)cs.x, ci = (W)cs.y;
     const bool k0 = (kx == 0 && ky == 0 && kz == 0);
-    if (a.energy) fint += 0.5 * w * F.kappa_c * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci);
+    if (a.energy) fint += (double)((W)0.5 * w * kapc * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci));
     // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
-    double ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+    W ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
     if (a.homog && !k0) {
-      double Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
+      W Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
       for (int v = 0; v < V; ++v)
 #pragma unroll
-        for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * F.sig0[v][q]; Si[q] += ti[v] * F.sig0[v][q]; }
+        for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * sgW[v][q]; Si[q] += ti[v] * sgW[v][q]; }
       // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
-      const double t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
-      const double t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
-      const double t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
-      const double Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
-      const double Kv[6] = {av[0] * av[0], av[1] * av[1], av[2] * av[2], b[1] * b[2], b[0] * b[2], b[0] * b[1]};
+      const W t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
+      const W t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
+      const W t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
+      const W Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
+      // Omega(k) in FP64 from the double k-vectors
+      double ad[3], bd[3];
+      kvec_n<N>(kx, ky, kz, ad, bd);
+      const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
       double Qs[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         double acc = 0;
 #pragma unroll
-        for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
+        for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
         Qs[q] = acc;
       }
       // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
-      const double qa = Qs[0], qb = Qs[1], qc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
-      const double i00 = qb * qc - qf * qf, i01 = qe * qf - qc * qd, i02 = qd * qf - qb * qe;
-      const double i11 = qa * qc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+      const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+      const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
+      const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
       const double det = qa * i00 + qd * i01 + qe * i02;
       if (det == 0.0) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
       const double rd = 1.0 / det;
-      const double Qi[3][3] = {{i00 * rd, i01 * rd, i02 * rd}, {i01 * rd, i11 * rd, i12 * rd}, {i02 * rd, i12 * rd, i22 * rd}};
+      const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
+                          {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
+                          {(W)(i02 * rd), (W)(i12 * rd), (W)(i22 * rd)}};
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
@@ -201,14 +244,14 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     }
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      double pr = 0, pi = 0;
+      W pr = 0, pi = 0;
       if (a.homog && !k0) {
-        const double* sg = F.sig0[v];
-        const double sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
-        const double sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
-        const double sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
-        const double dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
-        const double di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
+        const W* sg = sgW[v];
+        const W sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
+        const W sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
+        const W sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
+        const W dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
+        const W di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
         pr = -di;
         pi = dr;
       }
@@ -217,37 +260,40 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     if (a.homog && a.energy) {
       // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
       const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
-      double er[6], ei[6];
+      W er[6], ei[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         const int ii = I1[q], jj = J1[q];
-        double gr, gi;
+        W gr, gi;
         if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
         else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
 #pragma unroll
-        for (int v = 0; v < V; ++v) { gr -= tr[v] * F.eps_eng[v][q]; gi -= ti[v] * F.eps_eng[v][q]; }
-        if (k0) gr += F.ebar_eng[q];
+        for (int v = 0; v < V; ++v) { gr -= tr[v] * epW[v][q]; gi -= ti[v] * epW[v][q]; }
+        if (k0) gr += ebW[q];
         er[q] = gr;
         ei[q] = gi;
       }
-      double qq = 0;
+      W qq = 0;
 #pragma unroll
       for (int r = 0; r < 6; ++r) {
-        double cr2 = 0, ci2 = 0;
+        W cr2 = 0, ci2 = 0;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) { cr2 += F.c0m[r + j * 6] * er[j]; ci2 += F.c0m[r + j * 6] * ei[j]; }
+        for (int j = 0; j < 6; ++j) { cr2 += c0W[r + j * 6] * er[j]; ci2 += c0W[r + j * 6] * ei[j]; }
         qq += er[r] * cr2 + ei[r] * ci2;
       }
-      elen += 0.5 * w * qq;
+      elen += (double)((W)0.5 * w * qq);
     }
     // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
-    double nr = 0, ni = 0;
+    W nr = 0, ni = 0;
     if (!k0) {
-      const double k2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
-      const double mr = F.lan_a * cr - 0.5 * F.lan_b * str, mi = F.lan_a * ci - 0.5 * F.lan_b * sti;
-      const double den = 1.0 + F.dm * F.kappa_c * k2 * k2;
-      nr = (cr - F.dm * k2 * mr) / den;
-      ni = (ci - F.dm * k2 * mi) / den;
+      double ad[3], bd[3];
+      kvec_n<N>(kx, ky, kz, ad, bd);
+      const double k2d = ad[0] * ad[0] + ad[1] * ad[1] + ad[2] * ad[2];
+      const Damp<W> rden(1.0 / (1.0 + dmd * kapcd * k2d * k2d));
+      const W dk2 = (W)(dmd * k2d);
+      const W mr = lan_a * cr - hlb * str, mi = lan_a * ci - hlb * sti;
+      nr = rden(cr - dk2 * mr);
+      ni = rden(ci - dk2 * mi);
     }
     const C cn = mk((R)nr, (R)ni);
     *kc = cn;
@@ -262,26 +308,37 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
 }
 
 // ------------------------------------------------------------------ PB
-// Pointwise inputs (eta_0..V-1 and dc of this plane) stream through a two-deep
-// cp.async pipeline of PB_CH-row chunks; the first two chunks load during the
-// inverse transform.  Block (f, z): g_f of plane z -> forward transform.
+// Pointwise inputs (eta_0..V-1 and dc of this plane) either stream through a
+// two-deep cp.async pipeline of PB_CH-row chunks (the first two chunks load
+// during the inverse transform), or -- when that staging buffer is what keeps
+// the kernel below 3 blocks per SM -- are read straight from global memory
+// (mostly L2) by the pointwise loop.  Block (f, z): g_f of plane z -> forward transform.
 constexpr int PB_CH = 8;
+constexpr size_t SM_SMEM = 228 * 1024, BLOCK_RESERVED = 1024;
 
-template <typename R, int N, int PV, int NTP>
-constexpr size_t pb_smem(int V) {
-  return fz::Plane<R, N, NTP, PV>::smem_bytes() + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
+template <typename R, int N, int V>
+constexpr bool pb_direct() {
+  constexpr size_t plane = fz::Plane<R, N, 512, 0>::smem_bytes();
+  constexpr size_t staged = plane + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
+  return 3 * (staged + BLOCK_RESERVED) > SM_SMEM && 3 * (plane + BLOCK_RESERVED) <= SM_SMEM;
 }
 
 template <typename R, int N, int V, int PV, int NTP>
-__global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
+constexpr size_t pb_smem() {
+  return fz::Plane<R, N, NTP, PV>::smem_bytes() + (pb_direct<R, N, V>() ? 0 : 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R));
+}
+
+template <typename R, int N, int V, int PV, int NTP>
+__global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
   using P = fz::Plane<R, N, NTP, PV>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
+  constexpr bool DIRECT = pb_direct<R, N, V>();
   constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
-  R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR]
+  R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR] (staged mode)
   // field index fastest: the V+1 blocks of one plane, which read the same eta and
   // dc planes, are resident together and share those reads through L2
   const int f = blockIdx.x, z = blockIdx.y;
@@ -300,10 +357,13 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_m(buf, mp);
   fz::cp_async_commit();
-  issue(0);
-  issue(1);
+  if constexpr (!DIRECT) {
+    issue(0);
+    issue(1);
+  }
   P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_group<2>();
+  if constexpr (DIRECT) fz::cp_async_wait_all();
+  else fz::cp_async_wait_group<2>();
   __syncthreads();
   P::inverse(buf, tws);
   if (a.rec_phi) {
@@ -314,15 +374,57 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
       ((C*)(dst + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
     }
   }
-  // constants of the driving force in registers
+  // constants of the driving force in registers; pointwise math in the field precision W
+  using W = R;
   const LanFusedConst& F = *a.F;
-  const double cbar = F.cbar, lb = F.lan_b, lc2 = F.lan_c2, lc = F.lan_c, ld = F.lan_d, cw4 = 4.0 * F.cross_w;
-  const double s0f = F.sig0_ebar[f];
-  double Af[V];
+  const W cbar = (W)F.cbar, lb = (W)F.lan_b, lc2 = (W)F.lan_c2, lc = (W)F.lan_c, ld = (W)F.lan_d;
+  const W cw4 = (W)(4.0 * F.cross_w), s0f = (W)F.sig0_ebar[f];
+  W Af[V];
 #pragma unroll
-  for (int q = 0; q < V; ++q) Af[q] = F.A[f][q];
+  for (int q = 0; q < V; ++q) Af[q] = (W)F.A[f][q];
   const bool homog = a.homog != 0;
-  {
+  // g_f at the pair (x, x+1) of row y from eta_q (q < V), dc and phi_f
+  auto point = [&](const C* ev, C dcv, C ph) -> C {
+    W e2q[2][V], s2[2] = {0, 0}, ef[2];
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      const W x = ev[q].x, yv = ev[q].y;
+      e2q[0][q] = x * x;
+      e2q[1][q] = yv * yv;
+      s2[0] += e2q[0][q];
+      s2[1] += e2q[1][q];
+      if (q == f) { ef[0] = x; ef[1] = yv; }
+    }
+    const W cv[2] = {cbar + (W)dcv.x, cbar + (W)dcv.y};
+    const W phv[2] = {(W)ph.x, (W)ph.y};
+    W out[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const W e = ef[h], e2 = e * e;
+      W g = lb * (lc2 - cv[h]) * e - lc * e2 * e + ld * e2 * e2 * e + cw4 * e * (s2[h] - e2);
+      if (homog) {
+        W sacc = s0f + phv[h];
+#pragma unroll
+        for (int q = 0; q < V; ++q) sacc -= Af[q] * e2q[h][q];
+        g += (W)-2 * e * sacc;
+      }
+      out[h] = g;
+    }
+    return mk((R)out[0], (R)out[1]);
+  };
+  if constexpr (DIRECT) {
+#pragma unroll 2
+    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+      const int y = i / P::LX, n = i - y * P::LX;
+      const int64_t g0 = z * PL + (int64_t)y * N + 2 * n;
+      C ev[V];
+#pragma unroll
+      for (int q = 0; q < V; ++q) ev[q] = *(const C*)(a.eta + q * N3 + g0);
+      const C dcv = *(const C*)(a.c + g0);
+      buf[y * P::PITCH + n] = point(ev, dcv, buf[y * P::PITCH + n]);
+    }
+    __syncthreads();
+  } else {
 #pragma unroll 1
     for (int k = 0; k < NCH; ++k) {
       if (k + 1 < NCH) fz::cp_async_wait_group<1>();
@@ -332,37 +434,11 @@ __global__ void __launch_bounds__(NTP) k_lf_pb(const LanFusedArgs<R>* __restrict
 #pragma unroll 1
       for (int i = threadIdx.x; i < CH * P::LX; i += NTP) {
         const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
-        double e2q[2][V], s2[2] = {0, 0}, ef[2];
+        C ev[V];
 #pragma unroll
-        for (int q = 0; q < V; ++q) {
-          const C ev = ((const C*)(sb + q * CHR + yl * N))[n];
-          const double x = ev.x, yv = ev.y;
-          e2q[0][q] = x * x;
-          e2q[1][q] = yv * yv;
-          s2[0] += e2q[0][q];
-          s2[1] += e2q[1][q];
-          if (q == f) { ef[0] = x; ef[1] = yv; }
-        }
+        for (int q = 0; q < V; ++q) ev[q] = ((const C*)(sb + q * CHR + yl * N))[n];
         const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
-        const double cv[2] = {cbar + (double)dcv.x, cbar + (double)dcv.y};
-        {
-          const C ph = buf[y * P::PITCH + n];
-          const double phv[2] = {(double)ph.x, (double)ph.y};
-          double out[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const double ev = ef[h], e2 = ev * ev;
-            double g = lb * (lc2 - cv[h]) * ev - lc * e2 * ev + ld * e2 * e2 * ev + cw4 * ev * (s2[h] - e2);
-            if (homog) {
-              double sacc = s0f + phv[h];
-#pragma unroll
-              for (int q = 0; q < V; ++q) sacc -= Af[q] * e2q[h][q];
-              g += -2.0 * ev * sacc;
-            }
-            out[h] = g;
-          }
-          buf[y * P::PITCH + n] = mk((R)out[0], (R)out[1]);
-        }
+        buf[y * P::PITCH + n] = point(ev, dcv, buf[y * P::PITCH + n]);
       }
       __syncthreads();
       if (k + 2 < NCH) issue(k + 2);
@@ -383,19 +459,38 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
   C* buf = (C*)smraw;
   C* ks = buf + N * LN;  // eta^ state tiles [N][V][TM]
   C* tw = ks + N * LN;
+  using W = R;  // working precision of the update (the state's)
   __shared__ double g[V][9];
-  __shared__ double dtl;
+  __shared__ int sameg;  // every variant has the gradient coefficients of variant 0
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
   tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
-  for (int i = threadIdx.x; i < V * 9; i += NT) g[i / 9][i % 9] = a.F->g[i / 9][i % 9];
-  if (threadIdx.x == 0) dtl = a.F->dtl;
+  if (threadIdx.x == 0) {
+    int same = 1;
+    for (int v = 0; v < V; ++v)
+      for (int j = 0; j < 9; ++j) {
+        g[v][j] = a.F->g[v][j];
+        same &= a.F->g[v][j] == a.F->g[0][j];
+      }
+    sameg = same;
+  }
+  const double dtld = a.F->dtl;
+  const W dtl = (W)dtld;
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   fz::cp_async_wait_all();
   __syncthreads();
   fz::dif<C, N, LN, 1, LN, NT, PV>(buf, tw);
-  const double s = 1.0 / ((double)N * N * N);
+  const W ds = dtl * (W)(1.0 / ((double)N * N * N));
+  const bool one_g = sameg != 0;
   double fint = 0;
+  auto kappa_b = [&](const double* gv, const double* b) {
+    return gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
+           (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+  };
+  auto kappa_k = [&](const double* gv, const double* av, const double* b) {
+    return gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] + (gv[3] + gv[1]) * b[0] * b[1] +
+           (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
+  };
   for (int i = threadIdx.x; i < N * TM; i += NT) {
     const int p = i / TM, c = i - p * TM;
     const int64_t m = m0 + c;
@@ -403,28 +498,29 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
     const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
     double av[3], b[3];
     kvec_n<N>(kx, ky, kz, av, b);
-    const double w = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+    const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
     C* e = buf + p * LN + c;
+    W kb0 = 0;
+    double rd0 = 0;
+    if (one_g) {
+      if (a.energy) kb0 = (W)kappa_b(g[0], b);
+      rd0 = 1.0 / (1.0 + dtld * kappa_k(g[0], av, b));
+    }
+    W fk = 0;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      const double* gv = g[v];
       C* kst = ks + p * LN + v * TM + c;
       const C st = *kst;
-      const double hr = (double)st.x, hi = (double)st.y;
-      if (a.energy) {
-        const double kb = gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
-                          (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-        fint += 0.5 * w * kb * (hr * hr + hi * hi);
-      }
-      const double kk = gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] +
-                        (gv[3] + gv[1]) * b[0] * b[1] + (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-      const double rden = 1.0 / (1.0 + dtl * kk);
-      const double nr = (hr - dtl * s * (double)e[v * TM].x) * rden;
-      const double ni = (hi - dtl * s * (double)e[v * TM].y) * rden;
+      const W hr = (W)st.x, hi = (W)st.y;
+      if (a.energy) fk += (one_g ? kb0 : (W)kappa_b(g[v], b)) * (hr * hr + hi * hi);
+      const Damp<W> rden(one_g ? rd0 : 1.0 / (1.0 + dtld * kappa_k(g[v], av, b)));
+      const W nr = rden(hr - ds * (W)e[v * TM].x);
+      const W ni = rden(hi - ds * (W)e[v * TM].y);
       const C o = mk((R)nr, (R)ni);
       *kst = o;
       e[v * TM] = o;
     }
+    if (a.energy) fint += (double)((W)0.5 * w * fk);
   }
   __syncthreads();
   tile_store<C, N, TM>(ks, LN, 0, a.Keta_out, NK, PL, m0, V);
@@ -569,7 +665,7 @@ void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t 
   const size_t sp = P::smem_bytes();
   const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + (size_t)N * TM + N * Tw<C>::K);
   const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
-  const size_t spb = pb_smem<R, N, PV, NTP>(V);
+  const size_t spb = pb_smem<R, N, V, PV, NTP>();
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_pb<R, N, V, PV, NTP>, spb);
   ensure_smem(k_lf_pi<R, N, PV, NTP>, sp);
