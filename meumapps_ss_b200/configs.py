@@ -74,6 +74,26 @@ precipitate
 """
 
 
+def tetrahedral_rotations() -> List[np.ndarray]:
+    """The 12 proper rotations of the tetrahedral group (identity, three 180 degree
+    turns about the cube axes, eight 120 degree turns about the body diagonals),
+    as the 12 orientation matrices a `sym_var.inp` file lists for 12-variant KKS
+    decks (read at ModInitials.f:200-338).  The reference ships no such file."""
+    rots = [np.eye(3)]
+    for ax in range(3):
+        m = -np.eye(3)
+        m[ax, ax] = 1.0
+        rots.append(m)
+    for sx in (1, -1):
+        for sy in (1, -1):
+            d = np.array([1.0, sx, sy]) / np.sqrt(3.0)
+            for ang in (2 * np.pi / 3, -2 * np.pi / 3):
+                k = np.array([[0, -d[2], d[1]], [d[2], 0, -d[0]], [-d[1], d[0], 0]])
+                r = np.eye(3) + np.sin(ang) * k + (1 - np.cos(ang)) * (k @ k)
+                rots.append(np.round(r, 15))
+    return rots
+
+
 def cubic(c11: float, c12: float, c44: float) -> np.ndarray:
     c = np.zeros((6, 6))
     c[0, 0], c[0, 1], c[3, 3] = c11, c12, c44

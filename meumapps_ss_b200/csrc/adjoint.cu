@@ -202,8 +202,9 @@ void Engine<R>::adjoint(int T, int K, const double* cons_tgt, const double* phi_
       MEU_CUDA(cudaMemcpyAsync(B.dFwd, &fa, sizeof(fa), cudaMemcpyHostToDevice, st));
       up_homog = hg;
     }
-    if (!lan_fused_step<R>(N, 1, sched, B.dFwd, 1, false, st, &prof, nb))
+    if (!lan_fused_step<R>(N, 1, sched, B.dFwd, 1, theta_ready ? LS_THETA_READY : 0, st, &prof, nb))
       throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+    theta_ready = true;
   }
   step = step0 + T;
   // ---- loss and seed lam_T, nu_T (real) -> spectra
@@ -248,9 +249,11 @@ void Engine<R>::adjoint(int T, int K, const double* cons_tgt, const double* phi_
       B.hRec[j] = r;
     }
     MEU_CUDA(cudaMemcpyAsync(B.dRec, B.hRec, sizeof(LanFusedArgs<R>) * S, cudaMemcpyHostToDevice, st));
+    // the segment starts from a checkpoint: its first step transforms theta itself
     for (int j = 0; j < S; ++j)
-      if (!lan_fused_step<R>(N, 1, sched, B.dRec + j, 1, false, st, &prof, nb))
+      if (!lan_fused_step<R>(N, 1, sched, B.dRec + j, 1, j ? LS_THETA_READY : 0, st, &prof, nb))
         throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
+    theta_ready = false;  // the engine's M now holds a recomputed step's theta^
     for (int m = S - 1; m >= 0; --m) {
       const int g = i0 + m;
       AdjArgs<R> a;

@@ -241,8 +241,6 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       if (std::fabs(p.cela[0][i] - p.cela[1][i]) > 1e-12 * (std::fabs(p.cela[1][i]) + 1e-300))
         throw CudaError("MEU_ELAST_HOMOG needs equal matrix and precipitate moduli", MEU_ERR_BADARG);
   }
-  if (p.model == MEU_MODEL_KKS && sizeof(R) != 8)
-    throw CudaError("the KKS model runs in plain FP64 only", MEU_ERR_UNSUPPORTED);
   // ---- buffers
   c = dalloc<R>(E * n3);
   c2 = dalloc<R>(E * n3);
@@ -341,7 +339,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     MEU_CUDA(cudaMemset(sp, 0, sizeof(C) * (size_t)NS * nk));
     if (p.flags & MEU_FLAG_AUTOTUNE) {
       sync_args();
-      sched = lan_autotune<R>(p.nx, V, dA, 1, p.diag_energy != 0, d_ops, st, nullptr);
+      sched = lan_autotune<R>(p.nx, V, dA, 1, p.diag_energy != 0, st, nullptr);
       reset_fused_state();
     }
   }
@@ -375,6 +373,7 @@ void Engine<R>::reset_fused_state() {
   MEU_CUDA(cudaMemsetAsync(d_row, 0, 2 * sizeof(int), st));
   MEU_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   MEU_CUDA(cudaStreamSynchronize(st));
+  theta_ready = false;
 }
 
 template <typename R>
@@ -445,7 +444,10 @@ void Engine<R>::set_fields(const double* cons, const double* phi_in, const doubl
     }
   }
   if (phi_in) up(phi_in, phi, V, 0);
-  if (cons || phi_in) fields_set = true;
+  if (cons || phi_in) {
+    fields_set = true;
+    theta_ready = false;
+  }
   if (P.model == MEU_MODEL_LANDAU && (cons || phi_in)) {
     // spectral state of the step from the uploaded real fields
     if (fused) {
@@ -626,14 +628,13 @@ void Engine<R>::kks_step(meu_diag* d) {
     std::vector<const R*> in;
     for (int v = 0; v < V; ++v) in.push_back(field(phi, v));
     fwd_list(in, 0);
-    KLAUNCH("kks_grad", (double)5 * V * nk * sizeof(C), k_kks_grad<R><<<gridk(), 256, 0, st>>>(dK, specs(0, V), specs(V, 4 * V), V));
+    KLAUNCH("kks_grad", (double)5 * V * nk * sizeof(C), k_kks_grad<R><<<gridk(), 256, 0, st>>>(dK, spec(0), spec(V), V));
     std::vector<R*> out;
     for (int f = 0; f < 4 * V; ++f) out.push_back(field(wr, f));
     inv_list(V, out);
   }
   // local driving force (:619-845)
-  KLAUNCH("kks_point", (double)(7 * V + 4 * E) * n3 * sizeof(R), k_kks_point<<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, (const double*)phi, (const double*)c, (const double*)wr,
-                                                  (double*)pphi, (double*)fd, (double*)fc, partials, d_err));
+  KLAUNCH("kks_point", (double)(7 * V + 4 * E) * n3 * sizeof(R), k_kks_point<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, phi, c, wr, pphi, fd, fc, partials, d_err));
   // elasticity (:851-880)
   last_iters = 0;
   if (step >= P.elastep0 && P.elastic != MEU_ELAST_NONE) {
@@ -703,9 +704,10 @@ void Engine<R>::sync_args() {
 
 template <typename R>
 void Engine<R>::fused_step_launches() {
-  if (!lan_fused_step<R>(P.nx, V, sched, dA, 1, P.diag_energy != 0, st, &prof, fnb))
+  const int opts = (P.diag_energy ? LS_ENERGY : 0) | (theta_ready ? LS_THETA_READY : 0);
+  if (!lan_fused_step<R>(P.nx, V, sched, dA, 1, opts, st, &prof, fnb))
     throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
-  lan_fused_finalize<R>(dA, 1, fnb, d_ops, st, &prof);
+  theta_ready = true;
 }
 
 template <typename R>
@@ -721,8 +723,8 @@ void Engine<R>::fused_steps(int n) {
     sync_args();
     const bool homog_now = hA.homog != 0;
     const bool homog_later = P.elastic != MEU_ELAST_NONE && step + GRAPH_STEPS - 1 >= P.elastep0;
-    const bool graphable =
-        fused_warm && !prof.on && st != nullptr && n - done >= GRAPH_STEPS && homog_now == homog_later;
+    const bool graphable = fused_warm && theta_ready && !prof.on && st != nullptr && n - done >= GRAPH_STEPS &&
+                           homog_now == homog_later;
     if (graphable) {
       if (!gexec) {
         const int64_t l0 = prof.launches;

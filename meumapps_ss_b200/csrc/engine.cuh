@@ -181,28 +181,35 @@ class Engine : public EngineBase {
   unsigned gridk() const { return grid_for(nk, 256); }
   unsigned gridr() const { return grid_for(n3, 256); }
 
-  void fwd(std::initializer_list<const R*> in, int s0) {
-    PtrList<const R> a{};
-    PtrList<C> b{};
-    int n = 0;
-    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
-    fft->forward<R>(a, b, n, st);
-  }
+  // Batched transforms of any number of fields, issued in groups of at most
+  // MAXF (the pointer lists the transform kernels take by value hold MAXF entries).
+  void fwd(std::initializer_list<const R*> in, int s0) { fwd_list(std::vector<const R*>(in), s0); }
   void fwd_list(const std::vector<const R*>& in, int s0) {
-    PtrList<const R> a{};
-    PtrList<C> b{};
-    int n = 0;
-    for (const R* q : in) { a.p[n] = q; b.p[n] = spec(s0 + n); ++n; }
-    fft->forward<R>(a, b, n, st);
+    for (size_t g0 = 0; g0 < in.size(); g0 += MAXF) {
+      PtrList<const R> a{};
+      PtrList<C> b{};
+      int n = 0;
+      for (size_t i = g0; i < in.size() && n < MAXF; ++i, ++n) {
+        a.p[n] = in[i];
+        b.p[n] = spec(s0 + (int)i);
+      }
+      fft->forward<R>(a, b, n, st);
+    }
   }
   void inv_list(int s0, const std::vector<R*>& out) {
-    PtrList<C> a{};
-    PtrList<R> b{};
-    int n = 0;
-    for (R* q : out) { a.p[n] = spec(s0 + n); b.p[n] = q; ++n; }
-    fft->inverse<R>(a, b, n, st);
+    for (size_t g0 = 0; g0 < out.size(); g0 += MAXF) {
+      PtrList<C> a{};
+      PtrList<R> b{};
+      int n = 0;
+      for (size_t i = g0; i < out.size() && n < MAXF; ++i, ++n) {
+        a.p[n] = spec(s0 + (int)i);
+        b.p[n] = out[i];
+      }
+      fft->inverse<R>(a, b, n, st);
+    }
   }
   PtrList<C> specs(int s0, int n) const {
+    if (n > MAXF) throw CudaError("internal: more than MAXF spectra in one kernel argument", MEU_ERR_UNSUPPORTED);
     PtrList<C> l{};
     for (int i = 0; i < n; ++i) l.p[i] = spec(s0 + i);
     return l;
@@ -228,6 +235,7 @@ class Engine : public EngineBase {
   int fnb[Q_TOTAL] = {0};
   static constexpr int GRAPH_STEPS = 8;
   bool fused_warm = false;
+  bool theta_ready = false;  // sp holds theta^ of the current fields (written by the last step's PI)
   bool fields_set = false;  // the spectral-state layout is fixed from the first upload on
   std::unique_ptr<AdjBuffers<R>, void (*)(AdjBuffers<R>*)> adjb{nullptr, adj_buffers_free<R>};
   void reset_fused_state();

@@ -56,6 +56,7 @@ class EnsembleT : public EnsembleBase {
     int nb[Q_TOTAL] = {0};
     cudaStream_t bst = nullptr;
     cudaEvent_t done = nullptr;
+    bool theta_ready = false;  // the members' M holds theta^ of their current fields
   };
   std::vector<std::unique_ptr<Engine<R>>> mem;
   std::vector<Bucket> bk;
@@ -65,7 +66,6 @@ class EnsembleT : public EnsembleBase {
   cudaGraphExec_t gexec = nullptr;
   int64_t graph_launches = 0;
   bool warm = false;
-  const int* d_ops = nullptr;
 
   void sync_args();
   void step_launches();
@@ -107,7 +107,6 @@ EnsembleT<R>::EnsembleT(int n, const meu_params* ps, int flags) {
     bk[b].idx.push_back(m);
     bucket_of.push_back(b);
   }
-  d_ops = mem[0]->d_ops;
   MEU_CUDA(cudaStreamCreateWithFlags(&own_st, cudaStreamNonBlocking));
   st = own_st;
   MEU_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -120,9 +119,10 @@ EnsembleT<R>::EnsembleT(int n, const meu_params* ps, int flags) {
   sync_args();
   if (flags & MEU_ENS_AUTOTUNE) {
     for (Bucket& b : bk)
-      b.sched = lan_autotune<R>(b.N, b.V, b.dA, (int)b.idx.size(), b.energy, d_ops, st, nullptr);
+      b.sched = lan_autotune<R>(b.N, b.V, b.dA, (int)b.idx.size(), b.energy, st, nullptr);
     MEU_CUDA(cudaStreamSynchronize(st));
     for (auto& e : mem) e->reset_fused_state();
+    for (Bucket& b : bk) b.theta_ready = false;
   }
   for (Bucket& b : bk)
     for (int m : b.idx) mem[m]->sched = b.sched;  // the spectral-state layout follows the radix plan
@@ -160,16 +160,17 @@ void EnsembleT<R>::sync_args() {
   }
 }
 
-// one ensemble step: fork to the bucket streams, batched step + finalisation, join
+// one ensemble step: fork to the bucket streams, batched step, join
 template <typename R>
 void EnsembleT<R>::step_launches() {
   MEU_CUDA(cudaEventRecord(fork, st));
   for (Bucket& b : bk) {
     MEU_CUDA(cudaStreamWaitEvent(b.bst, fork, 0));
     const int nm = (int)b.idx.size();
-    if (!lan_fused_step<R>(b.N, b.V, b.sched, b.dA, nm, b.energy, b.bst, &prof, b.nb))
+    const int opts = (b.energy ? LS_ENERGY : 0) | (b.theta_ready ? LS_THETA_READY : 0);
+    if (!lan_fused_step<R>(b.N, b.V, b.sched, b.dA, nm, opts, b.bst, &prof, b.nb))
       throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
-    lan_fused_finalize<R>(b.dA, nm, b.nb, d_ops, b.bst, &prof);
+    b.theta_ready = true;
     MEU_CUDA(cudaEventRecord(b.done, b.bst));
     MEU_CUDA(cudaStreamWaitEvent(st, b.done, 0));
   }
@@ -200,7 +201,10 @@ void EnsembleT<R>::run(int nsteps, meu_diag* diag) {
     int i = 0;
     while (i < chunk) {
       sync_args();
-      const bool graphable = warm && !prof.on && st != nullptr && chunk - i >= GRAPH_STEPS && homog_stable(GRAPH_STEPS);
+      bool ready = true;
+      for (const Bucket& b : bk) ready = ready && b.theta_ready;
+      const bool graphable =
+          warm && ready && !prof.on && st != nullptr && chunk - i >= GRAPH_STEPS && homog_stable(GRAPH_STEPS);
       int k = 1;
       if (graphable) {
         if (!gexec) {
@@ -258,6 +262,7 @@ void EnsembleT<R>::set_fields(int m, const double* cons, const double* phi) {
   MEU_CUDA(cudaStreamSynchronize(st));
   mem[m]->step = step;
   mem[m]->set_fields(cons, phi, nullptr);
+  bk[bucket_of[m]].theta_ready = false;
   MEU_CUDA(cudaStreamSynchronize(mem[m]->st));
 }
 

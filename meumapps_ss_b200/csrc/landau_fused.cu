@@ -1,5 +1,5 @@
-// landau_fused.cu -- size dispatch, per-step finalisation and schedule
-// autotuning of the fused Landau step (kernels: landau_fused_kernels.cuh,
+// landau_fused.cu -- size dispatch and schedule autotuning of the fused
+// Landau step (kernels: landau_fused_kernels.cuh,
 // instantiated per (precision, N) in lf_inst_*.cu).
 #include <cstdio>
 #include <cstdlib>
@@ -13,33 +13,6 @@
 
 namespace meu {
 
-namespace {
-// Fixed-order reduction of member blockIdx.y's partials into its history row.
-// The last of the member's blocks advances the member's row counter, so graph
-// replays of the step need no host-side row index.
-template <typename R>
-__global__ void __launch_bounds__(256) k_lf_finalize(const LanFusedArgs<R>* __restrict__ A, NbList nb,
-                                                     const int* __restrict__ ops) {
-  const LanFusedArgs<R>& a = A[blockIdx.y];
-  const int q = blockIdx.x, op = ops[q];
-  const int row = *a.hist_row;
-  double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
-  for (int i = threadIdx.x; i < nb.nb[q]; i += blockDim.x) {
-    const double v = a.partials[(int64_t)q * PSTRIDE + i];
-    acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
-  }
-  const double x = block_reduce_value(acc, op);
-  if (threadIdx.x == 0) {
-    if (row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = x;
-    __threadfence();
-    if (atomicAdd(a.ticket, 1) == (int)gridDim.x - 1) {
-      *a.ticket = 0;
-      *a.hist_row = row + 1;
-    }
-  }
-}
-}  // namespace
-
 bool lan_fused_supported(const meu_params& p) {
   const int n = p.nx;
   const bool size_ok = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128) && p.ny == n && p.nz == n;
@@ -48,15 +21,15 @@ bool lan_fused_supported(const meu_params& p) {
 }
 
 template <typename R>
-bool lan_fused_step(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy,
+bool lan_fused_step(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, int opts,
                     cudaStream_t st, LaunchHook* hook, int* nb) {
   if (members < 1 || members > 65535) return false;
   switch (N) {
-    case 32: return lf_step_n<R, 32>(V, s, dA, members, energy, st, hook, nb);
-    case 48: return lf_step_n<R, 48>(V, s, dA, members, energy, st, hook, nb);
-    case 64: return lf_step_n<R, 64>(V, s, dA, members, energy, st, hook, nb);
-    case 96: return lf_step_n<R, 96>(V, s, dA, members, energy, st, hook, nb);
-    case 128: return lf_step_n<R, 128>(V, s, dA, members, energy, st, hook, nb);
+    case 32: return lf_step_n<R, 32>(V, s, dA, members, opts, st, hook, nb);
+    case 48: return lf_step_n<R, 48>(V, s, dA, members, opts, st, hook, nb);
+    case 64: return lf_step_n<R, 64>(V, s, dA, members, opts, st, hook, nb);
+    case 96: return lf_step_n<R, 96>(V, s, dA, members, opts, st, hook, nb);
+    case 128: return lf_step_n<R, 128>(V, s, dA, members, opts, st, hook, nb);
     default: return false;
   }
 }
@@ -73,19 +46,6 @@ bool lan_fused_init(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, 
     case 128: return lf_init_n<R, 128>(V, s, dA, members, st, hook);
     default: return false;
   }
-}
-
-template <typename R>
-void lan_fused_finalize(const LanFusedArgs<R>* dA, int members, const int* nb, const int* ops, cudaStream_t st,
-                        LaunchHook* hook) {
-  NbList l;
-  for (int q = 0; q < Q_TOTAL; ++q) l.nb[q] = q < Q_STEP_COUNT ? nb[q] : 0;
-  double bytes = 0;
-  for (int q = 0; q < Q_STEP_COUNT; ++q) bytes += 8.0 * nb[q];
-  if (hook) hook->begin("finalize", bytes * members, st);
-  k_lf_finalize<R><<<dim3(Q_STEP_COUNT, members), 256, 0, st>>>(dA, l, ops);
-  MEU_CHECK_LAUNCH();
-  if (hook) hook->end(st);
 }
 
 std::vector<LanSched> lan_sched_candidates(int N, bool f64) {
@@ -139,8 +99,8 @@ void tune_store(const std::string& key, const LanSched& s, double ms) {
 }  // namespace
 
 template <typename R>
-LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool energy, const int* d_ops,
-                      cudaStream_t st, double* best_ms) {
+LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st,
+                      double* best_ms) {
   const bool f64 = sizeof(R) == 8;
   const std::string key = tune_key(f64, N, V, members, energy);
   {
@@ -152,26 +112,28 @@ LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool
       return it->second;
     }
   }
-  constexpr int WARM = 2, TIMED = 5;
+  constexpr int WARM = 3, TIMED = 10, REPS = 2;  // best of REPS timings of TIMED steps
   cudaEvent_t e0, e1;
   MEU_CUDA(cudaEventCreate(&e0));
   MEU_CUDA(cudaEventCreate(&e1));
   LanSched best;
   double best_t = 1e300;
   int nb[Q_TOTAL];
+  const int eopt = energy ? LS_ENERGY : 0;
   for (const LanSched& s : lan_sched_candidates(N, f64)) {
-    for (int i = 0; i < WARM + TIMED; ++i) {
-      if (i == WARM) MEU_CUDA(cudaEventRecord(e0, st));
-      if (!lan_fused_step<R>(N, V, s, dA, members, energy, st, nullptr, nb)) break;
-      lan_fused_finalize<R>(dA, members, nb, d_ops, st, nullptr);
-    }
-    MEU_CUDA(cudaEventRecord(e1, st));
-    MEU_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms / TIMED < best_t) {
-      best_t = ms / TIMED;
-      best = s;
+    for (int i = 0; i < WARM; ++i)
+      if (!lan_fused_step<R>(N, V, s, dA, members, eopt | (i ? LS_THETA_READY : 0), st, nullptr, nb)) break;
+    for (int r = 0; r < REPS; ++r) {
+      MEU_CUDA(cudaEventRecord(e0, st));
+      for (int i = 0; i < TIMED; ++i) lan_fused_step<R>(N, V, s, dA, members, eopt | LS_THETA_READY, st, nullptr, nb);
+      MEU_CUDA(cudaEventRecord(e1, st));
+      MEU_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms / TIMED < best_t) {
+        best_t = ms / TIMED;
+        best = s;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -185,15 +147,11 @@ LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool
 
 template bool lan_fused_init<float>(int, int, const LanSched&, const LanFusedArgs<float>*, int, cudaStream_t, LaunchHook*);
 template bool lan_fused_init<double>(int, int, const LanSched&, const LanFusedArgs<double>*, int, cudaStream_t, LaunchHook*);
-template bool lan_fused_step<float>(int, int, const LanSched&, const LanFusedArgs<float>*, int, bool, cudaStream_t,
+template bool lan_fused_step<float>(int, int, const LanSched&, const LanFusedArgs<float>*, int, int, cudaStream_t,
                                     LaunchHook*, int*);
-template bool lan_fused_step<double>(int, int, const LanSched&, const LanFusedArgs<double>*, int, bool, cudaStream_t,
+template bool lan_fused_step<double>(int, int, const LanSched&, const LanFusedArgs<double>*, int, int, cudaStream_t,
                                      LaunchHook*, int*);
-template void lan_fused_finalize<float>(const LanFusedArgs<float>*, int, const int*, const int*, cudaStream_t, LaunchHook*);
-template void lan_fused_finalize<double>(const LanFusedArgs<double>*, int, const int*, const int*, cudaStream_t,
-                                         LaunchHook*);
-template LanSched lan_autotune<float>(int, int, const LanFusedArgs<float>*, int, bool, const int*, cudaStream_t, double*);
-template LanSched lan_autotune<double>(int, int, const LanFusedArgs<double>*, int, bool, const int*, cudaStream_t,
-                                       double*);
+template LanSched lan_autotune<float>(int, int, const LanFusedArgs<float>*, int, bool, cudaStream_t, double*);
+template LanSched lan_autotune<double>(int, int, const LanFusedArgs<double>*, int, bool, cudaStream_t, double*);
 
 }  // namespace meu

@@ -8,20 +8,22 @@
 // re-derived each step for the nonlinear terms and the output.  (Re-transforming
 // the real fields every step instead makes an FP32 forward/inverse pair act on
 // slowly varying data each step, whose rounding errors then add up coherently.)
-// Six launches per step (with the bulk-energy reduction) and one finalisation:
+// Four launches per step (five on the first step after new fields):
 //
-//   PF  plane:  theta_v = eta_v^2 -> x R2C + y FFT                         (+ bulk energy)
+//   PF  plane:  theta_v = eta_v^2 -> x R2C + y FFT   (first step after new fields only)
 //   Z1  column: z FFT of theta -> Green operator phi_v; Cahn-Hilliard update of
 //              the dc^ state (mu^ = A dc^ - B/2 sum theta^_v) -> z iFFT of phi_v, dc_new
 //   PB  plane:  y iFFT + x C2R of phi_v -> g_v = df/deta_v + el_grad_v -> x R2C + y FFT
+//              (+ bulk free energy of the start-of-step fields)
 //   Z2  column: z FFT of g -> eta^ state <- (eta^ - dt L g^) / (1 + dt L k.kappa.k) -> z iFFT
 //   PI  plane:  y iFFT + x C2R of eta_new, dc_new -> real eta, dc in place
-//              (+ end-of-step statistics)
+//              (+ end-of-step statistics; theta_v = eta_v^2 -> x R2C + y FFT for the
+//              next step; the last block reduces the step's partials into its history row)
 //
 // Set-up (after new fields are uploaded): PF in raw mode transforms eta_v and dc,
 // Z0 finishes the z transform into the spectral state.
 //
-// The real-field inputs of the step (eta and dc) are read by PF, FCH and PB and
+// The real-field inputs of the step (eta and dc) are read by PF and PB and
 // rewritten only by PI, the last launch, so both are updated in place.
 #pragma once
 #include <vector>
@@ -63,8 +65,8 @@ struct LanFusedArgs {
   const cplx<R>* twz;
   const cplx<R>* post;
   double* hist;   // per-step reduction rows [hist_rows][Q_STEP_COUNT]
-  int* hist_row;  // row of the current step (advanced by the finalisation)
-  int* ticket;    // completion counter of the finalisation
+  int* hist_row;  // row of the current step (advanced at the end of the step)
+  int* ticket;    // completion counter of the step's last kernel
   int hist_rows;
   // where the step writes the new state (equal to eta, c, Keta, Kc for an in-place step)
   R* eta_next;
@@ -88,21 +90,22 @@ enum LanQ : int {
   LQ_SOLID = Q_SOLID, LQ_CSUM = Q_CSUM0
 };
 
+// options of lan_fused_step
+enum LanStepOpt : int {
+  LS_ENERGY = 1,       // fort.98 energies of the step
+  LS_THETA_READY = 2,  // M holds theta^ of the current fields (written by the previous step's PI)
+};
+
 // Host launch entries (landau_fused.cu).  dA: device array of `members`
 // argument records.  Return false if (N, V, schedule) has no instantiation.
 // lan_fused_step writes the per-block reduction counts of the step into nb.
 template <typename R>
-bool lan_fused_step(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy,
+bool lan_fused_step(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, int opts,
                     cudaStream_t st, LaunchHook* hook, int* nb);
 // spectral state from the real fields eta and dc (after an upload)
 template <typename R>
 bool lan_fused_init(int N, int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st,
                     LaunchHook* hook);
-// fixed-order reduction of each member's partials into its history row
-// *hist_row; the last block to finish advances *hist_row
-template <typename R>
-void lan_fused_finalize(const LanFusedArgs<R>* dA, int members, const int* nb, const int* ops, cudaStream_t st,
-                        LaunchHook* hook);
 // the schedules instantiated for (N, precision)
 std::vector<LanSched> lan_sched_candidates(int N, bool f64);
 // Times every candidate schedule on the members' buffers (a few steps each, the
@@ -110,13 +113,13 @@ std::vector<LanSched> lan_sched_candidates(int N, bool f64);
 // fastest.  Results are cached per (precision, N, V, members, energy) for the
 // process and, when the environment names a file in MEU_AUTOTUNE_CACHE, in that file.
 template <typename R>
-LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool energy, const int* d_ops,
-                      cudaStream_t st, double* best_ms);
+LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st,
+                      double* best_ms);
 bool lan_fused_supported(const meu_params& p);
 
 // per-(R, N) entries, one translation unit each (lf_inst_*.cu)
 template <typename R, int N>
-bool lf_step_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st,
+bool lf_step_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
                LaunchHook* hook, int* nb);
 template <typename R, int N>
 bool lf_init_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st, LaunchHook* hook);

@@ -15,7 +15,6 @@ namespace meu {
 namespace lf {
 
 constexpr int NT = 256;   // column kernels
-constexpr int FCH_MAX_BLOCKS = 592;
 constexpr double TWO_PI = 6.283185307179586476925286766559;
 
 template <int N>
@@ -383,6 +382,28 @@ __global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(con
 #pragma unroll
   for (int q = 0; q < V; ++q) Af[q] = (W)F.A[f][q];
   const bool homog = a.homog != 0;
+  // bulk free energy of the start-of-step fields, summed by the f == 0 block of each plane
+  const bool bulk = a.energy && f == 0;
+  const W la2 = (W)(0.5 * F.lan_a), lc1 = (W)F.lan_c1, lb2 = (W)(0.5 * F.lan_b), lc4 = (W)(0.25 * F.lan_c);
+  const W ld6 = (W)(F.lan_d / 6.0), cw = (W)F.cross_w;
+  double fch = 0;
+  auto bulk_energy = [&](const C* ev, C dcv) {
+    W acc = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      W s2 = 0, s4 = 0, s6 = 0;
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        const W x = h ? ev[q].y : ev[q].x, e2 = x * x;
+        s2 += e2;
+        s4 += e2 * e2;
+        s6 += e2 * e2 * e2;
+      }
+      const W cv = cbar + (W)(h ? dcv.y : dcv.x), dc1 = cv - lc1;
+      acc += la2 * dc1 * dc1 + lb2 * (lc2 - cv) * s2 - lc4 * s4 + ld6 * s6 + cw * (s2 * s2 - s4);
+    }
+    fch += (double)acc;
+  };
   // g_f at the pair (x, x+1) of row y from eta_q (q < V), dc and phi_f
   auto point = [&](const C* ev, C dcv, C ph) -> C {
     W e2q[2][V], s2[2] = {0, 0}, ef[2];
@@ -421,6 +442,7 @@ __global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(con
 #pragma unroll
       for (int q = 0; q < V; ++q) ev[q] = *(const C*)(a.eta + q * N3 + g0);
       const C dcv = *(const C*)(a.c + g0);
+      if (bulk) bulk_energy(ev, dcv);
       buf[y * P::PITCH + n] = point(ev, dcv, buf[y * P::PITCH + n]);
     }
     __syncthreads();
@@ -438,12 +460,14 @@ __global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(con
 #pragma unroll
         for (int q = 0; q < V; ++q) ev[q] = ((const C*)(sb + q * CHR + yl * N))[n];
         const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
+        if (bulk) bulk_energy(ev, dcv);
         buf[y * P::PITCH + n] = point(ev, dcv, buf[y * P::PITCH + n]);
       }
       __syncthreads();
       if (k + 2 < NCH) issue(k + 2);
     }
   }
+  if (bulk) block_reduce_store(fch, 0, a.partials + LQ_FCH * PSTRIDE + z);
   P::forward(buf, tws);
   P::store_m(buf, mp);
 }
@@ -533,7 +557,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
 // Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
 // -> real, concentration statistics.
 template <typename R, int N, int PV, int NTP>
-__global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V) {
+__global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
   using P = fz::Plane<R, N, NTP, PV>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
@@ -571,48 +595,53 @@ __global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict
   block_reduce_store(cmin, 2, a.partials + LQ_CMIN * PSTRIDE + blk);
   block_reduce_store(cmax, 1, a.partials + LQ_CMAX * PSTRIDE + blk);
   block_reduce_store(csum, 0, a.partials + LQ_CSUM * PSTRIDE + blk);
-}
-
-// ------------------------------------------------------------------ FCH
-// bulk free energy of the start-of-step fields (all eta and dc), streamed with
-// 16-byte loads over the whole grid
-template <typename R>
-__global__ void __launch_bounds__(256) k_lf_fch(const LanFusedArgs<R>* __restrict__ A, int V, int64_t n3) {
-  using V4 = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
-  const LanFusedArgs<R> a = A[blockIdx.z];
-  constexpr int PER = 16 / sizeof(R);
-  const LanFusedConst& F = *a.F;
-  double fch = 0;
-  const int64_t nv = n3 / PER;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
-    R e[4][PER], d[PER];
-    {
-      const V4 t = ((const V4*)a.c)[i];
-      const R* tp = (const R*)&t;
-#pragma unroll
-      for (int h = 0; h < PER; ++h) d[h] = tp[h];
+  if (f < V) {
+    // theta^_f of the next step from the new eta_f still in shared memory (the
+    // next step then starts at its column kernel)
+    __syncthreads();
+#pragma unroll 1
+    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+      const int y = i / P::LX, n = i - y * P::LX;
+      const C e = buf[y * P::PITCH + n];
+      buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
     }
-    for (int q = 0; q < V; ++q) {
-      const V4 t = ((const V4*)(a.eta + q * n3))[i];
-      const R* tp = (const R*)&t;
-#pragma unroll
-      for (int h = 0; h < PER; ++h) e[q][h] = tp[h];
-    }
-#pragma unroll
-    for (int h = 0; h < PER; ++h) {
-      double s2 = 0, s4 = 0, s6 = 0;
-      for (int q = 0; q < V; ++q) {
-        const double e2 = (double)e[q][h] * (double)e[q][h];
-        s2 += e2;
-        s4 += e2 * e2;
-        s6 += e2 * e2 * e2;
-      }
-      const double cv = F.cbar + (double)d[h];
-      fch += 0.5 * F.lan_a * (cv - F.lan_c1) * (cv - F.lan_c1) + 0.5 * F.lan_b * (F.lan_c2 - cv) * s2 - 0.25 * F.lan_c * s4 +
-             F.lan_d / 6.0 * s6 + F.cross_w * (s2 * s2 - s4);
-    }
+    __syncthreads();
+    P::forward(buf, tws);
+    P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
   }
-  block_reduce_store(fch, 0, a.partials + LQ_FCH * PSTRIDE + blockIdx.x);
+  // ---- finalisation of the step: the member's last PI block reduces every block
+  // partial of the step in a fixed order into history row *hist_row and advances it
+  // (so graph replays need no host-side row index)
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(a.ticket, 1) == (int)(gridDim.x * gridDim.y) - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int row = *(volatile const int*)a.hist_row;
+  // one quantity per warp, lane-strided loads, fixed reduction order
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll 1
+  for (int q = wid; q < Q_STEP_COUNT; q += NTP / 32) {
+    const int op = (q == Q_CMIN) ? 2 : (q == Q_CMAX || q == Q_PHIMAX) ? 1 : 0;
+    double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
+    const double* src = a.partials + (int64_t)q * PSTRIDE;
+#pragma unroll 4
+    for (int i = lane; i < nb.nb[q]; i += 32) {
+      const double v = __ldcg(src + i);
+      acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
+    }
+    acc = op == 0 ? warp_sum(acc) : op == 1 ? warp_max(acc) : warp_min(acc);
+    if (lane == 0 && row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *a.ticket = 0;
+    *a.hist_row = row + 1;
+  }
 }
 
 // ------------------------------------------------------------------ launch sequence
@@ -644,22 +673,14 @@ void ensure_smem(K fn, size_t bytes) {
   done.push_back((const void*)fn);
 }
 
-// blocks of the bulk-energy reduction for an N^3 grid
-template <typename R, int N>
-constexpr int fch_blocks() {
-  constexpr int64_t vec = (int64_t)N * N * N / (16 / sizeof(R));
-  constexpr int64_t b = (vec + 255) / 256;
-  return b < FCH_MAX_BLOCKS ? (int)b : FCH_MAX_BLOCKS;
-}
-
 template <typename R, int N, int V, int PV, int NTP, int TM>
-void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st, LaunchHook* hook, int* nb) {
+void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st, LaunchHook* hook, int* nb) {
+  const bool energy = (opts & LS_ENERGY) != 0;
   using P = fz::Plane<R, N, NTP, PV>;
   using C = cplx<R>;
   constexpr int NXH = N / 2 + 1;
   constexpr int tiles = N * NXH / TM;
   static_assert(N * NXH % TM == 0 && tiles <= PSTRIDE, "column tiling");
-  constexpr int FB = fch_blocks<R, N>();
   const double mm = (double)members;
   const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
   const size_t sp = P::smem_bytes();
@@ -671,14 +692,10 @@ void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t 
   ensure_smem(k_lf_pi<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_z1<R, N, V, PV, TM>, s1);
   ensure_smem(k_lf_z2<R, N, V, PV, TM>, s2);
-  {
+  if (!(opts & LS_THETA_READY)) {
+    // theta^ of the first step after new fields (later steps get it from PI)
     Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
     k_lf_pf<R, N, PV, NTP><<<dim3(N, V, members), NTP, sp, st>>>(dA, V, 0);
-    MEU_CHECK_LAUNCH();
-  }
-  if (energy) {
-    Scope s(hook, "lf_bulk_energy", (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_fch<R><<<dim3(FB, 1, members), 256, 0, st>>>(dA, V, (int64_t)N * N * N);
     MEU_CHECK_LAUNCH();
   }
   {
@@ -696,17 +713,19 @@ void run_step(const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t 
     k_lf_z2<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s2, st>>>(dA);
     MEU_CHECK_LAUNCH();
   }
+  NbList l;
+  for (int q = 0; q < Q_TOTAL; ++q) l.nb[q] = 0;
+  l.nb[Q_FCH] = energy ? N : 0;
+  l.nb[Q_FINT] = tiles;
+  l.nb[Q_ELEN] = tiles;
+  l.nb[Q_FINT2] = tiles;
+  l.nb[Q_CMIN] = l.nb[Q_CMAX] = l.nb[Q_PHIMAX] = l.nb[Q_SOLID] = l.nb[Q_CSUM0] = N * (V + 1);
   {
-    Scope s(hook, "lf_plane_inv_stats", (V + 1.0) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pi<R, N, PV, NTP><<<dim3(N, V + 1, members), NTP, sp, st>>>(dA, V);
+    Scope s(hook, "lf_plane_inv_stats_theta", (2.0 * V + 1.0) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
+    k_lf_pi<R, N, PV, NTP><<<dim3(N, V + 1, members), NTP, sp, st>>>(dA, V, l);
     MEU_CHECK_LAUNCH();
   }
-  for (int q = 0; q < Q_TOTAL; ++q) nb[q] = 0;
-  nb[Q_FCH] = energy ? FB : 0;
-  nb[Q_FINT] = tiles;
-  nb[Q_ELEN] = tiles;
-  nb[Q_FINT2] = tiles;
-  nb[Q_CMIN] = nb[Q_CMAX] = nb[Q_PHIMAX] = nb[Q_SOLID] = nb[Q_CSUM0] = N * (V + 1);
+  for (int q = 0; q < Q_TOTAL; ++q) nb[q] = l.nb[q];
 }
 
 template <typename R, int N, int V, int PV, int NTP, int TM>
@@ -780,13 +799,13 @@ template <typename R, int N>
 struct StepFn {
   const LanFusedArgs<R>* dA;
   int members;
-  bool energy;
+  int opts;
   cudaStream_t st;
   LaunchHook* hook;
   int* nb;
   template <int V, int PV, int NTP, int TM>
   void operator()() const {
-    run_step<R, N, V, PV, NTP, TM>(dA, members, energy, st, hook, nb);
+    run_step<R, N, V, PV, NTP, TM>(dA, members, opts, st, hook, nb);
   }
 };
 template <typename R, int N>
@@ -803,9 +822,9 @@ struct InitFn {
 }  // namespace lf
 
 template <typename R, int N>
-bool lf_step_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, bool energy, cudaStream_t st,
+bool lf_step_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
                LaunchHook* hook, int* nb) {
-  return lf::with_sched<R, N>(V, s, lf::StepFn<R, N>{dA, members, energy, st, hook, nb});
+  return lf::with_sched<R, N>(V, s, lf::StepFn<R, N>{dA, members, opts, st, hook, nb});
 }
 template <typename R, int N>
 bool lf_init_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members, cudaStream_t st, LaunchHook* hook) {
@@ -816,7 +835,7 @@ bool lf_init_n(int V, const LanSched& s, const LanFusedArgs<R>* dA, int members,
 
 // one translation unit per (R, N)
 #define MEU_LF_INSTANTIATE(R, N)                                                                                    \
-  template bool meu::lf_step_n<R, N>(int, const meu::LanSched&, const meu::LanFusedArgs<R>*, int, bool, cudaStream_t, \
+  template bool meu::lf_step_n<R, N>(int, const meu::LanSched&, const meu::LanFusedArgs<R>*, int, int, cudaStream_t, \
                                      meu::LaunchHook*, int*);                                                       \
   template bool meu::lf_init_n<R, N>(int, const meu::LanSched&, const meu::LanFusedArgs<R>*, int, cudaStream_t,      \
                                      meu::LaunchHook*);

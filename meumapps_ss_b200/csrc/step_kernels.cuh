@@ -18,10 +18,11 @@ __device__ __forceinline__ void ld2(const C& v, double& re, double& im) {
 
 // ------------------------------------------------------------ KKS: gradients
 // dft_grad_{x,y,z} = kf * phi^, dft_k_del_sq = phi^ * (grad_coeff multiplier)
-// (Multi_MEUMAPPS.f:581-605).  out[4v+c].
+// (Multi_MEUMAPPS.f:581-605).  in: V spectra at in0 + v*nk; out: 4V spectra at
+// out0 + (4v+c)*nk (contiguous, so any variant count fits one launch).
 template <typename R>
-__global__ void __launch_bounds__(256) k_kks_grad(const DevConst* __restrict__ Kp, PtrList<cplx<R>> in,
-                                                  PtrList<cplx<R>> out, int V) {
+__global__ void __launch_bounds__(256) k_kks_grad(const DevConst* __restrict__ Kp, const cplx<R>* __restrict__ in0,
+                                                  cplx<R>* __restrict__ out0, int V) {
   const DevConst& K = *Kp;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < K.nk; id += (int64_t)gridDim.x * blockDim.x) {
     int kx, ky, kz;
@@ -29,22 +30,24 @@ __global__ void __launch_bounds__(256) k_kks_grad(const DevConst* __restrict__ K
     double a[3], b[3];
     kvec(K, kx, ky, kz, a, b);
     for (int v = 0; v < V; ++v) {
-      const cplx<R> val = in.p[v][id];
+      const cplx<R> val = in0[v * K.nk + id];
       const double re = val.x, im = val.y;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) out.p[4 * v + c][id] = mk((R)(-b[c] * im), (R)(b[c] * re));
+      for (int c = 0; c < 3; ++c) out0[(4 * v + c) * K.nk + id] = mk((R)(-b[c] * im), (R)(b[c] * re));
       const double m = -kkappak(K.p.grad_coeff[v], a, b);
-      out.p[4 * v + 3][id] = mk((R)(re * m), (R)(im * m));
+      out0[(4 * v + 3) * K.nk + id] = mk((R)(re * m), (R)(im * m));
     }
   }
 }
 
 // ------------------------------------------------- KKS: local driving force
 // Multi_MEUMAPPS.f:634-845 per voxel.  g4 = [gx_v, gy_v, gz_v, kds_v] per v.
-__global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __restrict__ Kp, const double* __restrict__ phi,
-                                                           const double* __restrict__ cons, const double* __restrict__ g4,
-                                                           double* __restrict__ pphi, double* __restrict__ fdiff,
-                                                           double* __restrict__ fc, double* partials, int* err) {
+// Fields in R; the local solve and the energies in FP64.
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
+                                                           const R* __restrict__ cons, const R* __restrict__ g4,
+                                                           R* __restrict__ pphi, R* __restrict__ fdiff,
+                                                           R* __restrict__ fc, double* partials, int* err) {
   const DevConst& K = *Kp;
   const meu_params& p = K.p;
   const int V = p.nvar, numel = p.numel, numph = p.numph, zdim = K.zdim;
@@ -53,12 +56,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
     double Pph[MEU_MAX_PH], Gph[MEU_MAX_PH], Ppr[MEU_MAX_VAR], fgrad[MEU_MAX_VAR], ph[MEU_MAX_VAR];
     for (int n = 0; n < MEU_MAX_PH; ++n) { Pph[n] = 0; Gph[n] = 0; }
-    for (int v = 0; v < V; ++v) ph[v] = phi[v * n3 + id];
+    for (int v = 0; v < V; ++v) ph[v] = (double)phi[v * n3 + id];
     for (int n = 2; n <= numph; ++n)
       for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
         const double fi = ph[v], fi_sq = fi * fi;
         const double pl = fi_sq * fi * (6.0 * fi_sq - 15.0 * fi + 10.0);
-        pphi[v * n3 + id] = pl;
+        pphi[v * n3 + id] = (R)pl;
         Ppr[v] = 30.0 * fi_sq * (fi_sq - 2.0 * fi + 1.0);
         Pph[0] += pl;
         Pph[n - 1] += pl;
@@ -73,7 +76,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
     for (int i = 0; i < zdim; ++i) Zr[i] = K.zr_const[i];
     for (int e = 1; e <= numel; ++e) {
       const int i0 = zdim - numel + e;
-      Zr[i0 - 1] = cons[(e - 1) * n3 + id];
+      Zr[i0 - 1] = (double)cons[(e - 1) * n3 + id];
       for (int n = 1; n <= numph; ++n) Z[(i0 - 1) + (numph * (e - 1) + n - 1) * zdim] = Pph[n - 1];
     }
     set_err(err, invert_small<12>(Z, zdim, MEU_ERR_Z_SINGULAR));
@@ -101,7 +104,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
     for (int n = 2; n <= numph; ++n) {
       for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
         const double* g = p.grad_coeff[v];
-        const double gx = g4[(4 * v + 0) * n3 + id], gy = g4[(4 * v + 1) * n3 + id], gz = g4[(4 * v + 2) * n3 + id];
+        const double gx = (double)g4[(4 * v + 0) * n3 + id], gy = (double)g4[(4 * v + 1) * n3 + id];
+        const double gz = (double)g4[(4 * v + 2) * n3 + id];
         const double term = g[0] * gx * gx + g[4] * gy * gy + g[8] * gz * gz + (g[3] + g[1]) * gx * gy +
                             (g[6] + g[2]) * gx * gz + (g[7] + g[5]) * gy * gz;
         fint += 0.5 * term;
@@ -125,7 +129,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
     }
     fch += fchloc;
     fw += fwloc;
-    for (int i = 0; i < 3 * numel; ++i) fc[(int64_t)i * n3 + id] = fcl[i];
+    for (int i = 0; i < 3 * numel; ++i) fc[(int64_t)i * n3 + id] = (R)fcl[i];
     // n_tilda projection (:824-841)
     for (int jv = 0; jv < V; ++jv) {
       double term11 = 0;
@@ -133,10 +137,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
       if (ph[jv] > 0.0)
         for (int iv = 0; iv < V; ++iv)
           if (ph[iv] > 0.0 && iv != jv) {
-            term11 += fgrad[iv] - g4[(4 * iv + 3) * n3 + id];
+            term11 += fgrad[iv] - (double)g4[(4 * iv + 3) * n3 + id];
             nt += 1;
           }
-      fdiff[jv * n3 + id] = fgrad[jv] - term11 / (double)nt;
+      fdiff[jv * n3 + id] = (R)(fgrad[jv] - term11 / (double)nt);
     }
   }
   block_reduce_store(fch, 0, partials + Q_FCH * PSTRIDE + blockIdx.x);

@@ -104,16 +104,16 @@ def test_kks_mass_conservation_and_clip():
 
 
 @pytest.mark.gpu
-def test_kks_rejects_fp32_and_bad_sizes():
+def test_kks_rejects_bad_sizes_and_precision():
     from meumapps_ss_b200._lib import MeuError
     _, p, _, _ = kks_case(n=16)
     q = p.copy()
-    q.precision = P.PREC_F32
+    q.nx = 10
     with pytest.raises(MeuError) as e:
         Simulation(q)
     assert e.value.code == 103
     q = p.copy()
-    q.nx = 10
+    q.precision = 7
     with pytest.raises(MeuError):
         Simulation(q)
 
@@ -129,3 +129,42 @@ def test_kks_equal_moduli_parity(oracle):
     assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(fg - fo)) <= TOL
     assert np.max(np.abs(eg - eo)) <= 1e-9 * np.max(np.abs(eo))
     assert np.array_equal(_cat(do, "el_iters"), _cat(dg, "el_iters"))
+
+
+def _kks12(n, precision=P.PREC_F64, steps=30):
+    from meumapps_ss_b200 import configs as CF
+    deck = P.parse_input_txt(CF.kks_input_txt(n, 12, steps, radius=4))
+    p = P.kks_params(deck, precision=precision, sym_var=CF.tetrahedral_rotations())
+    cons, phi = P.init_fields(deck)
+    return p, cons, phi
+
+
+@pytest.mark.gpu
+def test_kks_12_variants_parity(oracle):
+    # 12 orientation variants (sym_var rotations), heterogeneous moduli, plain FP64
+    p, cons, phi = _kks12(16)
+    assert p.nvar == 12
+    o, g, do, dg = _run_both(oracle, p, cons, phi, 30)
+    co, fo, _, _ = o.get_fields()
+    cg, fg, _, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(fg - fo)) <= TOL
+    assert np.array_equal(_cat(do, "el_iters"), _cat(dg, "el_iters"))
+
+
+@pytest.mark.gpu
+def test_kks_12_variants_fp32_against_fp64():
+    # the reference's production shape (12 variants) with FP32 fields: relative L2
+    # of the concentration and of the order parameters against the plain FP64 path
+    out = {}
+    for prec in (P.PREC_F64, P.PREC_F32):
+        p, cons, phi = _kks12(32, prec, 200)
+        g = Simulation(p)
+        g.set_fields(cons, phi)
+        g.run(200, diag=False)
+        out[prec] = g.get_fields()
+    c64, f64, _, _ = out[P.PREC_F64]
+    c32, f32, _, _ = out[P.PREC_F32]
+    rc = np.linalg.norm(c32 - c64) / np.linalg.norm(c64)
+    rf = np.linalg.norm(f32 - f64) / np.linalg.norm(f64)
+    print("kks12 fp32 rel", rc, rf)
+    assert rc <= 1e-5 and rf <= 1e-4, (rc, rf)
