@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--n", type=int, default=0, help="override the grid edge (tests only)")
+    ap.add_argument("--schedule", default="",
+                    help="pv,threads,tile: fixed schedule of the fused step instead of the autotuner's (profiling)")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed FP32 steps (for ncu launch lists and captures)")
     return ap.parse_args()
@@ -234,7 +236,8 @@ def run_ours(args):
 
     w = CF.landau_config(args.config, n=args.n or None, precision=P.PREC_F32)
     p32 = w.params
-    p32.flags |= P.FLAG_AUTOTUNE  # fused decks: fastest schedule variant (ignored on the generic path)
+    if not args.schedule:
+        p32.flags |= P.FLAG_AUTOTUNE  # fused decks: fastest schedule variant (ignored on the generic path)
     nx, ny, nz, V, E = p32.nx, p32.ny, p32.nz, p32.nvar, p32.numel
     n3 = nx * ny * nz
     seed = w.seed - rank
@@ -244,6 +247,8 @@ def run_ours(args):
     free0 = torch.cuda.mem_get_info(dev)[0]
     sim = Simulation(p32)
     footprint = free0 - torch.cuda.mem_get_info(dev)[0]
+    if args.schedule:
+        sim.set_schedule(*(int(x) for x in args.schedule.split(",")))
     schedule = sim.schedule
     sim.set_stream(stream.cuda_stream)
     sim.set_fields(c0, e0)

@@ -58,7 +58,7 @@ static void twiddle(int n, int L, long double& c, long double& s) {
 
 size_t FFT3::table_bytes(int nx, int ny, int nz, bool fp64) {
   const size_t csz = fp64 ? sizeof(double2) : sizeof(float2);
-  const int K = fp64 ? 1 : 2;
+  const int K = 1;
   return ((size_t)nx / 2 + ny + nz + nx / 2 + 1) * K * csz + sizeof(int) * ((size_t)nx / 2 + ny + nz) + 256;
 }
 
@@ -70,7 +70,7 @@ FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_, void* table_mem, size_t table_
   const int Lx = nx / 2;
   auto rvx = rev_table(Lx, rx), rvy = rev_table(ny, ry), rvz = rev_table(nz, rz);
   const size_t csz = fp64 ? sizeof(double2) : sizeof(float2);
-  const int K = fp64 ? 1 : 2;  // float tables hold hi then lo
+  const int K = 1;  // one correctly rounded entry per twiddle
   // layout: twx[Lx*K] twy[ny*K] twz[nz*K] post[nxh*K] | revx revy revz
   size_t ntw = ((size_t)Lx + ny + nz + nxh) * K;
   size_t bytes_tw = ntw * csz;
@@ -84,11 +84,8 @@ FFT3::FFT3(int nx_, int ny_, int nz_, bool fp64_, void* table_mem, size_t table_
         double2 v = make_double2((double)c, (double)s);
         memcpy(host.data() + (base + n) * csz, &v, csz);
       } else {
-        const float ch = (float)(double)c, sh = (float)(double)s;
-        float2 hi = make_float2(ch, sh);
-        float2 lo = make_float2((float)(double)(c - (long double)ch), (float)(double)(s - (long double)sh));
-        memcpy(host.data() + (base + n) * csz, &hi, csz);
-        memcpy(host.data() + (base + n_entries + n) * csz, &lo, csz);
+        float2 v = make_float2((float)(double)c, (float)(double)s);
+        memcpy(host.data() + (base + n) * csz, &v, csz);
       }
     }
   };

@@ -20,17 +20,12 @@ struct LinePlan {
   int L;       // transform length
   int ns;      // number of stages
   int r[12];   // radix of each DIF stage (product = L)
-  const void* tw;   // cplx<R>[L * Tw::K], tw[n] = exp(-2 pi i n / L) (float: hi then lo)
+  const void* tw;   // cplx<R>[L], tw[n] = exp(-2 pi i n / L)
   const int* rev;   // rev[p] = frequency index held at position p after DIF
 };
 
-// ------------------------------------------------------ compensated twiddles
-// FP32 transforms carry every twiddle as an unevaluated sum hi + lo of two
-// floats (hi = W rounded to float, lo = W - hi rounded to float) and multiply
-// x*hi + x*lo.  A forward/inverse pair then equals the identity up to random
-// rounding instead of a fixed bias |W_hi|^2 != 1 that every time step would
-// re-apply.  A twiddle table of length L stores hi at [0, L) and lo at [L, 2L)
-// for float; double tables have no lo part.
+// ------------------------------------------------------------------ twiddles
+// Twiddle tables hold exp(-2 pi i n / L) once per entry in the field precision.
 template <typename C> struct Tw;
 template <> struct Tw<double2> {
   static constexpr int K = 1;
@@ -38,14 +33,14 @@ template <> struct Tw<double2> {
   static __device__ __forceinline__ double2 mulc(double2 x, const double2* t, int i, int) { return cmulc(x, t[i]); }
   static __device__ __forceinline__ double2 scale(double2 x, double hi, double) { return cscale(x, hi); }
 };
+// FP32 twiddle tables hold the correctly rounded value only.  (A hi + lo split of
+// every table twiddle was measured to change nothing once the fused step keeps its
+// state spectral: config 1 after 1000 steps, eta error 1.28e-6 with, 1.30e-6 without.)
+// The radix-8 / radix-3 constants keep their hi + lo form (scale).
 template <> struct Tw<float2> {
-  static constexpr int K = 2;
-  static __device__ __forceinline__ float2 mul(float2 x, const float2* t, int i, int L) {
-    return cadd(cmul(x, t[i]), cmul(x, t[i + L]));
-  }
-  static __device__ __forceinline__ float2 mulc(float2 x, const float2* t, int i, int L) {
-    return cadd(cmulc(x, t[i]), cmulc(x, t[i + L]));
-  }
+  static constexpr int K = 1;
+  static __device__ __forceinline__ float2 mul(float2 x, const float2* t, int i, int) { return cmul(x, t[i]); }
+  static __device__ __forceinline__ float2 mulc(float2 x, const float2* t, int i, int) { return cmulc(x, t[i]); }
   static __device__ __forceinline__ float2 scale(float2 x, double hi, double lo) {
     return cadd(cscale(x, (float)hi), cscale(x, (float)lo));
   }
@@ -109,6 +104,43 @@ template <int S, typename C> struct Dft<8, S, C> {
     for (int q = 0; q < 4; ++q) {
       x[2 * q] = a[q];
       x[2 * q + 1] = b[q];
+    }
+  }
+};
+
+// 16 points as 4 x 4: radix-4 over a of x[4a+b], twiddle W16^(b c), radix-4 over b
+// (y[c + 4d] = sum_b W4^(bd) W16^(bc) sum_a W4^(ac) x[4a+b]).  Constants in the field
+// precision (the fused transforms only).
+template <int S, typename C> struct Dft<16, S, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    using R = decltype(x[0].x);
+    const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173, r2 = (R)0.70710678118654752440;
+    C t[16];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      C v[4] = {x[b], x[4 + b], x[8 + b], x[12 + b]};
+      Dft<4, S, C>::run(v);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) t[4 * b + c] = v[c];
+    }
+    // W16^k = (cos, S sin)(2 pi k / 16) for the exponents b*c in {1, 2, 3, 4, 6, 9}
+    auto w = [&](C v, R cr, R ci) { return mk(v.x * cr - v.y * ci, v.x * ci + v.y * cr); };
+    const R sg = (R)S;
+    t[5] = w(t[5], c1, sg * s1);        // b=1 c=1: W^1
+    t[6] = w(t[6], r2, sg * r2);        // b=1 c=2: W^2
+    t[7] = w(t[7], s1, sg * c1);        // b=1 c=3: W^3
+    t[9] = w(t[9], r2, sg * r2);        // b=2 c=1: W^2
+    t[10] = cmul_is<S>(t[10]);          // b=2 c=2: W^4 = S i
+    t[11] = w(t[11], -r2, sg * r2);     // b=2 c=3: W^6
+    t[13] = w(t[13], s1, sg * c1);      // b=3 c=1: W^3
+    t[14] = w(t[14], -r2, sg * r2);     // b=3 c=2: W^6
+    t[15] = w(t[15], -c1, -sg * s1);    // b=3 c=3: W^9
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      C v[4] = {t[c], t[4 + c], t[8 + c], t[12 + c]};
+      Dft<4, S, C>::run(v);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) x[c + 4 * d] = v[d];
     }
   }
 };
@@ -216,7 +248,7 @@ class FFT3 {
 
   LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
   LaunchHook* hook = nullptr;
-  const void* post_tw;  // cplx<R>[(nx/2+1) * Tw::K]: exp(-2 pi i k / nx) (float: hi then lo)
+  const void* post_tw;  // cplx<R>[nx/2+1]: exp(-2 pi i k / nx)
   bool fp64;
 
  private:

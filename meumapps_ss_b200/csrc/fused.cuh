@@ -24,10 +24,12 @@ struct RPlan {
   int ns;
   int r[8];
 };
-// Radix plans (product = L), two variants for the autotuner:
+// Radix plans (product = L), three variants for the autotuner:
 //   pv 0: radix 8 while the remainder does not end in a single factor 2
 //         (128 = 8*4*4, not 8*8*2), then 4s, at most one 2, then 3s;
-//   pv 1: radix 4 first (128 = 4*4*4*2), then at most one 2, then 3s.
+//   pv 1: radix 4 first (128 = 4*4*4*2), then at most one 2, then 3s;
+//   pv 2: radix 16 first, then 8s, 4s, at most one 2, 3s (128 = 16*8: one
+//         shared-memory pass fewer, more registers per butterfly).
 __host__ __device__ constexpr int twos(int n) {
   int k = 0;
   while (n > 0 && n % 2 == 0) { n /= 2; ++k; }
@@ -36,6 +38,10 @@ __host__ __device__ constexpr int twos(int n) {
 __host__ __device__ constexpr RPlan rplan(int L, int pv = 0) {
   RPlan p{0, {1, 1, 1, 1, 1, 1, 1, 1}};
   int n = L;
+  if (pv == 2) {
+    while (n % 16 == 0) { p.r[p.ns++] = 16; n /= 16; }
+    while (n % 8 == 0) { p.r[p.ns++] = 8; n /= 8; }
+  }
   if (pv == 0)
     while (n % 8 == 0 && twos(n / 8) != 1) { p.r[p.ns++] = 8; n /= 8; }
   while (n % 4 == 0) { p.r[p.ns++] = 4; n /= 4; }
@@ -193,7 +199,9 @@ struct Plane {
   static constexpr int ELEMS = NY * PITCH;
   // twiddles (hi then lo for float): twx[LX*K], twy[NY*K], post[NXH*K]
   static constexpr int K = Tw<C>::K;
-  static constexpr int TW_ELEMS = (LX + NY + NXH) * K;
+  // rounded up to 16 bytes: PB stages its inputs with 16-byte copies right after the twiddles
+  static constexpr int TW_ELEMS = (((LX + NY + NXH) * K * (int)sizeof(C) + 15) / 16) * 16 / (int)sizeof(C);
+  static_assert((ELEMS * sizeof(C)) % 16 == 0, "the twiddles follow the plane image on a 16-byte boundary");
   static constexpr size_t smem_bytes() { return sizeof(C) * (size_t)(ELEMS + TW_ELEMS); }
 
   static __device__ __forceinline__ void load_tw(C* tws, const C* __restrict__ gx, const C* __restrict__ gy,

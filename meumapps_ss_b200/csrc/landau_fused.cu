@@ -52,7 +52,7 @@ std::vector<LanSched> lan_sched_candidates(int N, bool f64) {
   std::vector<LanSched> v;
   const int wide = f64 ? 8 : 16;
   const int cols = N * (N / 2 + 1);
-  for (int pv = 0; pv < 2; ++pv)
+  for (int pv = 0; pv < 3; ++pv)
     for (int ntp : {512, 256})
       for (int tm : {wide, wide / 2}) {
         if (cols % tm != 0 || cols / tm > PSTRIDE) continue;

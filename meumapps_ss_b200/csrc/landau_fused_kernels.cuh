@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(con
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
   R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR] (staged mode)
+  static_assert(((P::ELEMS + P::TW_ELEMS) * sizeof(C)) % 16 == 0, "16-byte copies into the staging area");
   // field index fastest: the V+1 blocks of one plane, which read the same eta and
   // dc planes, are resident together and share those reads through L2
   const int f = blockIdx.x, z = blockIdx.y;
@@ -557,7 +558,8 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
 // Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
 // -> real, concentration statistics.
 template <typename R, int N, int PV, int NTP>
-__global__ void __launch_bounds__(NTP) k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
+__global__ void __launch_bounds__(NTP, 3 * (fz::Plane<R, N, NTP, PV>::smem_bytes() + BLOCK_RESERVED) <= SM_SMEM ? 3 : 1)
+    k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
   using P = fz::Plane<R, N, NTP, PV>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
@@ -773,12 +775,15 @@ bool with_sched_v(const LanSched& s, Fn&& f) {
   };
   using I0 = std::integral_constant<int, 0>;
   using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
   using T256 = std::integral_constant<int, 256>;
   using T512 = std::integral_constant<int, 512>;
   if (s.pv == 0 && s.ntp == 512) return pick_tm(I0{}, T512{});
   if (s.pv == 0 && s.ntp == 256) return pick_tm(I0{}, T256{});
   if (s.pv == 1 && s.ntp == 512) return pick_tm(I1{}, T512{});
   if (s.pv == 1 && s.ntp == 256) return pick_tm(I1{}, T256{});
+  if (s.pv == 2 && s.ntp == 512) return pick_tm(I2{}, T512{});
+  if (s.pv == 2 && s.ntp == 256) return pick_tm(I2{}, T256{});
   return false;
 }
 template <typename R, int N, typename Fn>

@@ -154,7 +154,7 @@ def schedule_candidates(n: int, f64: bool):
     """Schedules of the fused step instantiated for an n^3 grid (the autotuner's candidates)."""
     wide = 8 if f64 else 16
     cols = n * (n // 2 + 1)
-    return [(pv, ntp, tm) for pv in (0, 1) for ntp in (512, 256) for tm in (wide, wide // 2)
+    return [(pv, ntp, tm) for pv in (0, 1, 2) for ntp in (512, 256) for tm in (wide, wide // 2)
             if cols % tm == 0 and cols // tm <= 2048]
 
 
