@@ -80,6 +80,51 @@ module meu_iface
       import :: c_int, c_ptr
       type(c_ptr), value :: h
     end function
+    ! dparams(5): dJ/dbeta (kappa_eta scale), dJ/dkappa_c, dJ/db_mob, dJ/dcmobs(1), dJ/dalpha (eigenstrain scale)
+    integer(c_int) function meu_adjoint(h, nsteps, checkpoint_every, cons_target, phi_target, loss, dparams, dphi0) &
+        bind(C, name="meu_adjoint")
+      import :: c_int, c_int32_t, c_ptr, c_double
+      type(c_ptr), value :: h, cons_target, phi_target, dparams, dphi0
+      integer(c_int32_t), value :: nsteps, checkpoint_every
+      real(c_double), intent(out) :: loss
+    end function
+    integer(c_int) function meu_schedule(h, out3) bind(C, name="meu_schedule")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), intent(out) :: out3(3)
+    end function
+    integer(c_int) function meu_set_schedule(h, in3) bind(C, name="meu_set_schedule")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), intent(in) :: in3(3)
+    end function
+    ! ensembles: params(n) decks stepped together (flags: MEU_ENS_AUTOTUNE = 1)
+    integer(c_int) function meu_ensemble_create(n, params, flags, e) bind(C, name="meu_ensemble_create")
+      import :: c_int, c_int32_t, c_ptr, meu_params
+      integer(c_int32_t), value :: n, flags
+      type(meu_params), intent(in) :: params(*)
+      type(c_ptr), intent(out) :: e
+    end function
+    integer(c_int) function meu_ensemble_set_fields(e, member, cons, phi) bind(C, name="meu_ensemble_set_fields")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: e, cons, phi
+      integer(c_int32_t), value :: member
+    end function
+    ! diag: NULL or n_members * nsteps rows, member-major
+    integer(c_int) function meu_ensemble_run(e, nsteps, diag) bind(C, name="meu_ensemble_run")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: e, diag
+      integer(c_int32_t), value :: nsteps
+    end function
+    integer(c_int) function meu_ensemble_get_fields(e, member, cons, phi, el_en) bind(C, name="meu_ensemble_get_fields")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: e, cons, phi, el_en
+      integer(c_int32_t), value :: member
+    end function
+    integer(c_int) function meu_ensemble_destroy(e) bind(C, name="meu_ensemble_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: e
+    end function
   end interface
 
 contains
