@@ -188,6 +188,16 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     }
   }
   for (int i = 0; i < 36; ++i) hK.c0m[i] = p.cela[1][i];
+  {
+    // Q_il = -sum_{j,k} C0(voigt(i,j), voigt(k,l)) K_kj, K_kk = a_k^2, K_kj = b_k b_j (k != j)
+    auto vq = [](int i, int j) { return i == j ? i : 9 - i - j; };
+    const int mi[6] = {1, 2, 3, 2, 1, 1}, ml[6] = {1, 2, 3, 3, 3, 2};
+    auto kidx = [](int k, int j) { return k == j ? k - 1 : (k + j == 5 ? 3 : (k + j == 4 ? 4 : 5)); };
+    for (int m = 0; m < 6; ++m)
+      for (int j = 1; j <= 3; ++j)
+        for (int k = 1; k <= 3; ++k)
+          hK.qcoef[m][kidx(k, j)] -= p.cela[1][(vq(mi[m], j) - 1) + (vq(k, ml[m]) - 1) * 6];
+  }
   // proportional compliances: S_n = alpha_n S_1 for every phase (and a non-zero matrix)
   {
     bool prop = p.cela[0][0] > 0;
@@ -296,13 +306,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   if (fused) {
     LanFusedConst F;
     memset(&F, 0, sizeof(F));
-    // Q_il = -sum_{j,k} C0(voigt(i,j), voigt(k,l)) K_kj, K_kk = a_k^2, K_kj = b_k b_j (k != j)
-    const int mi[6] = {1, 2, 3, 2, 1, 1}, ml[6] = {1, 2, 3, 3, 3, 2};
-    auto kidx = [](int k, int j) { return k == j ? k - 1 : (k + j == 5 ? 3 : (k + j == 4 ? 4 : 5)); };
-    for (int m = 0; m < 6; ++m)
-      for (int j = 1; j <= 3; ++j)
-        for (int k = 1; k <= 3; ++k)
-          F.qcoef[m][kidx(k, j)] -= p.cela[1][(vg(mi[m], j) - 1) + (vg(k, ml[m]) - 1) * 6];
+    memcpy(F.qcoef, hK.qcoef, sizeof(F.qcoef));
     for (int v = 0; v < V; ++v) {
       for (int m = 0; m < 6; ++m) {
         F.sig0[v][m] = hK.sig0[v][m];
@@ -573,7 +577,10 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
       niter += 1;
       total += 1;
       if (total > 100000) throw CudaError("elastic iteration runaway", MEU_ERR_NOT_CONVERGED);
-      KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
+      if (hK.prop_moduli)
+        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R, true><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
+      else
+        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R, false><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
       std::vector<const R*> in;
       for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
       fwd_list(in, 0);
@@ -613,7 +620,12 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
     }
   }
   last_iters = total;
-  KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+  if (hK.prop_moduli)
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, true><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+                                                  (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
+                                                  partials, d_err));
+  else
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, false><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
                                                   partials, d_err));
 }

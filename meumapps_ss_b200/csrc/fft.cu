@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "fused.cuh"
 
 namespace meu {
 
@@ -146,10 +147,12 @@ __global__ void __launch_bounds__(256) k_rows_r2c(PtrList<const R> in, PtrList<c
   const int nr = (int)min((int64_t)rpb, nrows - row0);
   const R* src = in.p[blockIdx.y] + row0 * nx;
   C* dst = out.p[blockIdx.y] + row0 * nxh;
+  // asynchronous copies: every load of the tile is in flight at once
   for (int i = threadIdx.x; i < nr * L; i += blockDim.x) {
     int r = i / L, n = i - r * L;
-    buf[r * pitch + n] = ((const C*)(src + (int64_t)r * nx))[n];
+    fz::cp_async_c(buf + r * pitch + n, (const C*)(src + (int64_t)r * nx) + n);
   }
+  fz::cp_async_wait_all();
   __syncthreads();
   fft_dif(buf, pl, nr, pitch, 1);
   // split: X[k] = E + W^k O with E = (Z[k] + conj Z[L-k])/2, O = -i (Z[k] - conj Z[L-k])/2
@@ -195,6 +198,7 @@ __global__ void __launch_bounds__(256) k_rows_c2r(PtrList<const cplx<R>> in, Ptr
   for (int i = threadIdx.x; i < L; i += blockDim.x) posk[pl.rev[i]] = i;
   __syncthreads();
   const int npair = L / 2 + 1;
+#pragma unroll 4
   for (int i = threadIdx.x; i < nr * npair; i += blockDim.x) {
     int r = i / npair, k = i - r * npair;
     const C* srow = src + (int64_t)r * nxh;
@@ -239,8 +243,9 @@ __global__ void __launch_bounds__(256) k_cols(PtrList<cplx<R>> in, PtrList<cplx<
   for (int i = threadIdx.x; i < L * nc; i += blockDim.x) {
     int l = i / nc, c = i - l * nc;
     int gl = FWD ? l : rev[l];
-    buf[l * tm + c] = src[(int64_t)gl * inner + c];
+    fz::cp_async_c(buf + l * tm + c, src + (int64_t)gl * inner + c);
   }
+  fz::cp_async_wait_all();
   __syncthreads();
   if (FWD) fft_dif(buf, pl, nc, 1, tm);
   else fft_dit(buf, pl, nc, 1, tm);

@@ -230,9 +230,9 @@ struct Plane {
       o = mk(o.y, -o.x);
       const C xk = cadd(e, Tw<C>::mul(o, post, k, NXH));
       if (k == 0) {
-        // X[0] = E + O, X[LX] = E - O
-        rb[0] = xk;
-        rb[LX] = csub(e, o);
+        // X[0] = E + O and X[LX] = E - O are real: packed as X[0] + i X[LX] into
+        // column 0, so the y transform runs over LX columns instead of LX + 1
+        rb[0] = mk(xk.x, csub(e, o).x);
       } else {
         rb[pk] = xk;
         if (k != LX - k) {
@@ -244,7 +244,21 @@ struct Plane {
       }
     }
     __syncthreads();
-    dif<C, NY, NXH, 1, PITCH, NT, PV>(buf, twy);
+    dif<C, NY, LX, 1, PITCH, NT, PV>(buf, twy);
+    // unpack column 0: Z = Y0 + i YN  ->  Y0(ky) = (Z(ky) + conj Z(-ky)) / 2 into column 0,
+    // YN(ky) = -i (Z(ky) - conj Z(-ky)) / 2 into column LX (rows in digit-reversed order)
+    for (int ky = threadIdx.x; ky <= NY / 2; ky += NT) {
+      const int p1 = pos<NY, PV>(ky), p2 = pos<NY, PV>((NY - ky) % NY);
+      const C z1 = buf[p1 * PITCH], z2 = buf[p2 * PITCH];
+      const C y0 = cscale(cadd(z1, cconj(z2)), (R)0.5);
+      const C d = cscale(csub(z1, cconj(z2)), (R)0.5);
+      const C yn = mk(d.y, -d.x);
+      buf[p1 * PITCH] = y0;
+      buf[p1 * PITCH + LX] = yn;
+      buf[p2 * PITCH] = cconj(y0);
+      buf[p2 * PITCH + LX] = cconj(yn);
+    }
+    __syncthreads();
   }
 
   // inverse of forward(): M-form plane -> rows of (x[2n], x[2n+1]), unscaled.
@@ -252,7 +266,14 @@ struct Plane {
     const C* twx = tws;
     const C* twy = tws + LX * K;
     const C* post = tws + (LX + NY) * K;
-    dit<C, NY, NXH, 1, PITCH, NT, PV>(buf, twy);
+    // columns 0 and LX (Hermitian in ky) packed as X0 + i XN, so the inverse y
+    // transform runs over LX columns; its column 0 then holds x0 + i xN, both real
+    for (int y = threadIdx.x; y < NY; y += NT) {
+      const C x0 = buf[y * PITCH], xn = buf[y * PITCH + LX];
+      buf[y * PITCH] = mk(x0.x - xn.y, x0.y + xn.x);
+    }
+    __syncthreads();
+    dit<C, NY, LX, 1, PITCH, NT, PV>(buf, twy);
     constexpr int NP = LX / 2 + 1;
 #pragma unroll 1
     for (int i = threadIdx.x; i < NY * NP; i += NT) {
@@ -260,8 +281,15 @@ struct Plane {
       C* rb = buf + row * PITCH;
       const int pk = (k == 0) ? 0 : pos<LX, PV>(k);
       const int pm = (k == 0) ? LX : pos<LX, PV>(LX - k);
-      C xk = rb[pk], xm = rb[pm];
-      if (k == 0) { xk.y = 0; xm.y = 0; }
+      C xk, xm;
+      if (k == 0) {
+        const C z = rb[0];
+        xk = mk(z.x, (R)0);
+        xm = mk(z.y, (R)0);
+      } else {
+        xk = rb[pk];
+        xm = rb[pm];
+      }
       {
         const C ex = cadd(xk, cconj(xm));
         const C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, NXH);

@@ -31,6 +31,9 @@ struct DevConst {
   double sig0_ebar[MEU_MAX_VAR];       // sig0_v : e_mean
   double ebar_eng[6];                  // e_mean with engineering shear
   double c0m[36];                      // C0 = CEla(:,:,2) (column-major)
+  // Q(k) as 6 unique entries (11,22,33,23,13,12): Q_m = sum_n qcoef[m][n] Kv_n,
+  // Kv = (a1^2, a2^2, a3^2, b2 b3, b1 b3, b1 b2) (the fused Landau kernels' form)
+  double qcoef[6][6];
   int use_var[MEU_MAX_VAR];            // elener: variant contributes (transsum > 1e-9)
   // prop_moduli: every phase's compliance is alpha[n] * SEla(:,:,1), so the mixed
   // stiffness (sum_v P_v S_n(v) + w S_1)^-1 is CEla(:,:,1) / (sum_v alpha P_v + w)
@@ -108,6 +111,15 @@ __device__ __forceinline__ void block_reduce_store(double v, int op, double* out
 
 // --------------------------------------------------------------- k helpers
 __device__ __forceinline__ void kdecode(const DevConst& K, int64_t id, int& kx, int& ky, int& kz) {
+  if (K.nk < ((int64_t)1 << 31)) {
+    // 32-bit division (a 64-bit one is a long software sequence on the GPU)
+    const unsigned u = (unsigned)id, nxh = (unsigned)K.nxh, ny = (unsigned)K.ny;
+    const unsigned r = u / nxh;
+    kx = (int)(u - r * nxh);
+    kz = (int)(r / ny);
+    ky = (int)(r - (unsigned)kz * ny);
+    return;
+  }
   kx = (int)(id % K.nxh);
   int64_t r = id / K.nxh;
   ky = (int)(r % K.ny);
@@ -208,8 +220,7 @@ __device__ int invert_small(double* a, int n, int flag) {
     for (int i = 0; i < n; ++i) s += fabs(a[i + j * n]);
     inorm = fmax(inorm, s);
   }
-  const double rcond = 1.0 / (anorm * inorm);
-  if (!(rcond > 1e-16)) return flag;
+  if (!(anorm * inorm < 1e16)) return flag;  // rcond = 1 / (|A| |A^-1|) > 1e-16
   return 0;
 }
 
@@ -258,7 +269,7 @@ __device__ __forceinline__ int invert6(double* a, int flag) {
       anorm = fmax(anorm, sa);
       inorm = fmax(inorm, si);
     }
-    if (1.0 / (anorm * inorm) > 1e-16) {
+    if (anorm * inorm < 1e16) {  // rcond > 1e-16
 #pragma unroll
       for (int i = 0; i < 36; ++i) a[i] = b[i];
       return 0;
@@ -281,8 +292,8 @@ __device__ __forceinline__ int invert3(double* q, int flag) {
   o[2] = Cc * r; o[5] = -(a * h - b * g) * r; o[8] = (a * e - b * d) * r;
   const double inorm = fmax(fabs(o[0]) + fabs(o[1]) + fabs(o[2]), fmax(fabs(o[3]) + fabs(o[4]) + fabs(o[5]), fabs(o[6]) + fabs(o[7]) + fabs(o[8])));
   for (int k = 0; k < 9; ++k) q[k] = o[k];
-  const double rcond = 1.0 / (anorm * inorm);
-  if (!(rcond > 1e-16)) return flag;
+  // rcond = 1 / (|Q| |Q^-1|) > 1e-16, tested without a second division
+  if (!(anorm * inorm < 1e16)) return flag;
   return 0;
 }
 

@@ -206,8 +206,10 @@ __global__ void __launch_bounds__(256) k_el_zeroth(const DevConst* __restrict__ 
 
 // --------------------------------------------------- elastic: polarisation x
 // ModElastic.f:248-327.  strain = engineering gamma (6), xs out (6).
-template <typename R>
-__global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
+// PROP: every phase compliance is a multiple of the matrix's (K.prop_moduli); the
+// general variant carries the per-voxel 6x6 inversion and its registers.
+template <typename R, bool PROP>
+__global__ void __launch_bounds__(256, PROP ? 4 : 1) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
                                               const R* __restrict__ strain, R* __restrict__ xs, double cfac, int* err) {
   const DevConst& K = *Kp;
   const meu_params& p = K.p;
@@ -220,7 +222,8 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
 #pragma unroll
       for (int m = 0; m < 6; ++m) e0[m] += pv * K.eps_eng[v][m];
     }
-    if (K.prop_moduli) {
+    if constexpr (PROP) {
+      // C(x) = C_1 / s: x = cfac C0 gamma + (C_1 / s)(e0 - cfac gamma), no 6x6 matrix per voxel
       double sc = 0;
       for (int n = 2; n <= p.numph; ++n)
         for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
@@ -231,8 +234,23 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
       if (psum < 1.0) sc += 1.0 - psum;
       if (!(sc != 0.0)) set_err(err, MEU_ERR_C_SINGULAR);
       const double r = 1.0 / sc;
+      double gam[6], d[6];
 #pragma unroll
-      for (int i = 0; i < 36; ++i) Cm[i] = p.cela[0][i] * r;
+      for (int m = 0; m < 6; ++m) {
+        gam[m] = (double)strain[(int64_t)m * n3 + id] + K.ebar_eng[m];
+        d[m] = e0[m] - cfac * gam[m];
+      }
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        double a0 = 0, a1 = 0;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          a0 += K.c0m[i + m * 6] * gam[m];
+          a1 += p.cela[0][i + m * 6] * d[m];
+        }
+        xs[(int64_t)i * n3 + id] = (R)(cfac * a0 + r * a1);
+      }
+      continue;
     } else {
 #pragma unroll
       for (int i = 0; i < 36; ++i) Cm[i] = 0;
@@ -269,7 +287,7 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
 // ModElastic.f:340-394: u^ = Qinv (kf . x^), gamma^ of u^ written over x^.
 // Convergence sums (ModElastic.f:413-430) by Parseval against the previous u^.
 template <typename R>
-__global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict__ Kp, PtrList<cplx<R>> xk,
+__global__ void __launch_bounds__(RED_THREADS, 3) k_el_k(const DevConst* __restrict__ Kp, PtrList<cplx<R>> xk,
                                                       cplx<R>* __restrict__ uk, double* partials, int* err) {
   const DevConst& K = *Kp;
   const int64_t nk = K.nk;
@@ -325,8 +343,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict
 // -------------------------------------------------------------- elener
 // ModElastic.f:540-687.  mode 0 (KKS): fdiff += el_grad; mode 1 (Landau): elg = el_grad.
 // theta' = 30 f^2 (f^2 - 2f + 1) (KKS and Landau h coupling) or 2 eta (eta^2 coupling).
-template <typename R>
-__global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
+template <typename R, bool PROP>
+__global__ void __launch_bounds__(RED_THREADS, PROP ? 4 : 1) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
                                                         const R* __restrict__ pphi, const R* __restrict__ strain,
                                                         R* __restrict__ el_en, R* __restrict__ elg, int mode, int eta2,
                                                         double* partials, int* err) {
@@ -349,15 +367,21 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
       const double gm = (double)strain[(int64_t)m * n3 + id];
       eps[m] = (m < 3) ? (p.e_mean[m] + gm - te[m]) : (2.0 * p.e_mean[m] + gm - 2.0 * te[m]);
     }
-    double Cm[36];
-    if (K.prop_moduli) {
+    double Cm[36], sig[6];
+    if constexpr (PROP) {
+      // C(x) = C_1 / s: sigma = (C_1 eps) / s without a per-voxel matrix
       double sc = 1.0 - psum;
       for (int n = 2; n <= p.numph; ++n)
         for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) sc += K.alpha[n - 1] * P[v];
       if (!(sc != 0.0)) set_err(err, MEU_ERR_C_ELENER_SINGULAR);
       const double r = 1.0 / sc;
 #pragma unroll
-      for (int i = 0; i < 36; ++i) Cm[i] = p.cela[0][i] * r;
+      for (int i = 0; i < 6; ++i) {
+        double a = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) a += p.cela[0][i + j * 6] * eps[j];
+        sig[i] = a * r;
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < 36; ++i) Cm[i] = (1.0 - psum) * p.sela[0][i];
@@ -367,14 +391,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
           for (int i = 0; i < 36; ++i) Cm[i] += P[v] * p.sela[n - 1][i];
         }
       set_err(err, invert6(Cm, MEU_ERR_C_ELENER_SINGULAR));
-    }
-    double sig[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      double s = 0;
+      for (int i = 0; i < 6; ++i) {
+        double s = 0;
 #pragma unroll
-      for (int j = 0; j < 6; ++j) s += Cm[i + j * 6] * eps[j];
-      sig[i] = s;
+        for (int j = 0; j < 6; ++j) s += Cm[i + j * 6] * eps[j];
+        sig[i] = s;
+      }
     }
     double elmat = 0;
 #pragma unroll
@@ -390,7 +413,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
       for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
         if (!K.use_var[v]) continue;
         double elp = 0;
-        if (K.prop_moduli) {
+        if constexpr (PROP) {
           elp = K.alpha[n - 1] * elmat;
         } else {
 #pragma unroll
