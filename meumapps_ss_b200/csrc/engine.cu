@@ -339,6 +339,19 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   if (uk) MEU_CUDA(cudaMemset(uk, 0, sizeof(C) * 3 * nk));
   stage_elems = std::min<int64_t>(n3 * std::max(std::max(V, E), 1), (int64_t)32 << 20);
   stage = dalloc<double>(stage_elems);
+  {
+    int dev = 0, sms = 0;
+    MEU_CUDA(cudaGetDevice(&dev));
+    MEU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    auto resident = [&](const void* fn) {
+      int nb = 0;
+      MEU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, RED_THREADS, 0));
+      return std::max(1, std::min(RED_BLOCKS, nb * sms));
+    };
+    g_el_k = resident((const void*)k_el_k<R>);
+    g_lan_k1 = resident((const void*)k_lan_k1<R>);
+    g_elener = hK.prop_moduli ? resident((const void*)k_elener<R, true>) : resident((const void*)k_elener<R, false>);
+  }
   if (fused) {
     MEU_CUDA(cudaMemset(sp, 0, sizeof(C) * (size_t)NS * nk));
     if (p.flags & MEU_FLAG_AUTOTUNE) {
@@ -584,7 +597,7 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
       std::vector<const R*> in;
       for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
       fwd_list(in, 0);
-      KLAUNCH("el_k", 18.0 * nk * sizeof(C), k_el_k<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, 6), uk, partials, d_err));
+      KLAUNCH("el_k", 18.0 * nk * sizeof(C), k_el_k<R><<<g_el_k, RED_THREADS, 0, st>>>(dK, specs(0, 6), uk, partials, d_err));
       std::vector<R*> out;
       for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
       inv_list(0, out);
@@ -621,11 +634,11 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
   }
   last_iters = total;
   if (hK.prop_moduli)
-    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, true><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, true><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
                                                   partials, d_err));
   else
-    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, false><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, false><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
                                                   partials, d_err));
 }
@@ -802,7 +815,7 @@ void Engine<R>::landau_step(meu_diag* d) {
     fwd_list(in, 0);
   }
   KLAUNCH("lan_k1", (double)(homog ? 3 * V + 4 : 2 * V + 4) * nk * sizeof(C),
-          k_lan_k1<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, specs(0, V + 1), V, kc, keta, homog ? 1 : 0,
+          k_lan_k1<R><<<g_lan_k1, RED_THREADS, 0, st>>>(dK, specs(0, V + 1), V, kc, keta, homog ? 1 : 0,
                                                           P.diag_energy, partials, d_err));
   R* phel = field(wr, 1);  // V fields: strain interaction (homog) or el_grad (hetero)
   {

@@ -234,6 +234,9 @@ class Engine : public EngineBase {
   int* d_ticket = nullptr;
   int fnb[Q_TOTAL] = {0};
   static constexpr int GRAPH_STEPS = 8;
+  // grids of grid-stride reduction kernels sized to the blocks that fit at once (a
+  // partial second wave would redo a whole share of the loop); <= RED_BLOCKS
+  int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS;
   bool fused_warm = false;
   bool theta_ready = false;  // sp holds theta^ of the current fields (written by the last step's PI)
   bool fields_set = false;  // the spectral-state layout is fixed from the first upload on

@@ -287,19 +287,37 @@ __global__ void __launch_bounds__(256, PROP ? 4 : 1) k_el_x(const DevConst* __re
 // ModElastic.f:340-394: u^ = Qinv (kf . x^), gamma^ of u^ written over x^.
 // Convergence sums (ModElastic.f:413-430) by Parseval against the previous u^.
 template <typename R>
-__global__ void __launch_bounds__(RED_THREADS, 3) k_el_k(const DevConst* __restrict__ Kp, PtrList<cplx<R>> xk,
+__global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict__ Kp, PtrList<cplx<R>> xk,
                                                       cplx<R>* __restrict__ uk, double* partials, int* err) {
+  using C = cplx<R>;
   const DevConst& K = *Kp;
-  const int64_t nk = K.nk;
+  const int64_t nk = K.nk, stride = (int64_t)gridDim.x * blockDim.x;
   double e[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < nk; id += (int64_t)gridDim.x * blockDim.x) {
+  // software pipeline: the next k's nine loads are in flight during this k's FP64 work
+  int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  C x[6], u[3];
+  if (id < nk) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) x[m] = xk.p[m][id];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) u[i] = uk[(int64_t)i * nk + id];
+  }
+  for (; id < nk; id += stride) {
+    const int64_t nid = id + stride;
+    C xn[6], un[3];
+    if (nid < nk) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) xn[m] = xk.p[m][nid];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) un[i] = uk[(int64_t)i * nk + nid];
+    }
     int kx, ky, kz;
     kdecode(K, id, kx, ky, kz);
     double a[3], b[3];
     kvec(K, kx, ky, kz, a, b);
     double xr[6], xi[6];
 #pragma unroll
-    for (int m = 0; m < 6; ++m) ld2(xk.p[m][id], xr[m], xi[m]);
+    for (int m = 0; m < 6; ++m) { xr[m] = (double)x[m].x; xi[m] = (double)x[m].y; }
     // R = kf . x (Voigt 1..6 -> x1 x2 x3 x4 x5 x6)
     const double tr1 = xr[0] * b[0] + xr[5] * b[1] + xr[4] * b[2], ti1 = xi[0] * b[0] + xi[5] * b[1] + xi[4] * b[2];
     const double tr2 = xr[5] * b[0] + xr[1] * b[1] + xr[3] * b[2], ti2 = xi[5] * b[0] + xi[1] * b[1] + xi[3] * b[2];
@@ -319,8 +337,7 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_el_k(const DevConst* __restr
     const double w = hweight(K, kx);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      double orr, oi;
-      ld2(uk[(int64_t)i * nk + id], orr, oi);
+      const double orr = (double)u[i].x, oi = (double)u[i].y;
       const double dr = ur[i] - orr, di = ui[i] - oi;
       e[2 * i] += w * (dr * dr + di * di);
       e[2 * i + 1] += w * (orr * orr + oi * oi);
@@ -335,6 +352,10 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_el_k(const DevConst* __restr
       else { gr = -(b[i] * ui[j] + b[j] * ui[i]); gi = b[i] * ur[j] + b[j] * ur[i]; }
       xk.p[m][id] = mk((R)gr, (R)gi);
     }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) x[m] = xn[m];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) u[i] = un[i];
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) block_reduce_store(e[q], 0, partials + (Q_ERR0 + q) * PSTRIDE + blockIdx.x);
