@@ -350,7 +350,48 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     };
     g_el_k = resident((const void*)k_el_k<R>);
     g_lan_k1 = resident((const void*)k_lan_k1<R>);
-    g_elener = hK.prop_moduli ? resident((const void*)k_elener<R, true>) : resident((const void*)k_elener<R, false>);
+    g_elener = resident((const void*)k_elener<R, false>);
+    if (hK.prop_moduli) {
+      ElxProp& X = el_prop;
+      for (int i = 0; i < 36; ++i) {
+        X.c0[i] = hK.c0m[i];
+        X.c1[i] = p.cela[0][i];
+      }
+      for (int m = 0; m < 6; ++m) X.ebar[m] = hK.ebar_eng[m];
+      for (int v = 0; v < V; ++v) {
+        const int n = hK.var_phase[v];
+        for (int m = 0; m < 6; ++m) X.ep[v][m] = hK.eps_eng[v][m];
+        X.av[v] = n >= 2 ? hK.alpha[n - 1] : 0.0;
+        X.inc[v] = n >= 2 ? 1.0 : 0.0;
+      }
+      X.nvar = V;
+      ElenProp& Y = en_prop;
+      for (int i = 0; i < 36; ++i) {
+        Y.c1[i] = p.cela[0][i];
+        Y.s1[i] = p.sela[0][i];
+      }
+      for (int m = 0; m < 6; ++m) Y.emean[m] = p.e_mean[m];
+      for (int v = 0; v < V; ++v) {
+        const int n = hK.var_phase[v];
+        for (int m = 0; m < 6; ++m) Y.tp[v][m] = p.trans_ppt[v][m];
+        Y.av[v] = n >= 2 ? hK.alpha[n - 1] : 0.0;
+        Y.use[v] = (n >= 2 && hK.use_var[v]) ? 1 : 0;
+      }
+      Y.nvar = V;
+      g_elener = V == 1   ? resident((const void*)k_elener_prop<R, 1>)
+                 : V == 2 ? resident((const void*)k_elener_prop<R, 2>)
+                 : V == 3 ? resident((const void*)k_elener_prop<R, 3>)
+                 : V == 4 ? resident((const void*)k_elener_prop<R, 4>)
+                          : resident((const void*)k_elener_prop<R, 0>);
+      const void* fn = V == 1   ? (const void*)k_el_x_prop<R, 1>
+                       : V == 2 ? (const void*)k_el_x_prop<R, 2>
+                       : V == 3 ? (const void*)k_el_x_prop<R, 3>
+                       : V == 4 ? (const void*)k_el_x_prop<R, 4>
+                                : (const void*)k_el_x_prop<R, 0>;
+      int nb = 0;
+      MEU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 256, 0));
+      g_el_x = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(nb, 1) * sms, (n3 + 255) / 256));
+    }
   }
   if (fused) {
     MEU_CUDA(cudaMemset(sp, 0, sizeof(C) * (size_t)NS * nk));
@@ -590,10 +631,22 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
       niter += 1;
       total += 1;
       if (total > 100000) throw CudaError("elastic iteration runaway", MEU_ERR_NOT_CONVERGED);
-      if (hK.prop_moduli)
-        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R, true><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
-      else
-        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R, false><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
+      if (hK.prop_moduli) {
+        const ElxProp& E = el_prop;
+        switch (V) {
+#define MEU_ELX(VV)                                                                                            \
+  case VV:                                                                                                      \
+    KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),                                                          \
+            k_el_x_prop<R, VV><<<g_el_x, 256, 0, st>>>(E, (int64_t)n3, pphi, strain, xs, cfac, d_err));         \
+    break;
+          MEU_ELX(1) MEU_ELX(2) MEU_ELX(3) MEU_ELX(4)
+#undef MEU_ELX
+          default:
+            KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
+                    k_el_x_prop<R, 0><<<g_el_x, 256, 0, st>>>(E, (int64_t)n3, pphi, strain, xs, cfac, d_err));
+        }
+      } else
+        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
       std::vector<const R*> in;
       for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
       fwd_list(in, 0);
@@ -633,11 +686,24 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
     }
   }
   last_iters = total;
-  if (hK.prop_moduli)
-    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, true><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
-                                                  (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
-                                                  partials, d_err));
-  else
+  const int eta2 = (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0;
+  if (hK.prop_moduli) {
+    const ElenProp& E = en_prop;
+    switch (V) {
+#define MEU_ELEN(VV)                                                                                                 \
+  case VV:                                                                                                           \
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R),                                                  \
+            k_elener_prop<R, VV><<<g_elener, RED_THREADS, 0, st>>>(E, (int64_t)n3, ph_for_ppr, pphi, strain, el_en,  \
+                                                                   elg, mode, eta2, partials, d_err));                \
+    break;
+      MEU_ELEN(1) MEU_ELEN(2) MEU_ELEN(3) MEU_ELEN(4)
+#undef MEU_ELEN
+      default:
+        KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R),
+                k_elener_prop<R, 0><<<g_elener, RED_THREADS, 0, st>>>(E, (int64_t)n3, ph_for_ppr, pphi, strain, el_en,
+                                                                      elg, mode, eta2, partials, d_err));
+    }
+  } else
     KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, false><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
                                                   partials, d_err));

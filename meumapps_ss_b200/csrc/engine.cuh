@@ -13,6 +13,25 @@
 #include "landau_fused.cuh"
 
 namespace meu {
+// proportional-moduli polarization coefficients, passed by value to k_el_x_prop
+struct ElxProp {
+  double c0[36], c1[36], ebar[6];
+  double ep[MEU_MAX_VAR][6];
+  double av[MEU_MAX_VAR];   // alpha of the variant's phase, 0 for phase-1 variants
+  double inc[MEU_MAX_VAR];  // 1 when the variant counts toward sum P (phase >= 2)
+  int nvar;
+};
+// proportional-moduli elastic-energy coefficients, passed by value to k_elener_prop
+struct ElenProp {
+  double c1[36], s1[36], emean[6];
+  double tp[MEU_MAX_VAR][6];  // trans_ppt (tensor shear)
+  double av[MEU_MAX_VAR];     // alpha of the variant's phase, 0 for phase-1 variants
+  int use[MEU_MAX_VAR];       // phase >= 2 and use_var: gets an energy share and a driving force
+  int nvar;
+};
+}  // namespace meu
+
+namespace meu {
 
 // ==========================================================================
 // Launch counter and per-kernel CUDA-event timing (off unless requested).
@@ -236,7 +255,9 @@ class Engine : public EngineBase {
   static constexpr int GRAPH_STEPS = 8;
   // grids of grid-stride reduction kernels sized to the blocks that fit at once (a
   // partial second wave would redo a whole share of the loop); <= RED_BLOCKS
-  int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS;
+  int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS, g_el_x = RED_BLOCKS;
+  ElxProp el_prop{};  // proportional-moduli polarization coefficients (host-built)
+  ElenProp en_prop{};  // proportional-moduli energy coefficients (host-built)
   bool fused_warm = false;
   bool theta_ready = false;  // sp holds theta^ of the current fields (written by the last step's PI)
   bool fields_set = false;  // the spectral-state layout is fixed from the first upload on

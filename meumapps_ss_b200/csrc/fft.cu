@@ -1,5 +1,6 @@
 // fft.cu -- batched 3-D R2C / C2R transforms (see fft.cuh).
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "fft.cuh"
@@ -258,6 +259,121 @@ __global__ void __launch_bounds__(256) k_cols(PtrList<cplx<R>> in, PtrList<cplx<
   }
 }
 
+// ----------------------------------------------- compile-time specialisations
+// The same transforms with the length, radix plan and line count as template
+// constants (the stage loops of fused.cuh): index arithmetic folds to shifts and
+// constant multiplies, and the digit reversal is computed instead of read from
+// the table.  Lengths 32..512 (powers of two) take these; other lengths keep the
+// run-time plan above.
+constexpr int rows_per_block_c(int L) { return 2048 / L < 1 ? 1 : (2048 / L > 64 ? 64 : 2048 / L); }
+
+template <typename R, int L, int PV>
+__global__ void __launch_bounds__(256) k_rows_r2c_s(PtrList<const R> in, PtrList<cplx<R>> out, int64_t nrows,
+                                                    const cplx<R>* __restrict__ tw, const cplx<R>* __restrict__ post) {
+  using C = cplx<R>;
+  constexpr int NR = rows_per_block_c(L), P = L + 1, NXH = L + 1, NP = L / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  const int64_t row0 = (int64_t)blockIdx.x * NR;
+  const int nr = (int)min((int64_t)NR, nrows - row0);
+  const C* src = (const C*)(in.p[blockIdx.y] + row0 * (2 * L));
+  C* dst = out.p[blockIdx.y] + row0 * NXH;
+  // a tile of nr rows is nr * L contiguous complex pairs of reals
+  for (int i = threadIdx.x; i < nr * L; i += 256) fz::cp_async_c(buf + (i / L) * P + (i % L), src + i);
+  fz::cp_async_wait_all();
+  __syncthreads();
+  fz::dif<C, L, NR, P, 1, 256, PV>(buf, tw);
+  for (int i = threadIdx.x; i < nr * NP; i += 256) {
+    const int r = i / NP, k = i - r * NP;
+    const int km = k == 0 ? 0 : L - k;
+    const C zk = buf[r * P + fz::pos<L, PV>(k)], zm = buf[r * P + fz::pos<L, PV>(km)];
+    C* drow = dst + (int64_t)r * NXH;
+    {
+      C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
+      C o = cscale(csub(zk, cconj(zm)), (R)0.5);
+      o = mk(o.y, -o.x);
+      drow[k] = cadd(e, Tw<C>::mul(o, post, k, NXH));
+    }
+    if (k != L - k) {
+      C e = cscale(cadd(zm, cconj(zk)), (R)0.5);
+      C o = cscale(csub(zm, cconj(zk)), (R)0.5);
+      o = mk(o.y, -o.x);
+      drow[L - k] = cadd(e, Tw<C>::mul(o, post, L - k, NXH));
+    }
+  }
+}
+
+template <typename R, int L, int PV>
+__global__ void __launch_bounds__(256) k_rows_c2r_s(PtrList<const cplx<R>> in, PtrList<R> out, int64_t nrows,
+                                                    const cplx<R>* __restrict__ tw, const cplx<R>* __restrict__ post) {
+  using C = cplx<R>;
+  constexpr int NR = rows_per_block_c(L), P = L + 1, NXH = L + 1, NP = L / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  const int64_t row0 = (int64_t)blockIdx.x * NR;
+  const int nr = (int)min((int64_t)NR, nrows - row0);
+  const C* src = in.p[blockIdx.y] + row0 * NXH;
+  C* dst = (C*)(out.p[blockIdx.y] + row0 * (2 * L));
+  for (int i = threadIdx.x; i < nr * NP; i += 256) {
+    const int r = i / NP, k = i - r * NP;
+    const C* srow = src + (int64_t)r * NXH;
+    C xk = srow[k], xm = srow[L - k];
+    if (k == 0) { xk.y = 0; xm.y = 0; }
+    {
+      C ex = cadd(xk, cconj(xm));
+      C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, NXH);
+      buf[r * P + fz::pos<L, PV>(k)] = cadd(ex, mk(-ox.y, ox.x));
+    }
+    if (k != 0 && k != L - k) {
+      C ex = cadd(xm, cconj(xk));
+      C ox = Tw<C>::mulc(csub(xm, cconj(xk)), post, L - k, NXH);
+      buf[r * P + fz::pos<L, PV>(L - k)] = cadd(ex, mk(-ox.y, ox.x));
+    }
+  }
+  __syncthreads();
+  fz::dit<C, L, NR, P, 1, 256, PV>(buf, tw);
+  for (int i = threadIdx.x; i < nr * L; i += 256) dst[i] = buf[(i / L) * P + (i % L)];
+}
+
+// TM columns of length L per block; element l of column (o, c) at o*ostride + l*inner + c.
+template <typename R, bool FWD, int L, int TM, int PV>
+__global__ void __launch_bounds__(256) k_cols_s(PtrList<cplx<R>> in, PtrList<cplx<R>> out, int inner, int64_t ostride,
+                                                const cplx<R>* __restrict__ tw, R scale) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  const int tiles = (inner + TM - 1) / TM;
+  const int o = blockIdx.x / tiles, t = blockIdx.x - o * tiles;
+  const int c0 = t * TM, nc = min(TM, inner - c0);
+  const C* src = in.p[blockIdx.y] + (int64_t)o * ostride + c0;
+  C* dst = out.p[blockIdx.y] + (int64_t)o * ostride + c0;
+  if (nc == TM) {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < L * TM; i += 256) {
+      const int l = i / TM, c = i % TM;
+      fz::cp_async_c(buf + i, src + (int64_t)(FWD ? l : fz::rev<L, PV>(l)) * inner + c);
+    }
+  } else {
+    for (int i = threadIdx.x; i < L * TM; i += 256) {
+      const int l = i / TM, c = i % TM;
+      if (c < nc) fz::cp_async_c(buf + i, src + (int64_t)(FWD ? l : fz::rev<L, PV>(l)) * inner + c);
+    }
+  }
+  fz::cp_async_wait_all();
+  __syncthreads();
+  if constexpr (FWD) fz::dif<C, L, TM, 1, TM, 256, PV>(buf, tw);
+  else fz::dit<C, L, TM, 1, TM, 256, PV>(buf, tw);
+#pragma unroll 4
+  for (int i = threadIdx.x; i < L * TM; i += 256) {
+    const int l = i / TM, c = i % TM;
+    if (nc == TM || c < nc) {
+      C v = buf[i];
+      if (FWD) v = cscale(v, scale);
+      dst[(int64_t)(FWD ? fz::rev<L, PV>(l) : l) * inner + c] = v;
+    }
+  }
+}
+
 // Raise a kernel's dynamic shared-memory limit to the opt-in maximum once
 // (227 KB per block on sm_100 minus the kernel's static shared memory).
 template <typename R>
@@ -275,6 +391,67 @@ static void set_smem(const void* fn, size_t bytes) {
   if ((int)bytes > lim) throw CudaError("transform tile exceeds shared memory", 103);
   MEU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
   done.push_back(fn);
+}
+
+// columns per block of the specialised column kernels: about 32 KB of tile
+template <typename R>
+constexpr int col_tile_s(int L) {
+  const int t = 32768 / (L * 2 * (int)sizeof(R));
+  return t < 4 ? 4 : (t > 16 ? 16 : t);
+}
+
+// Launch the specialised kernel for this length; false when L has none.
+template <typename R>
+static bool rows_s(bool fwd, int L, int nf, int64_t nrows, const void* in, const void* out, const void* tw,
+                   const void* post, cudaStream_t st) {
+  using C = cplx<R>;
+  auto go = [&](auto Lc) {
+    constexpr int LL = decltype(Lc)::value;
+    constexpr int NR = rows_per_block_c(LL);
+    const size_t sm = (size_t)NR * (LL + 1) * sizeof(C);
+    const dim3 g((unsigned)((nrows + NR - 1) / NR), nf);
+    if (fwd) {
+      set_smem<R>((const void*)k_rows_r2c_s<R, LL, 0>, sm);
+      k_rows_r2c_s<R, LL, 0><<<g, 256, sm, st>>>(*(const PtrList<const R>*)in, *(const PtrList<C>*)out, nrows,
+                                                  (const C*)tw, (const C*)post);
+    } else {
+      set_smem<R>((const void*)k_rows_c2r_s<R, LL, 0>, sm);
+      k_rows_c2r_s<R, LL, 0><<<g, 256, sm, st>>>(*(const PtrList<const C>*)in, *(const PtrList<R>*)out, nrows,
+                                                  (const C*)tw, (const C*)post);
+    }
+    return true;
+  };
+  switch (L) {
+    case 32: return go(std::integral_constant<int, 32>{});
+    case 64: return go(std::integral_constant<int, 64>{});
+    case 128: return go(std::integral_constant<int, 128>{});
+    case 256: return go(std::integral_constant<int, 256>{});
+    case 512: return go(std::integral_constant<int, 512>{});
+    default: return false;
+  }
+}
+
+template <typename R, bool FWD>
+static bool cols_s(int L, int nf, int outer, int inner, int64_t ostride, const PtrList<cplx<R>>& buf, const void* tw,
+                   R scale, cudaStream_t st) {
+  using C = cplx<R>;
+  auto go = [&](auto Lc) {
+    constexpr int LL = decltype(Lc)::value;
+    constexpr int TM = col_tile_s<R>(LL);
+    const size_t sm = (size_t)LL * TM * sizeof(C);
+    set_smem<R>((const void*)k_cols_s<R, FWD, LL, TM, 0>, sm);
+    const dim3 g((unsigned)(outer * ((inner + TM - 1) / TM)), nf);
+    k_cols_s<R, FWD, LL, TM, 0><<<g, 256, sm, st>>>(buf, buf, inner, ostride, (const C*)tw, scale);
+    return true;
+  };
+  switch (L) {
+    case 32: return go(std::integral_constant<int, 32>{});
+    case 64: return go(std::integral_constant<int, 64>{});
+    case 128: return go(std::integral_constant<int, 128>{});
+    case 256: return go(std::integral_constant<int, 256>{});
+    case 512: return go(std::integral_constant<int, 512>{});
+    default: return false;
+  }
 }
 
 static inline int col_tile(int L, bool fp64) {
@@ -303,7 +480,8 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
   set_smem<R>((const void*)k_rows_r2c<R>, sm);
   dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
   { HookScope hs_(hook, "fft_x_r2c", (double)nf * (n3() * sizeof(R) + nk() * sizeof(C)), st);
-  k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw); }
+  if (!rows_s<R>(true, Lx, nf, nrows, &in, &out, px.tw, post_tw, st))
+    k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
   // y columns: outer = z, inner = nxh
   {
@@ -312,7 +490,8 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     set_smem<R>((const void*)k_cols<R, true>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
     { HookScope hs_(hook, "fft_y_fwd", 2.0 * nf * nk() * sizeof(C), st);
-  k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
+  if (!cols_s<R, true>(ny, nf, nz, nxh, (int64_t)ny * nxh, out, py.tw, (R)1, st))
+    k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
   // z columns: outer = 1, inner = ny*nxh
@@ -323,7 +502,9 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     int inner = ny * nxh;
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
     { HookScope hs_(hook, "fft_z_fwd", 2.0 * nf * nk() * sizeof(C), st);
-  k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, (R)(1.0 / ((double)nx * ny * nz))); }
+  const R scale = (R)(1.0 / ((double)nx * ny * nz));
+  if (!cols_s<R, true>(nz, nf, 1, inner, 0, out, pz.tw, scale, st))
+    k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, scale); }
     MEU_CHECK_LAUNCH();
   }
 }
@@ -338,7 +519,8 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     int inner = ny * nxh;
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
     { HookScope hs_(hook, "fft_z_inv", 2.0 * nf * nk() * sizeof(C), st);
-  k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1); }
+  if (!cols_s<R, false>(nz, nf, 1, inner, 0, in, pz.tw, (R)1, st))
+    k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1); }
     MEU_CHECK_LAUNCH();
   }
   {
@@ -347,7 +529,8 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     set_smem<R>((const void*)k_cols<R, false>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
     { HookScope hs_(hook, "fft_y_inv", 2.0 * nf * nk() * sizeof(C), st);
-  k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
+  if (!cols_s<R, false>(ny, nf, nz, nxh, (int64_t)ny * nxh, in, py.tw, (R)1, st))
+    k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
   const int Lx = px.L;
@@ -359,7 +542,8 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
   for (int f = 0; f < MAXF; ++f) cin.p[f] = in.p[f];
   dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
   { HookScope hs_(hook, "fft_x_c2r", (double)nf * (n3() * sizeof(R) + nk() * sizeof(C)), st);
-  k_rows_c2r<R><<<g, 256, sm, st>>>(cin, out, nx, nrows, px, (const C*)post_tw); }
+  if (!rows_s<R>(false, Lx, nf, nrows, &cin, &out, px.tw, post_tw, st))
+    k_rows_c2r<R><<<g, 256, sm, st>>>(cin, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
 }
 

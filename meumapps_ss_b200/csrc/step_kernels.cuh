@@ -205,11 +205,11 @@ __global__ void __launch_bounds__(256) k_el_zeroth(const DevConst* __restrict__ 
 }
 
 // --------------------------------------------------- elastic: polarisation x
-// ModElastic.f:248-327.  strain = engineering gamma (6), xs out (6).
-// PROP: every phase compliance is a multiple of the matrix's (K.prop_moduli); the
-// general variant carries the per-voxel 6x6 inversion and its registers.
-template <typename R, bool PROP>
-__global__ void __launch_bounds__(256, PROP ? 4 : 1) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
+// ModElastic.f:248-327.  strain = engineering gamma (6), xs out (6).  General
+// moduli: the per-voxel mixed compliance is inverted (6x6); the proportional case
+// goes through k_el_x_prop below.
+template <typename R>
+__global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
                                               const R* __restrict__ strain, R* __restrict__ xs, double cfac, int* err) {
   const DevConst& K = *Kp;
   const meu_params& p = K.p;
@@ -222,36 +222,7 @@ __global__ void __launch_bounds__(256, PROP ? 4 : 1) k_el_x(const DevConst* __re
 #pragma unroll
       for (int m = 0; m < 6; ++m) e0[m] += pv * K.eps_eng[v][m];
     }
-    if constexpr (PROP) {
-      // C(x) = C_1 / s: x = cfac C0 gamma + (C_1 / s)(e0 - cfac gamma), no 6x6 matrix per voxel
-      double sc = 0;
-      for (int n = 2; n <= p.numph; ++n)
-        for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
-          const double pv = (double)pphi[v * n3 + id];
-          psum += pv;
-          sc += K.alpha[n - 1] * pv;
-        }
-      if (psum < 1.0) sc += 1.0 - psum;
-      if (!(sc != 0.0)) set_err(err, MEU_ERR_C_SINGULAR);
-      const double r = 1.0 / sc;
-      double gam[6], d[6];
-#pragma unroll
-      for (int m = 0; m < 6; ++m) {
-        gam[m] = (double)strain[(int64_t)m * n3 + id] + K.ebar_eng[m];
-        d[m] = e0[m] - cfac * gam[m];
-      }
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        double a0 = 0, a1 = 0;
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-          a0 += K.c0m[i + m * 6] * gam[m];
-          a1 += p.cela[0][i + m * 6] * d[m];
-        }
-        xs[(int64_t)i * n3 + id] = (R)(cfac * a0 + r * a1);
-      }
-      continue;
-    } else {
+    {
 #pragma unroll
       for (int i = 0; i < 36; ++i) Cm[i] = 0;
       for (int n = 2; n <= p.numph; ++n)
@@ -279,6 +250,64 @@ __global__ void __launch_bounds__(256, PROP ? 4 : 1) k_el_x(const DevConst* __re
         s += cfac * (K.c0m[r + m * 6] - c) * gam[m] + c * e0[m];
       }
       xs[(int64_t)r * n3 + id] = (R)s;
+    }
+  }
+}
+
+// Proportional moduli (K.prop_moduli): C(x) = C_1 / s(x), so
+// x = cfac C0 gamma + (C_1 / s)(e0 - cfac gamma), s = sum_v alpha_v P_v (+ 1 - sum P).
+// The coefficients travel as a kernel parameter, so the FP64 products read their
+// constants straight from the parameter bank; VT > 0 fixes the variant count at
+// compile time so the order-parameter loads are issued together, VT == 0 loops.
+template <typename R, int VT>
+__global__ void __launch_bounds__(256, 3) k_el_x_prop(const __grid_constant__ ElxProp E, int64_t n3,
+                                                      const R* __restrict__ pphi, const R* __restrict__ strain,
+                                                      R* __restrict__ xs, double cfac, int* err) {
+  const int V = VT > 0 ? VT : E.nvar;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    R st[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) st[m] = strain[(int64_t)m * n3 + id];
+    double e0[6] = {0, 0, 0, 0, 0, 0}, psum = 0, sc = 0;
+    if constexpr (VT > 0) {
+      R pv[VT > 0 ? VT : 1];
+#pragma unroll
+      for (int v = 0; v < VT; ++v) pv[v] = pphi[v * n3 + id];
+#pragma unroll
+      for (int v = 0; v < VT; ++v) {
+        const double q = (double)pv[v];
+        psum += E.inc[v] * q;
+        sc += E.av[v] * q;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) e0[m] += q * E.ep[v][m];
+      }
+    } else {
+      for (int v = 0; v < V; ++v) {
+        const double q = (double)pphi[v * n3 + id];
+        psum += E.inc[v] * q;
+        sc += E.av[v] * q;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) e0[m] += q * E.ep[v][m];
+      }
+    }
+    if (psum < 1.0) sc += 1.0 - psum;
+    if (!(sc != 0.0)) set_err(err, MEU_ERR_C_SINGULAR);
+    const double r = 1.0 / sc;
+    double gam[6], d[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      gam[m] = (double)st[m] + E.ebar[m];
+      d[m] = e0[m] - cfac * gam[m];
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double a0 = 0, a1 = 0;
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        a0 += E.c0[i + m * 6] * gam[m];
+        a1 += E.c1[i + m * 6] * d[m];
+      }
+      xs[(int64_t)i * n3 + id] = (R)(cfac * a0 + r * a1);
     }
   }
 }
@@ -455,6 +484,86 @@ __global__ void __launch_bounds__(RED_THREADS, PROP ? 4 : 1) k_elener(const DevC
         if (mode == 0) elg[v * n3 + id] += (R)eg;
         else elg[v * n3 + id] = (R)eg;
       }
+    el_en[id] = (R)en;
+    esum += en;
+  }
+  block_reduce_store(esum, 0, partials + Q_ELEN * PSTRIDE + blockIdx.x);
+}
+
+// Proportional moduli (K.prop_moduli) form of k_elener: sigma = (C_1 eps) / s with
+// s = 1 - sum P + sum_v alpha_v P_v, and each variant's energy alpha_v * elmat.
+// Coefficients as a kernel parameter; VT > 0 fixes the variant count.
+template <typename R, int VT>
+__global__ void __launch_bounds__(RED_THREADS, 2) k_elener_prop(const __grid_constant__ ElenProp E, int64_t n3,
+                                                                const R* __restrict__ phi, const R* __restrict__ pphi,
+                                                                const R* __restrict__ strain, R* __restrict__ el_en,
+                                                                R* __restrict__ elg, int mode, int eta2,
+                                                                double* partials, int* err) {
+  constexpr int NV = VT > 0 ? VT : MEU_MAX_VAR;
+  const int V = VT > 0 ? VT : E.nvar;
+  double esum = 0;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
+    R st[6], pr_[NV];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) st[m] = strain[(int64_t)m * n3 + id];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+      if (v < V) pr_[v] = pphi[v * n3 + id];
+    double te[6] = {0, 0, 0, 0, 0, 0}, psum = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (v >= V) break;
+      const double q = (double)pr_[v];
+      psum += q;
+#pragma unroll
+      for (int m = 0; m < 6; ++m) te[m] += q * E.tp[v][m];
+    }
+    double eps[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const double gm = (double)st[m];
+      eps[m] = (m < 3) ? (E.emean[m] + gm - te[m]) : (2.0 * E.emean[m] + gm - 2.0 * te[m]);
+    }
+    double sc = 1.0 - psum;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (v >= V) break;
+      sc += E.av[v] * (double)pr_[v];
+    }
+    if (!(sc != 0.0)) set_err(err, MEU_ERR_C_ELENER_SINGULAR);
+    const double r = 1.0 / sc;
+    double sig[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double a = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) a += E.c1[i + j * 6] * eps[j];
+      sig[i] = a * r;
+    }
+    double elmat = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double em = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) em += E.s1[i + j * 6] * sig[j];
+      elmat += sig[i] * em;
+    }
+    elmat *= 0.5;
+    double en = (1.0 - psum) * elmat;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (v >= V) break;
+      if (!E.use[v]) continue;
+      const double elp = E.av[v] * elmat;
+      en += elp * (double)pr_[v];
+      const double* t = E.tp[v];
+      const double g = sig[0] * t[0] + sig[1] * t[1] + sig[2] * t[2] + 2.0 * (sig[3] * t[3] + sig[4] * t[4] + sig[5] * t[5]);
+      const double f = (double)phi[v * n3 + id];
+      const double pr = eta2 ? 2.0 * f : 30.0 * f * f * (f * f - 2.0 * f + 1.0);
+      const double eg = pr * (elmat - elp) - g * pr;
+      if (mode == 0) elg[v * n3 + id] += (R)eg;
+      else elg[v * n3 + id] = (R)eg;
+    }
     el_en[id] = (R)en;
     esum += en;
   }

@@ -5,8 +5,11 @@ import pytest
 from meumapps_ss_b200 import _lib
 from meumapps_ss_b200 import params as P
 
+# (nz, ny, nx).  Power-of-two lengths 32..512 (x: nx/2) take the compile-time
+# kernels, the rest the run-time plan; the last three put lengths 512/256 on every
+# axis and leave a partial column tile (ny = 512 with nx/2+1 = 9 columns).
 SHAPES = [(8, 8, 8), (16, 16, 16), (12, 24, 6), (48, 48, 48), (32, 96, 64), (64, 64, 128), (128, 128, 128),
-          (4, 6, 8), (9, 3, 12), (96, 96, 96)]
+          (4, 6, 8), (9, 3, 12), (96, 96, 96), (16, 32, 1024), (512, 16, 36), (32, 512, 16), (256, 64, 512)]
 
 
 @pytest.mark.gpu
