@@ -237,7 +237,7 @@ def run_ours(args):
     w = CF.landau_config(args.config, n=args.n or None, precision=P.PREC_F32)
     p32 = w.params
     if not args.schedule:
-        p32.flags |= P.FLAG_AUTOTUNE  # fused decks: fastest schedule variant (ignored on the generic path)
+        p32.flags |= P.FLAG_AUTOTUNE  # fused decks: fastest schedule; generic path: fastest transform radix plan
     nx, ny, nz, V, E = p32.nx, p32.ny, p32.nz, p32.nvar, p32.numel
     n3 = nx * ny * nz
     seed = w.seed - rank

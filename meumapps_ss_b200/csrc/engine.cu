@@ -17,6 +17,15 @@
 
 namespace meu {
 
+// A 6x6 stiffness or compliance with decoupled normal / shear parts and independent
+// shears (the zero pattern mv6<true> skips).
+static bool ortho6(const double* c) {
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j)
+      if (!((i < 3 && j < 3) || i == j) && c[i + j * 6] != 0.0) return false;
+  return true;
+}
+
 // Fixed-order finalisation: block q reduces partials[q*PSTRIDE .. + nb[q]) with ops[q].
 __global__ void k_finalize(const double* __restrict__ partials, NbList nb, const int* __restrict__ ops, double* out) {
   const int q = blockIdx.x, op = ops[q];
@@ -350,7 +359,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     };
     g_el_k = resident((const void*)k_el_k<R>);
     g_lan_k1 = resident((const void*)k_lan_k1<R>);
-    g_elener = resident((const void*)k_elener<R, false>);
+    g_elener = resident((const void*)k_elener<R>);
     if (hK.prop_moduli) {
       ElxProp& X = el_prop;
       for (int i = 0; i < 36; ++i) {
@@ -378,19 +387,22 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
         Y.use[v] = (n >= 2 && hK.use_var[v]) ? 1 : 0;
       }
       Y.nvar = V;
-      g_elener = V == 1   ? resident((const void*)k_elener_prop<R, 1>)
-                 : V == 2 ? resident((const void*)k_elener_prop<R, 2>)
-                 : V == 3 ? resident((const void*)k_elener_prop<R, 3>)
-                 : V == 4 ? resident((const void*)k_elener_prop<R, 4>)
-                          : resident((const void*)k_elener_prop<R, 0>);
-      const void* fn = V == 1   ? (const void*)k_el_x_prop<R, 1>
-                       : V == 2 ? (const void*)k_el_x_prop<R, 2>
-                       : V == 3 ? (const void*)k_el_x_prop<R, 3>
-                       : V == 4 ? (const void*)k_el_x_prop<R, 4>
-                                : (const void*)k_el_x_prop<R, 0>;
-      int nb = 0;
-      MEU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 256, 0));
-      g_el_x = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(nb, 1) * sms, (n3 + 255) / 256));
+      const bool ortho = ortho6(hK.c0m) && ortho6(p.cela[0]) && ortho6(p.sela[0]);
+      fn_el_x = ortho ? k_el_x_prop<R, true> : k_el_x_prop<R, false>;
+      fn_elener = ortho ? k_elener_prop<R, true> : k_elener_prop<R, false>;
+      sm_el_x = (size_t)2 * (6 + V) * PF_TILE * sizeof(R);
+      sm_elener = (size_t)2 * (6 + 2 * V) * PF_TILE * sizeof(R);
+      const int64_t ntiles = (n3 + PF_TILE - 1) / PF_TILE;
+      // grid: the blocks that fit at once (each loops over tiles), at most one per tile
+      auto fit = [&](const void* fn, size_t smem) {
+        if (smem > 48 * 1024)
+          MEU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int nb = 0;
+        MEU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, PF_TILE, smem));
+        return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(nb, 1) * sms, ntiles));
+      };
+      g_el_x = fit((const void*)fn_el_x, sm_el_x);
+      g_elener = std::min(fit((const void*)fn_elener, sm_elener), RED_BLOCKS);
     }
   }
   if (fused) {
@@ -400,12 +412,65 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       sched = lan_autotune<R>(p.nx, V, dA, 1, p.diag_energy != 0, st, nullptr);
       reset_fused_state();
     }
+  } else if (p.flags & MEU_FLAG_AUTOTUNE) {
+    tune_transforms();
   }
+}
+
+// Generic path: time the radix plans of the compile-time transforms (forward and
+// inverse of V fields, the batch of the driving-force transforms) and keep the faster.
+template <typename R>
+void Engine<R>::tune_transforms() {
+  const int nf = std::min(V, NS);
+  MEU_CUDA(cudaMemsetAsync(pphi, 0, sizeof(R) * V * n3, st));
+  std::vector<const R*> in;
+  std::vector<R*> out;
+  for (int v = 0; v < nf; ++v) {
+    in.push_back(field(pphi, v));
+    out.push_back(field(fd, v));
+  }
+  cudaEvent_t e0, e1;
+  MEU_CUDA(cudaEventCreate(&e0));
+  MEU_CUDA(cudaEventCreate(&e1));
+  float best = 0;
+  int best_pv = 0;
+  for (int pv : {0, 2}) {
+    fft->pv = pv;
+    for (int i = 0; i < 2; ++i) {
+      fwd_list(in, 0);
+      inv_list(0, out);
+    }
+    MEU_CUDA(cudaEventRecord(e0, st));
+    for (int i = 0; i < 4; ++i) {
+      fwd_list(in, 0);
+      inv_list(0, out);
+    }
+    MEU_CUDA(cudaEventRecord(e1, st));
+    MEU_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (pv == 0 || ms < best) {
+      best = ms;
+      best_pv = pv;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  fft->pv = best_pv;
+  MEU_CUDA(cudaMemsetAsync(sp, 0, sizeof(C) * (size_t)NS * nk, st));
+  MEU_CUDA(cudaMemsetAsync(fd, 0, sizeof(R) * V * n3, st));
+  MEU_CUDA(cudaStreamSynchronize(st));
 }
 
 template <typename R>
 void Engine<R>::set_schedule(const int32_t* in3) {
-  if (!fused) throw CudaError("the handle runs the generic path (no schedule)", MEU_ERR_UNSUPPORTED);
+  if (!fused) {
+    // the transforms keep no state between calls, so the plan may change at any time
+    if ((in3[0] != 0 && in3[0] != 2) || in3[1] != 0 || in3[2] != 0)
+      throw CudaError("generic path: the schedule is (radix plan 0 or 2, 0, 0)", MEU_ERR_UNSUPPORTED);
+    fft->pv = in3[0];
+    return;
+  }
   if (fields_set) throw CudaError("set the schedule before the first meu_set_fields", MEU_ERR_BADARG);
   for (const LanSched& c : lan_sched_candidates(P.nx, sizeof(R) == 8)) {
     if (c.pv == in3[0] && c.ntp == in3[1] && c.tm == in3[2]) {
@@ -632,19 +697,8 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
       total += 1;
       if (total > 100000) throw CudaError("elastic iteration runaway", MEU_ERR_NOT_CONVERGED);
       if (hK.prop_moduli) {
-        const ElxProp& E = el_prop;
-        switch (V) {
-#define MEU_ELX(VV)                                                                                            \
-  case VV:                                                                                                      \
-    KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),                                                          \
-            k_el_x_prop<R, VV><<<g_el_x, 256, 0, st>>>(E, (int64_t)n3, pphi, strain, xs, cfac, d_err));         \
-    break;
-          MEU_ELX(1) MEU_ELX(2) MEU_ELX(3) MEU_ELX(4)
-#undef MEU_ELX
-          default:
-            KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
-                    k_el_x_prop<R, 0><<<g_el_x, 256, 0, st>>>(E, (int64_t)n3, pphi, strain, xs, cfac, d_err));
-        }
+        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
+                fn_el_x<<<g_el_x, PF_TILE, sm_el_x, st>>>(el_prop, (int64_t)n3, pphi, strain, xs, cfac, d_err));
       } else
         KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
       std::vector<const R*> in;
@@ -688,23 +742,11 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
   last_iters = total;
   const int eta2 = (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0;
   if (hK.prop_moduli) {
-    const ElenProp& E = en_prop;
-    switch (V) {
-#define MEU_ELEN(VV)                                                                                                 \
-  case VV:                                                                                                           \
-    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R),                                                  \
-            k_elener_prop<R, VV><<<g_elener, RED_THREADS, 0, st>>>(E, (int64_t)n3, ph_for_ppr, pphi, strain, el_en,  \
-                                                                   elg, mode, eta2, partials, d_err));                \
-    break;
-      MEU_ELEN(1) MEU_ELEN(2) MEU_ELEN(3) MEU_ELEN(4)
-#undef MEU_ELEN
-      default:
-        KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R),
-                k_elener_prop<R, 0><<<g_elener, RED_THREADS, 0, st>>>(E, (int64_t)n3, ph_for_ppr, pphi, strain, el_en,
-                                                                      elg, mode, eta2, partials, d_err));
-    }
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R),
+            fn_elener<<<g_elener, PF_TILE, sm_elener, st>>>(en_prop, (int64_t)n3, ph_for_ppr, pphi, strain, el_en, elg,
+                                                            mode, eta2, partials, d_err));
   } else
-    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R, false><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
                                                   partials, d_err));
 }
@@ -1135,7 +1177,7 @@ int meu_set_schedule(meu_handle* h, const int32_t* in3) {
 
 int meu_schedule(meu_handle* h, int32_t* out3) {
   if (!h || !out3) return MEU_ERR_BADARG;
-  if (!h->eng->schedule(out3)) return fail(h, MEU_ERR_UNSUPPORTED, "the handle runs the generic path (no schedule)");
+  if (!h->eng->schedule(out3)) return fail(h, MEU_ERR_UNSUPPORTED, "the handle has no schedule");
   return MEU_OK;
 }
 

@@ -152,7 +152,12 @@ class Engine : public EngineBase {
   void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
   void set_stream(cudaStream_t s) override { st = s ? s : own_st; }
   bool schedule(int32_t* out3) const override {
-    if (!fused) return false;
+    if (!fused) {  // generic path: the radix plan of its transforms
+      out3[0] = fft->pv;
+      out3[1] = 0;
+      out3[2] = 0;
+      return true;
+    }
     out3[0] = sched.pv;
     out3[1] = sched.ntp;
     out3[2] = sched.tm ? sched.tm : (sizeof(R) == 4 ? 16 : 8);
@@ -258,11 +263,16 @@ class Engine : public EngineBase {
   int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS, g_el_x = RED_BLOCKS;
   ElxProp el_prop{};  // proportional-moduli polarization coefficients (host-built)
   ElenProp en_prop{};  // proportional-moduli energy coefficients (host-built)
+  // the instantiation of the proportional kernels for this stiffness form
+  void (*fn_el_x)(ElxProp, int64_t, const R*, const R*, R*, double, int*) = nullptr;
+  void (*fn_elener)(ElenProp, int64_t, const R*, const R*, const R*, R*, R*, int, int, double*, int*) = nullptr;
+  size_t sm_el_x = 0, sm_elener = 0;  // their dynamic shared memory (prefetch tiles)
   bool fused_warm = false;
   bool theta_ready = false;  // sp holds theta^ of the current fields (written by the last step's PI)
   bool fields_set = false;  // the spectral-state layout is fixed from the first upload on
   std::unique_ptr<AdjBuffers<R>, void (*)(AdjBuffers<R>*)> adjb{nullptr, adj_buffers_free<R>};
   void reset_fused_state();
+  void tune_transforms();  // generic path: pick FFT3::pv by timing
   cudaGraphExec_t gexec = nullptr;
   int64_t graph_launches = 0;  // kernels in gexec
   void end_step(meu_diag* d, int clip);

@@ -267,26 +267,80 @@ __global__ void __launch_bounds__(256) k_cols(PtrList<cplx<R>> in, PtrList<cplx<
 // run-time plan above.
 constexpr int rows_per_block_c(int L) { return 2048 / L < 1 ? 1 : (2048 / L > 64 ? 64 : 2048 / L); }
 
+// One radix stage over NL lines with caller-supplied element access: ld(line, e)
+// and st(line, e, v) address element e of a line in whatever memory the stage
+// reads or writes.  FWD: DIF butterfly then twiddle; else twiddle then DIT butterfly.
+template <typename C, int L, int S, int NL, int NT, int PV, bool FWD, typename LD, typename ST>
+__device__ __forceinline__ void stage_io(const C* __restrict__ tw, LD&& ld, ST&& st) {
+  constexpr int R = fz::rplan(L, PV).r[S];
+  constexpr int SPAN = fz::span_of(L, S, PV);
+  constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
+#pragma unroll 1
+  for (int t = threadIdx.x; t < NBF; t += NT) {
+    const int line = t % NL, u = t / NL, j = u % M, b = u / M;
+    const int e0 = b * SPAN + j;
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = ld(line, e0 + r * M);
+    if constexpr (FWD) {
+      Dft<R, -1, C>::run(x);
+      if (M > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) x[q] = Tw<C>::mul(x[q], tw, j * q * TWS, L);
+      }
+    } else {
+      if (M > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) x[q] = Tw<C>::mulc(x[q], tw, j * q * TWS, L);
+      }
+      Dft<R, 1, C>::run(x);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) st(line, e0 + q * M, x[q]);
+  }
+}
+
+// Stages S, S+1, .. (FWD) or S, S-1, .. (inverse), up to but excluding SEND, in
+// shared memory (element e of line l at buf[e * ES + l]); each ends with a barrier.
+template <typename C, int L, int NL, int ES, int NT, int PV, bool FWD, int S, int SEND>
+__device__ __forceinline__ void stages_smem(C* buf, const C* tw) {
+  if constexpr (FWD ? (S < SEND) : (S > SEND)) {
+    stage_io<C, L, S, NL, NT, PV, FWD>(
+        tw, [&](int l, int e) { return buf[e * ES + l]; }, [&](int l, int e, C v) { buf[e * ES + l] = v; });
+    __syncthreads();
+    stages_smem<C, L, NL, ES, NT, PV, FWD, FWD ? S + 1 : S - 1, SEND>(buf, tw);
+  }
+}
+
+// Rows interleaved in shared memory: element e of row r at e * ES + r with
+// ES = NR + 1 (the odd stride keeps the split step's digit-reversed reads spread
+// over the banks).  The stages and the split put the row index in the fastest
+// lanes.  The forward transform's first stage reads the rows from global memory,
+// the inverse's last stage writes them there.
 template <typename R, int L, int PV>
 __global__ void __launch_bounds__(256) k_rows_r2c_s(PtrList<const R> in, PtrList<cplx<R>> out, int64_t nrows,
                                                     const cplx<R>* __restrict__ tw, const cplx<R>* __restrict__ post) {
   using C = cplx<R>;
-  constexpr int NR = rows_per_block_c(L), P = L + 1, NXH = L + 1, NP = L / 2 + 1;
+  constexpr int NR = rows_per_block_c(L), ES = NR + 1, NXH = L + 1, NP = L / 2 + 1;
+  constexpr int NS = fz::rplan(L, PV).ns;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   const int64_t row0 = (int64_t)blockIdx.x * NR;
   const int nr = (int)min((int64_t)NR, nrows - row0);
   const C* src = (const C*)(in.p[blockIdx.y] + row0 * (2 * L));
   C* dst = out.p[blockIdx.y] + row0 * NXH;
-  // a tile of nr rows is nr * L contiguous complex pairs of reals
-  for (int i = threadIdx.x; i < nr * L; i += 256) fz::cp_async_c(buf + (i / L) * P + (i % L), src + i);
-  fz::cp_async_wait_all();
+  // a row of 2L reals is L complex pairs (rows past nr read row 0, never stored)
+  stage_io<C, L, 0, NR, 256, PV, true>(
+      tw, [&](int r, int e) { return src[(int64_t)(r < nr ? r : 0) * L + e]; },
+      [&](int r, int e, C v) { buf[e * ES + r] = v; });
   __syncthreads();
-  fz::dif<C, L, NR, P, 1, 256, PV>(buf, tw);
-  for (int i = threadIdx.x; i < nr * NP; i += 256) {
-    const int r = i / NP, k = i - r * NP;
+  stages_smem<C, L, NR, ES, 256, PV, true, 1, NS>(buf, tw);
+  // split: X[k] = E + W^k O with E = (Z[k] + conj Z[L-k])/2, O = -i (Z[k] - conj Z[L-k])/2
+  for (int i = threadIdx.x; i < NR * NP; i += 256) {
+    const int r = i % NR, k = i / NR;
+    if (r >= nr) continue;
     const int km = k == 0 ? 0 : L - k;
-    const C zk = buf[r * P + fz::pos<L, PV>(k)], zm = buf[r * P + fz::pos<L, PV>(km)];
+    const C zk = buf[fz::pos<L, PV>(k) * ES + r], zm = buf[fz::pos<L, PV>(km) * ES + r];
     C* drow = dst + (int64_t)r * NXH;
     {
       C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
@@ -307,39 +361,51 @@ template <typename R, int L, int PV>
 __global__ void __launch_bounds__(256) k_rows_c2r_s(PtrList<const cplx<R>> in, PtrList<R> out, int64_t nrows,
                                                     const cplx<R>* __restrict__ tw, const cplx<R>* __restrict__ post) {
   using C = cplx<R>;
-  constexpr int NR = rows_per_block_c(L), P = L + 1, NXH = L + 1, NP = L / 2 + 1;
+  constexpr int NR = rows_per_block_c(L), ES = NR + 1, NXH = L + 1, NP = L / 2 + 1;
+  constexpr int NS = fz::rplan(L, PV).ns;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   const int64_t row0 = (int64_t)blockIdx.x * NR;
   const int nr = (int)min((int64_t)NR, nrows - row0);
   const C* src = in.p[blockIdx.y] + row0 * NXH;
   C* dst = (C*)(out.p[blockIdx.y] + row0 * (2 * L));
-  for (int i = threadIdx.x; i < nr * NP; i += 256) {
-    const int r = i / NP, k = i - r * NP;
+  // Z[k] = (X[k] + conj X[L-k]) + i (X[k] - conj X[L-k]) W^-k, into digit-reversed positions
+  for (int i = threadIdx.x; i < NR * NP; i += 256) {
+    const int r = i % NR, k = i / NR;
+    if (r >= nr) continue;
     const C* srow = src + (int64_t)r * NXH;
     C xk = srow[k], xm = srow[L - k];
     if (k == 0) { xk.y = 0; xm.y = 0; }
     {
       C ex = cadd(xk, cconj(xm));
       C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, NXH);
-      buf[r * P + fz::pos<L, PV>(k)] = cadd(ex, mk(-ox.y, ox.x));
+      buf[fz::pos<L, PV>(k) * ES + r] = cadd(ex, mk(-ox.y, ox.x));
     }
     if (k != 0 && k != L - k) {
       C ex = cadd(xm, cconj(xk));
       C ox = Tw<C>::mulc(csub(xm, cconj(xk)), post, L - k, NXH);
-      buf[r * P + fz::pos<L, PV>(L - k)] = cadd(ex, mk(-ox.y, ox.x));
+      buf[fz::pos<L, PV>(L - k) * ES + r] = cadd(ex, mk(-ox.y, ox.x));
     }
   }
   __syncthreads();
-  fz::dit<C, L, NR, P, 1, 256, PV>(buf, tw);
-  for (int i = threadIdx.x; i < nr * L; i += 256) dst[i] = buf[(i / L) * P + (i % L)];
+  stages_smem<C, L, NR, ES, 256, PV, false, NS - 1, 0>(buf, tw);
+  stage_io<C, L, 0, NR, 256, PV, false>(
+      tw, [&](int r, int e) { return buf[e * ES + r]; },
+      [&](int r, int e, C v) {
+        if (r < nr) dst[(int64_t)r * L + e] = v;
+      });
 }
 
 // TM columns of length L per block; element l of column (o, c) at o*ostride + l*inner + c.
+// The first stage reads its butterflies straight from global memory and the last
+// writes straight to global memory (digit reversal and forward scale folded into
+// the addressing); only the stages between them go through shared memory.
 template <typename R, bool FWD, int L, int TM, int PV>
 __global__ void __launch_bounds__(256) k_cols_s(PtrList<cplx<R>> in, PtrList<cplx<R>> out, int inner, int64_t ostride,
                                                 const cplx<R>* __restrict__ tw, R scale) {
   using C = cplx<R>;
+  constexpr int NS = fz::rplan(L, PV).ns;
+  static_assert(NS >= 2, "first and last stage must differ");
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   const int tiles = (inner + TM - 1) / TM;
@@ -347,30 +413,26 @@ __global__ void __launch_bounds__(256) k_cols_s(PtrList<cplx<R>> in, PtrList<cpl
   const int c0 = t * TM, nc = min(TM, inner - c0);
   const C* src = in.p[blockIdx.y] + (int64_t)o * ostride + c0;
   C* dst = out.p[blockIdx.y] + (int64_t)o * ostride + c0;
-  if (nc == TM) {
-#pragma unroll 4
-    for (int i = threadIdx.x; i < L * TM; i += 256) {
-      const int l = i / TM, c = i % TM;
-      fz::cp_async_c(buf + i, src + (int64_t)(FWD ? l : fz::rev<L, PV>(l)) * inner + c);
-    }
+  // lines past nc (a partial last tile) read column 0 and are never stored
+  auto gld = [&](int l, int e) {
+    const int c = l < nc ? l : 0;
+    return src[(int64_t)(FWD ? e : fz::rev<L, PV>(e)) * inner + c];
+  };
+  auto sst = [&](int l, int e, C v) { buf[e * TM + l] = v; };
+  auto sld = [&](int l, int e) { return buf[e * TM + l]; };
+  auto gst = [&](int l, int e, C v) {
+    if (l < nc) dst[(int64_t)(FWD ? fz::rev<L, PV>(e) : e) * inner + l] = FWD ? cscale(v, scale) : v;
+  };
+  if constexpr (FWD) {
+    stage_io<C, L, 0, TM, 256, PV, true>(tw, gld, sst);
+    __syncthreads();
+    stages_smem<C, L, TM, TM, 256, PV, true, 1, NS - 1>(buf, tw);
+    stage_io<C, L, NS - 1, TM, 256, PV, true>(tw, sld, gst);
   } else {
-    for (int i = threadIdx.x; i < L * TM; i += 256) {
-      const int l = i / TM, c = i % TM;
-      if (c < nc) fz::cp_async_c(buf + i, src + (int64_t)(FWD ? l : fz::rev<L, PV>(l)) * inner + c);
-    }
-  }
-  fz::cp_async_wait_all();
-  __syncthreads();
-  if constexpr (FWD) fz::dif<C, L, TM, 1, TM, 256, PV>(buf, tw);
-  else fz::dit<C, L, TM, 1, TM, 256, PV>(buf, tw);
-#pragma unroll 4
-  for (int i = threadIdx.x; i < L * TM; i += 256) {
-    const int l = i / TM, c = i % TM;
-    if (nc == TM || c < nc) {
-      C v = buf[i];
-      if (FWD) v = cscale(v, scale);
-      dst[(int64_t)(FWD ? fz::rev<L, PV>(l) : l) * inner + c] = v;
-    }
+    stage_io<C, L, NS - 1, TM, 256, PV, false>(tw, gld, sst);
+    __syncthreads();
+    stages_smem<C, L, TM, TM, 256, PV, false, NS - 2, 0>(buf, tw);
+    stage_io<C, L, 0, TM, 256, PV, false>(tw, sld, gst);
   }
 }
 
@@ -400,58 +462,60 @@ constexpr int col_tile_s(int L) {
   return t < 4 ? 4 : (t > 16 ? 16 : t);
 }
 
-// Launch the specialised kernel for this length; false when L has none.
-template <typename R>
-static bool rows_s(bool fwd, int L, int nf, int64_t nrows, const void* in, const void* out, const void* tw,
-                   const void* post, cudaStream_t st) {
-  using C = cplx<R>;
-  auto go = [&](auto Lc) {
-    constexpr int LL = decltype(Lc)::value;
-    constexpr int NR = rows_per_block_c(LL);
-    const size_t sm = (size_t)NR * (LL + 1) * sizeof(C);
-    const dim3 g((unsigned)((nrows + NR - 1) / NR), nf);
-    if (fwd) {
-      set_smem<R>((const void*)k_rows_r2c_s<R, LL, 0>, sm);
-      k_rows_r2c_s<R, LL, 0><<<g, 256, sm, st>>>(*(const PtrList<const R>*)in, *(const PtrList<C>*)out, nrows,
-                                                  (const C*)tw, (const C*)post);
-    } else {
-      set_smem<R>((const void*)k_rows_c2r_s<R, LL, 0>, sm);
-      k_rows_c2r_s<R, LL, 0><<<g, 256, sm, st>>>(*(const PtrList<const C>*)in, *(const PtrList<R>*)out, nrows,
-                                                  (const C*)tw, (const C*)post);
-    }
-    return true;
+// Call go(length, plan) as integral constants for the lengths with compile-time
+// kernels; false when L has none.  Launch helpers for those kernels follow.
+template <typename F>
+static bool dispatch_len(int L, int pv, F&& go) {
+  auto with_pv = [&](auto Lc) {
+    return pv == 2 ? go(Lc, std::integral_constant<int, 2>{}) : go(Lc, std::integral_constant<int, 0>{});
   };
   switch (L) {
-    case 32: return go(std::integral_constant<int, 32>{});
-    case 64: return go(std::integral_constant<int, 64>{});
-    case 128: return go(std::integral_constant<int, 128>{});
-    case 256: return go(std::integral_constant<int, 256>{});
-    case 512: return go(std::integral_constant<int, 512>{});
+    case 32: return with_pv(std::integral_constant<int, 32>{});
+    case 64: return with_pv(std::integral_constant<int, 64>{});
+    case 128: return with_pv(std::integral_constant<int, 128>{});
+    case 256: return with_pv(std::integral_constant<int, 256>{});
+    case 512: return with_pv(std::integral_constant<int, 512>{});
     default: return false;
   }
 }
 
-template <typename R, bool FWD>
-static bool cols_s(int L, int nf, int outer, int inner, int64_t ostride, const PtrList<cplx<R>>& buf, const void* tw,
-                   R scale, cudaStream_t st) {
+template <typename R>
+static bool rows_s(bool fwd, int L, int pv, int nf, int64_t nrows, const void* in, const void* out, const void* tw,
+                   const void* post, cudaStream_t st) {
   using C = cplx<R>;
-  auto go = [&](auto Lc) {
-    constexpr int LL = decltype(Lc)::value;
-    constexpr int TM = col_tile_s<R>(LL);
-    const size_t sm = (size_t)LL * TM * sizeof(C);
-    set_smem<R>((const void*)k_cols_s<R, FWD, LL, TM, 0>, sm);
-    const dim3 g((unsigned)(outer * ((inner + TM - 1) / TM)), nf);
-    k_cols_s<R, FWD, LL, TM, 0><<<g, 256, sm, st>>>(buf, buf, inner, ostride, (const C*)tw, scale);
+  auto go = [&](auto Lc, auto Pc) {
+    constexpr int LL = decltype(Lc)::value, PV = decltype(Pc)::value;
+    constexpr int NR = rows_per_block_c(LL);
+    const size_t sm = (size_t)(NR + 1) * LL * sizeof(C);
+    const dim3 g((unsigned)((nrows + NR - 1) / NR), nf);
+    if (fwd) {
+      set_smem<R>((const void*)k_rows_r2c_s<R, LL, PV>, sm);
+      k_rows_r2c_s<R, LL, PV><<<g, 256, sm, st>>>(*(const PtrList<const R>*)in, *(const PtrList<C>*)out, nrows,
+                                                   (const C*)tw, (const C*)post);
+    } else {
+      set_smem<R>((const void*)k_rows_c2r_s<R, LL, PV>, sm);
+      k_rows_c2r_s<R, LL, PV><<<g, 256, sm, st>>>(*(const PtrList<const C>*)in, *(const PtrList<R>*)out, nrows,
+                                                   (const C*)tw, (const C*)post);
+    }
     return true;
   };
-  switch (L) {
-    case 32: return go(std::integral_constant<int, 32>{});
-    case 64: return go(std::integral_constant<int, 64>{});
-    case 128: return go(std::integral_constant<int, 128>{});
-    case 256: return go(std::integral_constant<int, 256>{});
-    case 512: return go(std::integral_constant<int, 512>{});
-    default: return false;
-  }
+  return dispatch_len(L, pv, go);
+}
+
+template <typename R, bool FWD>
+static bool cols_s(int L, int pv, int nf, int outer, int inner, int64_t ostride, const PtrList<cplx<R>>& buf,
+                   const void* tw, R scale, cudaStream_t st) {
+  using C = cplx<R>;
+  auto go = [&](auto Lc, auto Pc) {
+    constexpr int LL = decltype(Lc)::value, PV = decltype(Pc)::value;
+    constexpr int TM = col_tile_s<R>(LL);
+    const size_t sm = (size_t)LL * TM * sizeof(C);
+    set_smem<R>((const void*)k_cols_s<R, FWD, LL, TM, PV>, sm);
+    const dim3 g((unsigned)(outer * ((inner + TM - 1) / TM)), nf);
+    k_cols_s<R, FWD, LL, TM, PV><<<g, 256, sm, st>>>(buf, buf, inner, ostride, (const C*)tw, scale);
+    return true;
+  };
+  return dispatch_len(L, pv, go);
 }
 
 static inline int col_tile(int L, bool fp64) {
@@ -480,7 +544,7 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
   set_smem<R>((const void*)k_rows_r2c<R>, sm);
   dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
   { HookScope hs_(hook, "fft_x_r2c", (double)nf * (n3() * sizeof(R) + nk() * sizeof(C)), st);
-  if (!rows_s<R>(true, Lx, nf, nrows, &in, &out, px.tw, post_tw, st))
+  if (!rows_s<R>(true, Lx, pv, nf, nrows, &in, &out, px.tw, post_tw, st))
     k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
   // y columns: outer = z, inner = nxh
@@ -490,7 +554,7 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     set_smem<R>((const void*)k_cols<R, true>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
     { HookScope hs_(hook, "fft_y_fwd", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, true>(ny, nf, nz, nxh, (int64_t)ny * nxh, out, py.tw, (R)1, st))
+  if (!cols_s<R, true>(ny, pv, nf, nz, nxh, (int64_t)ny * nxh, out, py.tw, (R)1, st))
     k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
@@ -503,7 +567,7 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
     { HookScope hs_(hook, "fft_z_fwd", 2.0 * nf * nk() * sizeof(C), st);
   const R scale = (R)(1.0 / ((double)nx * ny * nz));
-  if (!cols_s<R, true>(nz, nf, 1, inner, 0, out, pz.tw, scale, st))
+  if (!cols_s<R, true>(nz, pv, nf, 1, inner, 0, out, pz.tw, scale, st))
     k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, scale); }
     MEU_CHECK_LAUNCH();
   }
@@ -519,7 +583,7 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     int inner = ny * nxh;
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
     { HookScope hs_(hook, "fft_z_inv", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, false>(nz, nf, 1, inner, 0, in, pz.tw, (R)1, st))
+  if (!cols_s<R, false>(nz, pv, nf, 1, inner, 0, in, pz.tw, (R)1, st))
     k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1); }
     MEU_CHECK_LAUNCH();
   }
@@ -529,7 +593,7 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     set_smem<R>((const void*)k_cols<R, false>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
     { HookScope hs_(hook, "fft_y_inv", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, false>(ny, nf, nz, nxh, (int64_t)ny * nxh, in, py.tw, (R)1, st))
+  if (!cols_s<R, false>(ny, pv, nf, nz, nxh, (int64_t)ny * nxh, in, py.tw, (R)1, st))
     k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
@@ -542,7 +606,7 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
   for (int f = 0; f < MAXF; ++f) cin.p[f] = in.p[f];
   dim3 g((unsigned)((nrows + rpb - 1) / rpb), nf);
   { HookScope hs_(hook, "fft_x_c2r", (double)nf * (n3() * sizeof(R) + nk() * sizeof(C)), st);
-  if (!rows_s<R>(false, Lx, nf, nrows, &cin, &out, px.tw, post_tw, st))
+  if (!rows_s<R>(false, Lx, pv, nf, nrows, &cin, &out, px.tw, post_tw, st))
     k_rows_c2r<R><<<g, 256, sm, st>>>(cin, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
 }

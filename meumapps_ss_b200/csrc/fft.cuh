@@ -247,6 +247,9 @@ class FFT3 {
   void inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
 
   LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
+  // radix plan of the compile-time kernels (power-of-two lengths 32..512): 0 = radix 8
+  // first, 2 = radix 16 first (one shared-memory pass fewer, more registers)
+  int pv = 0;
   LaunchHook* hook = nullptr;
   const void* post_tw;  // cplx<R>[nx/2+1]: exp(-2 pi i k / nx)
   bool fp64;

@@ -254,61 +254,95 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
   }
 }
 
+// 6x6 (column-major) times 6-vector.  ORTHO: normal and shear parts decouple and the
+// shears are independent (C[i][j] = 0 for i < 3 <= j, j < 3 <= i and 3 <= i != j,
+// every cubic or orthotropic stiffness in its crystal frame).  The skipped terms are
+// exact zeros, so the sums are bit-identical to the full product.
+template <bool ORTHO>
+__device__ __forceinline__ void mv6(const double* __restrict__ c, const double* x, double* y) {
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double a = 0;
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+      if (!ORTHO || (i < 3 && m < 3) || i == m) a += c[i + m * 6] * x[m];
+    y[i] = a;
+  }
+}
+
+// Per-voxel prefetch through shared memory: each thread copies its own voxel's
+// values of the next tile with cp.async while it works on the current one, so the
+// loads of a whole tile are in flight during the FP64 work without holding
+// registers.  Thread i of a block owns voxel i of every tile; no barrier needed.
+constexpr int PF_TILE = 256;
+template <typename R>
+__device__ __forceinline__ void pf_copy(R* smem, const R* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (sizeof(R) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void pf_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void pf_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 // Proportional moduli (K.prop_moduli): C(x) = C_1 / s(x), so
 // x = cfac C0 gamma + (C_1 / s)(e0 - cfac gamma), s = sum_v alpha_v P_v (+ 1 - sum P).
 // The coefficients travel as a kernel parameter, so the FP64 products read their
-// constants straight from the parameter bank; VT > 0 fixes the variant count at
-// compile time so the order-parameter loads are issued together, VT == 0 loops.
-template <typename R, int VT>
-__global__ void __launch_bounds__(256, 3) k_el_x_prop(const __grid_constant__ ElxProp E, int64_t n3,
-                                                      const R* __restrict__ pphi, const R* __restrict__ strain,
-                                                      R* __restrict__ xs, double cfac, int* err) {
-  const int V = VT > 0 ? VT : E.nvar;
-  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
-    R st[6];
+// constants straight from the parameter bank.  Dynamic shared memory:
+// 2 * (6 + V) * PF_TILE elements of R (double-buffered tiles, field-major).
+template <typename R, bool ORTHO>
+__global__ void __launch_bounds__(PF_TILE, 4) k_el_x_prop(const __grid_constant__ ElxProp E, int64_t n3,
+                                                          const R* __restrict__ pphi, const R* __restrict__ strain,
+                                                          R* __restrict__ xs, double cfac, int* err) {
+  constexpr int NV = MEU_MAX_VAR;
+  const int V = E.nvar;
+  const int NF = 6 + V;
+  extern __shared__ __align__(16) unsigned char pf_raw[];
+  R* buf = (R*)pf_raw;
+  const int tid = threadIdx.x;
+  auto issue = [&](int64_t tile, int slot) {
+    const int64_t id = tile * PF_TILE + tid;
+    R* b = buf + (int64_t)slot * NF * PF_TILE + tid;
+    if (id < n3) {
 #pragma unroll
-    for (int m = 0; m < 6; ++m) st[m] = strain[(int64_t)m * n3 + id];
+      for (int m = 0; m < 6; ++m) pf_copy(b + m * PF_TILE, strain + (int64_t)m * n3 + id);
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        if (v < V) pf_copy(b + (6 + v) * PF_TILE, pphi + (int64_t)v * n3 + id);
+    }
+    pf_commit();
+  };
+  const int64_t ntiles = (n3 + PF_TILE - 1) / PF_TILE;
+  int64_t tile = blockIdx.x;
+  issue(tile, 0);
+  for (int k = 0; tile < ntiles; tile += gridDim.x, ++k) {
+    issue(tile + gridDim.x, (k + 1) & 1);
+    pf_wait_prev();
+    const int64_t id = tile * PF_TILE + tid;
+    if (id >= n3) continue;
+    const R* b = buf + (int64_t)(k & 1) * NF * PF_TILE + tid;
     double e0[6] = {0, 0, 0, 0, 0, 0}, psum = 0, sc = 0;
-    if constexpr (VT > 0) {
-      R pv[VT > 0 ? VT : 1];
 #pragma unroll
-      for (int v = 0; v < VT; ++v) pv[v] = pphi[v * n3 + id];
+    for (int v = 0; v < NV; ++v) {
+      if (v >= V) break;
+      const double q = (double)b[(6 + v) * PF_TILE];
+      psum += E.inc[v] * q;
+      sc += E.av[v] * q;
 #pragma unroll
-      for (int v = 0; v < VT; ++v) {
-        const double q = (double)pv[v];
-        psum += E.inc[v] * q;
-        sc += E.av[v] * q;
-#pragma unroll
-        for (int m = 0; m < 6; ++m) e0[m] += q * E.ep[v][m];
-      }
-    } else {
-      for (int v = 0; v < V; ++v) {
-        const double q = (double)pphi[v * n3 + id];
-        psum += E.inc[v] * q;
-        sc += E.av[v] * q;
-#pragma unroll
-        for (int m = 0; m < 6; ++m) e0[m] += q * E.ep[v][m];
-      }
+      for (int m = 0; m < 6; ++m) e0[m] += q * E.ep[v][m];
     }
     if (psum < 1.0) sc += 1.0 - psum;
     if (!(sc != 0.0)) set_err(err, MEU_ERR_C_SINGULAR);
     const double r = 1.0 / sc;
-    double gam[6], d[6];
+    double gam[6], d[6], a0[6], a1[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) {
-      gam[m] = (double)st[m] + E.ebar[m];
+      gam[m] = (double)b[m * PF_TILE] + E.ebar[m];
       d[m] = e0[m] - cfac * gam[m];
     }
+    mv6<ORTHO>(E.c0, gam, a0);
+    mv6<ORTHO>(E.c1, d, a1);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      double a0 = 0, a1 = 0;
-#pragma unroll
-      for (int m = 0; m < 6; ++m) {
-        a0 += E.c0[i + m * 6] * gam[m];
-        a1 += E.c1[i + m * 6] * d[m];
-      }
-      xs[(int64_t)i * n3 + id] = (R)(cfac * a0 + r * a1);
-    }
+    for (int i = 0; i < 6; ++i) xs[(int64_t)i * n3 + id] = (R)(cfac * a0[i] + r * a1[i]);
   }
 }
 
@@ -393,8 +427,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict
 // -------------------------------------------------------------- elener
 // ModElastic.f:540-687.  mode 0 (KKS): fdiff += el_grad; mode 1 (Landau): elg = el_grad.
 // theta' = 30 f^2 (f^2 - 2f + 1) (KKS and Landau h coupling) or 2 eta (eta^2 coupling).
-template <typename R, bool PROP>
-__global__ void __launch_bounds__(RED_THREADS, PROP ? 4 : 1) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
                                                         const R* __restrict__ pphi, const R* __restrict__ strain,
                                                         R* __restrict__ el_en, R* __restrict__ elg, int mode, int eta2,
                                                         double* partials, int* err) {
@@ -418,21 +452,7 @@ __global__ void __launch_bounds__(RED_THREADS, PROP ? 4 : 1) k_elener(const DevC
       eps[m] = (m < 3) ? (p.e_mean[m] + gm - te[m]) : (2.0 * p.e_mean[m] + gm - 2.0 * te[m]);
     }
     double Cm[36], sig[6];
-    if constexpr (PROP) {
-      // C(x) = C_1 / s: sigma = (C_1 eps) / s without a per-voxel matrix
-      double sc = 1.0 - psum;
-      for (int n = 2; n <= p.numph; ++n)
-        for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) sc += K.alpha[n - 1] * P[v];
-      if (!(sc != 0.0)) set_err(err, MEU_ERR_C_ELENER_SINGULAR);
-      const double r = 1.0 / sc;
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        double a = 0;
-#pragma unroll
-        for (int j = 0; j < 6; ++j) a += p.cela[0][i + j * 6] * eps[j];
-        sig[i] = a * r;
-      }
-    } else {
+    {
 #pragma unroll
       for (int i = 0; i < 36; ++i) Cm[i] = (1.0 - psum) * p.sela[0][i];
       for (int n = 2; n <= p.numph; ++n)
@@ -463,9 +483,7 @@ __global__ void __launch_bounds__(RED_THREADS, PROP ? 4 : 1) k_elener(const DevC
       for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
         if (!K.use_var[v]) continue;
         double elp = 0;
-        if constexpr (PROP) {
-          elp = K.alpha[n - 1] * elmat;
-        } else {
+        {
 #pragma unroll
           for (int i = 0; i < 6; ++i) {
             double ep = 0;
@@ -492,28 +510,52 @@ __global__ void __launch_bounds__(RED_THREADS, PROP ? 4 : 1) k_elener(const DevC
 
 // Proportional moduli (K.prop_moduli) form of k_elener: sigma = (C_1 eps) / s with
 // s = 1 - sum P + sum_v alpha_v P_v, and each variant's energy alpha_v * elmat.
-// Coefficients as a kernel parameter; VT > 0 fixes the variant count.
-template <typename R, int VT>
-__global__ void __launch_bounds__(RED_THREADS, 2) k_elener_prop(const __grid_constant__ ElenProp E, int64_t n3,
-                                                                const R* __restrict__ phi, const R* __restrict__ pphi,
-                                                                const R* __restrict__ strain, R* __restrict__ el_en,
-                                                                R* __restrict__ elg, int mode, int eta2,
-                                                                double* partials, int* err) {
-  constexpr int NV = VT > 0 ? VT : MEU_MAX_VAR;
-  const int V = VT > 0 ? VT : E.nvar;
+// Coefficients as a kernel parameter; ORTHO as in mv6.  Loads prefetched through
+// shared memory as in k_el_x_prop: dynamic shared memory 2 * (6 + 2V) * PF_TILE
+// elements of R.
+template <typename R, bool ORTHO>
+__global__ void __launch_bounds__(PF_TILE, 3) k_elener_prop(const __grid_constant__ ElenProp E, int64_t n3,
+                                                            const R* __restrict__ phi, const R* __restrict__ pphi,
+                                                            const R* __restrict__ strain, R* __restrict__ el_en,
+                                                            R* __restrict__ elg, int mode, int eta2, double* partials,
+                                                            int* err) {
+  static_assert(PF_TILE == RED_THREADS, "one voxel per reduction thread");
+  constexpr int NV = MEU_MAX_VAR;
+  const int V = E.nvar;
+  const int NF = 6 + 2 * V;
+  extern __shared__ __align__(16) unsigned char pf_raw[];
+  R* buf = (R*)pf_raw;
+  const int tid = threadIdx.x;
+  auto issue = [&](int64_t tile, int slot) {
+    const int64_t id = tile * PF_TILE + tid;
+    R* b = buf + (int64_t)slot * NF * PF_TILE + tid;
+    if (id < n3) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) pf_copy(b + m * PF_TILE, strain + (int64_t)m * n3 + id);
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        if (v < V) {
+          pf_copy(b + (6 + v) * PF_TILE, pphi + (int64_t)v * n3 + id);
+          if (E.use[v]) pf_copy(b + (6 + V + v) * PF_TILE, phi + (int64_t)v * n3 + id);
+        }
+    }
+    pf_commit();
+  };
   double esum = 0;
-  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
-    R st[6], pr_[NV];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) st[m] = strain[(int64_t)m * n3 + id];
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-      if (v < V) pr_[v] = pphi[v * n3 + id];
+  const int64_t ntiles = (n3 + PF_TILE - 1) / PF_TILE;
+  int64_t tile = blockIdx.x;
+  issue(tile, 0);
+  for (int k = 0; tile < ntiles; tile += gridDim.x, ++k) {
+    issue(tile + gridDim.x, (k + 1) & 1);
+    pf_wait_prev();
+    const int64_t id = tile * PF_TILE + tid;
+    if (id >= n3) continue;
+    const R* b = buf + (int64_t)(k & 1) * NF * PF_TILE + tid;
     double te[6] = {0, 0, 0, 0, 0, 0}, psum = 0;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       if (v >= V) break;
-      const double q = (double)pr_[v];
+      const double q = (double)b[(6 + v) * PF_TILE];
       psum += q;
 #pragma unroll
       for (int m = 0; m < 6; ++m) te[m] += q * E.tp[v][m];
@@ -521,33 +563,25 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_elener_prop(const __grid_con
     double eps[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) {
-      const double gm = (double)st[m];
+      const double gm = (double)b[m * PF_TILE];
       eps[m] = (m < 3) ? (E.emean[m] + gm - te[m]) : (2.0 * E.emean[m] + gm - 2.0 * te[m]);
     }
     double sc = 1.0 - psum;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       if (v >= V) break;
-      sc += E.av[v] * (double)pr_[v];
+      sc += E.av[v] * (double)b[(6 + v) * PF_TILE];
     }
     if (!(sc != 0.0)) set_err(err, MEU_ERR_C_ELENER_SINGULAR);
     const double r = 1.0 / sc;
-    double sig[6];
+    double sig[6], em[6];
+    mv6<ORTHO>(E.c1, eps, sig);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      double a = 0;
-#pragma unroll
-      for (int j = 0; j < 6; ++j) a += E.c1[i + j * 6] * eps[j];
-      sig[i] = a * r;
-    }
+    for (int i = 0; i < 6; ++i) sig[i] *= r;
+    mv6<ORTHO>(E.s1, sig, em);
     double elmat = 0;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      double em = 0;
-#pragma unroll
-      for (int j = 0; j < 6; ++j) em += E.s1[i + j * 6] * sig[j];
-      elmat += sig[i] * em;
-    }
+    for (int i = 0; i < 6; ++i) elmat += sig[i] * em[i];
     elmat *= 0.5;
     double en = (1.0 - psum) * elmat;
 #pragma unroll
@@ -555,10 +589,10 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_elener_prop(const __grid_con
       if (v >= V) break;
       if (!E.use[v]) continue;
       const double elp = E.av[v] * elmat;
-      en += elp * (double)pr_[v];
+      en += elp * (double)b[(6 + v) * PF_TILE];
       const double* t = E.tp[v];
       const double g = sig[0] * t[0] + sig[1] * t[1] + sig[2] * t[2] + 2.0 * (sig[3] * t[3] + sig[4] * t[4] + sig[5] * t[5]);
-      const double f = (double)phi[v * n3 + id];
+      const double f = (double)b[(6 + V + v) * PF_TILE];
       const double pr = eta2 ? 2.0 * f : 30.0 * f * f * (f * f - 2.0 * f + 1.0);
       const double eg = pr * (elmat - elp) - g * pr;
       if (mode == 0) elg[v * n3 + id] += (R)eg;

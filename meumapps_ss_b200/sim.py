@@ -121,7 +121,8 @@ class Simulation:
 
     @property
     def schedule(self) -> Optional[Tuple[int, int, int]]:
-        """(radix plan variant, plane threads, column tile) of the fused step, None on the generic path."""
+        """(radix plan variant, plane threads, column tile) of the fused step; on the
+        generic path (radix plan of the power-of-two transforms, 0, 0)."""
         out = (C.c_int32 * 3)()
         if lib().meu_schedule(self.h, out):
             return None
@@ -146,7 +147,8 @@ class Simulation:
         return float(loss.value), grads, field
 
     def set_schedule(self, pv: int, ntp: int, tm: int) -> None:
-        """Pick the fused step's schedule (before the first set_fields)."""
+        """Pick the fused step's schedule (before the first set_fields), or the generic
+        path's transform radix plan as (0 or 2, 0, 0)."""
         self._check(lib().meu_set_schedule(self.h, (C.c_int32 * 3)(pv, ntp, tm)))
 
 

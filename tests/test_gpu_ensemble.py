@@ -114,7 +114,12 @@ def test_set_schedule_rules():
         g.set_schedule(1, 256, 4)  # the spectral-state layout is fixed by then
     q = CF.landau_params(32, 1, [[0.01, 0.01, 0.01]])
     q.flags = P.FLAG_GENERIC
-    assert Simulation(q).schedule is None
+    h = Simulation(q)
+    assert h.schedule == (0, 0, 0)  # generic path: the transforms' radix plan
+    h.set_schedule(2, 0, 0)
+    assert h.schedule == (2, 0, 0)
+    with pytest.raises(_lib.MeuError):
+        h.set_schedule(1, 0, 0)
 
 
 @pytest.mark.gpu

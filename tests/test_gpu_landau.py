@@ -53,6 +53,33 @@ def test_landau_hetero_parity(oracle):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ortho,pv", [(True, 0), (False, 2)])
+def test_landau_hetero_kernels_parity(oracle, ortho, pv):
+    """Proportional moduli through the matrix-free kernels on a 64^3 grid (the
+    compile-time transforms), with the normal / shear blocks decoupled (cubic) or
+    coupled (an off-block term added to the stiffness), under both radix plans."""
+    p, c, e = active_landau(n=64, nvar=2, elastic=P.ELAST_HETERO, coupling=P.EIG_H, ppt_scale=1.5, el_tol=1e-8)
+    if not ortho:
+        cm = p.matrix("cela", 0, 6)
+        cm[0, 3] = cm[3, 0] = 7.0
+        cm[1, 5] = cm[5, 1] = -4.0
+        for ph, scale in ((0, 1.0), (1, 1.0 / 1.5)):
+            p.set_matrix("cela", ph, cm / scale)
+            p.set_matrix("sela", ph, np.linalg.inv(cm / scale))
+    o = oracle.OracleSim(p)
+    o.set_fields(c, e)
+    g = Simulation(p)
+    g.set_schedule(pv, 0, 0)
+    g.set_fields(c, e)
+    do, dg = o.run(6), g.run(6)
+    assert np.array_equal(do["el_iters"], dg["el_iters"])
+    co, eo, elo, _ = o.get_fields()
+    cg, eg, elg, _ = g.get_fields()
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(eg - eo)) <= TOL
+    assert np.max(np.abs(elg - elo)) <= 1e-9 * np.max(np.abs(elo))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("k", [0, 1, 2])
 def test_landau_configs_small_parity(oracle, k):
     w = CF.landau_config(k, n=16, precision=P.PREC_F64)
