@@ -270,18 +270,33 @@ constexpr int rows_per_block_c(int L) { return 2048 / L < 1 ? 1 : (2048 / L > 64
 // One radix stage over NL lines with caller-supplied element access: ld(line, e)
 // and st(line, e, v) address element e of a line in whatever memory the stage
 // reads or writes.  FWD: DIF butterfly then twiddle; else twiddle then DIT butterfly.
-template <typename C, int L, int S, int NL, int NT, int PV, bool FWD, typename LD, typename ST>
+// JFAST: consecutive threads take consecutive butterflies of one line (consecutive
+// elements, for row-contiguous global memory) instead of the same butterfly of
+// consecutive lines.  HOLD: every thread loads and transforms all of its
+// butterflies, the block synchronises, then all store -- for a stage whose
+// stores land on other threads' inputs (a permuting, in-place stage).
+template <typename C, int L, int S, int NL, int NT, int PV, bool FWD, bool JFAST = false, bool HOLD = false,
+          typename LD, typename ST>
 __device__ __forceinline__ void stage_io(const C* __restrict__ tw, LD&& ld, ST&& st) {
   constexpr int R = fz::rplan(L, PV).r[S];
   constexpr int SPAN = fz::span_of(L, S, PV);
   constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
-#pragma unroll 1
-  for (int t = threadIdx.x; t < NBF; t += NT) {
-    const int line = t % NL, u = t / NL, j = u % M, b = u / M;
-    const int e0 = b * SPAN + j;
-    C x[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = ld(line, e0 + r * M);
+  auto map = [](int t, int& line, int& j, int& e0) {
+    int b;
+    if constexpr (JFAST) {
+      j = t % M;
+      const int u = t / M;
+      line = u % NL;
+      b = u / NL;
+    } else {
+      line = t % NL;
+      const int u = t / NL;
+      j = u % M;
+      b = u / M;
+    }
+    e0 = b * SPAN + j;
+  };
+  auto butterfly = [&](C* x, int j) {
     if constexpr (FWD) {
       Dft<R, -1, C>::run(x);
       if (M > 1) {
@@ -295,8 +310,41 @@ __device__ __forceinline__ void stage_io(const C* __restrict__ tw, LD&& ld, ST&&
       }
       Dft<R, 1, C>::run(x);
     }
+  };
+  if constexpr (HOLD) {
+    constexpr int IT = (NBF + NT - 1) / NT;
+    C x[IT][R];
+    int ln[IT], ee[IT];
 #pragma unroll
-    for (int q = 0; q < R; ++q) st(line, e0 + q * M, x[q]);
+    for (int it = 0; it < IT; ++it) {
+      const int t = threadIdx.x + it * NT;
+      if (t < NBF) {
+        int j;
+        map(t, ln[it], j, ee[it]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[it][r] = ld(ln[it], ee[it] + r * M);
+        butterfly(x[it], j);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; ++it)
+      if (threadIdx.x + it * NT < NBF) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) st(ln[it], ee[it] + q * M, x[it][q]);
+      }
+  } else {
+#pragma unroll 1
+    for (int t = threadIdx.x; t < NBF; t += NT) {
+      int line, j, e0;
+      map(t, line, j, e0);
+      C x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = ld(line, e0 + r * M);
+      butterfly(x, j);
+#pragma unroll
+      for (int q = 0; q < R; ++q) st(line, e0 + q * M, x[q]);
+    }
   }
 }
 
@@ -312,17 +360,19 @@ __device__ __forceinline__ void stages_smem(C* buf, const C* tw) {
   }
 }
 
-// Rows interleaved in shared memory: element e of row r at e * ES + r with
-// ES = NR + 1 (the odd stride keeps the split step's digit-reversed reads spread
-// over the banks).  The stages and the split put the row index in the fastest
-// lanes.  The forward transform's first stage reads the rows from global memory,
-// the inverse's last stage writes them there.
+// Rows interleaved in shared memory: element e of row r at e * ES + r with the odd
+// stride ES = NR + 1, so that runs of consecutive e and runs of consecutive r both
+// spread over the banks.  The global-facing stage walks consecutive elements of a
+// row (JFAST); the stage next to the split step permutes between digit-reversed
+// positions and natural frequency order (HOLD), so the split reads and writes
+// consecutive frequencies, in shared and in global memory alike.
 template <typename R, int L, int PV>
 __global__ void __launch_bounds__(256) k_rows_r2c_s(PtrList<const R> in, PtrList<cplx<R>> out, int64_t nrows,
                                                     const cplx<R>* __restrict__ tw, const cplx<R>* __restrict__ post) {
   using C = cplx<R>;
   constexpr int NR = rows_per_block_c(L), ES = NR + 1, NXH = L + 1, NP = L / 2 + 1;
   constexpr int NS = fz::rplan(L, PV).ns;
+  static_assert(NS >= 2, "first and last stage must differ");
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   const int64_t row0 = (int64_t)blockIdx.x * NR;
@@ -330,17 +380,22 @@ __global__ void __launch_bounds__(256) k_rows_r2c_s(PtrList<const R> in, PtrList
   const C* src = (const C*)(in.p[blockIdx.y] + row0 * (2 * L));
   C* dst = out.p[blockIdx.y] + row0 * NXH;
   // a row of 2L reals is L complex pairs (rows past nr read row 0, never stored)
-  stage_io<C, L, 0, NR, 256, PV, true>(
+  stage_io<C, L, 0, NR, 256, PV, true, true>(
       tw, [&](int r, int e) { return src[(int64_t)(r < nr ? r : 0) * L + e]; },
       [&](int r, int e, C v) { buf[e * ES + r] = v; });
   __syncthreads();
-  stages_smem<C, L, NR, ES, 256, PV, true, 1, NS>(buf, tw);
+  stages_smem<C, L, NR, ES, 256, PV, true, 1, NS - 1>(buf, tw);
+  // last stage: position e holds frequency rev(e); store it at its frequency
+  stage_io<C, L, NS - 1, NR, 256, PV, true, false, true>(
+      tw, [&](int r, int e) { return buf[e * ES + r]; },
+      [&](int r, int e, C v) { buf[fz::rev<L, PV>(e) * ES + r] = v; });
+  __syncthreads();
   // split: X[k] = E + W^k O with E = (Z[k] + conj Z[L-k])/2, O = -i (Z[k] - conj Z[L-k])/2
   for (int i = threadIdx.x; i < NR * NP; i += 256) {
-    const int r = i % NR, k = i / NR;
+    const int r = i / NP, k = i - r * NP;
     if (r >= nr) continue;
     const int km = k == 0 ? 0 : L - k;
-    const C zk = buf[fz::pos<L, PV>(k) * ES + r], zm = buf[fz::pos<L, PV>(km) * ES + r];
+    const C zk = buf[k * ES + r], zm = buf[km * ES + r];
     C* drow = dst + (int64_t)r * NXH;
     {
       C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
@@ -363,15 +418,16 @@ __global__ void __launch_bounds__(256) k_rows_c2r_s(PtrList<const cplx<R>> in, P
   using C = cplx<R>;
   constexpr int NR = rows_per_block_c(L), ES = NR + 1, NXH = L + 1, NP = L / 2 + 1;
   constexpr int NS = fz::rplan(L, PV).ns;
+  static_assert(NS >= 2, "first and last stage must differ");
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   const int64_t row0 = (int64_t)blockIdx.x * NR;
   const int nr = (int)min((int64_t)NR, nrows - row0);
   const C* src = in.p[blockIdx.y] + row0 * NXH;
   C* dst = (C*)(out.p[blockIdx.y] + row0 * (2 * L));
-  // Z[k] = (X[k] + conj X[L-k]) + i (X[k] - conj X[L-k]) W^-k, into digit-reversed positions
+  // Z[k] = (X[k] + conj X[L-k]) + i (X[k] - conj X[L-k]) W^-k, in natural order
   for (int i = threadIdx.x; i < NR * NP; i += 256) {
-    const int r = i % NR, k = i / NR;
+    const int r = i / NP, k = i - r * NP;
     if (r >= nr) continue;
     const C* srow = src + (int64_t)r * NXH;
     C xk = srow[k], xm = srow[L - k];
@@ -379,17 +435,22 @@ __global__ void __launch_bounds__(256) k_rows_c2r_s(PtrList<const cplx<R>> in, P
     {
       C ex = cadd(xk, cconj(xm));
       C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, NXH);
-      buf[fz::pos<L, PV>(k) * ES + r] = cadd(ex, mk(-ox.y, ox.x));
+      buf[k * ES + r] = cadd(ex, mk(-ox.y, ox.x));
     }
     if (k != 0 && k != L - k) {
       C ex = cadd(xm, cconj(xk));
       C ox = Tw<C>::mulc(csub(xm, cconj(xk)), post, L - k, NXH);
-      buf[fz::pos<L, PV>(L - k) * ES + r] = cadd(ex, mk(-ox.y, ox.x));
+      buf[(L - k) * ES + r] = cadd(ex, mk(-ox.y, ox.x));
     }
   }
   __syncthreads();
-  stages_smem<C, L, NR, ES, 256, PV, false, NS - 1, 0>(buf, tw);
-  stage_io<C, L, 0, NR, 256, PV, false>(
+  // first DIT stage: position e takes frequency rev(e)
+  stage_io<C, L, NS - 1, NR, 256, PV, false, false, true>(
+      tw, [&](int r, int e) { return buf[fz::rev<L, PV>(e) * ES + r]; },
+      [&](int r, int e, C v) { buf[e * ES + r] = v; });
+  __syncthreads();
+  stages_smem<C, L, NR, ES, 256, PV, false, NS - 2, 0>(buf, tw);
+  stage_io<C, L, 0, NR, 256, PV, false, true>(
       tw, [&](int r, int e) { return buf[e * ES + r]; },
       [&](int r, int e, C v) {
         if (r < nr) dst[(int64_t)r * L + e] = v;
