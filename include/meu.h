@@ -166,13 +166,14 @@ int meu_destroy(meu_handle* h);
  * first, 1: radix 4 first, 2: radix 16 first), threads of the plane kernels,
  * complex columns per column-kernel block.  Handles on the generic path (KKS,
  * heterogeneous or non-cubic Landau) report (radix plan of their power-of-two
- * transforms, 0, 0); MEU_FLAG_AUTOTUNE picks that plan by timing at meu_create. */
+ * transforms, 0, column-tile factor 1 or 2); MEU_FLAG_AUTOTUNE picks both by
+ * timing at meu_create. */
 int meu_schedule(meu_handle* h, int32_t* out3);
 /* Choose the schedule (same three values) of a fused Landau handle before its
  * first meu_set_fields; MEU_ERR_UNSUPPORTED if the grid and precision have no
  * such variant (the variants: radix plan 0, 1 or 2, 512 or 256 plane threads,
  * column tile 16 or 8 in FP32, 8 or 4 in FP64 where the tiles fit).  A generic
- * handle takes (0 or 2, 0, 0) at any time. */
+ * handle takes (0 or 2, 0, 1 or 2) at any time. */
 int meu_set_schedule(meu_handle* h, const int32_t* in3);
 
 /* Adjoint. ---------------------------------------------------------------

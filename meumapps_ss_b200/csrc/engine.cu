@@ -417,8 +417,9 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
   }
 }
 
-// Generic path: time the radix plans of the compile-time transforms (forward and
-// inverse of V fields, the batch of the driving-force transforms) and keep the faster.
+// Generic path: time the radix plans and column tiles of the compile-time transforms
+// (forward and inverse of V fields, the batch of the driving-force transforms) and
+// keep the fastest.
 template <typename R>
 void Engine<R>::tune_transforms() {
   const int nf = std::min(V, NS);
@@ -433,9 +434,11 @@ void Engine<R>::tune_transforms() {
   MEU_CUDA(cudaEventCreate(&e0));
   MEU_CUDA(cudaEventCreate(&e1));
   float best = 0;
-  int best_pv = 0;
-  for (int pv : {0, 2}) {
+  int best_pv = 0, best_ct = 1;
+  for (int cand = 0; cand < 4; ++cand) {
+    const int pv = (cand & 1) ? 2 : 0, ct = (cand & 2) ? 2 : 1;
     fft->pv = pv;
+    fft->ct = ct;
     for (int i = 0; i < 2; ++i) {
       fwd_list(in, 0);
       inv_list(0, out);
@@ -449,14 +452,16 @@ void Engine<R>::tune_transforms() {
     MEU_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
     MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (pv == 0 || ms < best) {
+    if (cand == 0 || ms < best) {
       best = ms;
       best_pv = pv;
+      best_ct = ct;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   fft->pv = best_pv;
+  fft->ct = best_ct;
   MEU_CUDA(cudaMemsetAsync(sp, 0, sizeof(C) * (size_t)NS * nk, st));
   MEU_CUDA(cudaMemsetAsync(fd, 0, sizeof(R) * V * n3, st));
   MEU_CUDA(cudaStreamSynchronize(st));
@@ -466,9 +471,11 @@ template <typename R>
 void Engine<R>::set_schedule(const int32_t* in3) {
   if (!fused) {
     // the transforms keep no state between calls, so the plan may change at any time
-    if ((in3[0] != 0 && in3[0] != 2) || in3[1] != 0 || in3[2] != 0)
-      throw CudaError("generic path: the schedule is (radix plan 0 or 2, 0, 0)", MEU_ERR_UNSUPPORTED);
+    if ((in3[0] != 0 && in3[0] != 2) || in3[1] != 0 || (in3[2] != 1 && in3[2] != 2))
+      throw CudaError("generic path: the schedule is (radix plan 0 or 2, 0, column-tile factor 1 or 2)",
+                      MEU_ERR_UNSUPPORTED);
     fft->pv = in3[0];
+    fft->ct = in3[2];
     return;
   }
   if (fields_set) throw CudaError("set the schedule before the first meu_set_fields", MEU_ERR_BADARG);

@@ -152,10 +152,10 @@ class Engine : public EngineBase {
   void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
   void set_stream(cudaStream_t s) override { st = s ? s : own_st; }
   bool schedule(int32_t* out3) const override {
-    if (!fused) {  // generic path: the radix plan of its transforms
+    if (!fused) {  // generic path: radix plan and column-tile factor of its transforms
       out3[0] = fft->pv;
       out3[1] = 0;
-      out3[2] = 0;
+      out3[2] = fft->ct;
       return true;
     }
     out3[0] = sched.pv;

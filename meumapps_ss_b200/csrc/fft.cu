@@ -564,17 +564,21 @@ static bool rows_s(bool fwd, int L, int pv, int nf, int64_t nrows, const void* i
 }
 
 template <typename R, bool FWD>
-static bool cols_s(int L, int pv, int nf, int outer, int inner, int64_t ostride, const PtrList<cplx<R>>& buf,
+static bool cols_s(int L, int pv, int ct, int nf, int outer, int inner, int64_t ostride, const PtrList<cplx<R>>& buf,
                    const void* tw, R scale, cudaStream_t st) {
   using C = cplx<R>;
   auto go = [&](auto Lc, auto Pc) {
     constexpr int LL = decltype(Lc)::value, PV = decltype(Pc)::value;
-    constexpr int TM = col_tile_s<R>(LL);
-    const size_t sm = (size_t)LL * TM * sizeof(C);
-    set_smem<R>((const void*)k_cols_s<R, FWD, LL, TM, PV>, sm);
-    const dim3 g((unsigned)(outer * ((inner + TM - 1) / TM)), nf);
-    k_cols_s<R, FWD, LL, TM, PV><<<g, 256, sm, st>>>(buf, buf, inner, ostride, (const C*)tw, scale);
-    return true;
+    auto launch = [&](auto Tc) {
+      constexpr int TM = decltype(Tc)::value;
+      const size_t sm = (size_t)LL * TM * sizeof(C);
+      set_smem<R>((const void*)k_cols_s<R, FWD, LL, TM, PV>, sm);
+      const dim3 g((unsigned)(outer * ((inner + TM - 1) / TM)), nf);
+      k_cols_s<R, FWD, LL, TM, PV><<<g, 256, sm, st>>>(buf, buf, inner, ostride, (const C*)tw, scale);
+      return true;
+    };
+    constexpr int TM1 = col_tile_s<R>(LL);
+    return ct == 2 ? launch(std::integral_constant<int, 2 * TM1>{}) : launch(std::integral_constant<int, TM1>{});
   };
   return dispatch_len(L, pv, go);
 }
@@ -615,7 +619,7 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     set_smem<R>((const void*)k_cols<R, true>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
     { HookScope hs_(hook, "fft_y_fwd", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, true>(ny, pv, nf, nz, nxh, (int64_t)ny * nxh, out, py.tw, (R)1, st))
+  if (!cols_s<R, true>(ny, pv, ct, nf, nz, nxh, (int64_t)ny * nxh, out, py.tw, (R)1, st))
     k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
@@ -628,7 +632,7 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
     { HookScope hs_(hook, "fft_z_fwd", 2.0 * nf * nk() * sizeof(C), st);
   const R scale = (R)(1.0 / ((double)nx * ny * nz));
-  if (!cols_s<R, true>(nz, pv, nf, 1, inner, 0, out, pz.tw, scale, st))
+  if (!cols_s<R, true>(nz, pv, ct, nf, 1, inner, 0, out, pz.tw, scale, st))
     k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, scale); }
     MEU_CHECK_LAUNCH();
   }
@@ -644,7 +648,7 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     int inner = ny * nxh;
     dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
     { HookScope hs_(hook, "fft_z_inv", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, false>(nz, pv, nf, 1, inner, 0, in, pz.tw, (R)1, st))
+  if (!cols_s<R, false>(nz, pv, ct, nf, 1, inner, 0, in, pz.tw, (R)1, st))
     k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1); }
     MEU_CHECK_LAUNCH();
   }
@@ -654,7 +658,7 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     set_smem<R>((const void*)k_cols<R, false>, s2);
     dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
     { HookScope hs_(hook, "fft_y_inv", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, false>(ny, pv, nf, nz, nxh, (int64_t)ny * nxh, in, py.tw, (R)1, st))
+  if (!cols_s<R, false>(ny, pv, ct, nf, nz, nxh, (int64_t)ny * nxh, in, py.tw, (R)1, st))
     k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }

@@ -250,6 +250,9 @@ class FFT3 {
   // radix plan of the compile-time kernels (power-of-two lengths 32..512): 0 = radix 8
   // first, 2 = radix 16 first (one shared-memory pass fewer, more registers)
   int pv = 0;
+  // columns per block of the compile-time column kernels: ct = 1 about 32 KB of tile,
+  // ct = 2 twice as many columns (longer contiguous runs, fewer blocks per SM)
+  int ct = 1;
   LaunchHook* hook = nullptr;
   const void* post_tw;  // cplx<R>[nx/2+1]: exp(-2 pi i k / nx)
   bool fp64;

@@ -122,7 +122,7 @@ class Simulation:
     @property
     def schedule(self) -> Optional[Tuple[int, int, int]]:
         """(radix plan variant, plane threads, column tile) of the fused step; on the
-        generic path (radix plan of the power-of-two transforms, 0, 0)."""
+        generic path (radix plan of the power-of-two transforms, 0, column-tile factor)."""
         out = (C.c_int32 * 3)()
         if lib().meu_schedule(self.h, out):
             return None
@@ -148,7 +148,7 @@ class Simulation:
 
     def set_schedule(self, pv: int, ntp: int, tm: int) -> None:
         """Pick the fused step's schedule (before the first set_fields), or the generic
-        path's transform radix plan as (0 or 2, 0, 0)."""
+        path's transform plan as (0 or 2, 0, 1 or 2)."""
         self._check(lib().meu_set_schedule(self.h, (C.c_int32 * 3)(pv, ntp, tm)))
 
 

@@ -115,11 +115,11 @@ def test_set_schedule_rules():
     q = CF.landau_params(32, 1, [[0.01, 0.01, 0.01]])
     q.flags = P.FLAG_GENERIC
     h = Simulation(q)
-    assert h.schedule == (0, 0, 0)  # generic path: the transforms' radix plan
-    h.set_schedule(2, 0, 0)
-    assert h.schedule == (2, 0, 0)
+    assert h.schedule == (0, 0, 1)  # generic path: radix plan, column-tile factor
+    h.set_schedule(2, 0, 2)
+    assert h.schedule == (2, 0, 2)
     with pytest.raises(_lib.MeuError):
-        h.set_schedule(1, 0, 0)
+        h.set_schedule(1, 0, 1)
 
 
 @pytest.mark.gpu

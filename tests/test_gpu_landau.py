@@ -53,8 +53,8 @@ def test_landau_hetero_parity(oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ortho,pv", [(True, 0), (False, 2)])
-def test_landau_hetero_kernels_parity(oracle, ortho, pv):
+@pytest.mark.parametrize("ortho,pv,ct", [(True, 0, 1), (False, 2, 2)])
+def test_landau_hetero_kernels_parity(oracle, ortho, pv, ct):
     """Proportional moduli through the matrix-free kernels on a 64^3 grid (the
     compile-time transforms), with the normal / shear blocks decoupled (cubic) or
     coupled (an off-block term added to the stiffness), under both radix plans."""
@@ -69,7 +69,7 @@ def test_landau_hetero_kernels_parity(oracle, ortho, pv):
     o = oracle.OracleSim(p)
     o.set_fields(c, e)
     g = Simulation(p)
-    g.set_schedule(pv, 0, 0)
+    g.set_schedule(pv, 0, ct)
     g.set_fields(c, e)
     do, dg = o.run(6), g.run(6)
     assert np.array_equal(do["el_iters"], dg["el_iters"])
