@@ -388,8 +388,12 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       }
       Y.nvar = V;
       const bool ortho = ortho6(hK.c0m) && ortho6(p.cela[0]) && ortho6(p.sela[0]);
-      fn_el_x = ortho ? k_el_x_prop<R, true> : k_el_x_prop<R, false>;
-      fn_elener = ortho ? k_elener_prop<R, true> : k_elener_prop<R, false>;
+      // 16-byte tile copies when every field starts on a 16-byte boundary
+      const bool vec = n3 % (16 / (int64_t)sizeof(R)) == 0;
+      fn_el_x = ortho ? (vec ? k_el_x_prop<R, true, true> : k_el_x_prop<R, true, false>)
+                      : (vec ? k_el_x_prop<R, false, true> : k_el_x_prop<R, false, false>);
+      fn_elener = ortho ? (vec ? k_elener_prop<R, true, true> : k_elener_prop<R, true, false>)
+                        : (vec ? k_elener_prop<R, false, true> : k_elener_prop<R, false, false>);
       sm_el_x = (size_t)2 * (6 + V) * PF_TILE * sizeof(R);
       sm_elener = (size_t)2 * (6 + 2 * V) * PF_TILE * sizeof(R);
       const int64_t ntiles = (n3 + PF_TILE - 1) / PF_TILE;

@@ -273,13 +273,19 @@ __device__ __forceinline__ void mv6(const double* __restrict__ c, const double* 
 // Per-voxel prefetch through shared memory: each thread copies its own voxel's
 // values of the next tile with cp.async while it works on the current one, so the
 // loads of a whole tile are in flight during the FP64 work without holding
-// registers.  Thread i of a block owns voxel i of every tile; no barrier needed.
+// registers.  Per element (VEC = false): thread i copies and uses voxel i of every
+// tile, no barrier needed.  VEC (n3 a multiple of 16 bytes of R): the tile moves in
+// 16-byte copies spread over the block, and barriers order copies and uses.
 constexpr int PF_TILE = 256;
 template <typename R>
 __device__ __forceinline__ void pf_copy(R* smem, const R* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   if constexpr (sizeof(R) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
   else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void pf_copy16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void pf_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void pf_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
@@ -289,7 +295,7 @@ __device__ __forceinline__ void pf_wait_prev() { asm volatile("cp.async.wait_gro
 // The coefficients travel as a kernel parameter, so the FP64 products read their
 // constants straight from the parameter bank.  Dynamic shared memory:
 // 2 * (6 + V) * PF_TILE elements of R (double-buffered tiles, field-major).
-template <typename R, bool ORTHO>
+template <typename R, bool ORTHO, bool VEC>
 __global__ void __launch_bounds__(PF_TILE, 4) k_el_x_prop(const __grid_constant__ ElxProp E, int64_t n3,
                                                           const R* __restrict__ pphi, const R* __restrict__ strain,
                                                           R* __restrict__ xs, double cfac, int* err) {
@@ -300,14 +306,25 @@ __global__ void __launch_bounds__(PF_TILE, 4) k_el_x_prop(const __grid_constant_
   R* buf = (R*)pf_raw;
   const int tid = threadIdx.x;
   auto issue = [&](int64_t tile, int slot) {
-    const int64_t id = tile * PF_TILE + tid;
-    R* b = buf + (int64_t)slot * NF * PF_TILE + tid;
-    if (id < n3) {
+    if constexpr (VEC) {
+      constexpr int PER = 16 / (int)sizeof(R), CPF = PF_TILE / PER;
+      const int64_t base = tile * PF_TILE;
+      R* b = buf + (int64_t)slot * NF * PF_TILE;
+      for (int c = tid; c < NF * CPF; c += PF_TILE) {
+        const int f = c / CPF, j = (c - f * CPF) * PER;
+        const R* src = f < 6 ? strain + (int64_t)f * n3 : pphi + (int64_t)(f - 6) * n3;
+        if (base + j < n3) pf_copy16(b + f * PF_TILE + j, src + base + j);
+      }
+    } else {
+      const int64_t id = tile * PF_TILE + tid;
+      R* b = buf + (int64_t)slot * NF * PF_TILE + tid;
+      if (id < n3) {
 #pragma unroll
-      for (int m = 0; m < 6; ++m) pf_copy(b + m * PF_TILE, strain + (int64_t)m * n3 + id);
+        for (int m = 0; m < 6; ++m) pf_copy(b + m * PF_TILE, strain + (int64_t)m * n3 + id);
 #pragma unroll
-      for (int v = 0; v < NV; ++v)
-        if (v < V) pf_copy(b + (6 + v) * PF_TILE, pphi + (int64_t)v * n3 + id);
+        for (int v = 0; v < NV; ++v)
+          if (v < V) pf_copy(b + (6 + v) * PF_TILE, pphi + (int64_t)v * n3 + id);
+      }
     }
     pf_commit();
   };
@@ -315,8 +332,10 @@ __global__ void __launch_bounds__(PF_TILE, 4) k_el_x_prop(const __grid_constant_
   int64_t tile = blockIdx.x;
   issue(tile, 0);
   for (int k = 0; tile < ntiles; tile += gridDim.x, ++k) {
+    if (VEC) __syncthreads();  // every thread is done with the slot the next copies fill
     issue(tile + gridDim.x, (k + 1) & 1);
     pf_wait_prev();
+    if (VEC) __syncthreads();  // the other threads' copies of this tile have landed
     const int64_t id = tile * PF_TILE + tid;
     if (id >= n3) continue;
     const R* b = buf + (int64_t)(k & 1) * NF * PF_TILE + tid;
@@ -513,7 +532,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
 // Coefficients as a kernel parameter; ORTHO as in mv6.  Loads prefetched through
 // shared memory as in k_el_x_prop: dynamic shared memory 2 * (6 + 2V) * PF_TILE
 // elements of R.
-template <typename R, bool ORTHO>
+template <typename R, bool ORTHO, bool VEC>
 __global__ void __launch_bounds__(PF_TILE, 3) k_elener_prop(const __grid_constant__ ElenProp E, int64_t n3,
                                                             const R* __restrict__ phi, const R* __restrict__ pphi,
                                                             const R* __restrict__ strain, R* __restrict__ el_en,
@@ -527,17 +546,29 @@ __global__ void __launch_bounds__(PF_TILE, 3) k_elener_prop(const __grid_constan
   R* buf = (R*)pf_raw;
   const int tid = threadIdx.x;
   auto issue = [&](int64_t tile, int slot) {
-    const int64_t id = tile * PF_TILE + tid;
-    R* b = buf + (int64_t)slot * NF * PF_TILE + tid;
-    if (id < n3) {
+    if constexpr (VEC) {
+      constexpr int PER = 16 / (int)sizeof(R), CPF = PF_TILE / PER;
+      const int64_t base = tile * PF_TILE;
+      R* b = buf + (int64_t)slot * NF * PF_TILE;
+      for (int c = tid; c < NF * CPF; c += PF_TILE) {
+        const int f = c / CPF, j = (c - f * CPF) * PER;
+        const R* src = f < 6 ? strain + (int64_t)f * n3
+                             : (f < 6 + V ? pphi + (int64_t)(f - 6) * n3 : phi + (int64_t)(f - 6 - V) * n3);
+        if (base + j < n3 && (f < 6 + V || E.use[f - 6 - V])) pf_copy16(b + f * PF_TILE + j, src + base + j);
+      }
+    } else {
+      const int64_t id = tile * PF_TILE + tid;
+      R* b = buf + (int64_t)slot * NF * PF_TILE + tid;
+      if (id < n3) {
 #pragma unroll
-      for (int m = 0; m < 6; ++m) pf_copy(b + m * PF_TILE, strain + (int64_t)m * n3 + id);
+        for (int m = 0; m < 6; ++m) pf_copy(b + m * PF_TILE, strain + (int64_t)m * n3 + id);
 #pragma unroll
-      for (int v = 0; v < NV; ++v)
-        if (v < V) {
-          pf_copy(b + (6 + v) * PF_TILE, pphi + (int64_t)v * n3 + id);
-          if (E.use[v]) pf_copy(b + (6 + V + v) * PF_TILE, phi + (int64_t)v * n3 + id);
-        }
+        for (int v = 0; v < NV; ++v)
+          if (v < V) {
+            pf_copy(b + (6 + v) * PF_TILE, pphi + (int64_t)v * n3 + id);
+            if (E.use[v]) pf_copy(b + (6 + V + v) * PF_TILE, phi + (int64_t)v * n3 + id);
+          }
+      }
     }
     pf_commit();
   };
@@ -546,8 +577,10 @@ __global__ void __launch_bounds__(PF_TILE, 3) k_elener_prop(const __grid_constan
   int64_t tile = blockIdx.x;
   issue(tile, 0);
   for (int k = 0; tile < ntiles; tile += gridDim.x, ++k) {
+    if (VEC) __syncthreads();  // every thread is done with the slot the next copies fill
     issue(tile + gridDim.x, (k + 1) & 1);
     pf_wait_prev();
+    if (VEC) __syncthreads();  // the other threads' copies of this tile have landed
     const int64_t id = tile * PF_TILE + tid;
     if (id >= n3) continue;
     const R* b = buf + (int64_t)(k & 1) * NF * PF_TILE + tid;
