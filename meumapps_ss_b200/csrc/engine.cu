@@ -374,6 +374,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
         X.inc[v] = n >= 2 ? 1.0 : 0.0;
       }
       X.nvar = V;
+      el_prop_r.assign(X);
       ElenProp& Y = en_prop;
       for (int i = 0; i < 36; ++i) {
         Y.c1[i] = p.cela[0][i];
@@ -388,6 +389,8 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       }
       Y.nvar = V;
       const bool ortho = ortho6(hK.c0m) && ortho6(p.cela[0]) && ortho6(p.sela[0]);
+      el_ortho = ortho;
+      el_fused_rows = el_rows_ok(p.nx);
       // 16-byte tile copies when every field starts on a 16-byte boundary
       const bool vec = n3 % (16 / (int64_t)sizeof(R)) == 0;
       fn_el_x = ortho ? (vec ? k_el_x_prop<R, true, true> : k_el_x_prop<R, true, false>)
@@ -703,22 +706,34 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
     double newfac = 0.5, cfac = 1.0, err_old[6] = {0, 0, 0, 0, 0, 0};
     int niter = 0;
     bool converged = false;
+    std::vector<R*> out;
+    for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
+    // spec(0..5) holds the strain spectrum of the last el_k and the real strain is not
+    // formed yet: the next iteration runs its x passes and el_x as one kernel
+    bool spec_pending = false;
     for (;;) {
       niter += 1;
       total += 1;
       if (total > 100000) throw CudaError("elastic iteration runaway", MEU_ERR_NOT_CONVERGED);
-      if (hK.prop_moduli) {
-        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
-                fn_el_x<<<g_el_x, PF_TILE, sm_el_x, st>>>(el_prop, (int64_t)n3, pphi, strain, xs, cfac, d_err));
-      } else
-        KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
-      std::vector<const R*> in;
-      for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
-      fwd_list(in, 0);
+      if (spec_pending) {
+        fft->inverse_cols<R>(specs(0, 6), 6, st);
+        KLAUNCH("el_rows", 6.0 * 2 * nk * sizeof(C) + (double)V * n3 * sizeof(R),
+                el_rows_launch<R>(*fft, specs(0, 6), pphi, el_prop_r, el_ortho, cfac, d_err, st));
+        fft->forward_cols<R>(specs(0, 6), 6, st);
+        spec_pending = false;
+      } else {
+        if (hK.prop_moduli) {
+          KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
+                  fn_el_x<<<g_el_x, PF_TILE, sm_el_x, st>>>(el_prop, (int64_t)n3, pphi, strain, xs, cfac, d_err));
+        } else
+          KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
+        std::vector<const R*> in;
+        for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
+        fwd_list(in, 0);
+      }
       KLAUNCH("el_k", 18.0 * nk * sizeof(C), k_el_k<R><<<g_el_k, RED_THREADS, 0, st>>>(dK, specs(0, 6), uk, partials, d_err));
-      std::vector<R*> out;
-      for (int m = 0; m < 6; ++m) out.push_back(field(strain, m));
-      inv_list(0, out);
+      if (el_fused_rows) spec_pending = true;
+      else inv_list(0, out);
       finalize(Q_ERR0, 6);
       MEU_CUDA(cudaMemcpyAsync(h_results + Q_ERR0, results + Q_ERR0, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
       check_err();  // synchronises
@@ -749,6 +764,7 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
       }
       break;
     }
+    if (spec_pending) inv_list(0, out);
   }
   last_iters = total;
   const int eta2 = (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0;

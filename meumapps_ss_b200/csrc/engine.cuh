@@ -14,13 +14,30 @@
 
 namespace meu {
 // proportional-moduli polarization coefficients, passed by value to k_el_x_prop
-struct ElxProp {
-  double c0[36], c1[36], ebar[6];
-  double ep[MEU_MAX_VAR][6];
-  double av[MEU_MAX_VAR];   // alpha of the variant's phase, 0 for phase-1 variants
-  double inc[MEU_MAX_VAR];  // 1 when the variant counts toward sum P (phase >= 2)
+// (W = double) and to the fused row kernel (W = the field precision)
+template <typename W>
+struct ElxCoef {
+  W c0[36], c1[36], ebar[6];
+  W ep[MEU_MAX_VAR][6];
+  W av[MEU_MAX_VAR];   // alpha of the variant's phase, 0 for phase-1 variants
+  W inc[MEU_MAX_VAR];  // 1 when the variant counts toward sum P (phase >= 2)
   int nvar;
+  template <typename U>
+  void assign(const ElxCoef<U>& o) {
+    for (int i = 0; i < 36; ++i) {
+      c0[i] = (W)o.c0[i];
+      c1[i] = (W)o.c1[i];
+    }
+    for (int m = 0; m < 6; ++m) ebar[m] = (W)o.ebar[m];
+    for (int v = 0; v < MEU_MAX_VAR; ++v) {
+      for (int m = 0; m < 6; ++m) ep[v][m] = (W)o.ep[v][m];
+      av[v] = (W)o.av[v];
+      inc[v] = (W)o.inc[v];
+    }
+    nvar = o.nvar;
+  }
 };
+using ElxProp = ElxCoef<double>;
 // proportional-moduli elastic-energy coefficients, passed by value to k_elener_prop
 struct ElenProp {
   double c1[36], s1[36], emean[6];
@@ -29,6 +46,13 @@ struct ElenProp {
   int use[MEU_MAX_VAR];       // phase >= 2 and use_var: gets an energy share and a driving force
   int nvar;
 };
+// x-direction work of one elastic iteration in one pass (el_rows.cu): x C2R of the six
+// strain spectra, polarisation, x R2C into the same spectra; row length nx/2 a power
+// of two in 32..512 (el_rows_ok)
+bool el_rows_ok(int nx);
+template <typename R>
+void el_rows_launch(const FFT3& f, const PtrList<cplx<R>>& sp, const R* pphi, const ElxCoef<R>& E, bool ortho,
+                    double cfac, int* err, cudaStream_t st);
 }  // namespace meu
 
 namespace meu {
@@ -262,11 +286,14 @@ class Engine : public EngineBase {
   // partial second wave would redo a whole share of the loop); <= RED_BLOCKS
   int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS, g_el_x = RED_BLOCKS;
   ElxProp el_prop{};  // proportional-moduli polarization coefficients (host-built)
+  ElxCoef<R> el_prop_r{};  // the same in the field precision (fused row kernel)
   ElenProp en_prop{};  // proportional-moduli energy coefficients (host-built)
   // the instantiation of the proportional kernels for this stiffness form
   void (*fn_el_x)(ElxProp, int64_t, const R*, const R*, R*, double, int*) = nullptr;
   void (*fn_elener)(ElenProp, int64_t, const R*, const R*, const R*, R*, R*, int, int, double*, int*) = nullptr;
   size_t sm_el_x = 0, sm_elener = 0;  // their dynamic shared memory (prefetch tiles)
+  bool el_ortho = false;              // stiffnesses with decoupled normal / shear blocks
+  bool el_fused_rows = false;         // iterations run the x passes and el_x as one kernel
   bool fused_warm = false;
   bool theta_ready = false;  // sp holds theta^ of the current fields (written by the last step's PI)
   bool fields_set = false;  // the spectral-state layout is fixed from the first upload on

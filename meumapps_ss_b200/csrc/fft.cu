@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "fft_stages.cuh"
 #include "fused.cuh"
 
 namespace meu {
@@ -267,99 +268,6 @@ __global__ void __launch_bounds__(256) k_cols(PtrList<cplx<R>> in, PtrList<cplx<
 // run-time plan above.
 constexpr int rows_per_block_c(int L) { return 2048 / L < 1 ? 1 : (2048 / L > 64 ? 64 : 2048 / L); }
 
-// One radix stage over NL lines with caller-supplied element access: ld(line, e)
-// and st(line, e, v) address element e of a line in whatever memory the stage
-// reads or writes.  FWD: DIF butterfly then twiddle; else twiddle then DIT butterfly.
-// JFAST: consecutive threads take consecutive butterflies of one line (consecutive
-// elements, for row-contiguous global memory) instead of the same butterfly of
-// consecutive lines.  HOLD: every thread loads and transforms all of its
-// butterflies, the block synchronises, then all store -- for a stage whose
-// stores land on other threads' inputs (a permuting, in-place stage).
-template <typename C, int L, int S, int NL, int NT, int PV, bool FWD, bool JFAST = false, bool HOLD = false,
-          typename LD, typename ST>
-__device__ __forceinline__ void stage_io(const C* __restrict__ tw, LD&& ld, ST&& st) {
-  constexpr int R = fz::rplan(L, PV).r[S];
-  constexpr int SPAN = fz::span_of(L, S, PV);
-  constexpr int M = SPAN / R, NBF = NL * (L / R), TWS = L / SPAN;
-  auto map = [](int t, int& line, int& j, int& e0) {
-    int b;
-    if constexpr (JFAST) {
-      j = t % M;
-      const int u = t / M;
-      line = u % NL;
-      b = u / NL;
-    } else {
-      line = t % NL;
-      const int u = t / NL;
-      j = u % M;
-      b = u / M;
-    }
-    e0 = b * SPAN + j;
-  };
-  auto butterfly = [&](C* x, int j) {
-    if constexpr (FWD) {
-      Dft<R, -1, C>::run(x);
-      if (M > 1) {
-#pragma unroll
-        for (int q = 1; q < R; ++q) x[q] = Tw<C>::mul(x[q], tw, j * q * TWS, L);
-      }
-    } else {
-      if (M > 1) {
-#pragma unroll
-        for (int q = 1; q < R; ++q) x[q] = Tw<C>::mulc(x[q], tw, j * q * TWS, L);
-      }
-      Dft<R, 1, C>::run(x);
-    }
-  };
-  if constexpr (HOLD) {
-    constexpr int IT = (NBF + NT - 1) / NT;
-    C x[IT][R];
-    int ln[IT], ee[IT];
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-      const int t = threadIdx.x + it * NT;
-      if (t < NBF) {
-        int j;
-        map(t, ln[it], j, ee[it]);
-#pragma unroll
-        for (int r = 0; r < R; ++r) x[it][r] = ld(ln[it], ee[it] + r * M);
-        butterfly(x[it], j);
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int it = 0; it < IT; ++it)
-      if (threadIdx.x + it * NT < NBF) {
-#pragma unroll
-        for (int q = 0; q < R; ++q) st(ln[it], ee[it] + q * M, x[it][q]);
-      }
-  } else {
-#pragma unroll 1
-    for (int t = threadIdx.x; t < NBF; t += NT) {
-      int line, j, e0;
-      map(t, line, j, e0);
-      C x[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) x[r] = ld(line, e0 + r * M);
-      butterfly(x, j);
-#pragma unroll
-      for (int q = 0; q < R; ++q) st(line, e0 + q * M, x[q]);
-    }
-  }
-}
-
-// Stages S, S+1, .. (FWD) or S, S-1, .. (inverse), up to but excluding SEND, in
-// shared memory (element e of line l at buf[e * ES + l]); each ends with a barrier.
-template <typename C, int L, int NL, int ES, int NT, int PV, bool FWD, int S, int SEND>
-__device__ __forceinline__ void stages_smem(C* buf, const C* tw) {
-  if constexpr (FWD ? (S < SEND) : (S > SEND)) {
-    stage_io<C, L, S, NL, NT, PV, FWD>(
-        tw, [&](int l, int e) { return buf[e * ES + l]; }, [&](int l, int e, C v) { buf[e * ES + l] = v; });
-    __syncthreads();
-    stages_smem<C, L, NL, ES, NT, PV, FWD, FWD ? S + 1 : S - 1, SEND>(buf, tw);
-  }
-}
-
 // Rows interleaved in shared memory: element e of row r at e * ES + r with the odd
 // stride ES = NR + 1, so that runs of consecutive e and runs of consecutive r both
 // spread over the banks.  The global-facing stage walks consecutive elements of a
@@ -612,6 +520,12 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
   if (!rows_s<R>(true, Lx, pv, nf, nrows, &in, &out, px.tw, post_tw, st))
     k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
+  forward_cols<R>(out, nf, st);
+}
+
+template <typename R>
+void FFT3::forward_cols(const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const {
+  using C = cplx<R>;
   // y columns: outer = z, inner = nxh
   {
     int tm = col_tile(ny, sizeof(R) == 8);
@@ -640,6 +554,12 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
 
 template <typename R>
 void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const {
+  inverse_cols<R>(in, nf, st);
+  inverse_rows<R>(in, out, nf, st);
+}
+
+template <typename R>
+void FFT3::inverse_cols(const PtrList<cplx<R>>& in, int nf, cudaStream_t st) const {
   using C = cplx<R>;
   {
     int tm = col_tile(nz, sizeof(R) == 8);
@@ -662,6 +582,11 @@ void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cu
     k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
     MEU_CHECK_LAUNCH();
   }
+}
+
+template <typename R>
+void FFT3::inverse_rows(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const {
+  using C = cplx<R>;
   const int Lx = px.L;
   const int64_t nrows = (int64_t)ny * nz;
   const int rpb = rows_per_block(Lx);
@@ -680,5 +605,9 @@ template void FFT3::forward<float>(const PtrList<const float>&, const PtrList<fl
 template void FFT3::forward<double>(const PtrList<const double>&, const PtrList<double2>&, int, cudaStream_t) const;
 template void FFT3::inverse<float>(const PtrList<float2>&, const PtrList<float>&, int, cudaStream_t) const;
 template void FFT3::inverse<double>(const PtrList<double2>&, const PtrList<double>&, int, cudaStream_t) const;
+template void FFT3::forward_cols<float>(const PtrList<float2>&, int, cudaStream_t) const;
+template void FFT3::forward_cols<double>(const PtrList<double2>&, int, cudaStream_t) const;
+template void FFT3::inverse_cols<float>(const PtrList<float2>&, int, cudaStream_t) const;
+template void FFT3::inverse_cols<double>(const PtrList<double2>&, int, cudaStream_t) const;
 
 }  // namespace meu

@@ -245,6 +245,12 @@ class FFT3 {
   // scratch and holds garbage afterwards.
   template <typename R>
   void inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
+  // the y and z passes alone (forward: after the x pass, scaled; inverse: before it),
+  // for callers that do the x pass themselves
+  template <typename R>
+  void forward_cols(const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const;
+  template <typename R>
+  void inverse_cols(const PtrList<cplx<R>>& in, int nf, cudaStream_t st) const;
 
   LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
   // radix plan of the compile-time kernels (power-of-two lengths 32..512): 0 = radix 8
@@ -258,6 +264,8 @@ class FFT3 {
   bool fp64;
 
  private:
+  template <typename R>
+  void inverse_rows(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
   void* dev_mem = nullptr;
   bool owns_mem = false;
 };

@@ -258,11 +258,11 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
 // shears are independent (C[i][j] = 0 for i < 3 <= j, j < 3 <= i and 3 <= i != j,
 // every cubic or orthotropic stiffness in its crystal frame).  The skipped terms are
 // exact zeros, so the sums are bit-identical to the full product.
-template <bool ORTHO>
-__device__ __forceinline__ void mv6(const double* __restrict__ c, const double* x, double* y) {
+template <bool ORTHO, typename W>
+__device__ __forceinline__ void mv6(const W* __restrict__ c, const W* x, W* y) {
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
-    double a = 0;
+    W a = 0;
 #pragma unroll
     for (int m = 0; m < 6; ++m)
       if (!ORTHO || (i < 3 && m < 3) || i == m) a += c[i + m * 6] * x[m];

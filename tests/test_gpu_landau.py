@@ -80,6 +80,27 @@ def test_landau_hetero_kernels_parity(oracle, ortho, pv, ct):
 
 
 @pytest.mark.gpu
+def test_landau_hetero_fp32_fused_rows():
+    """FP32 heterogeneous step on 64^3, where each fixed-point iteration runs its x
+    transforms and the polarisation as one kernel, against the FP64 step."""
+    p64, c, e = active_landau(n=64, nvar=2, elastic=P.ELAST_HETERO, coupling=P.EIG_H, ppt_scale=1.5, el_tol=1e-8)
+    p32 = p64.copy()
+    p32.precision = P.PREC_F32
+    out = {}
+    for name, p in (("f64", p64), ("f32", p32)):
+        with Simulation(p) as g:
+            g.set_fields(c, e)
+            g.timing(True)
+            g.run(10)
+            assert "el_rows" in g.timing_report()
+            out[name] = g.get_fields()
+    rc = np.linalg.norm(out["f32"][0] - out["f64"][0]) / np.linalg.norm(out["f64"][0])
+    re = np.linalg.norm(out["f32"][1] - out["f64"][1]) / np.linalg.norm(out["f64"][1])
+    rl = np.linalg.norm(out["f32"][2] - out["f64"][2]) / np.linalg.norm(out["f64"][2])
+    assert rc <= 1e-5 and re <= 1e-5 and rl <= 1e-4, (rc, re, rl)
+
+
+@pytest.mark.gpu
 def test_landau_hetero_fp32_odd_cell_count():
     """FP32 heterogeneous step on an 18 x 9 x 9 grid: 1458 cells is no multiple of four
     floats, so the elastic kernels copy their tiles element by element; checked
