@@ -14,20 +14,22 @@
 namespace meu {
 
 // rows per block: 6 * NR lines of L complex in shared memory
-constexpr int el_rows_per_block(int L) { return 1024 / L < 1 ? 1 : (1024 / L > 16 ? 16 : 1024 / L); }
+constexpr int el_rows_per_block(int L) { return 512 / L < 1 ? 1 : (512 / L > 16 ? 16 : 512 / L); }
+// order parameters prefetched into shared memory up to this many variants
+constexpr int EL_ROWS_PF_VAR = 4;
 
 // polarisation of one voxel from its engineering strain g[6] (k_el_x_prop's formula,
 // in the field precision R: FP64 for the plain path, FP32 for the FP32-bulk path;
 // order parameters at pp[v * n3])
 template <typename R, bool ORTHO>
-__device__ __forceinline__ void elx_voxel(const ElxCoef<R>& E, R cfac, const R* g, const R* pp, int64_t n3, R* x,
+__device__ __forceinline__ void elx_voxel(const ElxCoef<R>& E, R cfac, const R* g, const R* pp, int64_t pstride, R* x,
                                           int* err) {
   const int V = E.nvar;
   R e0[6] = {0, 0, 0, 0, 0, 0}, psum = 0, sc = 0;
 #pragma unroll
   for (int v = 0; v < MEU_MAX_VAR; ++v) {
     if (v >= V) break;
-    const R q = pp[(int64_t)v * n3];
+    const R q = pp[(int64_t)v * pstride];
     psum += E.inc[v] * q;
     sc += E.av[v] * q;
 #pragma unroll
@@ -50,8 +52,10 @@ __device__ __forceinline__ void elx_voxel(const ElxCoef<R>& E, R cfac, const R* 
 
 // Shared memory: element e of line l = m * NR + r (component m of row r) at
 // buf[e * ES + l], ES = 6 NR + 1.  sp.p[m] holds component m's spectrum, rows of
-// L + 1 complex, in place (read whole before written).
-template <typename R, int L, int PV, bool ORTHO>
+// L + 1 complex, in place (read whole before written).  PF: the block's order
+// parameters (V <= EL_ROWS_PF_VAR rows of 2L reals each) follow buf, copied with
+// cp.async at the start so that they arrive during the inverse transform.
+template <typename R, int L, int PV, bool ORTHO, bool PF>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 4) k_el_rows(PtrList<cplx<R>> sp, const R* __restrict__ pphi, int64_t nrows,
                                                  const cplx<R>* __restrict__ tw, const cplx<R>* __restrict__ post,
                                                  const __grid_constant__ ElxCoef<R> E, int64_t n3, R cfac, int* err) {
@@ -63,6 +67,18 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 4) k_el_rows(PtrList
   C* buf = (C*)smraw;
   const int64_t row0 = (int64_t)blockIdx.x * NR;
   const int nr = (int)min((int64_t)NR, nrows - row0);
+  R* pbuf = (R*)(buf + ES * L);
+  if constexpr (PF) {
+    // rows row0 .. row0 + nr - 1 of each order parameter: 16-byte pieces (2L reals
+    // per row, a multiple of 16 bytes; n3 a multiple of 2L)
+    constexpr int PER = 16 / (int)sizeof(R), CPR = 2 * L / PER;
+    const int nchunk = E.nvar * nr * CPR;
+    for (int c = threadIdx.x; c < nchunk; c += 256) {
+      const int v = c / (nr * CPR), rem = c - v * nr * CPR, r = rem / CPR, j = (rem - r * CPR) * PER;
+      fz::cp_async16(pbuf + (v * NR + r) * (2 * L) + j, pphi + (int64_t)v * n3 + (row0 + r) * (2 * L) + j);
+    }
+    fz::cp_async_commit();
+  }
 
   // ---- x C2R of the six strain components: split into natural order ...
   for (int i = threadIdx.x; i < NL * NP; i += 256) {
@@ -91,6 +107,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 4) k_el_rows(PtrList
   stages_smem<C, L, NL, ES, 256, PV, false, NS - 2, 0>(buf, tw);
   stage_io<C, L, 0, NL, 256, PV, false>(
       tw, [&](int l, int e) { return buf[e * ES + l]; }, [&](int l, int e, C v) { buf[e * ES + l] = v; });
+  if constexpr (PF) fz::cp_async_wait_all();
   __syncthreads();
 
   // ---- polarisation: element e of row r holds voxels 2e and 2e+1
@@ -101,10 +118,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 4) k_el_rows(PtrList
     R g[6], x0[6], x1[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) g[m] = buf[e * ES + m * NR + r].x;
-    elx_voxel<R, ORTHO>(E, cfac, g, pphi + id, n3, x0, err);
+    const R* pp = PF ? pbuf + r * (2 * L) + 2 * e : pphi + id;
+    const int64_t ps = PF ? (int64_t)NR * 2 * L : n3;
+    elx_voxel<R, ORTHO>(E, cfac, g, pp, ps, x0, err);
 #pragma unroll
     for (int m = 0; m < 6; ++m) g[m] = buf[e * ES + m * NR + r].y;
-    elx_voxel<R, ORTHO>(E, cfac, g, pphi + id + 1, n3, x1, err);
+    elx_voxel<R, ORTHO>(E, cfac, g, pp + 1, ps, x1, err);
 #pragma unroll
     for (int m = 0; m < 6; ++m) buf[e * ES + m * NR + r] = mk((R)x0[m], (R)x1[m]);
   }
@@ -150,12 +169,13 @@ void el_rows_launch(const FFT3& f, const PtrList<cplx<R>>& sp, const R* pphi, co
                     double cfac, int* err, cudaStream_t st) {
   using C = cplx<R>;
   const int64_t nrows = (int64_t)f.ny * f.nz, n3 = f.n3();
+  const bool pf = E.nvar <= EL_ROWS_PF_VAR;
   auto go = [&](auto Lc, auto Pc, auto Oc) {
     constexpr int L = decltype(Lc)::value, PV = decltype(Pc)::value;
     constexpr bool O = decltype(Oc)::value;
     constexpr int NR = el_rows_per_block(L);
-    auto fn = k_el_rows<R, L, PV, O>;
-    const size_t sm = (size_t)(6 * NR + 1) * L * sizeof(C);
+    auto fn = pf ? k_el_rows<R, L, PV, O, true> : k_el_rows<R, L, PV, O, false>;
+    const size_t sm = (size_t)(6 * NR + 1) * L * sizeof(C) + (pf ? (size_t)E.nvar * NR * 2 * L * sizeof(R) : 0);
     if (sm > 48 * 1024) {
       static thread_local std::vector<const void*> done;
       bool have = false;
