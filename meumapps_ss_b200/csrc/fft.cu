@@ -509,6 +509,12 @@ struct HookScope {
 
 template <typename R>
 void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const {
+  forward_x<R>(in, out, nf, st);
+  forward_cols<R>(out, nf, st);
+}
+
+template <typename R>
+void FFT3::forward_x(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const {
   using C = cplx<R>;
   const int Lx = px.L;
   const int64_t nrows = (int64_t)ny * nz;
@@ -520,72 +526,74 @@ void FFT3::forward(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int 
   if (!rows_s<R>(true, Lx, pv, nf, nrows, &in, &out, px.tw, post_tw, st))
     k_rows_r2c<R><<<g, 256, sm, st>>>(in, out, nx, nrows, px, (const C*)post_tw); }
   MEU_CHECK_LAUNCH();
-  forward_cols<R>(out, nf, st);
 }
 
 template <typename R>
 void FFT3::forward_cols(const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const {
+  pass_y<R>(out, nf, true, st);
+  pass_z<R>(out, nf, true, st);
+}
+
+// y columns: outer = z, inner = nxh
+template <typename R>
+void FFT3::pass_y(const PtrList<cplx<R>>& buf, int nf, bool fwd, cudaStream_t st) const {
   using C = cplx<R>;
-  // y columns: outer = z, inner = nxh
-  {
-    int tm = col_tile(ny, sizeof(R) == 8);
-    size_t s2 = (size_t)ny * tm * sizeof(C);
-    set_smem<R>((const void*)k_cols<R, true>, s2);
-    dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
-    { HookScope hs_(hook, "fft_y_fwd", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, true>(ny, pv, ct, nf, nz, nxh, (int64_t)ny * nxh, out, py.tw, (R)1, st))
-    k_cols<R, true><<<g2, 256, s2, st>>>(out, out, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
-    MEU_CHECK_LAUNCH();
+  const int tm = col_tile(ny, sizeof(R) == 8);
+  const size_t s2 = (size_t)ny * tm * sizeof(C);
+  const dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
+  HookScope hs_(hook, fwd ? "fft_y_fwd" : "fft_y_inv", 2.0 * nf * nk() * sizeof(C), st);
+  if (fwd) {
+    if (!cols_s<R, true>(ny, pv, ct, nf, nz, nxh, (int64_t)ny * nxh, buf, py.tw, (R)1, st)) {
+      set_smem<R>((const void*)k_cols<R, true>, s2);
+      k_cols<R, true><<<g2, 256, s2, st>>>(buf, buf, nxh, (int64_t)ny * nxh, tm, py, (R)1);
+    }
+  } else {
+    if (!cols_s<R, false>(ny, pv, ct, nf, nz, nxh, (int64_t)ny * nxh, buf, py.tw, (R)1, st)) {
+      set_smem<R>((const void*)k_cols<R, false>, s2);
+      k_cols<R, false><<<g2, 256, s2, st>>>(buf, buf, nxh, (int64_t)ny * nxh, tm, py, (R)1);
+    }
   }
-  // z columns: outer = 1, inner = ny*nxh
-  {
-    int tm = col_tile(nz, sizeof(R) == 8);
-    size_t s3 = (size_t)nz * tm * sizeof(C);
-    set_smem<R>((const void*)k_cols<R, true>, s3);
-    int inner = ny * nxh;
-    dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
-    { HookScope hs_(hook, "fft_z_fwd", 2.0 * nf * nk() * sizeof(C), st);
-  const R scale = (R)(1.0 / ((double)nx * ny * nz));
-  if (!cols_s<R, true>(nz, pv, ct, nf, 1, inner, 0, out, pz.tw, scale, st))
-    k_cols<R, true><<<g3, 256, s3, st>>>(out, out, inner, 0, tm, pz, scale); }
-    MEU_CHECK_LAUNCH();
+  MEU_CHECK_LAUNCH();
+}
+
+// z columns: outer = 1, inner = ny*nxh; the forward pass applies the 1/(Nx Ny Nz) scale
+template <typename R>
+void FFT3::pass_z(const PtrList<cplx<R>>& buf, int nf, bool fwd, cudaStream_t st) const {
+  using C = cplx<R>;
+  const int tm = col_tile(nz, sizeof(R) == 8);
+  const size_t s3 = (size_t)nz * tm * sizeof(C);
+  const int inner = ny * nxh;
+  const dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
+  HookScope hs_(hook, fwd ? "fft_z_fwd" : "fft_z_inv", 2.0 * nf * nk() * sizeof(C), st);
+  if (fwd) {
+    const R scale = (R)(1.0 / ((double)nx * ny * nz));
+    if (!cols_s<R, true>(nz, pv, ct, nf, 1, inner, 0, buf, pz.tw, scale, st)) {
+      set_smem<R>((const void*)k_cols<R, true>, s3);
+      k_cols<R, true><<<g3, 256, s3, st>>>(buf, buf, inner, 0, tm, pz, scale);
+    }
+  } else {
+    if (!cols_s<R, false>(nz, pv, ct, nf, 1, inner, 0, buf, pz.tw, (R)1, st)) {
+      set_smem<R>((const void*)k_cols<R, false>, s3);
+      k_cols<R, false><<<g3, 256, s3, st>>>(buf, buf, inner, 0, tm, pz, (R)1);
+    }
   }
+  MEU_CHECK_LAUNCH();
 }
 
 template <typename R>
 void FFT3::inverse(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const {
   inverse_cols<R>(in, nf, st);
-  inverse_rows<R>(in, out, nf, st);
+  inverse_x<R>(in, out, nf, st);
 }
 
 template <typename R>
 void FFT3::inverse_cols(const PtrList<cplx<R>>& in, int nf, cudaStream_t st) const {
-  using C = cplx<R>;
-  {
-    int tm = col_tile(nz, sizeof(R) == 8);
-    size_t s3 = (size_t)nz * tm * sizeof(C);
-    set_smem<R>((const void*)k_cols<R, false>, s3);
-    int inner = ny * nxh;
-    dim3 g3((unsigned)((inner + tm - 1) / tm), nf);
-    { HookScope hs_(hook, "fft_z_inv", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, false>(nz, pv, ct, nf, 1, inner, 0, in, pz.tw, (R)1, st))
-    k_cols<R, false><<<g3, 256, s3, st>>>(in, in, inner, 0, tm, pz, (R)1); }
-    MEU_CHECK_LAUNCH();
-  }
-  {
-    int tm = col_tile(ny, sizeof(R) == 8);
-    size_t s2 = (size_t)ny * tm * sizeof(C);
-    set_smem<R>((const void*)k_cols<R, false>, s2);
-    dim3 g2((unsigned)(nz * ((nxh + tm - 1) / tm)), nf);
-    { HookScope hs_(hook, "fft_y_inv", 2.0 * nf * nk() * sizeof(C), st);
-  if (!cols_s<R, false>(ny, pv, ct, nf, nz, nxh, (int64_t)ny * nxh, in, py.tw, (R)1, st))
-    k_cols<R, false><<<g2, 256, s2, st>>>(in, in, nxh, (int64_t)ny * nxh, tm, py, (R)1); }
-    MEU_CHECK_LAUNCH();
-  }
+  pass_z<R>(in, nf, false, st);
+  pass_y<R>(in, nf, false, st);
 }
 
 template <typename R>
-void FFT3::inverse_rows(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const {
+void FFT3::inverse_x(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const {
   using C = cplx<R>;
   const int Lx = px.L;
   const int64_t nrows = (int64_t)ny * nz;
@@ -609,5 +617,13 @@ template void FFT3::forward_cols<float>(const PtrList<float2>&, int, cudaStream_
 template void FFT3::forward_cols<double>(const PtrList<double2>&, int, cudaStream_t) const;
 template void FFT3::inverse_cols<float>(const PtrList<float2>&, int, cudaStream_t) const;
 template void FFT3::inverse_cols<double>(const PtrList<double2>&, int, cudaStream_t) const;
+template void FFT3::forward_x<float>(const PtrList<const float>&, const PtrList<float2>&, int, cudaStream_t) const;
+template void FFT3::forward_x<double>(const PtrList<const double>&, const PtrList<double2>&, int, cudaStream_t) const;
+template void FFT3::inverse_x<float>(const PtrList<float2>&, const PtrList<float>&, int, cudaStream_t) const;
+template void FFT3::inverse_x<double>(const PtrList<double2>&, const PtrList<double>&, int, cudaStream_t) const;
+template void FFT3::pass_y<float>(const PtrList<float2>&, int, bool, cudaStream_t) const;
+template void FFT3::pass_y<double>(const PtrList<double2>&, int, bool, cudaStream_t) const;
+template void FFT3::pass_z<float>(const PtrList<float2>&, int, bool, cudaStream_t) const;
+template void FFT3::pass_z<double>(const PtrList<double2>&, int, bool, cudaStream_t) const;
 
 }  // namespace meu

@@ -251,6 +251,16 @@ class FFT3 {
   void forward_cols(const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const;
   template <typename R>
   void inverse_cols(const PtrList<cplx<R>>& in, int nf, cudaStream_t st) const;
+  // single passes: x forward (real in, spectrum rows out), x inverse (spectrum rows
+  // in, used as scratch; real out), y and z in place
+  template <typename R>
+  void forward_x(const PtrList<const R>& in, const PtrList<cplx<R>>& out, int nf, cudaStream_t st) const;
+  template <typename R>
+  void inverse_x(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
+  template <typename R>
+  void pass_y(const PtrList<cplx<R>>& buf, int nf, bool fwd, cudaStream_t st) const;
+  template <typename R>
+  void pass_z(const PtrList<cplx<R>>& buf, int nf, bool fwd, cudaStream_t st) const;
 
   LinePlan px, py, pz;  // px: length nx/2 (complex half-length transform)
   // radix plan of the compile-time kernels (power-of-two lengths 32..512): 0 = radix 8
@@ -264,8 +274,6 @@ class FFT3 {
   bool fp64;
 
  private:
-  template <typename R>
-  void inverse_rows(const PtrList<cplx<R>>& in, const PtrList<R>& out, int nf, cudaStream_t st) const;
   void* dev_mem = nullptr;
   bool owns_mem = false;
 };
