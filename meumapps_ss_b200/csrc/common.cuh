@@ -6,6 +6,8 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace meu {
 
@@ -73,5 +75,27 @@ constexpr int MAXF = 32;
 template <typename T> struct PtrList {
   T* p[MAXF];
 };
+
+// Raise a kernel's dynamic shared-memory limit to the opt-in maximum (227 KB per block
+// on sm_100 minus the kernel's static shared memory), once per kernel and device, and
+// return that limit.  Raising it to the maximum (not to one launch's need) keeps every
+// later launch of the kernel valid whatever size it asks for.
+inline int smem_optin(const void* fn) {
+  static thread_local std::vector<std::pair<const void*, int>> done;  // (kernel, device)
+  int dev = 0;
+  MEU_CUDA(cudaGetDevice(&dev));
+  static thread_local std::vector<int> lims;
+  for (size_t i = 0; i < done.size(); ++i)
+    if (done[i].first == fn && done[i].second == dev) return lims[i];
+  int optin = 0;
+  MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  MEU_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const int lim = optin - (int)fa.sharedSizeBytes;
+  MEU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  done.push_back({fn, dev});
+  lims.push_back(lim);
+  return lim;
+}
 
 }  // namespace meu

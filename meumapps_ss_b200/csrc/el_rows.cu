@@ -21,13 +21,13 @@ constexpr int EL_ROWS_PF_VAR = 4;
 // polarisation of one voxel from its engineering strain g[6] (k_el_x_prop's formula,
 // in the field precision R: FP64 for the plain path, FP32 for the FP32-bulk path;
 // order parameters at pp[v * n3])
-template <typename R, bool ORTHO>
+template <typename R, bool ORTHO, int NVMAX = MEU_MAX_VAR>
 __device__ __forceinline__ void elx_voxel(const ElxCoef<R>& E, R cfac, const R* g, const R* pp, int64_t pstride, R* x,
                                           int* err) {
   const int V = E.nvar;
   R e0[6] = {0, 0, 0, 0, 0, 0}, psum = 0, sc = 0;
 #pragma unroll
-  for (int v = 0; v < MEU_MAX_VAR; ++v) {
+  for (int v = 0; v < NVMAX; ++v) {
     if (v >= V) break;
     const R q = pp[(int64_t)v * pstride];
     psum += E.inc[v] * q;
@@ -118,12 +118,26 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 4) k_el_rows(PtrList
     R g[6], x0[6], x1[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) g[m] = buf[e * ES + m * NR + r].x;
-    const R* pp = PF ? pbuf + r * (2 * L) + 2 * e : pphi + id;
-    const int64_t ps = PF ? (int64_t)NR * 2 * L : n3;
-    elx_voxel<R, ORTHO>(E, cfac, g, pp, ps, x0, err);
+    if constexpr (PF) {
+      // the pair's order parameters as one 2-element load per variant
+      R q0[EL_ROWS_PF_VAR], q1[EL_ROWS_PF_VAR];
+      const C* pq = (const C*)(pbuf + r * (2 * L)) + e;
 #pragma unroll
-    for (int m = 0; m < 6; ++m) g[m] = buf[e * ES + m * NR + r].y;
-    elx_voxel<R, ORTHO>(E, cfac, g, pp + 1, ps, x1, err);
+      for (int v = 0; v < EL_ROWS_PF_VAR; ++v) {
+        const C q = v < E.nvar ? pq[v * NR * L] : mk((R)0, (R)0);
+        q0[v] = q.x;
+        q1[v] = q.y;
+      }
+      elx_voxel<R, ORTHO, EL_ROWS_PF_VAR>(E, cfac, g, q0, 1, x0, err);
+#pragma unroll
+      for (int m = 0; m < 6; ++m) g[m] = buf[e * ES + m * NR + r].y;
+      elx_voxel<R, ORTHO, EL_ROWS_PF_VAR>(E, cfac, g, q1, 1, x1, err);
+    } else {
+      elx_voxel<R, ORTHO>(E, cfac, g, pphi + id, n3, x0, err);
+#pragma unroll
+      for (int m = 0; m < 6; ++m) g[m] = buf[e * ES + m * NR + r].y;
+      elx_voxel<R, ORTHO>(E, cfac, g, pphi + id + 1, n3, x1, err);
+    }
 #pragma unroll
     for (int m = 0; m < 6; ++m) buf[e * ES + m * NR + r] = mk((R)x0[m], (R)x1[m]);
   }
@@ -176,15 +190,8 @@ void el_rows_launch(const FFT3& f, const PtrList<cplx<R>>& sp, const R* pphi, co
     constexpr int NR = el_rows_per_block(L);
     auto fn = pf ? k_el_rows<R, L, PV, O, true> : k_el_rows<R, L, PV, O, false>;
     const size_t sm = (size_t)(6 * NR + 1) * L * sizeof(C) + (pf ? (size_t)E.nvar * NR * 2 * L * sizeof(R) : 0);
-    if (sm > 48 * 1024) {
-      static thread_local std::vector<const void*> done;
-      bool have = false;
-      for (const void* q : done) have = have || q == (const void*)fn;
-      if (!have) {
-        MEU_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        done.push_back((const void*)fn);
-      }
-    }
+    if (sm > 48 * 1024 && (int)sm > smem_optin((const void*)fn))
+      throw CudaError("fused elastic rows exceed shared memory", MEU_ERR_UNSUPPORTED);
     fn<<<(unsigned)((nrows + NR - 1) / NR), 256, sm, st>>>(sp, pphi, nrows, (const C*)f.px.tw, (const C*)f.post_tw, E,
                                                           n3, (R)cfac, err);
   };

@@ -402,8 +402,8 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       const int64_t ntiles = (n3 + PF_TILE - 1) / PF_TILE;
       // grid: the blocks that fit at once (each loops over tiles), at most one per tile
       auto fit = [&](const void* fn, size_t smem) {
-        if (smem > 48 * 1024)
-          MEU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (smem > 48 * 1024 && (int)smem > smem_optin(fn))
+          throw CudaError("elastic prefetch tiles exceed shared memory", MEU_ERR_UNSUPPORTED);
         int nb = 0;
         MEU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, PF_TILE, smem));
         return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(nb, 1) * sms, ntiles));

@@ -410,18 +410,7 @@ __global__ void __launch_bounds__(256) k_cols_s(PtrList<cplx<R>> in, PtrList<cpl
 template <typename R>
 static void set_smem(const void* fn, size_t bytes) {
   if (bytes <= 48 * 1024) return;
-  static thread_local std::vector<const void*> done;
-  for (const void* f : done)
-    if (f == fn) return;
-  int dev = 0, optin = 0;
-  MEU_CUDA(cudaGetDevice(&dev));
-  MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes fa;
-  MEU_CUDA(cudaFuncGetAttributes(&fa, fn));
-  const int lim = optin - (int)fa.sharedSizeBytes;
-  if ((int)bytes > lim) throw CudaError("transform tile exceeds shared memory", 103);
-  MEU_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  done.push_back(fn);
+  if ((int)bytes > smem_optin(fn)) throw CudaError("transform tile exceeds shared memory", 103);
 }
 
 // columns per block of the specialised column kernels: about 32 KB of tile

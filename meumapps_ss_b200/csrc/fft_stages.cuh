@@ -7,6 +7,7 @@
 
 namespace meu {
 
+
 // One radix stage over NL lines with caller-supplied element access: ld(line, e)
 // and st(line, e, v) address element e of a line in whatever memory the stage
 // reads or writes.  FWD: DIF butterfly then twiddle; else twiddle then DIT butterfly.
