@@ -1,6 +1,7 @@
 // el_rows.cu -- the x-direction work of one elastic fixed-point iteration in one
-// pass (proportional moduli, ModElastic.f:248-327 between the transforms of
-// ModElastic.f:330-345).  For a block of rows of the six strain spectra (after
+// pass (proportional moduli: the polarisation of ModElastic.f:248-327 between the
+// strain's inverse transforms, ModElastic.f:396-411, and the forward transforms of
+// x, ModElastic.f:329-334).  For a block of rows of the six strain spectra (after
 // their z and y inverse passes) the kernel runs the x C2R transform, forms the
 // polarisation x of every voxel pair from the strain and the order parameters,
 // and runs the x R2C transform of x back into the same spectral rows, which the
