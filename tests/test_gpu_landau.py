@@ -80,6 +80,29 @@ def test_landau_hetero_kernels_parity(oracle, ortho, pv, ct):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ny,nz", [(12, 9), (32, 48)])
+def test_landau_hetero_fused_rows_noncubic_parity(oracle, ny, nz):
+    """Fused elastic rows on non-cubic grids against the oracle in FP64: 12 x 9 = 108
+    rows leave a partial last block of rows; nz = 48 runs the run-time z plan."""
+    p, _, _ = active_landau(n=64, nvar=2, elastic=P.ELAST_HETERO, coupling=P.EIG_H, ppt_scale=1.5, el_tol=1e-8)
+    p.ny, p.nz = ny, nz
+    c, e = py_uniform(64, ny, nz, 2, -5, 0.8, 0.05, 0.5)
+    o = oracle.OracleSim(p)
+    o.set_fields(c, e)
+    do = o.run(4)
+    with Simulation(p) as g:
+        g.set_fields(c, e)
+        g.timing(True)
+        dg = g.run(4)
+        assert "el_rows" in g.timing_report()
+        cg, eg, elg, _ = g.get_fields()
+    co, eo, elo, _ = o.get_fields()
+    assert np.array_equal(do["el_iters"], dg["el_iters"])
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(eg - eo)) <= TOL
+    assert np.max(np.abs(elg - elo)) <= 1e-9 * np.max(np.abs(elo))
+
+
+@pytest.mark.gpu
 def test_landau_hetero_fp32_fused_rows():
     """FP32 heterogeneous step on 64^3, where each fixed-point iteration runs its x
     transforms and the polarisation as one kernel, against the FP64 step."""
