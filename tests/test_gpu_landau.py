@@ -103,6 +103,27 @@ def test_landau_hetero_fused_rows_noncubic_parity(oracle, ny, nz):
 
 
 @pytest.mark.gpu
+def test_landau_hetero_fused_rows_many_variants_parity(oracle):
+    """Six variants: more order parameters than the fused rows prefetch into shared
+    memory, so the polarisation reads them from global memory; FP64 against the oracle."""
+    p, c, e = active_landau(n=64, nvar=6, elastic=P.ELAST_HETERO, coupling=P.EIG_H, ppt_scale=1.5, el_tol=1e-8)
+    p.ny, p.nz = 16, 16
+    c, e = py_uniform(64, 16, 16, 6, -3, 0.8, 0.05, 0.5)
+    o = oracle.OracleSim(p)
+    o.set_fields(c, e)
+    do = o.run(3)
+    with Simulation(p) as g:
+        g.set_fields(c, e)
+        g.timing(True)
+        dg = g.run(3)
+        assert "el_rows" in g.timing_report()
+        cg, eg, _, _ = g.get_fields()
+    co, eo, _, _ = o.get_fields()
+    assert np.array_equal(do["el_iters"], dg["el_iters"])
+    assert np.max(np.abs(cg - co)) <= TOL and np.max(np.abs(eg - eo)) <= TOL
+
+
+@pytest.mark.gpu
 def test_landau_hetero_fp32_fused_rows():
     """FP32 heterogeneous step on 64^3, where each fixed-point iteration runs its x
     transforms and the polarisation as one kernel, against the FP64 step."""
