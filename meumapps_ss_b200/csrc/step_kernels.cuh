@@ -913,8 +913,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_stats(const DevConst* __restric
   const int64_t n3 = K.n3;
   const int V = K.p.nvar, E = K.p.numel;
   double cmin = 1.0, cmax = 0.0, pmax = 0.0, solid = 0.0, cs[MEU_MAX_EL] = {0, 0, 0};
+#pragma unroll 4
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
-    for (int e = 0; e < E; ++e) {
+#pragma unroll
+    for (int e = 0; e < MEU_MAX_EL; ++e) {
+      if (e >= E) break;
       const double v = (K.c_shift ? K.c_mean[e] : 0.0) + (double)c[(int64_t)e * n3 + id];
       cmin = fmin(cmin, v);
       cmax = fmax(cmax, v);
