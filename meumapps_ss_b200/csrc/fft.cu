@@ -264,8 +264,8 @@ __global__ void __launch_bounds__(256) k_cols(PtrList<cplx<R>> in, PtrList<cplx<
 // The same transforms with the length, radix plan and line count as template
 // constants (stage_io of fft_stages.cuh on the radix plans of fused.cuh): index
 // arithmetic folds to shifts and constant multiplies, and the digit reversal is
-// computed instead of read from the table.  Lengths 32..512 (powers of two) take these; other lengths keep the
-// run-time plan above.
+// computed instead of read from the table.  Lengths 32..512 (powers of two) take
+// these; other lengths keep the run-time plan above.
 constexpr int rows_per_block_c(int L) { return 2048 / L < 1 ? 1 : (2048 / L > 64 ? 64 : 2048 / L); }
 
 // Rows interleaved in shared memory: element e of row r at e * ES + r with the odd
