@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="override the grid edge (tests only)")
     ap.add_argument("--schedule", default="",
                     help="pv,threads,tile: fixed schedule of the fused step instead of the autotuner's (profiling)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the extra decks (0 and 2) measured beside the headline")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed FP32 steps (for ncu launch lists and captures)")
     return ap.parse_args()
@@ -127,12 +129,14 @@ def cpu_sample(cfg: int, n_override: int, budget_s: float, min_steps: int, threa
     import math
     from meumapps_ss_b200 import configs as CF
     from meumapps_ss_b200 import params as P
-    from meumapps_ss_b200 import _lib
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
 
     def deck(n):
+        # inputs from the oracle's own ran_2: the CPU legs load nothing of the product library
         w = CF.landau_config(cfg, n=n, precision=P.PREC_F64)
         p = w.params
-        c, e = _lib.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed, w.c0, w.c_amp, w.eta_amp)
+        c, e = O.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed, w.c0, w.c_amp, w.eta_amp)
         return w, p, c, e
 
     w0, p0, c0, e0 = deck(32)
@@ -201,6 +205,72 @@ def read_traffic(kernel: str):
                 except ValueError:
                     return None
     return None
+
+
+def elasticity_label(p) -> str:
+    from meumapps_ss_b200 import params as P
+    if p.elastic == P.ELAST_NONE:
+        return "none"
+    if p.elastic == P.ELAST_HOMOG:
+        return "homogeneous cubic 250/150/100, Green operator"
+    return (f"heterogeneous: precipitate moduli {p.cela[1][0] / p.cela[0][0]:g}x matrix, compliance mix, "
+            f"fixed-point iteration to residual <= {p.el_tol:g} (FP64 residual)")
+
+
+def measure_deck(cfg: int, stream, K: int, W: int, K64: int, local: int):
+    """One more deck beside the headline: FP32-bulk and FP64 throughput (CUDA events
+    around meu_run, graph capture and autotuning outside the timed region), the
+    FP32 error against FP64 after W + K steps, the clocks during the FP32 window."""
+    import numpy as np
+    import torch
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200.sim import Simulation
+
+    w = CF.landau_config(cfg, precision=P.PREC_F32)
+    p32 = w.params
+    p32.flags |= P.FLAG_AUTOTUNE
+    n3 = p32.nx * p32.ny * p32.nz
+    c0, e0 = _lib.init_uniform(p32.nx, p32.ny, p32.nz, p32.nvar, w.seed, w.c0, w.c_amp, w.eta_amp)
+    out = {"workload": w.name, "grid": [p32.nx, p32.ny, p32.nz], "variants": p32.nvar,
+           "elasticity": elasticity_label(p32), "dt": p32.dt}
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fields = {}
+    for prec, k in ((P.PREC_F32, K), (P.PREC_F64, K64)):
+        q = p32.copy()
+        q.precision = prec
+        sim = Simulation(q)
+        sim.set_stream(stream.cuda_stream)
+        sim.set_fields(c0, e0)
+        sim.run(W, diag=True)
+        sampler = ClockSampler(local)
+        torch.cuda.synchronize()
+        if prec == P.PREC_F32:
+            sampler.start()
+            time.sleep(0.3)
+        a.record(stream)
+        d = sim.run(k, diag=True)
+        b.record(stream)
+        stream.synchronize()
+        ms = a.elapsed_time(b)
+        key = "fp32_bulk" if prec == P.PREC_F32 else "fp64_plain"
+        out[key] = {"value": n3 * k / (ms / 1e3) / 1e6, "unit": UNIT, "steps": k, "ms_per_step": ms / k}
+        if p32.elastic == P.ELAST_HETERO:
+            out[key]["elastic_iterations_per_step"] = float(np.mean(d["el_iters"]))
+        if prec == P.PREC_F32:
+            out["clocks"] = sampler.stop()
+            out["schedule"] = sim.schedule
+        if k < K:
+            sim.run(K - k, diag=False)
+        fields[prec] = sim.get_fields()[:2]
+        sim.close()
+    (c32, e32), (c64, e64) = fields[P.PREC_F32], fields[P.PREC_F64]
+    out["fp32_speedup"] = out["fp32_bulk"]["value"] / out["fp64_plain"]["value"]
+    out["err_vs_fp64"] = {"c_rel_l2": float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64)),
+                          "eta_rel_l2": float(np.linalg.norm(e32 - e64) / max(np.linalg.norm(e64), 1e-300)),
+                          "after_steps": W + K}
+    return out
 
 
 def run_ours(args):
@@ -375,6 +445,12 @@ def run_ours(args):
         adj = measure_adjoint(stream, fd=False)
         adj.pop("kernels_ms", None)
 
+    # ---------------- the other single-grid decks, measured in the same run (rank 0, default workload)
+    decks = {}
+    if rank == 0 and not args.n and args.config == 1 and not args.no_extra:
+        decks["deck0"] = measure_deck(0, stream, K=200, W=W, K64=200, local=local)
+        decks["deck2"] = measure_deck(2, stream, K=10, W=W, K64=10, local=local)
+
     # ---------------- CPU baseline (rank 0, N = 1): the oracle port on host cores
     cpu = None
     if rank == 0 and world == 1:
@@ -395,7 +471,7 @@ def run_ours(args):
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": f"synthetic (ran_2 uniform noise c0={w.c0}+-{w.c_amp}, eta+-{w.eta_amp}, seed {w.seed})",
         "config": {"workload": w.name, "grid": [nx, ny, nz], "variants": V, "free_energy": "landau",
-                   "elasticity": "homogeneous cubic 250/150/100, Green operator", "dt": p32.dt,
+                   "elasticity": elasticity_label(p32), "dt": p32.dt,
                    "precision": "FP32 bulk; FP64 Omega(k), k=0 mode, reductions",
                    "l2": f"device working set {footprint / 2**20:.0f} MiB > {l2_mb} MB L2, no flush",
                    "schedule": schedule,
@@ -406,6 +482,7 @@ def run_ours(args):
         # t(forward + adjoint, recomputation included) / t(forward) - 1
         "adjoint_forward_cost": None if adj is None else adj["reverse_over_forward"],
         "adjoint": adj,
+        "decks": decks,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes_per_launch": dr["bytes"] / dr["launches"],
@@ -551,9 +628,13 @@ def run_adjoint_bench(args):
 ENS_MEMBERS = 96
 
 
-def ensemble_fields(w, rank: int = 0):
-    from meumapps_ss_b200 import _lib
+def ensemble_fields(w, rank: int = 0, oracle_rng: bool = False):
     p = w.params
+    if oracle_rng:  # CPU legs: the oracle's own ran_2 (same numbers, no product library)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        return O.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed - 1000 * rank, w.c0, w.c_amp, w.eta_amp)
+    from meumapps_ss_b200 import _lib
     return _lib.init_uniform(p.nx, p.ny, p.nz, p.nvar, w.seed - 1000 * rank, w.c0, w.c_amp, w.eta_amp)
 
 
@@ -565,7 +646,7 @@ def ensemble_cpu_sample(budget_s: float, threads: int):
     ws = CF.ensemble_config(ENS_MEMBERS, precision=P.PREC_F64)
     cells, secs, used = 0, 0.0, []
     for w in ws:
-        c, e = ensemble_fields(w)
+        c, e = ensemble_fields(w, oracle_rng=True)
         _, dt1 = oracle_throughput(w.params, c, e, 1, threads)
         steps = max(1, min(50, int((budget_s - secs) / max(dt1, 1e-6) * 0.5)))
         v, dt = oracle_throughput(w.params, c, e, steps, threads)

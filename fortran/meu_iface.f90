@@ -125,6 +125,23 @@ module meu_iface
       import :: c_int, c_ptr
       type(c_ptr), value :: e
     end function
+    ! one f_trans / inv_trans pair of host arrays (transform tests)
+    integer(c_int) function meu_fft_roundtrip(nx, ny, nz, precision, in, spec_out, back_out) &
+        bind(C, name="meu_fft_roundtrip")
+      import :: c_int, c_int32_t, c_ptr
+      integer(c_int32_t), value :: nx, ny, nz, precision
+      type(c_ptr), value :: in, spec_out, back_out
+    end function
+    ! the same pair on the caller's device arrays with no device allocation, e.g. the
+    ! c_loc of arrays inside "!$acc host_data use_device(...)".  The three arrays must
+    ! be 16-byte aligned for MEU_PREC_F64 (8-byte for MEU_PREC_F32): an array section
+    ! or an offset into a pool may not be; such calls return MEU_ERR_BADARG (100).
+    integer(c_int) function meu_fft_roundtrip_noalloc(nx, ny, nz, precision, in_dev, spec_dev, back_dev) &
+        bind(C, name="meu_fft_roundtrip_noalloc")
+      import :: c_int, c_int32_t, c_ptr
+      integer(c_int32_t), value :: nx, ny, nz, precision
+      type(c_ptr), value :: in_dev, spec_dev, back_dev
+    end function
   end interface
 
 contains

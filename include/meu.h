@@ -278,8 +278,10 @@ int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t precision, con
  * memory belongs to its OpenACC / managed-memory runtime, a framework whose
  * allocator has already reserved the GPU, or code that must not add the device
  * synchronisation of cudaMalloc/cudaFree.  in_dev, spec_dev and back_dev are
- * device-accessible arrays of the caller (device or managed memory): in_dev
- * holds Nx*Ny*Nz doubles, spec_dev receives 2*Nz*Ny*(Nx/2+1) doubles (the scaled
+ * device-accessible arrays of the caller (device or managed memory), each
+ * 16-byte aligned for MEU_PREC_F64 and 8-byte aligned for MEU_PREC_F32 (an
+ * array section or an offset into a pool may not be; misaligned arrays return
+ * MEU_ERR_BADARG before any work is issued): in_dev holds Nx*Ny*Nz doubles, spec_dev receives 2*Nz*Ny*(Nx/2+1) doubles (the scaled
  * half spectrum, re,im interleaved), back_dev the unscaled inverse (Nx*Ny*Nz
  * doubles).  The library's own working memory is a fixed static device array of
  * about 3.3 MB that every GPU loading the library keeps until exit, so the grid

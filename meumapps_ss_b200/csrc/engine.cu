@@ -873,9 +873,36 @@ void Engine<R>::fused_step_launches() {
 template <typename R>
 void Engine<R>::landau_step_fused() { fused_steps(1); }
 
+// Captures GRAPH_STEPS fused steps into gexec without running them.
+template <typename R>
+void Engine<R>::capture_graph() {
+  const int64_t l0 = prof.launches;
+  cudaGraph_t g = nullptr;
+  MEU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (int i = 0; i < GRAPH_STEPS; ++i) fused_step_launches();
+  } catch (...) {
+    cudaStreamEndCapture(st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  MEU_CUDA(cudaStreamEndCapture(st, &g));
+  const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    gexec = nullptr;
+    throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), MEU_ERR_CUDA);
+  }
+  graph_launches = prof.launches - l0;
+  prof.launches = l0;  // captured, not run
+}
+
 // n fused steps into history rows hist_n .. hist_n + n - 1 (d_row == hist_n on entry).
 // Runs of GRAPH_STEPS steps with one elastic state (homog flag) replay a CUDA
-// graph when the per-kernel timer is off and the stream can be captured.
+// graph when the per-kernel timer is off and the stream can be captured. The
+// graph is captured at the end of the first call that leaves the step able to
+// replay one, so a later call of any length only replays (capture and
+// instantiation stay out of the caller's next timed run).
 template <typename R>
 void Engine<R>::fused_steps(int n) {
   int done = 0;
@@ -886,27 +913,7 @@ void Engine<R>::fused_steps(int n) {
     const bool graphable = fused_warm && theta_ready && !prof.on && st != nullptr && n - done >= GRAPH_STEPS &&
                            homog_now == homog_later;
     if (graphable) {
-      if (!gexec) {
-        const int64_t l0 = prof.launches;
-        cudaGraph_t g = nullptr;
-        MEU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        try {
-          for (int i = 0; i < GRAPH_STEPS; ++i) fused_step_launches();
-        } catch (...) {
-          cudaStreamEndCapture(st, &g);
-          if (g) cudaGraphDestroy(g);
-          throw;
-        }
-        MEU_CUDA(cudaStreamEndCapture(st, &g));
-        const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-          gexec = nullptr;
-          throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), MEU_ERR_CUDA);
-        }
-        graph_launches = prof.launches - l0;
-        prof.launches = l0;  // captured, not run
-      }
+      if (!gexec) capture_graph();
       MEU_CUDA(cudaGraphLaunch(gexec, st));
       prof.launches += graph_launches;
       for (int i = 0; i < GRAPH_STEPS; ++i) {
@@ -926,6 +933,7 @@ void Engine<R>::fused_steps(int n) {
       done += 1;
     }
   }
+  if (!gexec && fused_warm && theta_ready && !prof.on && st != nullptr) capture_graph();
   last_iters = 0;
 }
 
@@ -1217,18 +1225,40 @@ int meu_destroy(meu_handle* h) {
 }  // extern "C"
 
 // ---------------------------------------------------------- diagnostics
+namespace {
+// device buffer freed when the call returns, on success and on every error path
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+}  // namespace
+
 extern "C" int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t precision, const double* in,
                                  double* spec_out, double* back_out) {
   using namespace meu;
   try {
-    if (!fft_size_ok(nx, true) || !fft_size_ok(ny, false) || !fft_size_ok(nz, false)) return MEU_ERR_UNSUPPORTED;
+    if (!in || !spec_out || !back_out) {
+      set_thread_error("meu_fft_roundtrip: NULL array");
+      return MEU_ERR_BADARG;
+    }
+    if (!fft_size_ok(nx, true) || !fft_size_ok(ny, false) || !fft_size_ok(nz, false)) {
+      set_thread_error("meu_fft_roundtrip: grid sizes must be 2^a 3^b with Nx even");
+      return MEU_ERR_UNSUPPORTED;
+    }
     const bool f64 = precision == MEU_PREC_F64;
+    if (!f64 && precision != MEU_PREC_F32) {
+      set_thread_error("meu_fft_roundtrip: unknown precision");
+      return MEU_ERR_BADARG;
+    }
     FFT3 f(nx, ny, nz, f64);
     const int64_t n3 = f.n3(), nk = f.nk();
-    double* d_in = nullptr;
-    double* d_spec = nullptr;
-    MEU_CUDA(cudaMalloc(&d_in, sizeof(double) * n3));
-    MEU_CUDA(cudaMalloc(&d_spec, sizeof(double) * 2 * nk));
+    DevBuf b_in, b_spec, b_fin, b_fsp;
+    MEU_CUDA(cudaMalloc(&b_in.p, sizeof(double) * n3));
+    MEU_CUDA(cudaMalloc(&b_spec.p, sizeof(double) * 2 * nk));
+    double* d_in = (double*)b_in.p;
+    double* d_spec = (double*)b_spec.p;
     MEU_CUDA(cudaMemcpy(d_in, in, sizeof(double) * n3, cudaMemcpyHostToDevice));
     cudaStream_t st = 0;
     if (f64) {
@@ -1245,17 +1275,19 @@ extern "C" int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t pre
       f.inverse<double>(c, d, 1, st);
       MEU_CUDA(cudaMemcpy(back_out, d_in, sizeof(double) * n3, cudaMemcpyDeviceToHost));
     } else {
-      float* fin = nullptr;
-      float2* fsp = nullptr;
-      MEU_CUDA(cudaMalloc(&fin, sizeof(float) * n3));
-      MEU_CUDA(cudaMalloc(&fsp, sizeof(float2) * nk));
+      MEU_CUDA(cudaMalloc(&b_fin.p, sizeof(float) * n3));
+      MEU_CUDA(cudaMalloc(&b_fsp.p, sizeof(float2) * nk));
+      float* fin = (float*)b_fin.p;
+      float2* fsp = (float2*)b_fsp.p;
       k_convert_in<float><<<grid_for(n3, 256), 256>>>(d_in, fin, n3);
+      MEU_CHECK_LAUNCH();
       PtrList<const float> a{};
       PtrList<float2> b{};
       a.p[0] = fin;
       b.p[0] = fsp;
       f.forward<float>(a, b, 1, st);
       k_convert<float><<<grid_for(2 * nk, 256), 256>>>((const float*)fsp, d_spec, 2 * nk);
+      MEU_CHECK_LAUNCH();
       MEU_CUDA(cudaMemcpy(spec_out, d_spec, sizeof(double) * 2 * nk, cudaMemcpyDeviceToHost));
       PtrList<float2> c{};
       PtrList<float> d{};
@@ -1263,15 +1295,19 @@ extern "C" int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t pre
       d.p[0] = fin;
       f.inverse<float>(c, d, 1, st);
       k_convert<float><<<grid_for(n3, 256), 256>>>(fin, d_in, n3);
+      MEU_CHECK_LAUNCH();
       MEU_CUDA(cudaMemcpy(back_out, d_in, sizeof(double) * n3, cudaMemcpyDeviceToHost));
-      cudaFree(fin);
-      cudaFree(fsp);
     }
-    cudaFree(d_in);
-    cudaFree(d_spec);
     MEU_CUDA(cudaDeviceSynchronize());
   } catch (const CudaError& e) {
+    set_thread_error(std::string("meu_fft_roundtrip: ") + e.what());
     return e.code;
+  } catch (const std::bad_alloc&) {
+    set_thread_error("meu_fft_roundtrip: host allocation failed");
+    return MEU_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    set_thread_error(std::string("meu_fft_roundtrip: ") + e.what());
+    return MEU_ERR_CUDA;
   }
   return MEU_OK;
 }

@@ -272,6 +272,7 @@ class Engine : public EngineBase {
   void sync_args();           // upload fused_args() into dA when it changed
   void fused_steps(int n);    // n fused steps (CUDA graphs of GRAPH_STEPS steps where possible)
   void fused_step_launches(); // launches of one fused step (stream or capture)
+  void capture_graph();       // GRAPH_STEPS fused steps into gexec, not run
   C *keta = nullptr, *kc = nullptr;  // spectral state of the Landau step
   // fused Landau path: schedule, device argument record, history row counter
   LanSched sched;

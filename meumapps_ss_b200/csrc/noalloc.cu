@@ -7,7 +7,10 @@
 // own device arrays, and the library's working memory (transform tables and the
 // working spectrum) comes from the fixed array below, which every GPU that loads
 // the library holds until the process exits.
+#include <cstdint>
 #include <mutex>
+#include <new>
+#include <stdexcept>
 #include <string>
 
 #include "../../include/meu.h"
@@ -74,6 +77,14 @@ extern "C" int meu_fft_roundtrip_noalloc(int32_t nx, int32_t ny, int32_t nz, int
       set_thread_error("meu_fft_roundtrip_noalloc: unknown precision");
       return MEU_ERR_BADARG;
     }
+    // FP64 transforms read and write the caller's arrays as 16-byte (re,im) pairs and
+    // 16-byte asynchronous copies; the FP32 path reads and writes single doubles
+    const uintptr_t align = f64 ? 16 : 8;
+    if ((((uintptr_t)in_dev | (uintptr_t)spec_dev | (uintptr_t)back_dev) & (align - 1)) != 0) {
+      set_thread_error(std::string("meu_fft_roundtrip_noalloc: in_dev, spec_dev and back_dev must be ") +
+                       (f64 ? "16-byte aligned in FP64" : "8-byte aligned in FP32"));
+      return MEU_ERR_BADARG;
+    }
     unsigned char* base = (unsigned char*)scratch_address();
     FFT3 f(nx, ny, nz, f64, base, kTableBytes);
     unsigned char* work = base + kTableBytes;
@@ -118,6 +129,12 @@ extern "C" int meu_fft_roundtrip_noalloc(int32_t nx, int32_t ny, int32_t nz, int
   } catch (const CudaError& e) {
     set_thread_error(e.what());
     return e.code;
+  } catch (const std::bad_alloc&) {
+    set_thread_error("meu_fft_roundtrip_noalloc: host allocation failed");
+    return MEU_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    set_thread_error(std::string("meu_fft_roundtrip_noalloc: ") + e.what());
+    return MEU_ERR_CUDA;
   }
   return MEU_OK;
 }

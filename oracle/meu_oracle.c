@@ -287,6 +287,18 @@ void orc_ran2_init(meu_ran2_state* s, int32_t iseed) {
   s->idum2 = 123456789; /* DATA idum2 /123456789/ */
 }
 
+/* Uniform-noise initial fields of the Landau decks: per voxel in Fortran
+ * order, c = c0 + c_amp*(2u-1), then eta_v = eta_amp*(2u-1) for v = 1..nvar,
+ * u from ran_2.  cons is (Nx,Ny,Nz); phi is phi(nvar,Nx,Ny,Nz), component fastest. */
+void orc_init_uniform(meu_ran2_state* s, int nx, int ny, int nz, int nvar, double c0, double c_amp, double eta_amp,
+                      double* cons, double* phi) {
+  const int64_t n3 = (int64_t)nx * ny * nz;
+  for (int64_t i = 0; i < n3; ++i) {
+    cons[i] = c0 + c_amp * (2.0 * orc_ran2(s) - 1.0);
+    for (int v = 0; v < nvar; ++v) phi[i * nvar + v] = eta_amp * (2.0 * orc_ran2(s) - 1.0);
+  }
+}
+
 /* langevin (ModFunc.f:77-100) */
 double orc_langevin(meu_ran2_state* s, double sd) {
   for (;;) {

@@ -54,6 +54,8 @@ def lib():
         L.orc_ran2_init.argtypes = [C.c_void_p, C.c_int32]
         L.orc_langevin.restype = C.c_double
         L.orc_langevin.argtypes = [C.c_void_p, C.c_double]
+        L.orc_init_uniform.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.c_double, dp, dp]
         _LIB = L
     return _LIB
 
@@ -109,6 +111,19 @@ class OracleRan2:
 
     def langevin(self, sd: float) -> float:
         return lib().orc_langevin(C.byref(self.s), float(sd))
+
+
+def init_uniform(nx: int, ny: int, nz: int, nvar: int, seed: int, c0: float, c_amp: float,
+                 eta_amp: float) -> Tuple[np.ndarray, np.ndarray]:
+    """Uniform-noise initial fields drawn with the oracle's own ran_2 (SoA float64:
+    (1,nz,ny,nx), (nvar,nz,ny,nx))."""
+    s = Ran2State()
+    lib().orc_ran2_init(C.byref(s), int(seed))
+    n3 = nx * ny * nz
+    cons = np.empty(n3)
+    phi = np.empty(n3 * nvar)
+    lib().orc_init_uniform(C.byref(s), nx, ny, nz, nvar, c0, c_amp, eta_amp, _dp(cons), _dp(phi))
+    return cons.reshape(1, nz, ny, nx), P.from_fortran(phi, nvar, nx, ny, nz)
 
 
 class OracleSim:

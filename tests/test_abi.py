@@ -57,3 +57,26 @@ def test_ensemble_bad_arguments():
     assert L.meu_ensemble_run(None, 1, None) == 100  # MEU_ERR_BADARG
     assert L.meu_ensemble_get_step(None) == -1
     assert L.meu_set_schedule(None, None) == 100  # MEU_ERR_BADARG
+
+
+def test_transform_entry_points_validate_before_any_gpu_work():
+    """Argument checks of the transform entry points run on the host before any
+    device call, so they answer without a GPU (and never launch on bad input)."""
+    import pytest
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("host-only argument checks; the addresses below are not device memory")
+    L = _lib.lib()
+    buf = (C.c_double * 8)()
+    assert L.meu_fft_roundtrip(16, 16, 16, 7, buf, buf, buf) == 100  # unknown precision
+    assert L.meu_fft_roundtrip(16, 16, 16, P.PREC_F64, None, buf, buf) == 100
+    assert L.meu_fft_roundtrip(14, 16, 16, P.PREC_F64, buf, buf, buf) == 103  # 7 is not 2^a 3^b
+    # FP64 needs 16-byte aligned arrays, FP32 8-byte: an address 8 past a 16-byte boundary
+    # is rejected in FP64; one 4 past an 8-byte boundary in FP32
+    a16, off8, off4 = C.c_void_p(0x10000), C.c_void_p(0x10008), C.c_void_p(0x10004)
+    assert L.meu_fft_roundtrip_noalloc(16, 16, 16, P.PREC_F64, off8, a16, a16) == 100
+    assert b"16-byte aligned" in L.meu_last_error(None)
+    assert L.meu_fft_roundtrip_noalloc(16, 16, 16, P.PREC_F64, a16, a16, off8) == 100
+    assert L.meu_fft_roundtrip_noalloc(16, 16, 16, P.PREC_F32, a16, off4, a16) == 100
+    assert b"8-byte aligned" in L.meu_last_error(None)
+    assert L.meu_fft_roundtrip_noalloc(16, 16, 16, 7, a16, a16, a16) == 100

@@ -36,6 +36,14 @@ def test_langevin_agrees(oracle):
     assert abs(np.std(vals) - 0.3) < 0.03
 
 
+def test_oracle_initialiser_matches_library(oracle):
+    # the CPU legs of the benchmark draw their inputs with the oracle's own ran_2
+    for args in ((16, 16, 16, 3, -7, 0.2, 0.01, 0.001), (12, 8, 6, 1, -1, 0.15, 0.01, 0.001)):
+        c1, e1 = _lib.init_uniform(*args)
+        c2, e2 = oracle.init_uniform(*args)
+        assert np.array_equal(c1, c2) and np.array_equal(e1, e2)
+
+
 def test_init_uniform_matches_python():
     from helpers import py_uniform
     c, e = _lib.init_uniform(6, 5, 4, 3, -7, 0.2, 0.01, 0.001)
