@@ -8,10 +8,17 @@
  * Parity status: UNPINNED by reference artefacts.  The reference ships no test,
  * golden vector or example input, and its Fortran/MPI/P3DFFT/LINPACK build cannot
  * be compiled here (no Fortran compiler, no P3DFFT/FFTW/LINPACK).  The oracle is
- * pinned instead against numpy.fft (transforms), analytic known answers (single
- * Fourier-mode decay, uniform fields, mass conservation, closed-form
- * homogeneous elasticity) and an independent numpy mirror of the step
- * (tests/test_oracle_*.py).
+ * pinned instead, on the CPU, by:
+ *   tests/test_oracle_fft.py  f_trans / inv_trans against numpy.fft (incl. the
+ *                             c2r convention) and invert with its condition flag;
+ *   tests/test_oracle_kat.py  single Fourier-mode decay (Landau eta and c, KKS c),
+ *                             uniform fields (uniformity and the k = 0 recurrence),
+ *                             mass conservation (Landau and KKS), Khachaturyan's
+ *                             closed-form elastic energy of a dilatational inclusion
+ *                             in a cubic medium, and a numpy restatement of one
+ *                             Landau step (1 to 3 variants, eta^2 and h(eta)
+ *                             coupling, with and without elasticity) to 1e-12;
+ *   tests/test_host.py        ran_2 / langevin against two other restatements.
  *
  * It follows the reference statement by statement:
  *   KKS step              Multi_MEUMAPPS.f:548-1106

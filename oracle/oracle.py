@@ -3,8 +3,10 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline / reference arm of bench.py.  Parity status: unpinned by
 reference artefacts (the reference ships none and its Fortran build is not
-compilable here); pinned against numpy.fft, analytic known answers and a
-numpy mirror of the step.
+compilable here).  Pinned on the CPU against numpy.fft (tests/test_oracle_fft.py),
+known answers -- single-mode decay, uniform fields, mass conservation,
+Khachaturyan's closed-form inclusion energy -- and a numpy restatement of one
+Landau step (tests/test_oracle_kat.py).
 """
 from __future__ import annotations
 
