@@ -247,6 +247,22 @@ double meu_langevin(meu_ran2_state* s, double sd);
 void meu_init_uniform(meu_ran2_state* s, int32_t nx, int32_t ny, int32_t nz, int32_t nvar,
                       double c0, double c_amp, double eta_amp, double* cons, double* phi);
 
+/* Fills *out from the ModGparams state after the set-up of
+ * Multi_MEUMAPPS.f:153-417 (the reference's module variables, in their Fortran
+ * layout and units: grad_coeff(3,3,vartot) already divided by del_N**2,
+ * trans_ppt(6,vartot), CEla/SEla(6,6,numph), Gparams(2*numel+1,numph) after the
+ * molar-volume division, Wellph(numph), Cmobs(numel), e_mean(6), Nvar(numph)).
+ * The C twin of meu_fill_params in fortran/meu_iface.f90, for drivers written in
+ * C or C++: KKS model, plain FP64, heterogeneous elasticity, the reference's
+ * iteration controls (4..10 iterations, 1e-7), clipping and energies on.
+ * Returns MEU_ERR_BADARG when a size exceeds the MEU_MAX_* limits or a pointer
+ * is NULL.  No GPU work. */
+int meu_params_from_gparams(int32_t nx, int32_t ny, int32_t nz, int32_t vartot, int32_t numel, int32_t numph,
+                            const int32_t* nvar_ph, int64_t step, int64_t elastep0, int64_t noise_step,
+                            double t_step, double b_mob, const double* cmobs, const double* e_mean,
+                            const double* grad_coeff, const double* trans_ppt, const double* cela,
+                            const double* sela, const double* gparams, const double* wellph, meu_params* out);
+
 /* Diagnostics. --------------------------------------------------------- */
 
 /* Launch the handle's work on a caller-owned CUDA stream (cudaStream_t passed

@@ -63,6 +63,9 @@ def lib():
     L.meu_langevin.argtypes = [C.POINTER(Ran2State), C.c_double]
     L.meu_langevin.restype = C.c_double
     L.meu_init_uniform.argtypes = [C.POINTER(Ran2State), i32, i32, i32, i32, C.c_double, C.c_double, C.c_double, dp, dp]
+    L.meu_params_from_gparams.argtypes = [i32, i32, i32, i32, i32, i32, C.POINTER(C.c_int32), i64, i64, i64,
+                                          C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp, dp,
+                                          C.POINTER(P.MeuParams)]
     L.meu_fft_roundtrip.argtypes = [i32, i32, i32, i32, dp, dp, dp]
     L.meu_fft_roundtrip_noalloc.argtypes = [i32, i32, i32, i32, vp, vp, vp]
     L.meu_set_stream.argtypes = [vp, vp]

@@ -134,6 +134,55 @@ __device__ __forceinline__ void dit_stage_s(C* buf, const C* __restrict__ tw) {
   }
 }
 
+// One butterfly of DIF / DIT stage S on R elements held in registers; j is the
+// butterfly's index within its span (the twiddle exponent base).  A task of
+// stage S over one line is u in [0, L/R): j = u % M, b = u / M, and its elements
+// sit at (b*SPAN + j) + r*M, r in [0, R).
+template <int L, int S, int PV>
+struct StageOf {
+  static constexpr int R = rplan(L, PV).r[S];
+  static constexpr int SPAN = span_of(L, S, PV);
+  static constexpr int M = SPAN / R;
+  static constexpr int TWS = L / SPAN;
+  static constexpr int TASKS = L / R;
+};
+template <typename C, int L, int S, int PV>
+__device__ __forceinline__ void dif_regs(C* x, const C* __restrict__ tw, int j) {
+  using T = StageOf<L, S, PV>;
+  Dft<T::R, -1, C>::run(x);
+  if (T::M > 1) {
+#pragma unroll
+    for (int q = 1; q < T::R; ++q) x[q] = Tw<C>::mul(x[q], tw, j * q * T::TWS, L);
+  }
+}
+template <typename C, int L, int S, int PV>
+__device__ __forceinline__ void dit_regs(C* x, const C* __restrict__ tw, int j) {
+  using T = StageOf<L, S, PV>;
+  if (T::M > 1) {
+#pragma unroll
+    for (int q = 1; q < T::R; ++q) x[q] = Tw<C>::mulc(x[q], tw, j * q * T::TWS, L);
+  }
+  Dft<T::R, 1, C>::run(x);
+}
+
+// DIF stages S0 .. S1-1 (shared memory, sync after each); DIT stages S1-1 down to S0.
+template <typename C, int L, int NL, int LS, int ES, int NT, int PV, int S, int S1>
+__device__ __forceinline__ void dif_range(C* buf, const C* tw) {
+  if constexpr (S < S1) {
+    dif_stage_s<C, L, S, NL, LS, ES, NT, PV>(buf, tw);
+    __syncthreads();
+    dif_range<C, L, NL, LS, ES, NT, PV, S + 1, S1>(buf, tw);
+  }
+}
+template <typename C, int L, int NL, int LS, int ES, int NT, int PV, int S0, int S>
+__device__ __forceinline__ void dit_range(C* buf, const C* tw) {
+  if constexpr (S >= S0) {
+    dit_stage_s<C, L, S, NL, LS, ES, NT, PV>(buf, tw);
+    __syncthreads();
+    dit_range<C, L, NL, LS, ES, NT, PV, S0, S - 1>(buf, tw);
+  }
+}
+
 // Forward DIF over all stages (natural -> digit reversed); syncs after each stage.
 template <typename C, int L, int NL, int LS, int ES, int NT, int PV, int S = 0>
 __device__ __forceinline__ void dif(C* buf, const C* tw) {
@@ -303,6 +352,163 @@ struct Plane {
     }
     __syncthreads();
     dit<C, LX, NY, PITCH, 1, NT, PV>(buf, twx);
+  }
+
+  // ---- streaming form: the plane's first inverse stage reads global memory, its last
+  // forward stage writes it, and the x transform's stage 0 of the inverse and of the
+  // forward run on one butterfly's registers with the caller's pointwise work in
+  // between (x_stage0), so a plane makes about half the shared-memory round trips
+  // of inverse() + pointwise pass + forward().
+  static constexpr int NSX = rplan(LX, PV).ns, NSY = rplan(NY, PV).ns;
+
+  // Inverse of an M-form plane in global memory (src) into shared memory, every
+  // stage except the x transform's stage 0.  Ends with a barrier.
+  static __device__ __forceinline__ void inverse_head(C* buf, const C* tws, const C* __restrict__ src) {
+    const C* twx = tws;
+    const C* twy = tws + LX * K;
+    const C* post = tws + (LX + NY) * K;
+    static_assert(NSY >= 2, "the streaming plane needs a y plan of two stages or more");
+    using SY = StageOf<NY, NSY - 1, PV>;  // first executed y stage (M = 1: no twiddles)
+    // columns 0 and LX (Hermitian in ky) are packed as X0 + i XN, so the y transform
+    // runs over LX columns; its column 0 then holds x0 + i xN, both real
+#pragma unroll 1
+    for (int t = threadIdx.x; t < LX * SY::TASKS; t += NT) {
+      const int c = t % LX, b = t / LX;
+      C x[SY::R];
+#pragma unroll
+      for (int q = 0; q < SY::R; ++q) {
+        const C* row = src + (b * SY::R + q) * NXH;
+        x[q] = row[c];
+        if (c == 0) {
+          const C xn = row[LX];
+          x[q] = mk(x[q].x - xn.y, x[q].y + xn.x);
+        }
+      }
+      Dft<SY::R, 1, C>::run(x);
+#pragma unroll
+      for (int q = 0; q < SY::R; ++q) buf[(b * SY::R + q) * PITCH + c] = x[q];
+    }
+    __syncthreads();
+    dit_range<C, NY, LX, 1, PITCH, NT, PV, 0, NSY - 2>(buf, twy);
+    constexpr int NP = LX / 2 + 1;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < NY * NP; i += NT) {
+      const int row = i % NY, k = i / NY;
+      C* rb = buf + row * PITCH;
+      const int pk = (k == 0) ? 0 : pos<LX, PV>(k);
+      const int pm = (k == 0) ? LX : pos<LX, PV>(LX - k);
+      C xk, xm;
+      if (k == 0) {
+        const C z = rb[0];
+        xk = mk(z.x, (R)0);
+        xm = mk(z.y, (R)0);
+      } else {
+        xk = rb[pk];
+        xm = rb[pm];
+      }
+      {
+        const C ex = cadd(xk, cconj(xm));
+        const C ox = Tw<C>::mulc(csub(xk, cconj(xm)), post, k, NXH);
+        rb[pk] = cadd(ex, mk(-ox.y, ox.x));
+      }
+      if (k != 0 && k != LX - k) {
+        const C ex = cadd(xm, cconj(xk));
+        const C ox = Tw<C>::mulc(csub(xm, cconj(xk)), post, LX - k, NXH);
+        rb[pm] = cadd(ex, mk(-ox.y, ox.x));
+      }
+    }
+    __syncthreads();
+    dit_range<C, LX, NY, PITCH, 1, NT, PV, 1, NSX - 1>(buf, twx);
+  }
+
+  // The x transform's stage 0 of the inverse on one butterfly's registers, then
+  // fn(y, n0, dn, x): x[r] holds the pair (x[2n], x[2n+1]) of row y at n = n0 + r*dn.
+  // With FWD the butterfly then runs the forward's stage 0 on what fn left in x and
+  // writes it back.  Ends with a barrier.
+  template <bool FWD, typename Fn>
+  static __device__ __forceinline__ void x_stage0(C* buf, const C* tws, Fn&& fn) {
+    using SX = StageOf<LX, 0, PV>;
+    const C* twx = tws;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < NY * SX::M; t += NT) {
+      const int j = t % SX::M, y = t / SX::M;
+      C* rb = buf + y * PITCH + j;
+      C x[SX::R];
+#pragma unroll
+      for (int q = 0; q < SX::R; ++q) x[q] = rb[q * SX::M];
+      dit_regs<C, LX, 0, PV>(x, twx, j);
+      fn(y, j, SX::M, x);
+      if constexpr (FWD) {
+        dif_regs<C, LX, 0, PV>(x, twx, j);
+#pragma unroll
+        for (int q = 0; q < SX::R; ++q) rb[q * SX::M] = x[q];
+      }
+    }
+    __syncthreads();
+  }
+
+  // Forward from rows whose x transform has run stage 0 (x_stage0<true>) to an M-form
+  // plane in global memory (dst).  buf is scratch afterwards.
+  static __device__ __forceinline__ void forward_tail(C* buf, const C* tws, C* __restrict__ dst) {
+    const C* twx = tws;
+    const C* twy = tws + LX * K;
+    const C* post = tws + (LX + NY) * K;
+    dif_range<C, LX, NY, PITCH, 1, NT, PV, 1, NSX>(buf, twx);
+    constexpr int NP = LX / 2 + 1;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < NY * NP; i += NT) {
+      const int row = i % NY, k = i / NY;
+      C* rb = buf + row * PITCH;
+      const int pk = pos<LX, PV>(k % LX), pm = pos<LX, PV>((LX - k) % LX);
+      const C zk = rb[pk], zm = rb[pm];
+      C e = cscale(cadd(zk, cconj(zm)), (R)0.5);
+      C o = cscale(csub(zk, cconj(zm)), (R)0.5);
+      o = mk(o.y, -o.x);
+      const C xk = cadd(e, Tw<C>::mul(o, post, k, NXH));
+      if (k == 0) {
+        rb[0] = mk(xk.x, csub(e, o).x);  // X[0] + i X[LX], both real
+      } else {
+        rb[pk] = xk;
+        if (k != LX - k) {
+          C e2 = cscale(cadd(zm, cconj(zk)), (R)0.5);
+          C o2 = cscale(csub(zm, cconj(zk)), (R)0.5);
+          o2 = mk(o2.y, -o2.x);
+          rb[pm] = cadd(e2, Tw<C>::mul(o2, post, LX - k, NXH));
+        }
+      }
+    }
+    __syncthreads();
+    dif_range<C, NY, LX, 1, PITCH, NT, PV, 0, NSY - 1>(buf, twy);
+    using SY = StageOf<NY, NSY - 1, PV>;  // last y stage (M = 1): straight to global memory
+#pragma unroll 1
+    for (int t = threadIdx.x; t < LX * SY::TASKS; t += NT) {
+      const int c = t % LX, b = t / LX;
+      C x[SY::R];
+#pragma unroll
+      for (int q = 0; q < SY::R; ++q) x[q] = buf[(b * SY::R + q) * PITCH + c];
+      Dft<SY::R, -1, C>::run(x);
+      if (c != 0) {
+#pragma unroll
+        for (int q = 0; q < SY::R; ++q) dst[(b * SY::R + q) * NXH + c] = x[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < SY::R; ++q) buf[(b * SY::R + q) * PITCH] = x[q];
+      }
+    }
+    __syncthreads();
+    // column 0 holds Z = Y0 + i YN: Y0(ky) = (Z(ky) + conj Z(-ky)) / 2 -> column 0,
+    // YN(ky) = -i (Z(ky) - conj Z(-ky)) / 2 -> column LX (rows in digit-reversed order)
+    for (int ky = threadIdx.x; ky <= NY / 2; ky += NT) {
+      const int p1 = pos<NY, PV>(ky), p2 = pos<NY, PV>((NY - ky) % NY);
+      const C z1 = buf[p1 * PITCH], z2 = buf[p2 * PITCH];
+      const C y0 = cscale(cadd(z1, cconj(z2)), (R)0.5);
+      const C d = cscale(csub(z1, cconj(z2)), (R)0.5);
+      const C yn = mk(d.y, -d.x);
+      dst[p1 * NXH] = y0;
+      dst[p1 * NXH + LX] = yn;
+      dst[p2 * NXH] = cconj(y0);
+      dst[p2 * NXH + LX] = cconj(yn);
+    }
   }
 
   // M-form plane <-> shared memory (rows of NXH complex, contiguous in both).

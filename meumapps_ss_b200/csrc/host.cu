@@ -75,4 +75,58 @@ void meu_init_uniform(meu_ran2_state* s, int32_t nx, int32_t ny, int32_t nz, int
   }
 }
 
+int meu_params_from_gparams(int32_t nx, int32_t ny, int32_t nz, int32_t vartot, int32_t numel, int32_t numph,
+                            const int32_t* nvar_ph, int64_t step, int64_t elastep0, int64_t noise_step,
+                            double t_step, double b_mob, const double* cmobs, const double* e_mean,
+                            const double* grad_coeff, const double* trans_ppt, const double* cela,
+                            const double* sela, const double* gparams, const double* wellph, meu_params* out) {
+  if (!out || !nvar_ph || !cmobs || !e_mean || !grad_coeff || !trans_ppt || !cela || !sela || !gparams || !wellph)
+    return MEU_ERR_BADARG;
+  if (vartot < 1 || vartot > MEU_MAX_VAR || numel < 1 || numel > MEU_MAX_EL || numph < 1 || numph > MEU_MAX_PH ||
+      nx < 1 || ny < 1 || nz < 1)
+    return MEU_ERR_BADARG;
+  meu_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.step = step;
+  p.elastep0 = elastep0;
+  p.noise_step = noise_step;
+  p.nx = nx;
+  p.ny = ny;
+  p.nz = nz;
+  p.model = MEU_MODEL_KKS;
+  p.precision = MEU_PREC_F64;
+  p.nvar = vartot;
+  p.numel = numel;
+  p.numph = numph;
+  for (int n = 0; n < numph; ++n) p.nvar_ph[n] = nvar_ph[n];
+  p.elastic = MEU_ELAST_HETERO;
+  p.el_min_iter = 4;   // ModElastic.f:469
+  p.el_max_iter = 10;  // ModElastic.f:462
+  p.clip_phi = 1;      // Multi_MEUMAPPS.f:1034-1035
+  p.diag_energy = 1;
+  p.dt = t_step;
+  p.b_mob = b_mob;
+  for (int e = 0; e < numel; ++e) p.cmobs[e] = cmobs[e];
+  p.el_tol = 1e-7;  // ModElastic.f:435
+  for (int i = 0; i < 6; ++i) p.e_mean[i] = e_mean[i];
+  // the Fortran arrays are column-major with the leading index fastest: element
+  // (i, j, v) of grad_coeff(3,3,vartot) sits at (i-1) + 3 (j-1) + 9 (v-1), which is
+  // the row-major [v][(j-1)*3 + (i-1)] of meu_params
+  for (int v = 0; v < vartot; ++v) {
+    for (int i = 0; i < 9; ++i) p.grad_coeff[v][i] = grad_coeff[9 * v + i];
+    for (int i = 0; i < 6; ++i) p.trans_ppt[v][i] = trans_ppt[6 * v + i];
+  }
+  const int ngp = 2 * numel + 1;
+  for (int n = 0; n < numph; ++n) {
+    for (int i = 0; i < 36; ++i) {
+      p.cela[n][i] = cela[36 * n + i];
+      p.sela[n][i] = sela[36 * n + i];
+    }
+    for (int j = 0; j < ngp; ++j) p.gparams[n][j] = gparams[ngp * n + j];
+    p.wellph[n] = wellph[n];
+  }
+  *out = p;
+  return MEU_OK;
+}
+
 }  // extern "C"

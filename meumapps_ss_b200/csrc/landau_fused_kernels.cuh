@@ -50,6 +50,22 @@ struct Damp {
   __device__ __forceinline__ W operator()(W x) const { return x * hi + x * lo; }
 };
 
+// 1/x for x >= 1 in FP64: a single-precision estimate refined by two Newton-Raphson
+// steps r <- r + r (1 - x r), each of which squares the relative error (2^-22 ->
+// 2^-44 -> below FP64 rounding).  Used for the semi-implicit factors 1/(1 + ...).
+__device__ __forceinline__ double recip_ge1(double x) {
+  double r = (double)__fdividef(1.0f, (float)x);
+  r = fma(r, fma(-x, r, 1.0), r);
+  r = fma(r, fma(-x, r, 1.0), r);
+  return r;
+}
+
+// one component of the k-vector a (m wrapped into (-N/2, N/2]); b = a except at Nyquist
+template <int N>
+__device__ __forceinline__ double kcomp(int m) {
+  return (double)((m <= N / 2) ? m : m - N) * (TWO_PI / (double)N);
+}
+
 template <typename R> constexpr int col_tile_default() { return sizeof(R) == 4 ? 16 : 8; }
 
 // Column tile of nf fields: smem [z][slot][TM] with LN complex per z row, global
@@ -137,23 +153,27 @@ __global__ void __launch_bounds__(NT) k_lf_z0(const LanFusedArgs<R>* __restrict_
 }
 
 // ------------------------------------------------------------------ Z1
+// z FFT of theta^_v (the first DIF stage straight from global memory), Green
+// operator and Cahn-Hilliard update of the dc^ state (read and written in global
+// memory by the k-space pass), z iFFT of phi^_v and dc^ (the last DIT stage
+// straight to global memory).
 template <typename R, int N, int V, int PV, int TM>
 __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
   const LanFusedArgs<R> a = A[blockIdx.z];
-  constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM;
+  constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM, LV = V * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  constexpr int NS = fz::rplan(N, PV).ns;
+  static_assert(NS >= 2, "the column kernels need a radix plan of two stages or more");
+  using S0 = fz::StageOf<N, 0, PV>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
-  C* ks = buf + N * LN;  // dc^ state tile [N][TM]
-  C* tw = ks + N * TM;
+  C* tw = buf + N * LN;
   // FP64 only for Omega(k) = Q^-1; every other k-space product in the field precision W
   using W = R;
   __shared__ double qc[6][6];
   __shared__ W sgW[V][6], epW[V][6], c0W[36], ebW[6];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
-  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
-  tile_load<C, N, TM>(ks, TM, 0, a.Kc, NK, PL, m0, 1);
   {
     const LanFusedConst& G = *a.F;
     for (int i = threadIdx.x; i < 36; i += NT) {
@@ -169,9 +189,20 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
   const double kapcd = a.F->kappa_c, dmd = a.F->dm;
   const W kapc = (W)kapcd, lan_a = (W)a.F->lan_a, hlb = (W)(0.5 * a.F->lan_b);
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  fz::cp_async_wait_all();
   __syncthreads();
-  fz::dif<C, N, V * TM, 1, LN, NT, PV>(buf, tw);
+#pragma unroll 1
+  for (int t = threadIdx.x; t < LV * S0::M; t += NT) {
+    const int line = t % LV, j = t / LV, f = line / TM, c = line - f * TM;
+    const C* src = a.M + f * NK + m0 + c;
+    C x[S0::R];
+#pragma unroll
+    for (int r = 0; r < S0::R; ++r) x[r] = src[(int64_t)(j + r * S0::M) * PL];
+    fz::dif_regs<C, N, 0, PV>(x, tw, j);
+#pragma unroll
+    for (int q = 0; q < S0::R; ++q) buf[(j + q * S0::M) * LN + line] = x[q];
+  }
+  __syncthreads();
+  fz::dif_range<C, N, LV, 1, LN, NT, PV, 1, NS>(buf, tw);
   const W s = (W)(1.0 / ((double)N * N * N));
   double fint = 0, elen = 0;
   for (int i = threadIdx.x; i < N * TM; i += NT) {
@@ -195,8 +226,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
 #pragma unroll
       for (int v = 0; v < V; ++v) a.rec_theta[v * NK + p * PL + m] = mk((R)tr[v], (R)ti[v]);
     }
-    C* kc = ks + p * TM + c;
-    const C cs = *kc;
+    const C cs = a.Kc[p * PL + m];
     const W cr = (W)cs.x, ci = (W)cs.y;
     const bool k0 = (kx == 0 && ky == 0 && kz == 0);
     if (a.energy) fint += (double)((W)0.5 * w * kapc * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci));
@@ -288,92 +318,72 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
       double ad[3], bd[3];
       kvec_n<N>(kx, ky, kz, ad, bd);
       const double k2d = ad[0] * ad[0] + ad[1] * ad[1] + ad[2] * ad[2];
-      const Damp<W> rden(1.0 / (1.0 + dmd * kapcd * k2d * k2d));
+      const Damp<W> rden(recip_ge1(1.0 + dmd * kapcd * k2d * k2d));
       const W dk2 = (W)(dmd * k2d);
       const W mr = lan_a * cr - hlb * str, mi = lan_a * ci - hlb * sti;
       nr = rden(cr - dk2 * mr);
       ni = rden(ci - dk2 * mi);
     }
     const C cn = mk((R)nr, (R)ni);
-    *kc = cn;
+    a.Kc_out[p * PL + m] = cn;
     e[V * TM] = cn;
   }
   __syncthreads();
-  tile_store<C, N, TM>(ks, TM, 0, a.Kc_out, NK, PL, m0, 1);
-  fz::dit<C, N, LN, 1, LN, NT, PV>(buf, tw);
-  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, NF);
+  fz::dit_range<C, N, LN, 1, LN, NT, PV, 1, NS - 1>(buf, tw);
+#pragma unroll 1
+  for (int t = threadIdx.x; t < LN * S0::M; t += NT) {
+    const int line = t % LN, j = t / LN, f = line / TM, c = line - f * TM;
+    C x[S0::R];
+#pragma unroll
+    for (int q = 0; q < S0::R; ++q) x[q] = buf[(j + q * S0::M) * LN + line];
+    fz::dit_regs<C, N, 0, PV>(x, tw, j);
+    C* dst = a.M + f * NK + m0 + c;
+#pragma unroll
+    for (int r = 0; r < S0::R; ++r) dst[(int64_t)(j + r * S0::M) * PL] = x[r];
+  }
   block_reduce_store(fint, 0, a.partials + LQ_FINT * PSTRIDE + blockIdx.x);
   block_reduce_store(elen, 0, a.partials + LQ_ELEN * PSTRIDE + blockIdx.x);
 }
 
 // ------------------------------------------------------------------ PB
-// Pointwise inputs (eta_0..V-1 and dc of this plane) either stream through a
-// two-deep cp.async pipeline of PB_CH-row chunks (the first two chunks load
-// during the inverse transform), or -- when that staging buffer is what keeps
-// the kernel below 3 blocks per SM -- are read straight from global memory
-// (mostly L2) by the pointwise loop.  Block (f, z): g_f of plane z -> forward transform.
-constexpr int PB_CH = 8;
+// Block (f, z): phi_f of plane z -> g_f -> forward transform.  The pointwise work
+// runs between the x transform's inverse and forward stage 0 on each butterfly's
+// registers (Plane::x_stage0); its inputs (eta_0..V-1 and dc of this plane) are
+// read straight from global memory (mostly L2).
 constexpr size_t SM_SMEM = 228 * 1024, BLOCK_RESERVED = 1024;
-
-template <typename R, int N, int V>
-constexpr bool pb_direct() {
-  constexpr size_t plane = fz::Plane<R, N, 512, 0>::smem_bytes();
-  constexpr size_t staged = plane + 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R);
-  return 3 * (staged + BLOCK_RESERVED) > SM_SMEM && 3 * (plane + BLOCK_RESERVED) <= SM_SMEM;
-}
 
 template <typename R, int N, int V, int PV, int NTP>
 constexpr size_t pb_smem() {
-  return fz::Plane<R, N, NTP, PV>::smem_bytes() + (pb_direct<R, N, V>() ? 0 : 2 * (size_t)(V + 1) * PB_CH * N * sizeof(R));
+  return fz::Plane<R, N, NTP, PV>::smem_bytes();
+}
+
+// resident blocks per SM the plane kernels are compiled for: as many as shared memory
+// allows, at most 768 threads (85 registers a thread at 256 threads, 64 at 512)
+template <typename R, int N, int PV, int NTP>
+constexpr int plane_min_blocks() {
+  constexpr size_t per = fz::Plane<R, N, NTP, PV>::smem_bytes() + BLOCK_RESERVED;
+  constexpr int by_smem = (int)(SM_SMEM / per);
+  constexpr int by_threads = NTP >= 512 ? 2 : 3;
+  return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
 }
 
 template <typename R, int N, int V, int PV, int NTP>
-__global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
+__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
+    k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
   using P = fz::Plane<R, N, NTP, PV>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
-  constexpr bool DIRECT = pb_direct<R, N, V>();
-  constexpr int CH = PB_CH, NCH = N / CH, CHR = CH * N, PER = 16 / sizeof(R);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
-  R* stg = (R*)(tws + P::TW_ELEMS);  // [2][V+1][CHR] (staged mode)
-  static_assert(((P::ELEMS + P::TW_ELEMS) * sizeof(C)) % 16 == 0, "16-byte copies into the staging area");
-  // field index fastest: the V+1 blocks of one plane, which read the same eta and
+  // field index fastest: the V blocks of one plane, which read the same eta and
   // dc planes, are resident together and share those reads through L2
   const int f = blockIdx.x, z = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  constexpr int NFI = V + 1;
-  auto issue = [&](int k) {
-    R* dst = stg + (k & 1) * NFI * CHR;
-#pragma unroll 1
-    for (int i = threadIdx.x; i < NFI * (CHR / PER); i += NTP) {
-      const int q = i / (CHR / PER), r = (i - q * (CHR / PER)) * PER;
-      const R* src = (q < V ? a.eta + q * N3 : a.c) + z * PL + (int64_t)k * CHR + r;
-      fz::cp_async16(dst + q * CHR + r, src);
-    }
-    fz::cp_async_commit();
-  };
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
-  P::load_m(buf, mp);
-  fz::cp_async_commit();
-  if constexpr (!DIRECT) {
-    issue(0);
-    issue(1);
-  }
   P::load_tw(tws, a.twx, a.twy, a.post);
-  if constexpr (DIRECT) fz::cp_async_wait_all();
-  else fz::cp_async_wait_group<2>();
   __syncthreads();
-  P::inverse(buf, tws);
-  if (a.rec_phi) {
-    R* dst = a.rec_phi + f * N3 + z * PL;
-#pragma unroll 1
-    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-      const int y = i / P::LX, n = i - y * P::LX;
-      ((C*)(dst + (int64_t)y * N))[n] = buf[y * P::PITCH + n];
-    }
-  }
+  P::inverse_head(buf, tws, mp);
   // constants of the driving force in registers; pointwise math in the field precision W
   using W = R;
   const LanFusedConst& F = *a.F;
@@ -434,62 +444,48 @@ __global__ void __launch_bounds__(NTP, pb_direct<R, N, V>() ? 3 : 1) k_lf_pb(con
     }
     return mk((R)out[0], (R)out[1]);
   };
-  if constexpr (DIRECT) {
-#pragma unroll 2
-    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-      const int y = i / P::LX, n = i - y * P::LX;
-      const int64_t g0 = z * PL + (int64_t)y * N + 2 * n;
+  R* rec = a.rec_phi ? a.rec_phi + f * N3 + z * PL : nullptr;
+  P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
+    const int64_t g0 = z * PL + (int64_t)y * N;
+#pragma unroll
+    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+      const int n = n0 + r * dn;
       C ev[V];
 #pragma unroll
-      for (int q = 0; q < V; ++q) ev[q] = *(const C*)(a.eta + q * N3 + g0);
-      const C dcv = *(const C*)(a.c + g0);
+      for (int q = 0; q < V; ++q) ev[q] = __ldg((const C*)(a.eta + q * N3 + g0) + n);
+      const C dcv = __ldg((const C*)(a.c + g0) + n);
+      if (rec) ((C*)(rec + (int64_t)y * N))[n] = x[r];
       if (bulk) bulk_energy(ev, dcv);
-      buf[y * P::PITCH + n] = point(ev, dcv, buf[y * P::PITCH + n]);
+      x[r] = point(ev, dcv, x[r]);
     }
-    __syncthreads();
-  } else {
-#pragma unroll 1
-    for (int k = 0; k < NCH; ++k) {
-      if (k + 1 < NCH) fz::cp_async_wait_group<1>();
-      else fz::cp_async_wait_group<0>();
-      __syncthreads();
-      const R* sb = stg + (k & 1) * NFI * CHR;
-#pragma unroll 1
-      for (int i = threadIdx.x; i < CH * P::LX; i += NTP) {
-        const int yl = i / P::LX, n = i - yl * P::LX, y = k * CH + yl;
-        C ev[V];
-#pragma unroll
-        for (int q = 0; q < V; ++q) ev[q] = ((const C*)(sb + q * CHR + yl * N))[n];
-        const C dcv = ((const C*)(sb + V * CHR + yl * N))[n];
-        if (bulk) bulk_energy(ev, dcv);
-        buf[y * P::PITCH + n] = point(ev, dcv, buf[y * P::PITCH + n]);
-      }
-      __syncthreads();
-      if (k + 2 < NCH) issue(k + 2);
-    }
-  }
+  });
   if (bulk) block_reduce_store(fch, 0, a.partials + LQ_FCH * PSTRIDE + z);
-  P::forward(buf, tws);
-  P::store_m(buf, mp);
+  P::forward_tail(buf, tws, mp);
 }
 
 // ------------------------------------------------------------------ Z2
+// z FFT of g_v, TDGL update of the eta^ state, z iFFT.  The first DIF stage takes
+// its butterflies straight from global memory and the last DIT stage (stage 0)
+// writes straight back; the last DIF stage, the state update and the first DIT
+// stage touch the same elements of one butterfly, so they run on its registers.
+// With a two-stage radix plan a column makes two shared-memory round trips.
 template <typename R, int N, int V, int PV, int TM>
 __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NXH = N / 2 + 1, LN = V * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  constexpr int NS = fz::rplan(N, PV).ns;
+  static_assert(NS >= 2, "the column kernels need a radix plan of two stages or more");
+  using S0 = fz::StageOf<N, 0, PV>;
+  using SL = fz::StageOf<N, NS - 1, PV>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;
-  C* ks = buf + N * LN;  // eta^ state tiles [N][V][TM]
-  C* tw = ks + N * LN;
+  C* buf = (C*)smraw;  // [N][V][TM]
+  C* tw = buf + N * LN;
   using W = R;  // working precision of the update (the state's)
   __shared__ double g[V][9];
   __shared__ int sameg;  // every variant has the gradient coefficients of variant 0
   const int64_t m0 = (int64_t)blockIdx.x * TM;
-  tile_load<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
-  tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
   if (threadIdx.x == 0) {
     int same = 1;
     for (int v = 0; v < V; ++v)
@@ -499,58 +495,80 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
       }
     sameg = same;
   }
-  const double dtld = a.F->dtl;
-  const W dtl = (W)dtld;
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
-  fz::cp_async_wait_all();
   __syncthreads();
-  fz::dif<C, N, LN, 1, LN, NT, PV>(buf, tw);
-  const W ds = dtl * (W)(1.0 / ((double)N * N * N));
+  // DIF stage 0: butterflies from global memory (column-fastest: coalesced rows)
+#pragma unroll 1
+  for (int t = threadIdx.x; t < LN * S0::M; t += NT) {
+    const int line = t % LN, j = t / LN, f = line / TM, c = line - f * TM;
+    const C* src = a.M + f * NK + m0 + c;
+    C x[S0::R];
+#pragma unroll
+    for (int r = 0; r < S0::R; ++r) x[r] = src[(int64_t)(j + r * S0::M) * PL];
+    fz::dif_regs<C, N, 0, PV>(x, tw, j);
+#pragma unroll
+    for (int q = 0; q < S0::R; ++q) buf[(j + q * S0::M) * LN + line] = x[q];
+  }
+  __syncthreads();
+  fz::dif_range<C, N, LN, 1, LN, NT, PV, 1, NS - 1>(buf, tw);
+  const double dtld = a.F->dtl;
+  const W ds = (W)dtld * (W)(1.0 / ((double)N * N * N));
   const bool one_g = sameg != 0;
   double fint = 0;
-  auto kappa_b = [&](const double* gv, const double* b) {
-    return gv[0] * b[0] * b[0] + gv[4] * b[1] * b[1] + gv[8] * b[2] * b[2] + (gv[3] + gv[1]) * b[0] * b[1] +
-           (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-  };
-  auto kappa_k = [&](const double* gv, const double* av, const double* b) {
-    return gv[0] * av[0] * av[0] + gv[4] * av[1] * av[1] + gv[8] * av[2] * av[2] + (gv[3] + gv[1]) * b[0] * b[1] +
-           (gv[7] + gv[5]) * b[1] * b[2] + (gv[2] + gv[6]) * b[2] * b[0];
-  };
-  for (int i = threadIdx.x; i < N * TM; i += NT) {
-    const int p = i / TM, c = i - p * TM;
+  // last DIF stage + update + first DIT stage on one butterfly (M = 1: no twiddles)
+#pragma unroll 1
+  for (int t = threadIdx.x; t < LN * SL::TASKS; t += NT) {
+    const int line = t % LN, b = t / LN, f = line / TM, c = line - f * TM;
     const int64_t m = m0 + c;
     const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
-    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
-    double av[3], b[3];
-    kvec_n<N>(kx, ky, kz, av, b);
+    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py);
+    const double* gv = one_g ? g[0] : g[f];
+    const double ax = kcomp<N>(kx), ay = kcomp<N>(ky);
+    const double bx = 2 * kx == N ? 0.0 : ax, by = 2 * ky == N ? 0.0 : ay;
+    // k.kappa.k = Kc + (terms in kz): constant part of this column
+    const double kk0 = gv[0] * ax * ax + gv[4] * ay * ay + (gv[3] + gv[1]) * bx * by;
+    const double kb0 = gv[0] * bx * bx + gv[4] * by * by + (gv[3] + gv[1]) * bx * by;
+    const double kz1 = (gv[7] + gv[5]) * by + (gv[2] + gv[6]) * bx;  // times bz
     const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
-    C* e = buf + p * LN + c;
-    W kb0 = 0;
-    double rd0 = 0;
-    if (one_g) {
-      if (a.energy) kb0 = (W)kappa_b(g[0], b);
-      rd0 = 1.0 / (1.0 + dtld * kappa_k(g[0], av, b));
-    }
+    C x[SL::R];
+#pragma unroll
+    for (int q = 0; q < SL::R; ++q) x[q] = buf[(b * SL::R + q) * LN + line];
+    Dft<SL::R, -1, C>::run(x);
+    const C* kst = a.Keta + f * NK + m;
+    C* kout = a.Keta_out + f * NK + m;
     W fk = 0;
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-      C* kst = ks + p * LN + v * TM + c;
-      const C st = *kst;
+    for (int q = 0; q < SL::R; ++q) {
+      const int p = b * SL::R + q;
+      const int kz = fz::rev<N, PV>(p);
+      const double az = kcomp<N>(kz), bz = 2 * kz == N ? 0.0 : az;
+      const C st = kst[(int64_t)p * PL];
       const W hr = (W)st.x, hi = (W)st.y;
-      if (a.energy) fk += (one_g ? kb0 : (W)kappa_b(g[v], b)) * (hr * hr + hi * hi);
-      const Damp<W> rden(one_g ? rd0 : 1.0 / (1.0 + dtld * kappa_k(g[v], av, b)));
-      const W nr = rden(hr - ds * (W)e[v * TM].x);
-      const W ni = rden(hi - ds * (W)e[v * TM].y);
-      const C o = mk((R)nr, (R)ni);
-      *kst = o;
-      e[v * TM] = o;
+      if (a.energy) fk += (W)(kb0 + gv[8] * bz * bz + kz1 * bz) * (hr * hr + hi * hi);
+      const Damp<W> rden(recip_ge1(1.0 + dtld * (kk0 + gv[8] * az * az + kz1 * bz)));
+      const C o = mk((R)rden(hr - ds * (W)x[q].x), (R)rden(hi - ds * (W)x[q].y));
+      kout[(int64_t)p * PL] = o;
+      x[q] = o;
     }
+    Dft<SL::R, 1, C>::run(x);
+#pragma unroll
+    for (int q = 0; q < SL::R; ++q) buf[(b * SL::R + q) * LN + line] = x[q];
     if (a.energy) fint += (double)((W)0.5 * w * fk);
   }
   __syncthreads();
-  tile_store<C, N, TM>(ks, LN, 0, a.Keta_out, NK, PL, m0, V);
-  fz::dit<C, N, LN, 1, LN, NT, PV>(buf, tw);
-  tile_store<C, N, TM>(buf, LN, 0, a.M, NK, PL, m0, V);
+  fz::dit_range<C, N, LN, 1, LN, NT, PV, 1, NS - 2>(buf, tw);
+  // DIT stage 0: butterflies straight to global memory
+#pragma unroll 1
+  for (int t = threadIdx.x; t < LN * S0::M; t += NT) {
+    const int line = t % LN, j = t / LN, f = line / TM, c = line - f * TM;
+    C x[S0::R];
+#pragma unroll
+    for (int q = 0; q < S0::R; ++q) x[q] = buf[(j + q * S0::M) * LN + line];
+    fz::dit_regs<C, N, 0, PV>(x, tw, j);
+    C* dst = a.M + f * NK + m0 + c;
+#pragma unroll
+    for (int r = 0; r < S0::R; ++r) dst[(int64_t)(j + r * S0::M) * PL] = x[r];
+  }
   block_reduce_store(fint, 0, a.partials + Q_FINT2 * PSTRIDE + blockIdx.x);
 }
 
@@ -558,7 +576,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
 // Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
 // -> real, concentration statistics.
 template <typename R, int N, int PV, int NTP>
-__global__ void __launch_bounds__(NTP, 3 * (fz::Plane<R, N, NTP, PV>::smem_bytes() + BLOCK_RESERVED) <= SM_SMEM ? 3 : 1)
+__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
     k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
   using P = fz::Plane<R, N, NTP, PV>;
   const LanFusedArgs<R> a = A[blockIdx.z];
@@ -568,28 +586,41 @@ __global__ void __launch_bounds__(NTP, 3 * (fz::Plane<R, N, NTP, PV>::smem_bytes
   C* tws = buf + P::ELEMS;
   const int z = blockIdx.x, f = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
-  P::load_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+  C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_all();
   __syncthreads();
-  P::inverse(buf, tws);
+  P::inverse_head(buf, tws, mp);
   R* dst = (f < V) ? a.eta_next + f * N3 + z * PL : a.c_next + z * PL;
   double emax = 0.0, s2 = 0.0, cmin = 1.0, cmax = 0.0, csum = 0.0;
   const double cbar = a.F->cbar;
-#pragma unroll 1
-  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-    const int y = i / P::LX, n = i - y * P::LX;
-    const C v = buf[y * P::PITCH + n];
-    ((C*)(dst + (int64_t)y * N))[n] = v;
-    if (f < V) {
-      emax = fmax(emax, fmax((double)v.x, (double)v.y));
-      s2 += (double)v.x * v.x + (double)v.y * v.y;
-    } else {
-      const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
-      cmin = fmin(cmin, fmin(c0, c1));
-      cmax = fmax(cmax, fmax(c0, c1));
-      csum += c0 + c1;
-    }
+  if (f < V) {
+    // new eta_f out, its statistics, and theta_f = eta_f^2 -> forward for the next
+    // step (which then starts at its column kernel)
+    P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
+      C* row = (C*)(dst + (int64_t)y * N);
+#pragma unroll
+      for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+        const C v = x[r];
+        row[n0 + r * dn] = v;
+        emax = fmax(emax, fmax((double)v.x, (double)v.y));
+        s2 += (double)v.x * v.x + (double)v.y * v.y;
+        x[r] = mk((R)((double)v.x * (double)v.x), (R)((double)v.y * (double)v.y));
+      }
+    });
+    P::forward_tail(buf, tws, mp);
+  } else {
+    P::template x_stage0<false>(buf, tws, [&](int y, int n0, int dn, C* x) {
+      C* row = (C*)(dst + (int64_t)y * N);
+#pragma unroll
+      for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+        const C v = x[r];
+        row[n0 + r * dn] = v;
+        const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
+        cmin = fmin(cmin, fmin(c0, c1));
+        cmax = fmax(cmax, fmax(c0, c1));
+        csum += c0 + c1;
+      }
+    });
   }
   const int blk = z * (V + 1) + f;
   block_reduce_store(emax, 1, a.partials + LQ_PHIMAX * PSTRIDE + blk);
@@ -597,20 +628,6 @@ __global__ void __launch_bounds__(NTP, 3 * (fz::Plane<R, N, NTP, PV>::smem_bytes
   block_reduce_store(cmin, 2, a.partials + LQ_CMIN * PSTRIDE + blk);
   block_reduce_store(cmax, 1, a.partials + LQ_CMAX * PSTRIDE + blk);
   block_reduce_store(csum, 0, a.partials + LQ_CSUM * PSTRIDE + blk);
-  if (f < V) {
-    // theta^_f of the next step from the new eta_f still in shared memory (the
-    // next step then starts at its column kernel)
-    __syncthreads();
-#pragma unroll 1
-    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-      const int y = i / P::LX, n = i - y * P::LX;
-      const C e = buf[y * P::PITCH + n];
-      buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
-    }
-    __syncthreads();
-    P::forward(buf, tws);
-    P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
-  }
   // ---- finalisation of the step: the member's last PI block reduces every block
   // partial of the step in a fixed order into history row *hist_row and advances it
   // (so graph replays need no host-side row index)
@@ -686,8 +703,8 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   const double mm = (double)members;
   const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
   const size_t sp = P::smem_bytes();
-  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + (size_t)N * TM + N * Tw<C>::K);
-  const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
+  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
+  const size_t s2 = sizeof(C) * ((size_t)N * V * TM + N * Tw<C>::K);
   const size_t spb = pb_smem<R, N, V, PV, NTP>();
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_pb<R, N, V, PV, NTP>, spb);

@@ -94,3 +94,36 @@ def test_fortran_layout_roundtrip():
     f = P.to_fortran(a)
     assert f[0] == a[0, 0, 0, 0] and f[1] == a[1, 0, 0, 0] and f[2] == a[0, 0, 0, 1]
     assert np.array_equal(P.from_fortran(f, 2, 5, 4, 3), a)
+
+
+@pytest.mark.parametrize("nvar,numel_in", [(1, 2), (3, 2), (3, 3)])
+def test_params_from_gparams_matches_host_setup(nvar, numel_in):
+    """The C fill of meu_params from the ModGparams arrays (Fortran layout) gives
+    the same block, byte for byte, as the host restatement of the set-up."""
+    deck = P.parse_input_txt(CF.kks_input_txt(16, nvar, 5, numel_in=numel_in))
+    ref = P.kks_params(deck)
+    V, E, NP = ref.nvar, ref.numel, ref.numph
+    f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))  # noqa: E731
+    grad = np.zeros((3, 3, V), order="F")
+    trans = np.zeros((6, V), order="F")
+    for v in range(V):
+        grad[:, :, v] = np.array(ref.grad_coeff[v][:]).reshape(3, 3, order="F")
+        trans[:, v] = ref.trans_ppt[v][:]
+    cela = np.zeros((6, 6, NP), order="F")
+    sela = np.zeros((6, 6, NP), order="F")
+    gpar = np.zeros((2 * E + 1, NP), order="F")
+    for n in range(NP):
+        cela[:, :, n] = ref.matrix("cela", n, 6)
+        sela[:, :, n] = ref.matrix("sela", n, 6)
+        gpar[:, n] = ref.gparams[n][:2 * E + 1]
+    arrays = [f([ref.cmobs[e] for e in range(E)]), f(ref.e_mean[:]), f(grad), f(trans), f(cela), f(sela), f(gpar),
+              f(ref.wellph[:NP])]
+    nv = (C.c_int32 * NP)(*[ref.nvar_ph[n] for n in range(NP)])
+    out = P.MeuParams()
+    st = _lib.lib().meu_params_from_gparams(ref.nx, ref.ny, ref.nz, V, E, NP, nv, ref.step, ref.elastep0,
+                                            ref.noise_step, ref.dt, ref.b_mob,
+                                            *[_lib.dptr(a) for a in arrays], C.byref(out))
+    assert st == 0
+    assert bytes(out) == bytes(ref)
+    assert _lib.lib().meu_params_from_gparams(16, 16, 16, 99, E, NP, nv, 1, 1, 0, 1.0, 1.0,
+                                              *[_lib.dptr(a) for a in arrays], C.byref(out)) == 100
