@@ -273,6 +273,49 @@ def measure_deck(cfg: int, stream, K: int, W: int, K64: int, local: int):
     return out
 
 
+def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
+    """The reference's own model (KKS, plain FP64, heterogeneous elasticity) on an n^3
+    deck in the reference's Input.txt format: Mcell-steps/s without noise and with the
+    Langevin noise of every step (ran_2 draws on a host thread, meu_run_noise)."""
+    import ctypes as C
+    import torch
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200 import _lib
+    from meumapps_ss_b200.sim import Simulation
+
+    deck = P.parse_input_txt(CF.kks_input_txt(n, nvar, 10 ** 6, radius=max(3, n // 10)))
+    p = P.kks_params(deck)
+    cons, phi = P.init_fields(deck)
+    n3 = n ** 3
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"workload": f"kks-{n}^3-{nvar}var-hetero", "grid": [n, n, n], "variants": nvar, "precision": "f64",
+           "elasticity": "heterogeneous cubic moduli, fixed point (ModElastic.f:241-481)",
+           "noise_draws_per_step": nvar * n3,
+           "noise_note": ("ran_2 is one serial chain: each step's vartot*N^3 langevin draws are made on one host "
+                          "thread, overlapped with the previous step on the GPU")}
+    for noisy in (False, True):
+        q = p.copy()
+        q.noise_step = q.step + 10 ** 6 if noisy else 0
+        with Simulation(q) as g:
+            g.set_stream(stream.cuda_stream)
+            g.set_fields(cons, phi)
+            st = _lib.Ran2State()
+            _lib.lib().meu_ran2_init(C.byref(st), -abs(deck.iseed) or -1)
+            run = (lambda k: g.run_noise(k, st, deck.sd)) if noisy else (lambda k: g.run(k))
+            run(W)
+            torch.cuda.synchronize()
+            a.record(stream)
+            d = run(K)
+            b.record(stream)
+            stream.synchronize()
+            ms = a.elapsed_time(b)
+        key = "noise_on" if noisy else "noise_off"
+        out[key] = {"value": n3 * K / (ms / 1e3) / 1e6, "unit": UNIT, "steps": K, "ms_per_step": ms / K,
+                    "elastic_iterations_per_step": float(sum(d["el_iters"]) / K)}
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -450,6 +493,7 @@ def run_ours(args):
     if rank == 0 and not args.n and args.config == 1 and not args.no_extra:
         decks["deck0"] = measure_deck(0, stream, K=200, W=W, K64=200, local=local)
         decks["deck2"] = measure_deck(2, stream, K=10, W=W, K64=10, local=local)
+        decks["kks"] = measure_kks(stream)
 
     # ---------------- CPU baseline (rank 0, N = 1): the oracle port on host cores
     cpu = None

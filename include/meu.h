@@ -132,6 +132,12 @@ typedef struct meu_diag {
   double cavg[MEU_MAX_EL];
 } meu_diag;
 
+/* State of the reference's ran_2 (ran_2.f:1-42), whose SAVE variables
+ * iv, iy, idum2 become explicit fields.  Initialise with meu_ran2_init. */
+typedef struct meu_ran2_state {
+  int32_t idum, idum2, iy, iv[32];
+} meu_ran2_state;
+
 typedef struct meu_handle meu_handle;
 
 /* Create a step engine on the current CUDA device.  Replaces the per-step
@@ -150,6 +156,15 @@ int meu_add_noise(meu_handle* h, const double* incr);
 
 /* Run nsteps time steps.  diag: NULL or nsteps rows. */
 int meu_run(meu_handle* h, int32_t nsteps, meu_diag* diag);
+
+/* meu_run with the reference's Langevin noise (Multi_MEUMAPPS.f:552-571): every
+ * step with step <= noise_step first adds vartot*Nx*Ny*Nz draws langevin(rng, sd)
+ * (ModFunc.f:77-100, ran_2.f) to phi_noise, in the reference's loop order
+ * (variant index fastest, then x, y, z) -- the same numbers as calling meu_langevin
+ * serially and passing them to meu_add_noise before each meu_run(h, 1, ..).  A host
+ * thread draws step s+1's increments while step s runs on the GPU; rng ends where
+ * the serial draws would leave it.  KKS model only (MEU_ERR_UNSUPPORTED otherwise). */
+int meu_run_noise(meu_handle* h, int32_t nsteps, meu_ran2_state* rng, double sd, meu_diag* diag);
 
 /* Download fields (any pointer may be NULL).  u_state as in meu_set_fields. */
 int meu_get_fields(meu_handle* h, double* cons, double* phi, double* el_en, double* u_state);
@@ -230,12 +245,7 @@ int meu_ensemble_destroy(meu_ensemble* e);
 
 /* Host-side helpers (no GPU work). ------------------------------------- */
 
-/* State of the reference's ran_2 (ran_2.f:1-42), whose SAVE variables
- * iv, iy, idum2 become explicit fields.  Initialise with meu_ran2_init. */
-typedef struct meu_ran2_state {
-  int32_t idum, idum2, iy, iv[32];
-} meu_ran2_state;
-
+/* ran_2 with the state meu_ran2_state (declared above). */
 void meu_ran2_init(meu_ran2_state* s, int32_t iseed);
 double meu_ran2(meu_ran2_state* s);
 /* langevin (ModFunc.f:77-100): one N(0,sd) draw by the polar method. */

@@ -51,6 +51,7 @@ def lib():
     L.meu_set_fields.argtypes = [vp, dp, dp, dp]
     L.meu_add_noise.argtypes = [vp, dp]
     L.meu_run.argtypes = [vp, i32, C.POINTER(P.MeuDiag)]
+    L.meu_run_noise.argtypes = [vp, i32, C.POINTER(Ran2State), C.c_double, C.POINTER(P.MeuDiag)]
     L.meu_get_fields.argtypes = [vp, dp, dp, dp, dp]
     L.meu_get_step.argtypes = [vp]
     L.meu_get_step.restype = i64

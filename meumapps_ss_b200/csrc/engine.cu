@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <memory>
 #include <string>
 #include <vector>
@@ -522,6 +523,10 @@ Engine<R>::~Engine() {
   for (void* q : allocs) cudaFree(q);
   if (h_results) cudaFreeHost(h_results);
   if (h_err) cudaFreeHost(h_err);
+  for (int b = 0; b < 2; ++b) {
+    if (noise_host[b]) cudaFreeHost(noise_host[b]);
+    if (noise_ev[b]) cudaEventDestroy(noise_ev[b]);
+  }
   fft.reset();
   if (own_st) cudaStreamDestroy(own_st);
 }
@@ -649,6 +654,65 @@ void Engine<R>::add_noise(const double* incr) {
     KLAUNCH("aos_to_soa", (double)nv * V * (8 + 2 * sizeof(R)), k_aos_to_soa<R><<<grid_for(nv * V, 256), 256, 0, st>>>(stage, noise, V, v0, nv, n3, 1, nullptr));
   }
   MEU_CUDA(cudaStreamSynchronize(st));
+}
+
+// phi_noise += one step's increments already in device memory (Fortran layout)
+template <typename R>
+void Engine<R>::upload_noise(const double* dev_incr) {
+  KLAUNCH("aos_to_soa", (double)n3 * V * (8 + 2 * sizeof(R)),
+          k_aos_to_soa<R><<<grid_for(n3 * V, 256), 256, 0, st>>>(dev_incr, noise, V, 0, n3, n3, 1, nullptr));
+}
+
+// The noise of Multi_MEUMAPPS.f:552-571: while step <= noise_step, every step first
+// adds V*n3 langevin draws (ran_2.f via ModFunc.f:77-100) to phi_noise, in the loop
+// order of the reference (variant index fastest, then x, y, z).  ran_2 is one serial
+// chain (each draw picks its shuffle-table slot from the previous one), so the draws
+// stay on the host; a host thread generates step s+1's increments into one pinned
+// buffer while step s runs, and each buffer goes up with one asynchronous copy.  The
+// caller's rng state ends exactly where the same number of serial draws leaves it.
+template <typename R>
+void Engine<R>::run_noise(int nsteps, meu_ran2_state* rng, double sd, meu_diag* diag) {
+  if (P.model != MEU_MODEL_KKS || !noise)
+    throw CudaError("run_noise: the Langevin noise belongs to the KKS model", MEU_ERR_UNSUPPORTED);
+  if (!rng) throw CudaError("run_noise: NULL ran_2 state", MEU_ERR_BADARG);
+  const int64_t cnt = (int64_t)V * n3;
+  int noisy = 0;  // the first `noisy` steps of the call draw noise (step <= noise_step)
+  while (noisy < nsteps && step + noisy <= P.noise_step) ++noisy;
+  if (noisy > 0 && !noise_dev) {
+    for (int b = 0; b < 2; ++b) {
+      void* hp = nullptr;
+      MEU_CUDA(cudaMallocHost(&hp, sizeof(double) * cnt));
+      noise_host[b] = (double*)hp;
+      MEU_CUDA(cudaEventCreateWithFlags(&noise_ev[b], cudaEventDisableTiming));
+    }
+    noise_dev = dalloc<double>(cnt);
+  }
+  auto generate = [rng, sd, cnt](double* dst, cudaEvent_t free_ev) {
+    cudaEventSynchronize(free_ev);  // the buffer's previous copy has run
+    for (int64_t i = 0; i < cnt; ++i) dst[i] = meu_langevin(rng, sd);
+  };
+  std::future<void> next;
+  if (noisy > 0) next = std::async(std::launch::async, generate, noise_host[0], noise_ev[0]);
+  int done = 0;
+  hist_n = 0;
+  while (done < nsteps) {
+    const int chunk = std::min(nsteps - done, HIST_MAX);
+    for (int i = 0; i < chunk; ++i) {
+      const int s = done + i;
+      if (s < noisy) {
+        const int b = s & 1;
+        next.get();
+        MEU_CUDA(cudaMemcpyAsync(noise_dev, noise_host[b], sizeof(double) * cnt, cudaMemcpyHostToDevice, st));
+        MEU_CUDA(cudaEventRecord(noise_ev[b], st));
+        upload_noise(noise_dev);
+        if (s + 1 < noisy) next = std::async(std::launch::async, generate, noise_host[b ^ 1], noise_ev[b ^ 1]);
+      }
+      kks_step(nullptr);
+    }
+    check_err();
+    flush_hist(diag ? diag + done : nullptr);
+    done += chunk;
+  }
 }
 
 template <typename R>
@@ -1130,6 +1194,12 @@ int meu_create(const meu_params* params, meu_handle** out) {
 int meu_set_fields(meu_handle* h, const double* cons, const double* phi, const double* u_state) {
   if (!h) return MEU_ERR_BADARG;
   MEU_TRY(h, h->eng->set_fields(cons, phi, u_state));
+  return MEU_OK;
+}
+
+int meu_run_noise(meu_handle* h, int32_t nsteps, meu_ran2_state* rng, double sd, meu_diag* diag) {
+  if (!h || nsteps < 0) return MEU_ERR_BADARG;
+  MEU_TRY(h, h->eng->run_noise(nsteps, rng, sd, diag));
   return MEU_OK;
 }
 

@@ -143,6 +143,9 @@ struct EngineBase {
   virtual void set_fields(const double* cons, const double* phi, const double* ustate) = 0;
   virtual void add_noise(const double* incr) = 0;
   virtual void run(int nsteps, meu_diag* diag) = 0;
+  // nsteps steps with the Langevin increments of the noisy steps drawn on a host
+  // thread from the caller's ran_2 state while the previous step runs
+  virtual void run_noise(int nsteps, meu_ran2_state* rng, double sd, meu_diag* diag) = 0;
   virtual void get_fields(double* cons, double* phi, double* el_en, double* ustate) = 0;
   virtual void set_stream(cudaStream_t s) = 0;
   virtual bool schedule(int32_t* out3) const = 0;
@@ -173,6 +176,7 @@ class Engine : public EngineBase {
   void set_fields(const double* cons, const double* phi, const double* ustate) override;
   void add_noise(const double* incr) override;
   void run(int nsteps, meu_diag* diag) override;
+  void run_noise(int nsteps, meu_ran2_state* rng, double sd, meu_diag* diag) override;
   void get_fields(double* cons, double* phi, double* el_en, double* ustate) override;
   void set_stream(cudaStream_t s) override { st = s ? s : own_st; }
   bool schedule(int32_t* out3) const override {
@@ -211,6 +215,12 @@ class Engine : public EngineBase {
   int* d_err = nullptr;
   int* h_err = nullptr;
   double* stage = nullptr;  // AoS staging (double)
+  // run_noise: two pinned host buffers of one step's increments (Fortran layout), their
+  // device copy, and the events that free a host buffer once its copy has run
+  double* noise_host[2] = {nullptr, nullptr};
+  double* noise_dev = nullptr;
+  cudaEvent_t noise_ev[2] = {nullptr, nullptr};
+  void upload_noise(const double* dev_incr);
   int64_t stage_elems = 0;
   std::vector<void*> allocs;
   // reference quirk state: values written on the next fort.98 line

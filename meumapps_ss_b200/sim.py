@@ -89,6 +89,15 @@ class Simulation:
             return None
         return P.diag_to_dict(list(rows)[:nsteps])
 
+    def run_noise(self, nsteps: int, rng, sd: float, diag: bool = True) -> Optional[Dict[str, np.ndarray]]:
+        """meu_run_noise: the steps with step <= noise_step draw their Langevin increments
+        from ``rng`` (a ``_lib.Ran2State``, advanced in place) on a host thread."""
+        rows = (P.MeuDiag * max(int(nsteps), 1))() if diag else None
+        self._check(lib().meu_run_noise(self.h, int(nsteps), C.byref(rng), float(sd), rows))
+        if not diag:
+            return None
+        return P.diag_to_dict(list(rows)[:nsteps])
+
     # -- instrumentation --
     def set_stream(self, stream_ptr: int) -> None:
         self._check(lib().meu_set_stream(self.h, C.c_void_p(int(stream_ptr)) if stream_ptr else None))

@@ -168,3 +168,37 @@ def test_kks_12_variants_fp32_against_fp64():
     rf = np.linalg.norm(f32 - f64) / np.linalg.norm(f64)
     print("kks12 fp32 rel", rc, rf)
     assert rc <= 1e-5 and rf <= 1e-4, (rc, rf)
+
+
+@pytest.mark.gpu
+def test_run_noise_matches_serial_draws(oracle):
+    """meu_run_noise (host thread drawing the next step's increments while a step runs)
+    against serial langevin draws passed to meu_add_noise before each single step: the
+    same fields bit for bit, the same final ran_2 state, and the oracle within 1e-10."""
+    import ctypes as C
+    from meumapps_ss_b200._lib import Ran2, Ran2State, dptr, lib
+    _, p, cons, phi = kks_case(n=16, nvar=3, steps=20)
+    p.noise_step = p.step + 4  # 5 noisy steps, then 3 without
+    sd, seed, steps = 2e-3, -23, 8
+    r1 = Ran2(seed)
+    o = oracle.OracleSim(p)
+    o.set_fields(cons, phi)
+    with Simulation(p) as g1, Simulation(p) as g2:
+        g1.set_fields(cons, phi)
+        g2.set_fields(cons, phi)
+        for s in range(steps):
+            if g1.step <= p.noise_step:
+                incr = np.array([r1.langevin(sd) for _ in range(phi.size)])  # Fortran order
+                assert lib().meu_add_noise(g1.h, dptr(incr)) == 0
+                o.add_noise(np.moveaxis(incr.reshape(phi.shape[1:] + (phi.shape[0],)), -1, 0))
+            g1.run(1)
+            o.run(1)
+        st = Ran2State()
+        lib().meu_ran2_init(C.byref(st), seed)
+        g2.run_noise(steps, st, sd)
+        c1, f1, _, _ = g1.get_fields()
+        c2, f2, _, _ = g2.get_fields()
+        assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
+        assert bytes(st) == bytes(r1.s)
+        co, fo, _, _ = o.get_fields()
+        assert np.max(np.abs(f2 - fo)) <= TOL and np.max(np.abs(c2 - co)) <= TOL
