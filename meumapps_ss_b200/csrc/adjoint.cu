@@ -102,7 +102,8 @@ struct AdjBuffers {
   std::vector<void*> allocs;
   int K = 0, nck = 0;
   std::vector<R*> ck_eta, ck_c, s_eta, s_c, s_phi;
-  std::vector<C*> ck_keta, ck_kc, s_keta, s_kc, s_theta;
+  std::vector<C*> ck_keta, ck_kc, ck_theta, s_keta, s_kc, s_theta;
+  std::vector<int> ck_has_theta;  // the checkpoint holds the forward's theta^ of its fields
   C *nu = nullptr, *lam_seed = nullptr, *M = nullptr;  // M: the adjoint's own M-form field (the
                                                        // recomputation uses the engine's)
   R *aw = nullptr, *lamT = nullptr, *nuT = nullptr, *lam0 = nullptr;
@@ -151,7 +152,9 @@ void Engine<R>::adjoint(int T, int K, const double* cons_tgt, const double* phi_
       b->ck_c.push_back(b->template alloc<R>(n3));
       b->ck_keta.push_back(b->template alloc<C>(nk));
       b->ck_kc.push_back(b->template alloc<C>(nk));
+      b->ck_theta.push_back(b->template alloc<C>(nk));  // V = 1: one M-form field
     }
+    b->ck_has_theta.assign(nck, 0);
     for (int j = 0; j <= K; ++j) {
       b->s_eta.push_back(b->template alloc<R>(n3));
       b->s_c.push_back(b->template alloc<R>(n3));
@@ -195,6 +198,10 @@ void Engine<R>::adjoint(int T, int K, const double* cons_tgt, const double* phi_
       MEU_CUDA(cudaMemcpyAsync(B.ck_c[s], c, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st));
       MEU_CUDA(cudaMemcpyAsync(B.ck_keta[s], keta, sizeof(C) * nk, cudaMemcpyDeviceToDevice, st));
       MEU_CUDA(cudaMemcpyAsync(B.ck_kc[s], kc, sizeof(C) * nk, cudaMemcpyDeviceToDevice, st));
+      // theta^ of these fields, as the previous forward step's PI wrote it: the recomputed
+      // segment then starts from the same numbers instead of transforming theta afresh
+      B.ck_has_theta[s] = theta_ready ? 1 : 0;
+      if (theta_ready) MEU_CUDA(cudaMemcpyAsync(B.ck_theta[s], sp, sizeof(C) * nk, cudaMemcpyDeviceToDevice, st));
     }
     const int hg = homog_at(step0 + i);
     if (hg != up_homog) {
@@ -249,9 +256,12 @@ void Engine<R>::adjoint(int T, int K, const double* cons_tgt, const double* phi_
       B.hRec[j] = r;
     }
     MEU_CUDA(cudaMemcpyAsync(B.dRec, B.hRec, sizeof(LanFusedArgs<R>) * S, cudaMemcpyHostToDevice, st));
-    // the segment starts from a checkpoint: its first step transforms theta itself
+    // the segment starts from a checkpoint with the forward's theta^ (or, at the very first
+    // step, transforms theta itself as the forward did), so it repeats the forward exactly
+    const bool ck_theta = B.ck_has_theta[seg] != 0;
+    if (ck_theta) MEU_CUDA(cudaMemcpyAsync(sp, B.ck_theta[seg], sizeof(C) * nk, cudaMemcpyDeviceToDevice, st));
     for (int j = 0; j < S; ++j)
-      if (!lan_fused_step<R>(N, 1, sched, B.dRec + j, 1, j ? LS_THETA_READY : 0, st, &prof, nb))
+      if (!lan_fused_step<R>(N, 1, sched, B.dRec + j, 1, (j || ck_theta) ? LS_THETA_READY : 0, st, &prof, nb))
         throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
     theta_ready = false;  // the engine's M now holds a recomputed step's theta^
     for (int m = S - 1; m >= 0; --m) {

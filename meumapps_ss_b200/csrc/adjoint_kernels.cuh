@@ -103,44 +103,43 @@ __global__ void __launch_bounds__(NTP) k_ad_b(AdjArgs<R> a) {
   const int z = blockIdx.x;
   constexpr int64_t PL = (int64_t)N * N;
   C* mp = a.M + z * (int64_t)N * P::NXH;
-  P::load_m(buf, mp);
   P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_all();
   __syncthreads();
-  P::inverse(buf, tws);
+  P::inverse_head(buf, tws, mp);
   const LanFusedConst& F = *a.F;
   const double dtl = F.dtl, cbar = F.cbar, s0 = F.sig0_ebar[0], A11 = F.A[0][0];
   double wg = 0, ea = 0;
   const int64_t off = z * PL;
-#pragma unroll 1
-  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-    const int y = i / P::LX, n = i - y * P::LX;
-    const int64_t g = off + (int64_t)y * N + 2 * n;
-    const C wv = buf[y * P::PITCH + n];
-    const C ev = *(const C*)(a.eta + g), cv = *(const C*)(a.c + g), pv = *(const C*)(a.phi + g);
-    const double w2[2] = {(double)wv.x, (double)wv.y}, e2v[2] = {(double)ev.x, (double)ev.y};
-    const double c2v[2] = {cbar + (double)cv.x, cbar + (double)cv.y}, p2v[2] = {(double)pv.x, (double)pv.y};
-    double ao[2], ho[2];
+  // pointwise adjoint between the x transform's inverse and forward stage 0
+  P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const double e = e2v[h], e2 = e * e, cc = c2v[h], ph = p2v[h], w = w2[h];
-      double G = F.lan_b * (F.lan_c2 - cc) * e - F.lan_c * e2 * e + F.lan_d * e2 * e2 * e;
-      double dG = F.lan_b * (F.lan_c2 - cc) - 3.0 * F.lan_c * e2 + 5.0 * F.lan_d * e2 * e2;
-      if (a.homog) {
-        G += -2.0 * e * (s0 + ph - A11 * e2);
-        dG += -2.0 * (s0 + ph) + 6.0 * A11 * e2;
-        ea += -dtl * w * (-2.0 * e * (s0 + 2.0 * ph - 2.0 * A11 * e2));
+    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+      const int n = n0 + r * dn;
+      const int64_t g = off + (int64_t)y * N + 2 * n;
+      const C wv = x[r];
+      const C ev = *(const C*)(a.eta + g), cv = *(const C*)(a.c + g), pv = *(const C*)(a.phi + g);
+      const double w2[2] = {(double)wv.x, (double)wv.y}, e2v[2] = {(double)ev.x, (double)ev.y};
+      const double c2v[2] = {cbar + (double)cv.x, cbar + (double)cv.y}, p2v[2] = {(double)pv.x, (double)pv.y};
+      double ao[2], ho[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double e = e2v[h], e2 = e * e, cc = c2v[h], ph = p2v[h], w = w2[h];
+        double G = F.lan_b * (F.lan_c2 - cc) * e - F.lan_c * e2 * e + F.lan_d * e2 * e2 * e;
+        double dG = F.lan_b * (F.lan_c2 - cc) - 3.0 * F.lan_c * e2 + 5.0 * F.lan_d * e2 * e2;
+        if (a.homog) {
+          G += -2.0 * e * (s0 + ph - A11 * e2);
+          dG += -2.0 * (s0 + ph) + 6.0 * A11 * e2;
+          ea += -dtl * w * (-2.0 * e * (s0 + 2.0 * ph - 2.0 * A11 * e2));
+        }
+        wg += w * G;
+        ao[h] = w * (1.0 - dtl * dG);
+        ho[h] = dtl * e * w;
       }
-      wg += w * G;
-      ao[h] = w * (1.0 - dtl * dG);
-      ho[h] = dtl * e * w;
+      *(C*)(a.aw + g) = mk((R)ao[0], (R)ao[1]);
+      x[r] = mk((R)ho[0], (R)ho[1]);
     }
-    *(C*)(a.aw + g) = mk((R)ao[0], (R)ao[1]);
-    buf[y * P::PITCH + n] = mk((R)ho[0], (R)ho[1]);
-  }
-  __syncthreads();
-  P::forward(buf, tws);
-  P::store_m(buf, mp);
+  });
+  P::forward_tail(buf, tws, mp);
   block_reduce_store(wg, 0, a.partials + AQ_WG * PSTRIDE + z);
   block_reduce_store(ea, 0, a.partials + AQ_EA * PSTRIDE + z);
 }
@@ -203,27 +202,32 @@ __global__ void __launch_bounds__(NTP) k_ad_d(AdjArgs<R> a) {
   const int z = blockIdx.x;
   constexpr int64_t PL = (int64_t)N * N;
   C* mp = a.M + z * (int64_t)N * P::NXH;
-  P::load_m(buf, mp);
   P::load_tw(tws, a.twx, a.twy, a.post);
-  fz::cp_async_wait_all();
   __syncthreads();
-  P::inverse(buf, tws);
+  P::inverse_head(buf, tws, mp);
   const int64_t off = z * PL;
-#pragma unroll 1
-  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-    const int y = i / P::LX, n = i - y * P::LX;
-    const int64_t g = off + (int64_t)y * N + 2 * n;
-    const C rv = buf[y * P::PITCH + n];
-    const C av = *(const C*)(a.aw + g), ev = *(const C*)(a.eta + g);
-    const C lam = mk((R)((double)av.x + 2.0 * (double)ev.x * (double)rv.x),
-                     (R)((double)av.y + 2.0 * (double)ev.y * (double)rv.y));
-    if (a.lam_out) *(C*)(a.lam_out + g) = lam;
-    else buf[y * P::PITCH + n] = lam;
+  auto lam = [&](int y, int n0, int dn, C* x) {
+#pragma unroll
+    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+      const int64_t g = off + (int64_t)y * N + 2 * (n0 + r * dn);
+      const C rv = x[r];
+      const C av = *(const C*)(a.aw + g), ev = *(const C*)(a.eta + g);
+      x[r] = mk((R)((double)av.x + 2.0 * (double)ev.x * (double)rv.x),
+                (R)((double)av.y + 2.0 * (double)ev.y * (double)rv.y));
+    }
+  };
+  if (a.lam_out) {
+    // lambda of the initial state: real space out, no forward transform
+    P::template x_stage0<false>(buf, tws, [&](int y, int n0, int dn, C* x) {
+      lam(y, n0, dn, x);
+#pragma unroll
+      for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r)
+        *(C*)(a.lam_out + off + (int64_t)y * N + 2 * (n0 + r * dn)) = x[r];
+    });
+    return;
   }
-  if (a.lam_out) return;
-  __syncthreads();
-  P::forward(buf, tws);
-  P::store_m(buf, mp);
+  P::template x_stage0<true>(buf, tws, lam);
+  P::forward_tail(buf, tws, mp);
 }
 
 }  // namespace adj

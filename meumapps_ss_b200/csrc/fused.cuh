@@ -447,6 +447,28 @@ struct Plane {
     __syncthreads();
   }
 
+  // Rows of (x[2n], x[2n+1]) already in shared memory (load_real): fn(y, n0, dn, x) on
+  // the butterfly's pairs, then the x transform's forward stage 0 on its registers --
+  // the same arithmetic as x_stage0<true> after its inverse stage.  Ends with a barrier.
+  template <typename Fn>
+  static __device__ __forceinline__ void x_forward0(C* buf, const C* tws, Fn&& fn) {
+    using SX = StageOf<LX, 0, PV>;
+    const C* twx = tws;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < NY * SX::M; t += NT) {
+      const int j = t % SX::M, y = t / SX::M;
+      C* rb = buf + y * PITCH + j;
+      C x[SX::R];
+#pragma unroll
+      for (int q = 0; q < SX::R; ++q) x[q] = rb[q * SX::M];
+      fn(y, j, SX::M, x);
+      dif_regs<C, LX, 0, PV>(x, twx, j);
+#pragma unroll
+      for (int q = 0; q < SX::R; ++q) rb[q * SX::M] = x[q];
+    }
+    __syncthreads();
+  }
+
   // Forward from rows whose x transform has run stage 0 (x_stage0<true>) to an M-form
   // plane in global memory (dst).  buf is scratch afterwards.
   static __device__ __forceinline__ void forward_tail(C* buf, const C* tws, C* __restrict__ dst) {

@@ -111,17 +111,17 @@ __global__ void __launch_bounds__(NTP) k_lf_pf(const LanFusedArgs<R>* __restrict
   P::load_tw(tws, a.twx, a.twy, a.post);
   fz::cp_async_wait_all();
   __syncthreads();
-  if (f < V && !raw) {
-    // theta_v = eta_v^2 in place
-    for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
-      const int y = i / P::LX, n = i - y * P::LX;
-      const C e = buf[y * P::PITCH + n];
-      buf[y * P::PITCH + n] = mk((R)((double)e.x * (double)e.x), (R)((double)e.y * (double)e.y));
+  // theta_v = eta_v^2 (raw: the fields themselves), then the same forward path as
+  // PI's theta transform, so a step after new fields sees bit-identical theta^
+  const bool square = f < V && !raw;
+  P::x_forward0(buf, tws, [&](int, int, int, C* x) {
+    if (square) {
+#pragma unroll
+      for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r)
+        x[r] = mk((R)((double)x[r].x * (double)x[r].x), (R)((double)x[r].y * (double)x[r].y));
     }
-    __syncthreads();
-  }
-  P::forward(buf, tws);
-  P::store_m(buf, a.M + f * NK + z * (int64_t)N * P::NXH);
+  });
+  P::forward_tail(buf, tws, a.M + f * NK + z * (int64_t)N * P::NXH);
 }
 
 // ------------------------------------------------------------------ Z0
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
   // FP64 only for Omega(k) = Q^-1; every other k-space product in the field precision W
   using W = R;
   __shared__ double qc[6][6];
-  __shared__ W sgW[V][6], epW[V][6], c0W[36], ebW[6];
+  __shared__ W sgW[V][6], epW[V][6], c0W[36], ebW[6], aW[V][V];
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   {
     const LanFusedConst& G = *a.F;
@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
       sgW[i / 6][i % 6] = (W)G.sig0[i / 6][i % 6];
       epW[i / 6][i % 6] = (W)G.eps_eng[i / 6][i % 6];
     }
+    for (int i = threadIdx.x; i < V * V; i += NT) aW[i / V][i % V] = (W)G.A[i / V][i % V];
     if (threadIdx.x < 6) ebW[threadIdx.x] = (W)G.ebar_eng[threadIdx.x];
   }
   const double kapcd = a.F->kappa_c, dmd = a.F->dm;
@@ -229,6 +230,9 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     const C cs = a.Kc[p * PL + m];
     const W cr = (W)cs.x, ci = (W)cs.y;
     const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+    const bool nyq = 2 * kx == N || 2 * ky == N || 2 * kz == N;
+    double ad[3], bd[3];
+    kvec_n<N>(kx, ky, kz, ad, bd);
     if (a.energy) fint += (double)((W)0.5 * w * kapc * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci));
     // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
     W ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
@@ -244,8 +248,6 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
       const W t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
       const W Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
       // Omega(k) in FP64 from the double k-vectors
-      double ad[3], bd[3];
-      kvec_n<N>(kx, ky, kz, ad, bd);
       const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
       double Qs[6];
 #pragma unroll
@@ -260,7 +262,11 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
       const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
       const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
       const double det = qa * i00 + qd * i01 + qe * i02;
-      if (det == 0.0) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
+      // the reference's rcond <= 1e-16 test (ModFunc.f:55-67) on the exact 1-norm
+      // condition number: ||Q|| ||adj Q|| >= 1e16 |det Q|
+      const double qn = fmax(fabs(qa) + fabs(qd) + fabs(qe), fmax(fabs(qd) + fabs(qb) + fabs(qf), fabs(qe) + fabs(qf) + fabs(qcc)));
+      const double an = fmax(fabs(i00) + fabs(i01) + fabs(i02), fmax(fabs(i01) + fabs(i11) + fabs(i12), fabs(i02) + fabs(i12) + fabs(i22)));
+      if (!(qn * an < 1e16 * fabs(det))) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
       const double rd = 1.0 / det;
       const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
                           {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
@@ -271,6 +277,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
         ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
       }
     }
+    W phr[V], phi_[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       W pr = 0, pi = 0;
@@ -284,9 +291,24 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
         pr = -di;
         pi = dr;
       }
+      phr[v] = pr;
+      phi_[v] = pi;
       e[v * TM] = mk((R)pr, (R)pi);
     }
-    if (a.homog && a.energy) {
+    if (a.homog && a.energy && !k0 && !nyq) {
+      // Khachaturyan's quadratic form: with equilibrium u^ and homogeneous C0,
+      // e*.C0.e = sum_pq A_pq Re(theta^_p* theta^_q) - sum_p Re(theta^_p* phi^_p),
+      // A_pq = eps0_p.C0.eps0_q.  It needs the strain's and Q(k)'s k-vectors to agree,
+      // which they do off the Nyquist planes (k_space zeroes b there but not a).
+      W qq = 0;
+#pragma unroll
+      for (int pv = 0; pv < V; ++pv) {
+        qq -= tr[pv] * phr[pv] + ti[pv] * phi_[pv];
+#pragma unroll
+        for (int qv = 0; qv < V; ++qv) qq += aW[pv][qv] * (tr[pv] * tr[qv] + ti[pv] * ti[qv]);
+      }
+      elen += (double)((W)0.5 * w * qq);
+    } else if (a.homog && a.energy) {
       // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
       const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
       W er[6], ei[6];
@@ -315,8 +337,6 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
     W nr = 0, ni = 0;
     if (!k0) {
-      double ad[3], bd[3];
-      kvec_n<N>(kx, ky, kz, ad, bd);
       const double k2d = ad[0] * ad[0] + ad[1] * ad[1] + ad[2] * ad[2];
       const Damp<W> rden(recip_ge1(1.0 + dmd * kapcd * k2d * k2d));
       const W dk2 = (W)(dmd * k2d);
