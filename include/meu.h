@@ -206,7 +206,8 @@ int meu_set_schedule(meu_handle* h, const int32_t* in3);
  *   dparams[4] = dJ/dalpha  (every eigenstrain scaled by alpha, at alpha = 1)
  *   dphi0      = dJ/deta_0 (layout as phi; may be NULL)
  * cons_target and phi_target hold c* and eta* (layouts as meu_set_fields).
- * Fused Landau handles with one order parameter on the default schedule only
+ * With several order parameters the loss sums (eta_v - eta_v*)^2 over them.
+ * Fused Landau handles with 1 to 4 order parameters on the default schedule only
  * (MEU_ERR_UNSUPPORTED otherwise).  The reference has no adjoint. */
 int meu_adjoint(meu_handle* h, int32_t nsteps, int32_t checkpoint_every, const double* cons_target,
                 const double* phi_target, double* loss, double* dparams, double* dphi0);

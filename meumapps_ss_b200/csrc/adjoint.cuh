@@ -1,6 +1,7 @@
-// adjoint.cuh -- hand-written adjoint of the fused Landau step for one order
-// parameter (V = 1), on the default schedule (radix plan 0, 512-thread planes,
-// default column tile).
+// adjoint.cuh -- hand-written adjoint of the fused Landau step, on the default
+// schedule (radix plan 0, 512-thread planes, default column tile).  The formulas
+// below are written for one order parameter; V variants (V >= 2, kernels *_v)
+// generalise them as set out after them.
 //
 // Forward step n (real fields eta, dc; spectra normalised, x = F^-1 x^):
 //   theta = eta^2
@@ -26,6 +27,22 @@
 //   B  plane:  xy iFFT of w -> a (real), h -> xy FFT (+ <w,G>, d/d(alpha) sums)
 //   C  column: z FFT of h -> nu^ update, r^ -> z iFFT
 //   D  plane:  xy iFFT of r -> lam_n = a + 2 eta r -> xy FFT (or lam_0 out)
+//
+// V variants (forward: theta_v = eta_v^2, phi_v = F^-1 [sum_q g_vq theta^_q] with the
+// symmetric g_vq(k) = -(sig0_v b)^T Q^-1 (sig0_q b), mu^ = A dc^ - (B/2) sum_v theta^_v,
+//   G_v = B(c2 - c) eta_v - C eta_v^3 + D eta_v^5 + 4 w eta_v sum_{q != v} eta_q^2
+//         - 2 eta_v (s0_v + phi_v - sum_q A_vq eta_q^2),   A_vq = eps0_v.C0.eps0_q,
+// H_v from variant v's gradient tensor):
+//   w_v = F^-1 [H_v lam^_v],  z_v = -dtL w_v,  h_v = -eta_v z_v
+//   a_u = w_u + sum_v z_v dG_v/deta_u, with
+//     dG_v/deta_v = B(c2 - c) - 3C eta_v^2 + 5D eta_v^4 + 4w sum_{q != v} eta_q^2
+//                   - 2 (s0_v + phi_v - sum_q A_vq eta_q^2) + 4 A_vv eta_v^2,
+//     dG_v/deta_u = 8 w eta_v eta_u + 4 A_vu eta_v eta_u   (u != v)
+//   r^_q = -2 (sig0_q b)^T Q^-1 sum_v (sig0_v b) h^_v + P dm k^2 (B/2) nu^_{n+1}
+//   lam_q = a_q + 2 eta_q r_q,   nu^_n = P (1 - dm A k^2) nu^_{n+1} + B sum_v h^_v
+// and the parameter sums add over the variants.  Six launches per adjoint step:
+//   EA_v column (V fields), B1_v plane (xy iFFT of w_v), B2_v pointwise (a_v, h_v, <w,G>,
+//   d/d(alpha)), B3_v plane (xy FFT of h_v), C_v column (V fields), D_v plane (per q).
 #pragma once
 #include "landau_fused_kernels.cuh"
 
@@ -44,7 +61,10 @@ struct AdjArgs {
   const R* eta;               // eta_n
   const R* c;                 // dc_n
   const R* phi;               // phi_n
-  R* aw;                      // a of the step (real scratch)
+  R* aw;                      // a of the step (real scratch; V fields)
+  R* wv;                      // w_v (V real fields; V >= 2 only)
+  R* hv;                      // h_v (V real fields; V >= 2 only)
+  int V;                      // variants
   R* lam_out;                 // lam_0 (last adjoint step), else NULL
   double* partials;           // [ADJ_Q][PSTRIDE]
   int homog;

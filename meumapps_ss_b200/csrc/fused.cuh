@@ -369,15 +369,19 @@ struct Plane {
     const C* post = tws + (LX + NY) * K;
     static_assert(NSY >= 2, "the streaming plane needs a y plan of two stages or more");
     using SY = StageOf<NY, NSY - 1, PV>;  // first executed y stage (M = 1: no twiddles)
-    // columns 0 and LX (Hermitian in ky) are packed as X0 + i XN, so the y transform
-    // runs over LX columns; its column 0 then holds x0 + i xN, both real
+    // the whole plane in flight at once (16-byte asynchronous copies), then the first
+    // stage in place; columns 0 and LX (Hermitian in ky) are packed as X0 + i XN, so the
+    // y transform runs over LX columns; its column 0 then holds x0 + i xN, both real
+    load_m(buf, src);
+    cp_async_wait_all();
+    __syncthreads();
 #pragma unroll 1
     for (int t = threadIdx.x; t < LX * SY::TASKS; t += NT) {
       const int c = t % LX, b = t / LX;
       C x[SY::R];
 #pragma unroll
       for (int q = 0; q < SY::R; ++q) {
-        const C* row = src + (b * SY::R + q) * NXH;
+        const C* row = buf + (b * SY::R + q) * PITCH;
         x[q] = row[c];
         if (c == 0) {
           const C xn = row[LX];
@@ -421,6 +425,25 @@ struct Plane {
     dit_range<C, LX, NY, PITCH, 1, NT, PV, 1, NSX - 1>(buf, twx);
   }
 
+  // Task t of the x transform's stage 0 -> (row y, butterfly j in [0, M)).  A shared-
+  // memory wavefront serves G = 128 B / sizeof(C) lanes; the pitch is odd, so the lanes'
+  // banks are distinct when (y + j) mod G is.  When M divides G (M < G), a group of G
+  // lanes takes rows spaced by M (y = y0 + h + M i) and all M butterflies of each, which
+  // also gives every row M consecutive pairs in global memory (full 32-byte sectors for
+  // the pointwise loads and stores); otherwise butterflies run fastest within a row.
+  static __device__ __forceinline__ void x_task(int t, int& y, int& j) {
+    constexpr int M = StageOf<LX, 0, PV>::M, G = 128 / (int)sizeof(C);
+    if constexpr (M >= G || G % M != 0) {
+      j = t % M;
+      y = t / M;
+    } else {
+      static_assert(NY % G == 0, "rows in groups of G");
+      const int grp = t / (G * M), rem = t - grp * (G * M), h = rem / G, l = rem - h * G;
+      j = l % M;
+      y = grp * G + h + M * (l / M);
+    }
+  }
+
   // The x transform's stage 0 of the inverse on one butterfly's registers, then
   // fn(y, n0, dn, x): x[r] holds the pair (x[2n], x[2n+1]) of row y at n = n0 + r*dn.
   // With FWD the butterfly then runs the forward's stage 0 on what fn left in x and
@@ -431,7 +454,8 @@ struct Plane {
     const C* twx = tws;
 #pragma unroll 1
     for (int t = threadIdx.x; t < NY * SX::M; t += NT) {
-      const int j = t % SX::M, y = t / SX::M;
+      int y, j;
+      x_task(t, y, j);
       C* rb = buf + y * PITCH + j;
       C x[SX::R];
 #pragma unroll
@@ -456,7 +480,8 @@ struct Plane {
     const C* twx = tws;
 #pragma unroll 1
     for (int t = threadIdx.x; t < NY * SX::M; t += NT) {
-      const int j = t % SX::M, y = t / SX::M;
+      int y, j;
+      x_task(t, y, j);
       C* rb = buf + y * PITCH + j;
       C x[SX::R];
 #pragma unroll

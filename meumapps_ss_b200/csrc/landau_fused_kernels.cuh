@@ -501,11 +501,14 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
   using SL = fz::StageOf<N, NS - 1, PV>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;  // [N][V][TM]
-  C* tw = buf + N * LN;
+  C* ks = buf + N * LN;  // eta^ state tile [N][V][TM], in flight from the start
+  C* tw = ks + N * LN;
   using W = R;  // working precision of the update (the state's)
   __shared__ double g[V][9];
   __shared__ int sameg;  // every variant has the gradient coefficients of variant 0
   const int64_t m0 = (int64_t)blockIdx.x * TM;
+  tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
+  fz::cp_async_commit();
   if (threadIdx.x == 0) {
     int same = 1;
     for (int v = 0; v < V; ++v)
@@ -531,6 +534,8 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
   }
   __syncthreads();
   fz::dif_range<C, N, LN, 1, LN, NT, PV, 1, NS - 1>(buf, tw);
+  fz::cp_async_wait_all();
+  __syncthreads();
   const double dtld = a.F->dtl;
   const W ds = (W)dtld * (W)(1.0 / ((double)N * N * N));
   const bool one_g = sameg != 0;
@@ -554,7 +559,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
 #pragma unroll
     for (int q = 0; q < SL::R; ++q) x[q] = buf[(b * SL::R + q) * LN + line];
     Dft<SL::R, -1, C>::run(x);
-    const C* kst = a.Keta + f * NK + m;
+    const C* kst = ks + line;
     C* kout = a.Keta_out + f * NK + m;
     W fk = 0;
 #pragma unroll
@@ -562,7 +567,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
       const int p = b * SL::R + q;
       const int kz = fz::rev<N, PV>(p);
       const double az = kcomp<N>(kz), bz = 2 * kz == N ? 0.0 : az;
-      const C st = kst[(int64_t)p * PL];
+      const C st = kst[p * LN];
       const W hr = (W)st.x, hi = (W)st.y;
       if (a.energy) fk += (W)(kb0 + gv[8] * bz * bz + kz1 * bz) * (hr * hr + hi * hi);
       const Damp<W> rden(recip_ge1(1.0 + dtld * (kk0 + gv[8] * az * az + kz1 * bz)));
@@ -724,7 +729,7 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
   const size_t sp = P::smem_bytes();
   const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
-  const size_t s2 = sizeof(C) * ((size_t)N * V * TM + N * Tw<C>::K);
+  const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
   const size_t spb = pb_smem<R, N, V, PV, NTP>();
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_pb<R, N, V, PV, NTP>, spb);

@@ -147,12 +147,17 @@ class Simulation:
         et = P.to_fortran(eta_target)
         loss = C.c_double()
         dpar = (C.c_double * 5)()
-        g = np.empty(p.nx * p.ny * p.nz) if want_field else None
+        g = np.empty(p.nvar * p.nx * p.ny * p.nz) if want_field else None
         self._check(lib().meu_adjoint(self.h, int(nsteps), int(checkpoint_every), dptr(ct), dptr(et),
                                       C.byref(loss), dpar, dptr(g)))
         names = ("beta_eta", "kappa_c", "L", "M", "alpha")
         grads = {k: float(v) for k, v in zip(names, dpar)}
-        field = None if g is None else g.reshape(p.nz, p.ny, p.nx)
+        if g is None:
+            field = None
+        elif p.nvar == 1:
+            field = g.reshape(p.nz, p.ny, p.nx)
+        else:  # (nvar, nz, ny, nx) from the phi(vartot,Nx,Ny,Nz) layout
+            field = P.from_fortran(g, p.nvar, p.nx, p.ny, p.nz)
         return float(loss.value), grads, field
 
     def set_schedule(self, pv: int, ntp: int, tm: int) -> None:
