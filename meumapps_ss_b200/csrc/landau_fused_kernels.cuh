@@ -465,20 +465,30 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
     return mk((R)out[0], (R)out[1]);
   };
   R* rec = a.rec_phi ? a.rec_phi + f * N3 + z * PL : nullptr;
-  P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
-    const int64_t g0 = z * PL + (int64_t)y * N;
+  // phi_f back to shared memory in real space, then one pass over the plane's pairs in
+  // row order (its global loads of eta_q and dc are coalesced rows with several pairs in
+  // flight per thread, which hides their L2 latency better than loading them inside the
+  // register stage), then the forward from shared memory
+  P::template x_stage0<false>(buf, tws, [&](int y, int n0, int dn, C* x) {
+    C* rb = buf + y * P::PITCH + n0;
 #pragma unroll
-    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
-      const int n = n0 + r * dn;
-      C ev[V];
-#pragma unroll
-      for (int q = 0; q < V; ++q) ev[q] = __ldg((const C*)(a.eta + q * N3 + g0) + n);
-      const C dcv = __ldg((const C*)(a.c + g0) + n);
-      if (rec) ((C*)(rec + (int64_t)y * N))[n] = x[r];
-      if (bulk) bulk_energy(ev, dcv);
-      x[r] = point(ev, dcv, x[r]);
-    }
+    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) rb[r * dn] = x[r];
   });
+#pragma unroll 2
+  for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
+    const int y = i / P::LX, n = i - y * P::LX;
+    const int64_t g0 = z * PL + (int64_t)y * N + 2 * n;
+    C ev[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) ev[q] = __ldg((const C*)(a.eta + q * N3 + g0));
+    const C dcv = __ldg((const C*)(a.c + g0));
+    const C ph = buf[y * P::PITCH + n];
+    if (rec) ((C*)(rec + (int64_t)y * N))[n] = ph;
+    if (bulk) bulk_energy(ev, dcv);
+    buf[y * P::PITCH + n] = point(ev, dcv, ph);
+  }
+  __syncthreads();
+  P::x_forward0(buf, tws, [](int, int, int, C*) {});
   if (bulk) block_reduce_store(fch, 0, a.partials + LQ_FCH * PSTRIDE + z);
   P::forward_tail(buf, tws, mp);
 }
@@ -666,20 +676,22 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   if (!last) return;
   __threadfence();
   const int row = *(volatile const int*)a.hist_row;
-  // one quantity per warp, lane-strided loads, fixed reduction order
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // every thread on each quantity in turn (thread-strided loads, all in flight together,
+  // then a block reduction): the tail of the step is one L2 round trip per quantity,
+  // not one per 32 partials; fixed reduction order
 #pragma unroll 1
-  for (int q = wid; q < Q_STEP_COUNT; q += NTP / 32) {
+  for (int q = 0; q < Q_STEP_COUNT; ++q) {
     const int op = (q == Q_CMIN) ? 2 : (q == Q_CMAX || q == Q_PHIMAX) ? 1 : 0;
     double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
     const double* src = a.partials + (int64_t)q * PSTRIDE;
+    const int n = nb.nb[q];
 #pragma unroll 4
-    for (int i = lane; i < nb.nb[q]; i += 32) {
+    for (int i = threadIdx.x; i < n; i += NTP) {
       const double v = __ldcg(src + i);
       acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
     }
-    acc = op == 0 ? warp_sum(acc) : op == 1 ? warp_max(acc) : warp_min(acc);
-    if (lane == 0 && row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = acc;
+    acc = block_reduce_value(acc, op);
+    if (threadIdx.x == 0 && row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = acc;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
