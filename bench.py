@@ -316,6 +316,56 @@ def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
     return out
 
 
+def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0):
+    """Deck 3 beside the headline: the 96-member ensemble (32^3..128^3 grids, one
+    variant) in FP32 bulk and plain FP64, CUDA events around meu_ensemble_run (graph
+    capture and autotuning outside the timed region), with the FP32 error against FP64
+    (worst member) and the clocks of the FP32 window."""
+    import numpy as np
+    import torch
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200.sim import Ensemble
+
+    out = {"workload": f"landau-ensemble-{ENS_MEMBERS}x1var"}
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fields_out = {}
+    for prec in (P.PREC_F32, P.PREC_F64):
+        ws = CF.ensemble_config(ENS_MEMBERS, precision=prec)
+        cells = sum(w.params.nx ** 3 for w in ws)
+        ens = Ensemble([w.params for w in ws], autotune=prec == P.PREC_F32)
+        ens.set_stream(stream.cuda_stream)
+        for i, w in enumerate(ws):
+            ens.set_fields(i, *ensemble_fields(w))
+        ens.run(W, diag=True)
+        sampler = ClockSampler(local)
+        torch.cuda.synchronize()
+        if prec == P.PREC_F32:
+            sampler.start()
+            time.sleep(0.3)
+        l0 = ens.launch_count
+        a.record(stream)
+        ens.run(K, diag=True)
+        b.record(stream)
+        stream.synchronize()
+        ms = a.elapsed_time(b)
+        key = "fp32_bulk" if prec == P.PREC_F32 else "fp64_plain"
+        out[key] = {"value": cells * K / (ms / 1e3) / 1e6, "unit": UNIT, "steps": K, "ms_per_step": ms / K,
+                    "gpu_launches_per_step": (ens.launch_count - l0) / K}
+        if prec == P.PREC_F32:
+            out["clocks"] = sampler.stop()
+            out["cells_per_step"] = cells
+        fields_out[prec] = [ens.get_fields(i)[:2] for i in range(len(ws))]
+        ens.close()
+    worst_c = max(float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64))
+                  for (c32, _), (c64, _) in zip(fields_out[P.PREC_F32], fields_out[P.PREC_F64]))
+    worst_e = max(float(np.linalg.norm(e32 - e64) / max(np.linalg.norm(e64), 1e-300))
+                  for (_, e32), (_, e64) in zip(fields_out[P.PREC_F32], fields_out[P.PREC_F64]))
+    out["fp32_speedup"] = out["fp32_bulk"]["value"] / out["fp64_plain"]["value"]
+    out["err_vs_fp64"] = {"c_rel_l2_max_member": worst_c, "eta_rel_l2_max_member": worst_e, "after_steps": W + K}
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -494,6 +544,7 @@ def run_ours(args):
         decks["deck0"] = measure_deck(0, stream, K=200, W=W, K64=200, local=local)
         decks["deck2"] = measure_deck(2, stream, K=10, W=W, K64=10, local=local)
         decks["kks"] = measure_kks(stream)
+        decks["deck3"] = measure_ensemble(stream, local=local)
 
     # ---------------- CPU baseline (rank 0, N = 1): the oracle port on host cores
     cpu = None

@@ -327,6 +327,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       F.sig0_ebar[v] = hK.sig0_ebar[v];
     }
     for (int i = 0; i < 36; ++i) F.c0m[i] = p.cela[1][i];
+    F.elastic_on = p.elastic != MEU_ELAST_NONE ? 1.0 : 0.0;
     for (int m = 0; m < 6; ++m) F.ebar_eng[m] = hK.ebar_eng[m];
     F.lan_a = p.lan_a; F.lan_b = p.lan_b; F.lan_c = p.lan_c; F.lan_d = p.lan_d;
     F.lan_c1 = p.lan_c1; F.lan_c2 = p.lan_c2; F.cross_w = p.cross_w; F.kappa_c = p.kappa_c;
@@ -928,7 +929,8 @@ void Engine<R>::sync_args() {
 
 template <typename R>
 void Engine<R>::fused_step_launches() {
-  const int opts = (P.diag_energy ? LS_ENERGY : 0) | (theta_ready ? LS_THETA_READY : 0);
+  const int opts = (P.diag_energy ? LS_ENERGY : 0) | (theta_ready ? LS_THETA_READY : 0) | (q_checked ? 0 : LS_QCHECK);
+  q_checked = true;  // the first step is never captured (fused_warm is false until it has run)
   if (!lan_fused_step<R>(P.nx, V, sched, dA, 1, opts, st, &prof, fnb))
     throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
   theta_ready = true;

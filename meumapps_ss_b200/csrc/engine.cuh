@@ -306,6 +306,7 @@ class Engine : public EngineBase {
   bool el_ortho = false;              // stiffnesses with decoupled normal / shear blocks
   bool el_fused_rows = false;         // iterations run the x passes and el_x as one kernel
   bool fused_warm = false;
+  bool q_checked = false;  // Q(k) of the fused step tested (LS_QCHECK on its first step)
   bool theta_ready = false;  // sp holds theta^ of the current fields (written by the last step's PI)
   bool fields_set = false;  // the spectral-state layout is fixed from the first upload on
   std::unique_ptr<AdjBuffers<R>, void (*)(AdjBuffers<R>*)> adjb{nullptr, adj_buffers_free<R>};

@@ -57,6 +57,7 @@ class EnsembleT : public EnsembleBase {
     cudaStream_t bst = nullptr;
     cudaEvent_t done = nullptr;
     bool theta_ready = false;  // the members' M holds theta^ of their current fields
+    bool q_checked = false;    // Q(k) tested (LS_QCHECK on the first, never captured, step)
   };
   std::vector<std::unique_ptr<Engine<R>>> mem;
   std::vector<Bucket> bk;
@@ -167,10 +168,11 @@ void EnsembleT<R>::step_launches() {
   for (Bucket& b : bk) {
     MEU_CUDA(cudaStreamWaitEvent(b.bst, fork, 0));
     const int nm = (int)b.idx.size();
-    const int opts = (b.energy ? LS_ENERGY : 0) | (b.theta_ready ? LS_THETA_READY : 0);
+    const int opts = (b.energy ? LS_ENERGY : 0) | (b.theta_ready ? LS_THETA_READY : 0) | (b.q_checked ? 0 : LS_QCHECK);
     if (!lan_fused_step<R>(b.N, b.V, b.sched, b.dA, nm, opts, b.bst, &prof, b.nb))
       throw CudaError("fused step not instantiated", MEU_ERR_UNSUPPORTED);
     b.theta_ready = true;
+    b.q_checked = true;
     MEU_CUDA(cudaEventRecord(b.done, b.bst));
     MEU_CUDA(cudaStreamWaitEvent(st, b.done, 0));
   }

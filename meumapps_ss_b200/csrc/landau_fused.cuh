@@ -44,6 +44,7 @@ struct LanFusedConst {
   double g[4][9];         // grad_coeff (kappa_eta) per variant
   double A[4][4], sig0_ebar[4];
   double lan_a, lan_b, lan_c, lan_d, lan_c1, lan_c2, cross_w, kappa_c, dm, dtl, cbar;
+  double elastic_on;  // 1: the deck has elasticity (Q(k) is checked once, LS_QCHECK)
 };
 
 // Device-side arguments of one simulation ("member").  Kernels read them from a
@@ -94,6 +95,7 @@ enum LanQ : int {
 enum LanStepOpt : int {
   LS_ENERGY = 1,       // fort.98 energies of the step
   LS_THETA_READY = 2,  // M holds theta^ of the current fields (written by the previous step's PI)
+  LS_QCHECK = 4,       // first step: test Q(k) of every k with the reference's rcond rule
 };
 
 // Host launch entries (landau_fused.cu).  dA: device array of `members`

@@ -60,6 +60,17 @@ __device__ __forceinline__ double recip_ge1(double x) {
   return r;
 }
 
+// 1/x in FP64 for any x whose reciprocal is a normal single: a single-precision
+// estimate and two Newton-Raphson steps (relative error 2^-22 -> 2^-44 -> FP64
+// rounding); other x take the FP64 division.
+__device__ __forceinline__ double recip_nr(double x) {
+  double r = (double)__fdividef(1.0f, (float)x);
+  if (!(fabs(r) < 1.0e37 && fabs(r) > 1.0e-37)) return 1.0 / x;
+  r = fma(r, fma(-x, r, 1.0), r);
+  r = fma(r, fma(-x, r, 1.0), r);
+  return r;
+}
+
 // one component of the k-vector a (m wrapped into (-N/2, N/2]); b = a except at Nyquist
 template <int N>
 __device__ __forceinline__ double kcomp(int m) {
@@ -149,6 +160,42 @@ __global__ void __launch_bounds__(NT) k_lf_z0(const LanFusedArgs<R>* __restrict_
     if (f == V && p == 0 && m0 + c == 0) o = mk((R)0, (R)0);  // dc has no k = 0 mode
     C* dst = (f < V) ? a.Keta + f * NK : a.Kc;
     dst[p * PL + m0 + c] = o;
+  }
+}
+
+// ------------------------------------------------------------------ QCHECK
+// Q(k) of every k (natural order) against the reference's rcond <= 1e-16 stop
+// (ModFunc.f:55-67 via ModElastic.f:187), on the exact 1-norm condition number from
+// the adjugate: ||Q|| ||adj Q|| >= 1e16 |det Q| sets MEU_ERR_Q_SINGULAR.  Q(k) does not
+// change in time, so the step tests it once (its first step) and Z1 only inverts.
+template <typename R, int N>
+__global__ void __launch_bounds__(256) k_lf_qcheck(const LanFusedArgs<R>* __restrict__ A) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  const LanFusedConst& F = *a.F;
+  if (F.elastic_on == 0.0) return;
+  constexpr int NXH = N / 2 + 1;
+  constexpr int64_t NKK = (int64_t)N * N * NXH;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < NKK; id += (int64_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(id % NXH), ky = (int)((id / NXH) % N), kz = (int)(id / ((int64_t)NXH * N));
+    if (kx == 0 && ky == 0 && kz == 0) continue;
+    double ad[3], bd[3];
+    kvec_n<N>(kx, ky, kz, ad, bd);
+    const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
+    double Qs[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      double acc = 0;
+#pragma unroll
+      for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
+      Qs[q] = acc;
+    }
+    const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+    const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
+    const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+    const double det = qa * i00 + qd * i01 + qe * i02;
+    const double qn = fmax(fabs(qa) + fabs(qd) + fabs(qe), fmax(fabs(qd) + fabs(qb) + fabs(qf), fabs(qe) + fabs(qf) + fabs(qcc)));
+    const double an = fmax(fabs(i00) + fabs(i01) + fabs(i02), fmax(fabs(i01) + fabs(i11) + fabs(i12), fabs(i02) + fabs(i12) + fabs(i22)));
+    if (!(qn * an < 1e16 * fabs(det))) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
   }
 }
 
@@ -261,13 +308,8 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
       const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
       const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
       const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
-      const double det = qa * i00 + qd * i01 + qe * i02;
-      // the reference's rcond <= 1e-16 test (ModFunc.f:55-67) on the exact 1-norm
-      // condition number: ||Q|| ||adj Q|| >= 1e16 |det Q|
-      const double qn = fmax(fabs(qa) + fabs(qd) + fabs(qe), fmax(fabs(qd) + fabs(qb) + fabs(qf), fabs(qe) + fabs(qf) + fabs(qcc)));
-      const double an = fmax(fabs(i00) + fabs(i01) + fabs(i02), fmax(fabs(i01) + fabs(i11) + fabs(i12), fabs(i02) + fabs(i12) + fabs(i22)));
-      if (!(qn * an < 1e16 * fabs(det))) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
-      const double rd = 1.0 / det;
+      const double det = qa * i00 + qd * i01 + qe * i02;  // singular Q(k): k_lf_qcheck's error
+      const double rd = recip_nr(det);
       const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
                           {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
                           {(W)(i02 * rd), (W)(i12 * rd), (W)(i22 * rd)}};
@@ -748,6 +790,11 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   ensure_smem(k_lf_pi<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_z1<R, N, V, PV, TM>, s1);
   ensure_smem(k_lf_z2<R, N, V, PV, TM>, s2);
+  if (opts & LS_QCHECK) {
+    Scope s(hook, "lf_qcheck", 0.0, st);
+    k_lf_qcheck<R, N><<<dim3(148, 1, members), 256, 0, st>>>(dA);
+    MEU_CHECK_LAUNCH();
+  }
   if (!(opts & LS_THETA_READY)) {
     // theta^ of the first step after new fields (later steps get it from PI)
     Scope s(hook, "lf_plane_fwd", (double)V * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
