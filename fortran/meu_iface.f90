@@ -34,6 +34,12 @@ module meu_iface
     real(c_double) :: lan_a, lan_b, lan_c, lan_d, lan_c1, lan_c2, kappa_c, cross_w
   end type meu_params
 
+  ! mirror of struct meu_ran2_state (ran_2's SAVE variables)
+  type, bind(C) :: meu_ran2_state
+    integer(c_int32_t) :: idum, idum2, iy
+    integer(c_int32_t) :: iv(32)
+  end type meu_ran2_state
+
   ! mirror of struct meu_diag: one fort.98 / fort.99 line
   type, bind(C) :: meu_diag
     integer(c_int64_t) :: step
@@ -63,6 +69,14 @@ module meu_iface
       type(c_ptr), value :: h
       integer(c_int32_t), value :: nsteps
       type(c_ptr), value :: diag
+    end function
+    ! meu_run with the Langevin noise drawn from the ran_2 state rng (type(meu_ran2_state))
+    integer(c_int) function meu_run_noise(h, nsteps, rng, sd, diag) bind(C, name="meu_run_noise")
+      import :: c_int, c_int32_t, c_ptr, c_double, meu_ran2_state
+      type(c_ptr), value :: h, diag
+      integer(c_int32_t), value :: nsteps
+      type(meu_ran2_state), intent(inout) :: rng
+      real(c_double), value :: sd
     end function
     integer(c_int) function meu_get_fields(h, cons, phi, el_en, u_state) bind(C, name="meu_get_fields")
       import :: c_int, c_ptr

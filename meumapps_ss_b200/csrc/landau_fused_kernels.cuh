@@ -163,6 +163,16 @@ __global__ void __launch_bounds__(NT) k_lf_z0(const LanFusedArgs<R>* __restrict_
   }
 }
 
+// Z1's tile row stride: NF*TM complex padded so that (stride * words) mod 32 = 16, i.e.
+// consecutive rows start half the 32 banks apart
+template <typename R, int N, int V, int TM>
+constexpr int z1_row_stride() {
+  constexpr int W = 2 * (int)sizeof(R) / 4, LN = (V + 1) * TM;
+  int ls = LN;
+  while ((ls * W) % 32 != 16) ++ls;
+  return ls;
+}
+
 // ------------------------------------------------------------------ QCHECK
 // Q(k) of every k (natural order) against the reference's rcond <= 1e-16 stop
 // (ModFunc.f:55-67 via ModElastic.f:187), on the exact 1-norm condition number from
@@ -209,13 +219,16 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
   using C = cplx<R>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM, LV = V * TM;
+  // row stride of the tile: LN padded so that consecutive rows start half the banks apart
+  // (the k-space pass reads TM columns of several rows per warp)
+  constexpr int LS = z1_row_stride<R, N, V, TM>();
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   constexpr int NS = fz::rplan(N, PV).ns;
   static_assert(NS >= 2, "the column kernels need a radix plan of two stages or more");
   using S0 = fz::StageOf<N, 0, PV>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  C* buf = (C*)smraw;  // [N][NF][TM]: theta^_v in slots 0..V-1, dc^ in slot V
-  C* tw = buf + N * LN;
+  C* buf = (C*)smraw;  // [N][LS >= NF*TM]: theta^_v in slots 0..V-1, dc^ in slot V
+  C* tw = buf + N * LS;
   // FP64 only for Omega(k) = Q^-1; every other k-space product in the field precision W
   using W = R;
   __shared__ double qc[6][6];
@@ -247,10 +260,10 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     for (int r = 0; r < S0::R; ++r) x[r] = src[(int64_t)(j + r * S0::M) * PL];
     fz::dif_regs<C, N, 0, PV>(x, tw, j);
 #pragma unroll
-    for (int q = 0; q < S0::R; ++q) buf[(j + q * S0::M) * LN + line] = x[q];
+    for (int q = 0; q < S0::R; ++q) buf[(j + q * S0::M) * LS + line] = x[q];
   }
   __syncthreads();
-  fz::dif_range<C, N, LV, 1, LN, NT, PV, 1, NS>(buf, tw);
+  fz::dif_range<C, N, LV, 1, LS, NT, PV, 1, NS>(buf, tw);
   const W s = (W)(1.0 / ((double)N * N * N));
   double fint = 0, elen = 0;
   for (int i = threadIdx.x; i < N * TM; i += NT) {
@@ -261,7 +274,7 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     W av[3], b[3];
     kvec_w<N, W>(kx, ky, kz, av, b);
     const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
-    C* e = buf + p * LN + c;
+    C* e = buf + p * LS + c;
     W tr[V], ti[V], str = 0, sti = 0;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -391,13 +404,13 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     e[V * TM] = cn;
   }
   __syncthreads();
-  fz::dit_range<C, N, LN, 1, LN, NT, PV, 1, NS - 1>(buf, tw);
+  fz::dit_range<C, N, LN, 1, LS, NT, PV, 1, NS - 1>(buf, tw);
 #pragma unroll 1
   for (int t = threadIdx.x; t < LN * S0::M; t += NT) {
     const int line = t % LN, j = t / LN, f = line / TM, c = line - f * TM;
     C x[S0::R];
 #pragma unroll
-    for (int q = 0; q < S0::R; ++q) x[q] = buf[(j + q * S0::M) * LN + line];
+    for (int q = 0; q < S0::R; ++q) x[q] = buf[(j + q * S0::M) * LS + line];
     fz::dit_regs<C, N, 0, PV>(x, tw, j);
     C* dst = a.M + f * NK + m0 + c;
 #pragma unroll
@@ -782,7 +795,7 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   const double mm = (double)members;
   const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
   const size_t sp = P::smem_bytes();
-  const size_t s1 = sizeof(C) * ((size_t)N * (V + 1) * TM + N * Tw<C>::K);
+  const size_t s1 = sizeof(C) * ((size_t)N * z1_row_stride<R, N, V, TM>() + N * Tw<C>::K);
   const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
   const size_t spb = pb_smem<R, N, V, PV, NTP>();
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
