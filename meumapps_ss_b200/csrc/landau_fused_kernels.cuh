@@ -731,22 +731,40 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   if (!last) return;
   __threadfence();
   const int row = *(volatile const int*)a.hist_row;
-  // every thread on each quantity in turn (thread-strided loads, all in flight together,
-  // then a block reduction): the tail of the step is one L2 round trip per quantity,
-  // not one per 32 partials; fixed reduction order
+  // every thread loads its strided share of every quantity at once (all loads in flight
+  // together: one L2 round trip), then one block reduction of the Q_STEP_COUNT values;
+  // fixed reduction order
+  constexpr int QN = Q_STEP_COUNT, NW = NTP / 32;
+  auto qop = [](int q) { return (q == Q_CMIN) ? 2 : (q == Q_CMAX || q == Q_PHIMAX) ? 1 : 0; };
+  double acc[QN];
+#pragma unroll
+  for (int q = 0; q < QN; ++q) acc[q] = qop(q) == 0 ? 0.0 : qop(q) == 1 ? -1.0e308 : 1.0e308;
+  int nmax = 0;
+#pragma unroll
+  for (int q = 0; q < QN; ++q) nmax = max(nmax, nb.nb[q]);
 #pragma unroll 1
-  for (int q = 0; q < Q_STEP_COUNT; ++q) {
-    const int op = (q == Q_CMIN) ? 2 : (q == Q_CMAX || q == Q_PHIMAX) ? 1 : 0;
-    double acc = op == 0 ? 0.0 : op == 1 ? -1.0e308 : 1.0e308;
-    const double* src = a.partials + (int64_t)q * PSTRIDE;
-    const int n = nb.nb[q];
-#pragma unroll 4
-    for (int i = threadIdx.x; i < n; i += NTP) {
-      const double v = __ldcg(src + i);
-      acc = op == 0 ? acc + v : op == 1 ? fmax(acc, v) : fmin(acc, v);
+  for (int i = threadIdx.x; i < nmax; i += NTP) {
+#pragma unroll
+    for (int q = 0; q < QN; ++q) {
+      if (i < nb.nb[q]) {
+        const double v = __ldcg(a.partials + (int64_t)q * PSTRIDE + i);
+        acc[q] = qop(q) == 0 ? acc[q] + v : qop(q) == 1 ? fmax(acc[q], v) : fmin(acc[q], v);
+      }
     }
-    acc = block_reduce_value(acc, op);
-    if (threadIdx.x == 0 && row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = acc;
+  }
+  __shared__ double wred[NW][QN];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < QN; ++q) {
+    const double v = qop(q) == 0 ? warp_sum(acc[q]) : qop(q) == 1 ? warp_max(acc[q]) : warp_min(acc[q]);
+    if (lane == 0) wred[wid][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < QN) {
+    const int q = threadIdx.x, op = qop(q);
+    double v = wred[0][q];
+    for (int w = 1; w < NW; ++w) v = op == 0 ? v + wred[w][q] : op == 1 ? fmax(v, wred[w][q]) : fmin(v, wred[w][q]);
+    if (row < a.hist_rows) a.hist[(int64_t)row * Q_STEP_COUNT + q] = v;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
