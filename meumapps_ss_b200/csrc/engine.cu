@@ -317,6 +317,23 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     LanFusedConst F;
     memset(&F, 0, sizeof(F));
     memcpy(F.qcoef, hK.qcoef, sizeof(F.qcoef));
+    {
+      // cubic pattern of qcoef (exact comparisons: the constants are copied, not refit)
+      const auto& q = hK.qcoef;
+      bool cub = true;
+      for (int m = 0; m < 3 && cub; ++m)
+        for (int n = 0; n < 6; ++n) {
+          const double want = n >= 3 ? 0.0 : (n == m ? q[0][0] : q[0][1]);
+          if (q[m][n] != want) cub = false;
+        }
+      for (int m = 3; m < 6 && cub; ++m)
+        for (int n = 0; n < 6; ++n)
+          if (q[m][n] != (n == m ? q[3][3] : 0.0)) cub = false;
+      F.q_cubic = cub ? 1.0 : 0.0;
+      F.q_own = q[0][0];
+      F.q_other = q[0][1];
+      F.q_off = q[3][3];
+    }
     for (int v = 0; v < V; ++v) {
       for (int m = 0; m < 6; ++m) {
         F.sig0[v][m] = hK.sig0[v][m];

@@ -45,6 +45,9 @@ struct LanFusedConst {
   double A[4][4], sig0_ebar[4];
   double lan_a, lan_b, lan_c, lan_d, lan_c1, lan_c2, cross_w, kappa_c, dm, dtl, cbar;
   double elastic_on;  // 1: the deck has elasticity (Q(k) is checked once, LS_QCHECK)
+  // 1 when qcoef has the cubic pattern Q_ii = q_own a_i^2 + q_other (|a|^2 - a_i^2),
+  // Q_ij = q_off b_i b_j (i != j), which Z1 then evaluates with these three constants
+  double q_cubic, q_own, q_other, q_off;
 };
 
 // Device-side arguments of one simulation ("member").  Kernels read them from a

@@ -248,6 +248,8 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     if (threadIdx.x < 6) ebW[threadIdx.x] = (W)G.ebar_eng[threadIdx.x];
   }
   const double kapcd = a.F->kappa_c, dmd = a.F->dm;
+  const bool qcub = a.F->q_cubic != 0.0;
+  const double q_own = a.F->q_own, q_other = a.F->q_other, q_off = a.F->q_off;
   const W kapc = (W)kapcd, lan_a = (W)a.F->lan_a, hlb = (W)(0.5 * a.F->lan_b);
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
   __syncthreads();
@@ -310,12 +312,20 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
       // Omega(k) in FP64 from the double k-vectors
       const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
       double Qs[6];
+      if (qcub) {
+        const double s2 = Kv[0] + Kv[1] + Kv[2];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        double acc = 0;
+        for (int q = 0; q < 3; ++q) Qs[q] = q_other * s2 + (q_own - q_other) * Kv[q];
 #pragma unroll
-        for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
-        Qs[q] = acc;
+        for (int q = 3; q < 6; ++q) Qs[q] = q_off * Kv[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          double acc = 0;
+#pragma unroll
+          for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
+          Qs[q] = acc;
+        }
       }
       // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
       const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
