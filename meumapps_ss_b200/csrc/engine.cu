@@ -508,8 +508,7 @@ void Engine<R>::set_schedule(const int32_t* in3) {
   for (const LanSched& c : lan_sched_candidates(P.nx, sizeof(R) == 8)) {
     if (c.pv == in3[0] && c.ntp == in3[1] && c.tm == in3[2]) {
       sched = c;
-      if (gexec) cudaGraphExecDestroy(gexec);
-      gexec = nullptr;
+      drop_graphs();
       fused_warm = false;
       return;
     }
@@ -536,7 +535,7 @@ template <typename R>
 Engine<R>::~Engine() {
   if (st) cudaStreamSynchronize(st);
   if (own_st) cudaStreamSynchronize(own_st);
-  if (gexec) cudaGraphExecDestroy(gexec);
+  drop_graphs();
   prof.reset();
   for (void* q : allocs) cudaFree(q);
   if (h_results) cudaFreeHost(h_results);
@@ -956,56 +955,75 @@ void Engine<R>::fused_step_launches() {
 template <typename R>
 void Engine<R>::landau_step_fused() { fused_steps(1); }
 
-// Captures GRAPH_STEPS fused steps into gexec without running them.
+// Captures 2^slot fused steps into gexec[slot] without running them.
 template <typename R>
-void Engine<R>::capture_graph() {
+void Engine<R>::capture_graph(int slot) {
+  const int k = 1 << slot;
   const int64_t l0 = prof.launches;
   cudaGraph_t g = nullptr;
   MEU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int i = 0; i < GRAPH_STEPS; ++i) fused_step_launches();
+    for (int i = 0; i < k; ++i) fused_step_launches();
   } catch (...) {
     cudaStreamEndCapture(st, &g);
     if (g) cudaGraphDestroy(g);
     throw;
   }
   MEU_CUDA(cudaStreamEndCapture(st, &g));
-  const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+  const cudaError_t e = cudaGraphInstantiate(&gexec[slot], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
-    gexec = nullptr;
+    gexec[slot] = nullptr;
     throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), MEU_ERR_CUDA);
   }
-  graph_launches = prof.launches - l0;
+  graph_launches[slot] = prof.launches - l0;
   prof.launches = l0;  // captured, not run
 }
 
+template <typename R>
+void Engine<R>::drop_graphs() {
+  for (auto& g : gexec) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+}
+
 // n fused steps into history rows hist_n .. hist_n + n - 1 (d_row == hist_n on entry).
-// Runs of GRAPH_STEPS steps with one elastic state (homog flag) replay a CUDA
-// graph when the per-kernel timer is off and the stream can be captured. The
-// graph is captured at the end of the first call that leaves the step able to
-// replay one, so a later call of any length only replays (capture and
-// instantiation stay out of the caller's next timed run).
+// Once the step is warm, every run of steps with one elastic state (homog flag) replays
+// CUDA graphs of 8, 4, 2 and 1 steps (largest first) when the per-kernel timer is off
+// and the stream can be captured.  The graphs are captured at the end of the first call
+// that leaves the step able to replay them, so a later call of any length only replays
+// (capture and instantiation stay out of the caller's next timed run).
 template <typename R>
 void Engine<R>::fused_steps(int n) {
   int done = 0;
   while (done < n) {
     sync_args();
-    const bool homog_now = hA.homog != 0;
-    const bool homog_later = P.elastic != MEU_ELAST_NONE && step + GRAPH_STEPS - 1 >= P.elastep0;
-    const bool graphable = fused_warm && theta_ready && !prof.on && st != nullptr && n - done >= GRAPH_STEPS &&
-                           homog_now == homog_later;
-    if (graphable) {
-      if (!gexec) capture_graph();
-      MEU_CUDA(cudaGraphLaunch(gexec, st));
-      prof.launches += graph_launches;
-      for (int i = 0; i < GRAPH_STEPS; ++i) {
+    const bool can = fused_warm && theta_ready && !prof.on && st != nullptr;
+    int slot = -1;
+    if (can) {
+      const bool homog_now = hA.homog != 0;
+      for (int sl = GRAPH_SLOTS - 1; sl >= 0; --sl) {
+        const int k = 1 << sl;
+        const bool homog_later = P.elastic != MEU_ELAST_NONE && step + k - 1 >= P.elastep0;
+        if (n - done >= k && homog_now == homog_later) {
+          slot = sl;
+          break;
+        }
+      }
+    }
+    if (slot >= 0) {
+      const int k = 1 << slot;
+      if (!gexec[slot]) capture_graph(slot);
+      MEU_CUDA(cudaGraphLaunch(gexec[slot], st));
+      prof.launches += graph_launches[slot];
+      for (int i = 0; i < k; ++i) {
         hist_step[hist_n] = step;
         hist_iters[hist_n] = 0;
         hist_n += 1;
         step += 1;
       }
-      done += GRAPH_STEPS;
+      done += k;
     } else {
       fused_step_launches();
       fused_warm = true;  // kernel attributes are set; capture is possible from here
@@ -1016,7 +1034,9 @@ void Engine<R>::fused_steps(int n) {
       done += 1;
     }
   }
-  if (!gexec && fused_warm && theta_ready && !prof.on && st != nullptr) capture_graph();
+  if (fused_warm && theta_ready && !prof.on && st != nullptr)
+    for (int sl = 0; sl < GRAPH_SLOTS; ++sl)
+      if (!gexec[sl]) capture_graph(sl);
   last_iters = 0;
 }
 

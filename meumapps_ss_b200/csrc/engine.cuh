@@ -282,7 +282,8 @@ class Engine : public EngineBase {
   void sync_args();           // upload fused_args() into dA when it changed
   void fused_steps(int n);    // n fused steps (CUDA graphs of GRAPH_STEPS steps where possible)
   void fused_step_launches(); // launches of one fused step (stream or capture)
-  void capture_graph();       // GRAPH_STEPS fused steps into gexec, not run
+  void capture_graph(int slot);  // 2^slot fused steps into gexec[slot], not run
+  void drop_graphs();
   C *keta = nullptr, *kc = nullptr;  // spectral state of the Landau step
   // fused Landau path: schedule, device argument record, history row counter
   LanSched sched;
@@ -292,7 +293,8 @@ class Engine : public EngineBase {
   int* d_row = nullptr;
   int* d_ticket = nullptr;
   int fnb[Q_TOTAL] = {0};
-  static constexpr int GRAPH_STEPS = 8;
+  static constexpr int GRAPH_STEPS = 8;   // ensemble graph length
+  static constexpr int GRAPH_SLOTS = 4;   // single-handle graphs of 1, 2, 4 and 8 steps
   // grids of grid-stride reduction kernels sized to the blocks that fit at once (a
   // partial second wave would redo a whole share of the loop); <= RED_BLOCKS
   int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS, g_el_x = RED_BLOCKS;
@@ -312,8 +314,8 @@ class Engine : public EngineBase {
   std::unique_ptr<AdjBuffers<R>, void (*)(AdjBuffers<R>*)> adjb{nullptr, adj_buffers_free<R>};
   void reset_fused_state();
   void tune_transforms();  // generic path: pick FFT3::pv by timing
-  cudaGraphExec_t gexec = nullptr;
-  int64_t graph_launches = 0;  // kernels in gexec
+  cudaGraphExec_t gexec[GRAPH_SLOTS] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t graph_launches[GRAPH_SLOTS] = {0, 0, 0, 0};  // kernels in each graph
   void end_step(meu_diag* d, int clip);
   void flush_hist(meu_diag* diag);
   static constexpr int HIST_MAX = 4096;

@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
 #pragma unroll
     for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) rb[r * dn] = x[r];
   });
-#pragma unroll 2
+#pragma unroll 4
   for (int i = threadIdx.x; i < N * P::LX; i += NTP) {
     const int y = i / P::LX, n = i - y * P::LX;
     const int64_t g0 = z * PL + (int64_t)y * N + 2 * n;

@@ -89,6 +89,11 @@ class Simulation:
             return None
         return P.diag_to_dict(list(rows)[:nsteps])
 
+    def run_into(self, nsteps: int, rows) -> None:
+        """meu_run into a caller-allocated ``(P.MeuDiag * nsteps)()`` buffer, with no
+        conversion afterwards: exactly the call a Fortran or C driver makes (for timing)."""
+        self._check(lib().meu_run(self.h, int(nsteps), rows))
+
     def run_noise(self, nsteps: int, rng, sd: float, diag: bool = True) -> Optional[Dict[str, np.ndarray]]:
         """meu_run_noise: the steps with step <= noise_step draw their Langevin increments
         from ``rng`` (a ``_lib.Ran2State``, advanced in place) on a host thread."""
@@ -248,6 +253,11 @@ class Ensemble:
     def get_fields_fortran(self, m: int, cons: Optional[np.ndarray], phi: Optional[np.ndarray],
                            el: Optional[np.ndarray] = None) -> None:
         self._check(lib().meu_ensemble_get_fields(self.h, int(m), dptr(cons), dptr(phi), dptr(el)))
+
+    def run_into(self, nsteps: int, rows) -> None:
+        """meu_ensemble_run into a caller-allocated ``(P.MeuDiag * (members * nsteps))()``
+        buffer, with no conversion afterwards (for timing)."""
+        self._check(lib().meu_ensemble_run(self.h, int(nsteps), rows))
 
     def run(self, nsteps: int, diag: bool = True):
         """Advance every member; returns one diagnostics dict per member (or None)."""
