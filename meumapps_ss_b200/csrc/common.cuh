@@ -68,6 +68,7 @@ struct LaunchHook {
   virtual ~LaunchHook() {}
   virtual void begin(const char* name, double bytes, cudaStream_t st) = 0;
   virtual void end(cudaStream_t st) = 0;
+  virtual bool timing() const { return false; }  // events around every kernel
 };
 
 // Up to MAXF field pointers passed by value to batched kernels.

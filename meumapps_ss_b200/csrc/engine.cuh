@@ -78,6 +78,7 @@ class Profiler : public LaunchHook {
     cur_a = get();
     MEU_CUDA(cudaEventRecord(cur_a, st));
   }
+  bool timing() const override { return on; }
   void end(cudaStream_t st) override {
     if (!on) return;
     cudaEvent_t e = get();
@@ -280,7 +281,7 @@ class Engine : public EngineBase {
   void landau_step_fused();
   LanFusedArgs<R> fused_args() const;
   void sync_args();           // upload fused_args() into dA when it changed
-  void fused_steps(int n);    // n fused steps (CUDA graphs of GRAPH_STEPS steps where possible)
+  void fused_steps(int n);    // n fused steps (CUDA graphs of 8, 4, 2 and 1 steps where possible)
   void fused_step_launches(); // launches of one fused step (stream or capture)
   void capture_graph(int slot);  // 2^slot fused steps into gexec[slot], not run
   void drop_graphs();
@@ -293,8 +294,7 @@ class Engine : public EngineBase {
   int* d_row = nullptr;
   int* d_ticket = nullptr;
   int fnb[Q_TOTAL] = {0};
-  static constexpr int GRAPH_STEPS = 8;   // ensemble graph length
-  static constexpr int GRAPH_SLOTS = 4;   // single-handle graphs of 1, 2, 4 and 8 steps
+  static constexpr int GRAPH_SLOTS = 4;   // graphs of 1, 2, 4 and 8 steps
   // grids of grid-stride reduction kernels sized to the blocks that fit at once (a
   // partial second wave would redo a whole share of the loop); <= RED_BLOCKS
   int g_el_k = RED_BLOCKS, g_elener = RED_BLOCKS, g_lan_k1 = RED_BLOCKS, g_el_x = RED_BLOCKS;

@@ -2,7 +2,7 @@
 // together.  Members with the same grid size, variant count, precision and
 // energy flag form a bucket; every kernel of the fused step covers all members
 // of its bucket in one launch (blockIdx.z = member), the buckets run as parallel
-// branches, and runs of GRAPH_STEPS whole-ensemble steps replay one CUDA graph.
+// branches, and runs of 8, 4, 2 or 1 whole-ensemble steps replay CUDA graphs.
 // An optional autotuner picks each bucket's schedule (radix plan, plane threads,
 // column tile) by timing the candidates on the bucket before the fields are set.
 #include <map>
@@ -45,7 +45,7 @@ class EnsembleT : public EnsembleBase {
   }
 
  private:
-  static constexpr int GRAPH_STEPS = Engine<R>::GRAPH_STEPS;
+  static constexpr int GRAPH_SLOTS = Engine<R>::GRAPH_SLOTS;
   struct Bucket {
     int N = 0, V = 0;
     bool energy = false;
@@ -64,13 +64,15 @@ class EnsembleT : public EnsembleBase {
   std::vector<int> bucket_of;
   cudaStream_t st = nullptr, own_st = nullptr;
   cudaEvent_t fork = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  int64_t graph_launches = 0;
+  cudaGraphExec_t gexec[GRAPH_SLOTS] = {};   // 2^slot whole-ensemble steps
+  int64_t graph_launches[GRAPH_SLOTS] = {};  // kernels in each graph
   bool warm = false;
 
   void sync_args();
   void step_launches();
   bool homog_stable(int n) const;
+  bool can_replay() const;
+  void capture_graph(int slot);  // captured and instantiated, not run
 };
 
 template <typename R>
@@ -132,7 +134,8 @@ EnsembleT<R>::EnsembleT(int n, const meu_params* ps, int flags) {
 template <typename R>
 EnsembleT<R>::~EnsembleT() {
   if (st) cudaStreamSynchronize(st);
-  if (gexec) cudaGraphExecDestroy(gexec);
+  for (cudaGraphExec_t g : gexec)
+    if (g) cudaGraphExecDestroy(g);
   for (Bucket& b : bk) {
     if (b.bst) cudaStreamSynchronize(b.bst);
     if (b.dA) cudaFree(b.dA);
@@ -188,6 +191,42 @@ bool EnsembleT<R>::homog_stable(int n) const {
   return true;
 }
 
+// the step is warm, every bucket's theta^ is current, the per-kernel timer is off and
+// the stream can be captured
+template <typename R>
+bool EnsembleT<R>::can_replay() const {
+  if (!warm || prof.on || st == nullptr) return false;
+  for (const Bucket& b : bk)
+    if (!b.theta_ready) return false;
+  return true;
+}
+
+template <typename R>
+void EnsembleT<R>::capture_graph(int slot) {
+  const int64_t l0 = prof.launches;
+  cudaGraph_t g = nullptr;
+  MEU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (int s = 0; s < (1 << slot); ++s) step_launches();
+  } catch (...) {
+    cudaStreamEndCapture(st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  MEU_CUDA(cudaStreamEndCapture(st, &g));
+  const cudaError_t e = cudaGraphInstantiate(&gexec[slot], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    gexec[slot] = nullptr;
+    throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), MEU_ERR_CUDA);
+  }
+  graph_launches[slot] = prof.launches - l0;
+  prof.launches = l0;
+}
+
+// Once warm, runs of steps with one elastic state replay graphs of 8, 4, 2 and 1 steps
+// (largest first).  The graphs are captured at the end of the first call that leaves the
+// ensemble able to replay them, so a later call of any length only replays.
 template <typename R>
 void EnsembleT<R>::run(int nsteps, meu_diag* diag) {
   if (nsteps < 0) throw CudaError("negative step count", MEU_ERR_BADARG);
@@ -203,36 +242,19 @@ void EnsembleT<R>::run(int nsteps, meu_diag* diag) {
     int i = 0;
     while (i < chunk) {
       sync_args();
-      bool ready = true;
-      for (const Bucket& b : bk) ready = ready && b.theta_ready;
-      const bool graphable =
-          warm && ready && !prof.on && st != nullptr && chunk - i >= GRAPH_STEPS && homog_stable(GRAPH_STEPS);
+      int slot = -1;
+      if (can_replay())
+        for (int sl = GRAPH_SLOTS - 1; sl >= 0; --sl)
+          if (chunk - i >= (1 << sl) && homog_stable(1 << sl)) {
+            slot = sl;
+            break;
+          }
       int k = 1;
-      if (graphable) {
-        if (!gexec) {
-          const int64_t l0 = prof.launches;
-          cudaGraph_t g = nullptr;
-          MEU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-          try {
-            for (int s = 0; s < GRAPH_STEPS; ++s) step_launches();
-          } catch (...) {
-            cudaStreamEndCapture(st, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-          }
-          MEU_CUDA(cudaStreamEndCapture(st, &g));
-          const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
-          cudaGraphDestroy(g);
-          if (e != cudaSuccess) {
-            gexec = nullptr;
-            throw CudaError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e), MEU_ERR_CUDA);
-          }
-          graph_launches = prof.launches - l0;
-          prof.launches = l0;
-        }
-        MEU_CUDA(cudaGraphLaunch(gexec, st));
-        prof.launches += graph_launches;
-        k = GRAPH_STEPS;
+      if (slot >= 0) {
+        if (!gexec[slot]) capture_graph(slot);
+        MEU_CUDA(cudaGraphLaunch(gexec[slot], st));
+        prof.launches += graph_launches[slot];
+        k = 1 << slot;
       } else {
         step_launches();
         warm = true;
@@ -256,6 +278,9 @@ void EnsembleT<R>::run(int nsteps, meu_diag* diag) {
     }
     done += chunk;
   }
+  if (can_replay())
+    for (int sl = 0; sl < GRAPH_SLOTS; ++sl)
+      if (!gexec[sl]) capture_graph(sl);
 }
 
 template <typename R>

@@ -236,3 +236,41 @@ def test_multivariant_adjoint_matches_central_differences(nvar):
     for k in g:
         assert rel(g32[k], g[k]) < 1e-3, (k, g32[k], g[k])
     assert np.linalg.norm(ge32 - ge) / np.linalg.norm(ge) < 1e-3
+
+
+@pytest.mark.gpu
+def test_deck4_full_size_central_differences():
+    """Deck 4 at its own size: 128^3, one variant, 200 steps, checkpoints every 20, target
+    from the FP64 forward at kappa 1.2, L 0.8, M 1.1, eps0 0.012.  FP64 gradients in
+    kappa, L, M, eps0 and eta_0 (along a seeded direction) against central differences
+    with h = 1e-4, within 1e-4."""
+    n, steps = 128, 200
+    every = CF.ADJOINT_CHECKPOINT_EVERY
+    w = CF.adjoint_config(n, P.PREC_F64, **CF.ADJOINT_TARGET)
+    c0, e0 = _lib.init_uniform(n, n, n, 1, w.seed, w.c0, w.c_amp, w.eta_amp)
+    t = Simulation(w.params)
+    t.set_fields(c0, e0)
+    t.run(steps, diag=False)
+    ct, et, _, _ = t.get_fields()
+
+    def loss(**kw):
+        return forward_loss(CF.adjoint_config(n, P.PREC_F64, **kw).params, c0, e0, ct, et, steps=steps)
+
+    st = dict(CF.ADJOINT_START)
+    s = Simulation(CF.adjoint_config(n, P.PREC_F64, **st).params)
+    s.set_fields(c0, e0)
+    J, g, ge = s.adjoint(steps, every, ct, et)
+    assert rel(J, loss(**st)) < 1e-12
+    adj = {"kappa": g["beta_eta"] / st["kappa"] + g["kappa_c"], "L": g["L"], "M": g["M"],
+           "eps0": g["alpha"] / st["eps0"]}
+    for k, v in adj.items():
+        up, dn = dict(st), dict(st)
+        up[k] += FD_H
+        dn[k] -= FD_H
+        fd = (loss(**up) - loss(**dn)) / (2 * FD_H)
+        assert rel(v, fd) < FD_TOL, (k, v, fd)
+    d = np.random.default_rng(8).standard_normal(e0.shape)
+    p = CF.adjoint_config(n, P.PREC_F64, **st).params
+    fd = (forward_loss(p, c0, e0 + FD_H * d, ct, et, steps=steps) -
+          forward_loss(p, c0, e0 - FD_H * d, ct, et, steps=steps)) / (2 * FD_H)
+    assert rel(float(np.sum(ge * d[0])), fd) < FD_TOL
