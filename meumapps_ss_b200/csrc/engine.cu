@@ -356,7 +356,10 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     d_row = dalloc<int>(2);
     d_ticket = d_row + 1;
     MEU_CUDA(cudaMemset(d_row, 0, 2 * sizeof(int)));
-
+    if (p.elastic != MEU_ELAST_NONE && V == 1) {
+      gtab = dalloc<R>(nk);
+      MEU_CUDA(cudaMemset(gtab, 0, sizeof(R) * nk));
+    }
   }
   MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
   MEU_CUDA(cudaMemset(c, 0, sizeof(R) * E * n3));
@@ -930,6 +933,7 @@ LanFusedArgs<R> Engine<R>::fused_args() const {
   a.c_next = c;
   a.Keta_out = keta;
   a.Kc_out = kc;
+  a.gtab = gtab;
   return a;
 }
 

@@ -286,6 +286,7 @@ class Engine : public EngineBase {
   void capture_graph(int slot);  // 2^slot fused steps into gexec[slot], not run
   void drop_graphs();
   C *keta = nullptr, *kc = nullptr;  // spectral state of the Landau step
+  R* gtab = nullptr;  // Green-operator table of the fused step (homogeneous elasticity)
   // fused Landau path: schedule, device argument record, history row counter
   LanSched sched;
   LanFusedArgs<R>* dA = nullptr;

@@ -77,6 +77,9 @@ struct LanFusedArgs {
   R* c_next;
   cplx<R>* Keta_out;
   cplx<R>* Kc_out;
+  // Green-operator table of homogeneous elasticity for one variant: one real plane in
+  // the dc^ state layout (k_lf_gtab); NULL without elasticity or with several variants
+  R* gtab;
   // optional records of the step for the adjoint (NULL: off): the real elastic
   // potential phi_v (V fields) and the normalised spectra theta^_v (V spectra)
   R* rec_phi;

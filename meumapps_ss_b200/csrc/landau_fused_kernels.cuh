@@ -79,6 +79,17 @@ __device__ __forceinline__ double kcomp(int m) {
 
 template <typename R> constexpr int col_tile_default() { return sizeof(R) == 4 ? 16 : 8; }
 
+// Programmatic dependent launch of the four per-step kernels (Z1, PB, Z2, PI): each is
+// launched while its predecessor in the stream still runs, so its blocks take the slots
+// the predecessor's last wave leaves free and load their constants and twiddles there.
+// step_dep_wait() blocks until the predecessor grid has completed and its writes are
+// visible; nothing the predecessor writes is read before it.  step_dep_release() comes
+// after the wait, so a successor's blocks start only once this grid's predecessor has
+// completed: a prologue overlaps one kernel at most (the one right before it).  A kernel
+// launched without the attribute passes both at once.
+__device__ __forceinline__ void step_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void step_dep_release() { asm volatile("griddepcontrol.launch_dependents;\n"); }
+
 // Column tile of nf fields: smem [z][slot][TM] with LN complex per z row, global
 // M-form (or state) field f at G + f*NK, row z at + z*PL, columns m0 .. m0+TM.
 // tile_load only issues cp.async copies; the caller waits.
@@ -173,6 +184,38 @@ constexpr int z1_row_stride() {
   return ls;
 }
 
+// a shared-memory load the compiler keeps in place (it is not moved across barriers)
+template <typename T>
+__device__ __forceinline__ T lds(const T* p);
+template <>
+__device__ __forceinline__ float lds<float>(const float* p) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"((unsigned)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+template <>
+__device__ __forceinline__ double lds<double>(const double* p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];\n" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+
+// With one variant, Z1 stages its tile of the Green-operator table and of the dc^ state
+// in shared memory (cp.async, issued before it waits for its predecessor) when both fit
+// beside the transform tile within a third of the SM's shared memory (three blocks per SM)
+template <typename R, int N, int V, int TM>
+constexpr size_t z1_smem_base() {
+  return sizeof(cplx<R>) * ((size_t)N * z1_row_stride<R, N, V, TM>() + N * Tw<cplx<R>>::K);
+}
+template <typename R, int N, int V, int TM>
+constexpr size_t z1_smem_stage() {
+  return sizeof(R) * (size_t)(V * (V + 1) / 2) * N * TM + sizeof(cplx<R>) * (size_t)N * TM;
+}
+template <typename R, int N, int V, int TM>
+constexpr bool z1_prefetch() {
+  return V == 1 && z1_smem_base<R, N, V, TM>() + z1_smem_stage<R, N, V, TM>() <= 74 * 1024;
+}
+
 // ------------------------------------------------------------------ QCHECK
 // Q(k) of every k (natural order) against the reference's rcond <= 1e-16 stop
 // (ModFunc.f:55-67 via ModElastic.f:187), on the exact 1-norm condition number from
@@ -207,6 +250,147 @@ __global__ void __launch_bounds__(256) k_lf_qcheck(const LanFusedArgs<R>* __rest
     const double an = fmax(fabs(i00) + fabs(i01) + fabs(i02), fmax(fabs(i01) + fabs(i11) + fabs(i12), fabs(i02) + fabs(i12) + fabs(i22)));
     if (!(qn * an < 1e16 * fabs(det))) atomicMax(a.err, (int)MEU_ERR_Q_SINGULAR);
   }
+}
+
+// ------------------------------------------------------------------ GTAB
+// The Green operator of homogeneous elasticity as a table, built once per upload in FP64
+// and stored in the field precision (used by the one-variant step).  With u^ = Omega(k) R, R = i sum_u theta^_u s_u,
+// s_v = sig0_v b and phi^_v = i s_v . u^, the elastic potential is
+//   phi^_v = sum_u T_vu theta^_u,   T_vu = -s_v . Omega(k) s_u   (real, symmetric),
+// Omega = Q(k)^-1.  Entry (v <= u) in pair order q goes to gtab[q * NK + p * PL + m],
+// the layout of the dc^ state (p: z row in the column kernels' digit-reversed order,
+// m: spectral column), so Z1 reads it beside dc^.  Q(k) and the moduli do not change in
+// time; k = 0 is left zero (Z1 does not read it).  Singular Q(k) is k_lf_qcheck's error.
+template <typename R, int N, int V, int PV>
+__global__ void __launch_bounds__(256) k_lf_gtab(const LanFusedArgs<R>* __restrict__ A) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  if (a.gtab == nullptr) return;
+  const LanFusedConst& F = *a.F;
+  constexpr int NXH = N / 2 + 1;
+  constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < NK; id += (int64_t)gridDim.x * blockDim.x) {
+    const int p = (int)(id / PL);
+    const int64_t m = id - (int64_t)p * PL;
+    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+    double T[V][V];
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int u = 0; u < V; ++u) T[v][u] = 0.0;
+    if (kx != 0 || ky != 0 || kz != 0) {
+      double ad[3], bd[3];
+      kvec_n<N>(kx, ky, kz, ad, bd);
+      const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
+      double Qs[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        double acc = 0;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) acc += F.qcoef[q][n] * Kv[n];
+        Qs[q] = acc;
+      }
+      const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+      const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
+      const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+      const double det = qa * i00 + qd * i01 + qe * i02;
+      const double Om[3][3] = {{i00 / det, i01 / det, i02 / det},
+                               {i01 / det, i11 / det, i12 / det},
+                               {i02 / det, i12 / det, i22 / det}};
+      double sb[V][3];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double* sg = F.sig0[v];
+        sb[v][0] = sg[0] * bd[0] + sg[5] * bd[1] + sg[4] * bd[2];
+        sb[v][1] = sg[5] * bd[0] + sg[1] * bd[1] + sg[3] * bd[2];
+        sb[v][2] = sg[4] * bd[0] + sg[3] * bd[1] + sg[2] * bd[2];
+      }
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        double w[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) w[r] = Om[r][0] * sb[u][0] + Om[r][1] * sb[u][1] + Om[r][2] * sb[u][2];
+#pragma unroll
+        for (int v = 0; v < V; ++v) T[v][u] = -(sb[v][0] * w[0] + sb[v][1] * w[1] + sb[v][2] * w[2]);
+      }
+    }
+    int q = 0;
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int u = v; u < V; ++u) {
+        // symmetric to rounding; the pair's mean keeps T_vu = T_uv exactly
+        a.gtab[q * NK + id] = (R)(0.5 * (T[v][u] + T[u][v]));
+        ++q;
+      }
+  }
+}
+
+// Elastic energy density 0.5 e*.C0.e (without the w factor) of one k on a Nyquist plane
+// or at k = 0, where the quadratic form in theta^ does not hold: u^ = Omega(k) R with
+// R_i = i sum_j b_j S_ij, S = sum_v theta^_v sig0_v (Voigt 11,22,33,23,13,12), then the
+// engineering strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0).
+template <typename W, int V>
+__device__ __forceinline__ W nyq_strain_energy(const W* tr, const W* ti, const W* b, const double* ad, const double* bd,
+                                            bool k0, bool green, const W (*sgW)[6], const W (*epW)[6], const W* c0W,
+                                            const W* ebW, const double (*qc)[6]) {
+  W ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
+  if (green) {
+    W Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * sgW[v][q]; Si[q] += ti[v] * sgW[v][q]; }
+    const W t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
+    const W t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
+    const W t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
+    const W Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
+    const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
+    double Qs[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      double acc = 0;
+#pragma unroll
+      for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
+      Qs[q] = acc;
+    }
+    const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+    const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
+    const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+    const double rd = 1.0 / (qa * i00 + qd * i01 + qe * i02);
+    const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
+                        {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
+                        {(W)(i02 * rd), (W)(i12 * rd), (W)(i22 * rd)}};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
+      ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
+    }
+  }
+  // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
+  const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+  W er[6], ei[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const int ii = I1[q], jj = J1[q];
+    W gr, gi;
+    if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
+    else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
+#pragma unroll
+    for (int v = 0; v < V; ++v) { gr -= tr[v] * epW[v][q]; gi -= ti[v] * epW[v][q]; }
+    if (k0) gr += ebW[q];
+    er[q] = gr;
+    ei[q] = gi;
+  }
+  W qq = 0;
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    W cr2 = 0, ci2 = 0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) { cr2 += c0W[r + j * 6] * er[j]; ci2 += c0W[r + j * 6] * ei[j]; }
+    qq += er[r] * cr2 + ei[r] * ci2;
+  }
+  return qq;
 }
 
 // ------------------------------------------------------------------ Z1
@@ -251,7 +435,33 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
   const bool qcub = a.F->q_cubic != 0.0;
   const double q_own = a.F->q_own, q_other = a.F->q_other, q_off = a.F->q_off;
   const W kapc = (W)kapcd, lan_a = (W)a.F->lan_a, hlb = (W)(0.5 * a.F->lan_b);
+  // staged tiles: table [q][z][TM] and dc^ state [z][TM].  Neither is written by the
+  // kernels this launch may overlap: the table only at upload, dc^ by the previous Z1,
+  // which has completed once this block runs (the predecessor released it after its wait)
+  // one variant: the Green operator from the table (one real per k); more variants:
+  // Omega(k) per k in FP64 (the table's V(V+1)/2 reals per k cost more than the solve)
+  constexpr bool TAB = V == 1;
+  constexpr bool PRE = TAB && z1_prefetch<R, N, V, TM>();
+  constexpr int NQ = V * (V + 1) / 2;
+  R* gts = (R*)(tw + N * Tw<C>::K);
+  C* kcs = (C*)(gts + NQ * N * TM);
+  if constexpr (PRE) {
+    constexpr int PR = 16 / sizeof(R), PC = 16 / sizeof(C);
+    if (a.homog) {
+      for (int i = threadIdx.x; i < NQ * N * (TM / PR); i += NT) {
+        const int row = i / (TM / PR), c = (i - row * (TM / PR)) * PR, q = row / N, z = row - q * N;
+        fz::cp_async16(gts + (q * N + z) * TM + c, a.gtab + q * NK + z * PL + m0 + c);
+      }
+    }
+    for (int i = threadIdx.x; i < N * (TM / PC); i += NT) {
+      const int z = i / (TM / PC), c = (i - z * (TM / PC)) * PC;
+      fz::cp_async16(kcs + z * TM + c, a.Kc + z * PL + m0 + c);
+    }
+    fz::cp_async_commit();
+  }
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  step_dep_wait();
+  step_dep_release();
   __syncthreads();
 #pragma unroll 1
   for (int t = threadIdx.x; t < LV * S0::M; t += NT) {
@@ -265,153 +475,273 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restri
     for (int q = 0; q < S0::R; ++q) buf[(j + q * S0::M) * LS + line] = x[q];
   }
   __syncthreads();
+  // the staged tiles are complete and visible after the barrier that ends the DIF stages
+  if constexpr (PRE) fz::cp_async_wait_all();
   fz::dif_range<C, N, LV, 1, LS, NT, PV, 1, NS>(buf, tw);
   const W s = (W)(1.0 / ((double)N * N * N));
   double fint = 0, elen = 0;
-  for (int i = threadIdx.x; i < N * TM; i += NT) {
-    const int p = i / TM, c = i - p * TM;
-    const int64_t m = m0 + c;
-    const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
-    const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
-    W av[3], b[3];
-    kvec_w<N, W>(kx, ky, kz, av, b);
-    const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
-    C* e = buf + p * LS + c;
-    W tr[V], ti[V], str = 0, sti = 0;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      tr[v] = (W)e[v * TM].x * s;
-      ti[v] = (W)e[v * TM].y * s;
-      str += tr[v];
-      sti += ti[v];
+  if constexpr (TAB) {
+    // Two passes over the tile's k-points, each thread on the same points in both (no
+    // barrier between them): the Cahn-Hilliard update reads theta^ and writes slot V, then
+    // the elastic pass overwrites theta^ with phi^.  Split, each pass keeps fewer values live.
+    // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
+  #pragma unroll 1
+    for (int i = threadIdx.x; i < N * TM; i += NT) {
+      const int p = i / TM, c = i - p * TM;
+      const int64_t m = m0 + c;
+      const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+      const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+      C* e = buf + p * LS + c;
+      W str = 0, sti = 0;
+  #pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const W tr = (W)e[v * TM].x * s, ti = (W)e[v * TM].y * s;
+        str += tr;
+        sti += ti;
+        if (a.rec_theta) a.rec_theta[v * NK + p * PL + m] = mk((R)tr, (R)ti);
+      }
+      const C cs = PRE ? kcs[p * TM + c] : a.Kc[p * PL + m];
+      const W cr = (W)cs.x, ci = (W)cs.y;
+      const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+      if (a.energy) {
+        W av[3], b[3];
+        kvec_w<N, W>(kx, ky, kz, av, b);
+        const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
+        fint += (double)((W)0.5 * w * kapc * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci));
+      }
+      W nr = 0, ni = 0;
+      if (!k0) {
+        const double a0 = kcomp<N>(kx), a1 = kcomp<N>(ky), a2 = kcomp<N>(kz);
+        const double k2d = a0 * a0 + a1 * a1 + a2 * a2;
+        const Damp<W> rden(recip_ge1(1.0 + dmd * kapcd * k2d * k2d));
+        const W dk2 = (W)(dmd * k2d);
+        const W mr = lan_a * cr - hlb * str, mi = lan_a * ci - hlb * sti;
+        nr = rden(cr - dk2 * mr);
+        ni = rden(ci - dk2 * mi);
+      }
+      const C cn = mk((R)nr, (R)ni);
+      a.Kc_out[p * PL + m] = cn;
+      e[V * TM] = cn;
     }
-    if (a.rec_theta) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) a.rec_theta[v * NK + p * PL + m] = mk((R)tr[v], (R)ti[v]);
-    }
-    const C cs = a.Kc[p * PL + m];
-    const W cr = (W)cs.x, ci = (W)cs.y;
-    const bool k0 = (kx == 0 && ky == 0 && kz == 0);
-    const bool nyq = 2 * kx == N || 2 * ky == N || 2 * kz == N;
-    double ad[3], bd[3];
-    kvec_n<N>(kx, ky, kz, ad, bd);
-    if (a.energy) fint += (double)((W)0.5 * w * kapc * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci));
-    // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
-    W ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
-    if (a.homog && !k0) {
-      W Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-      for (int v = 0; v < V; ++v)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * sgW[v][q]; Si[q] += ti[v] * sgW[v][q]; }
-      // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
-      const W t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
-      const W t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
-      const W t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
-      const W Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
-      // Omega(k) in FP64 from the double k-vectors
-      const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
-      double Qs[6];
-      if (qcub) {
-        const double s2 = Kv[0] + Kv[1] + Kv[2];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) Qs[q] = q_other * s2 + (q_own - q_other) * Kv[q];
-#pragma unroll
-        for (int q = 3; q < 6; ++q) Qs[q] = q_off * Kv[q];
-      } else {
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          double acc = 0;
-#pragma unroll
-          for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
-          Qs[q] = acc;
+    // ---- homogeneous elasticity: phi^_v = sum_u T_vu theta^_u from the Green-operator table
+  #pragma unroll 1
+    for (int i = threadIdx.x; i < N * TM; i += NT) {
+      const int p = i / TM, c = i - p * TM;
+      C* e = buf + p * LS + c;
+      if (!a.homog) {
+  #pragma unroll
+        for (int v = 0; v < V; ++v) e[v * TM] = mk((R)0, (R)0);
+        continue;
+      }
+      const int64_t m = m0 + c;
+      const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+      const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+      const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+      W tr[V], ti[V];
+  #pragma unroll
+      for (int v = 0; v < V; ++v) {
+        tr[v] = (W)e[v * TM].x * s;
+        ti[v] = (W)e[v * TM].y * s;
+      }
+      W phr[V], phi_[V];
+      {
+        W T[V][V];
+        int q = 0;
+  #pragma unroll
+        for (int v = 0; v < V; ++v)
+  #pragma unroll
+          for (int u = v; u < V; ++u) {
+            const W t = k0 ? (W)0 : PRE ? (W)lds<R>(gts + (q * N + p) * TM + c) : (W)__ldg(a.gtab + q * NK + p * PL + m);
+            T[v][u] = t;
+            T[u][v] = t;
+            ++q;
+          }
+  #pragma unroll
+        for (int v = 0; v < V; ++v) {
+          W pr = 0, pi = 0;
+  #pragma unroll
+          for (int u = 0; u < V; ++u) {
+            pr += T[v][u] * tr[u];
+            pi += T[v][u] * ti[u];
+          }
+          phr[v] = pr;
+          phi_[v] = pi;
+          e[v * TM] = mk((R)pr, (R)pi);
         }
       }
-      // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
-      const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
-      const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
-      const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
-      const double det = qa * i00 + qd * i01 + qe * i02;  // singular Q(k): k_lf_qcheck's error
-      const double rd = recip_nr(det);
-      const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
-                          {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
-                          {(W)(i02 * rd), (W)(i12 * rd), (W)(i22 * rd)}};
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
-        ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
+      if (!a.energy) continue;
+      const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
+      const bool nyq = 2 * kx == N || 2 * ky == N || 2 * kz == N;
+      if (!k0 && !nyq) {
+        // Khachaturyan's quadratic form: with equilibrium u^ and homogeneous C0,
+        // e*.C0.e = sum_pq A_pq Re(theta^_p* theta^_q) - sum_p Re(theta^_p* phi^_p),
+        // A_pq = eps0_p.C0.eps0_q.  It needs the strain's and Q(k)'s k-vectors to agree,
+        // which they do off the Nyquist planes (k_space zeroes b there but not a).
+        W qq = 0;
+  #pragma unroll
+        for (int pv = 0; pv < V; ++pv) {
+          qq -= tr[pv] * phr[pv] + ti[pv] * phi_[pv];
+  #pragma unroll
+          for (int qv = 0; qv < V; ++qv) qq += aW[pv][qv] * (tr[pv] * tr[qv] + ti[pv] * ti[qv]);
+        }
+        elen += (double)((W)0.5 * w * qq);
+      } else {
+        // Nyquist planes and k = 0: the strain itself
+        W av[3], b[3];
+        kvec_w<N, W>(kx, ky, kz, av, b);
+        double ad[3], bd[3];
+        kvec_n<N>(kx, ky, kz, ad, bd);
+        const W qq = nyq_strain_energy<W, V>(tr, ti, b, ad, bd, k0, !k0, sgW, epW, c0W, ebW, qc);
+        elen += (double)((W)0.5 * w * qq);
       }
     }
-    W phr[V], phi_[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      W pr = 0, pi = 0;
+  } else {
+    // one pass: theta^ sums and Cahn-Hilliard, Omega(k) = Q(k)^-1 in FP64 per k, phi^_v
+    for (int i = threadIdx.x; i < N * TM; i += NT) {
+      const int p = i / TM, c = i - p * TM;
+      const int64_t m = m0 + c;
+      const int py = (int)(m / NXH), cx = (int)(m - (int64_t)py * NXH);
+      const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
+      W av[3], b[3];
+      kvec_w<N, W>(kx, ky, kz, av, b);
+      const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
+      C* e = buf + p * LS + c;
+      W tr[V], ti[V], str = 0, sti = 0;
+  #pragma unroll
+      for (int v = 0; v < V; ++v) {
+        tr[v] = (W)e[v * TM].x * s;
+        ti[v] = (W)e[v * TM].y * s;
+        str += tr[v];
+        sti += ti[v];
+      }
+      if (a.rec_theta) {
+  #pragma unroll
+        for (int v = 0; v < V; ++v) a.rec_theta[v * NK + p * PL + m] = mk((R)tr[v], (R)ti[v]);
+      }
+      const C cs = a.Kc[p * PL + m];
+      const W cr = (W)cs.x, ci = (W)cs.y;
+      const bool k0 = (kx == 0 && ky == 0 && kz == 0);
+      const bool nyq = 2 * kx == N || 2 * ky == N || 2 * kz == N;
+      double ad[3], bd[3];
+      kvec_n<N>(kx, ky, kz, ad, bd);
+      if (a.energy) fint += (double)((W)0.5 * w * kapc * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * (cr * cr + ci * ci));
+      // ---- homogeneous elasticity: u^ = Q^-1 R, phi^_v = i (sig0_v b) . u^
+      W ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
       if (a.homog && !k0) {
-        const W* sg = sgW[v];
-        const W sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
-        const W sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
-        const W sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
-        const W dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
-        const W di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
-        pr = -di;
-        pi = dr;
+        W Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
+  #pragma unroll
+        for (int v = 0; v < V; ++v)
+  #pragma unroll
+          for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * sgW[v][q]; Si[q] += ti[v] * sgW[v][q]; }
+        // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
+        const W t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
+        const W t2r = b[0] * Sr[5] + b[1] * Sr[1] + b[2] * Sr[3], t2i = b[0] * Si[5] + b[1] * Si[1] + b[2] * Si[3];
+        const W t3r = b[0] * Sr[4] + b[1] * Sr[3] + b[2] * Sr[2], t3i = b[0] * Si[4] + b[1] * Si[3] + b[2] * Si[2];
+        const W Rr[3] = {-t1i, -t2i, -t3i}, Ri[3] = {t1r, t2r, t3r};
+        // Omega(k) in FP64 from the double k-vectors
+        const double Kv[6] = {ad[0] * ad[0], ad[1] * ad[1], ad[2] * ad[2], bd[1] * bd[2], bd[0] * bd[2], bd[0] * bd[1]};
+        double Qs[6];
+        if (qcub) {
+          const double s2 = Kv[0] + Kv[1] + Kv[2];
+  #pragma unroll
+          for (int q = 0; q < 3; ++q) Qs[q] = q_other * s2 + (q_own - q_other) * Kv[q];
+  #pragma unroll
+          for (int q = 3; q < 6; ++q) Qs[q] = q_off * Kv[q];
+        } else {
+  #pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            double acc = 0;
+  #pragma unroll
+            for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
+            Qs[q] = acc;
+          }
+        }
+        // symmetric [[a,d,e],[d,b,f],[e,f,c]] with a=Q11 b=Q22 c=Q33 d=Q12 e=Q13 f=Q23
+        const double qa = Qs[0], qb = Qs[1], qcc = Qs[2], qf = Qs[3], qe = Qs[4], qd = Qs[5];
+        const double i00 = qb * qcc - qf * qf, i01 = qe * qf - qcc * qd, i02 = qd * qf - qb * qe;
+        const double i11 = qa * qcc - qe * qe, i12 = qd * qe - qa * qf, i22 = qa * qb - qd * qd;
+        const double det = qa * i00 + qd * i01 + qe * i02;  // singular Q(k): k_lf_qcheck's error
+        const double rd = recip_nr(det);
+        const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
+                            {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
+                            {(W)(i02 * rd), (W)(i12 * rd), (W)(i22 * rd)}};
+  #pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
+          ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
+        }
       }
-      phr[v] = pr;
-      phi_[v] = pi;
-      e[v * TM] = mk((R)pr, (R)pi);
+      W phr[V], phi_[V];
+  #pragma unroll
+      for (int v = 0; v < V; ++v) {
+        W pr = 0, pi = 0;
+        if (a.homog && !k0) {
+          const W* sg = sgW[v];
+          const W sb0 = sg[0] * b[0] + sg[5] * b[1] + sg[4] * b[2];
+          const W sb1 = sg[5] * b[0] + sg[1] * b[1] + sg[3] * b[2];
+          const W sb2 = sg[4] * b[0] + sg[3] * b[1] + sg[2] * b[2];
+          const W dr = sb0 * ur[0] + sb1 * ur[1] + sb2 * ur[2];
+          const W di = sb0 * ui[0] + sb1 * ui[1] + sb2 * ui[2];
+          pr = -di;
+          pi = dr;
+        }
+        phr[v] = pr;
+        phi_[v] = pi;
+        e[v * TM] = mk((R)pr, (R)pi);
+      }
+      if (a.homog && a.energy && !k0 && !nyq) {
+        // Khachaturyan's quadratic form: with equilibrium u^ and homogeneous C0,
+        // e*.C0.e = sum_pq A_pq Re(theta^_p* theta^_q) - sum_p Re(theta^_p* phi^_p),
+        // A_pq = eps0_p.C0.eps0_q.  It needs the strain's and Q(k)'s k-vectors to agree,
+        // which they do off the Nyquist planes (k_space zeroes b there but not a).
+        W qq = 0;
+  #pragma unroll
+        for (int pv = 0; pv < V; ++pv) {
+          qq -= tr[pv] * phr[pv] + ti[pv] * phi_[pv];
+  #pragma unroll
+          for (int qv = 0; qv < V; ++qv) qq += aW[pv][qv] * (tr[pv] * tr[qv] + ti[pv] * ti[qv]);
+        }
+        elen += (double)((W)0.5 * w * qq);
+      } else if (a.homog && a.energy) {
+        // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
+        const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
+        W er[6], ei[6];
+  #pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const int ii = I1[q], jj = J1[q];
+          W gr, gi;
+          if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
+          else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
+  #pragma unroll
+          for (int v = 0; v < V; ++v) { gr -= tr[v] * epW[v][q]; gi -= ti[v] * epW[v][q]; }
+          if (k0) gr += ebW[q];
+          er[q] = gr;
+          ei[q] = gi;
+        }
+        W qq = 0;
+  #pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          W cr2 = 0, ci2 = 0;
+  #pragma unroll
+          for (int j = 0; j < 6; ++j) { cr2 += c0W[r + j * 6] * er[j]; ci2 += c0W[r + j * 6] * ei[j]; }
+          qq += er[r] * cr2 + ei[r] * ci2;
+        }
+        elen += (double)((W)0.5 * w * qq);
+      }
+      // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
+      W nr = 0, ni = 0;
+      if (!k0) {
+        const double k2d = ad[0] * ad[0] + ad[1] * ad[1] + ad[2] * ad[2];
+        const Damp<W> rden(recip_ge1(1.0 + dmd * kapcd * k2d * k2d));
+        const W dk2 = (W)(dmd * k2d);
+        const W mr = lan_a * cr - hlb * str, mi = lan_a * ci - hlb * sti;
+        nr = rden(cr - dk2 * mr);
+        ni = rden(ci - dk2 * mi);
+      }
+      const C cn = mk((R)nr, (R)ni);
+      a.Kc_out[p * PL + m] = cn;
+      e[V * TM] = cn;
     }
-    if (a.homog && a.energy && !k0 && !nyq) {
-      // Khachaturyan's quadratic form: with equilibrium u^ and homogeneous C0,
-      // e*.C0.e = sum_pq A_pq Re(theta^_p* theta^_q) - sum_p Re(theta^_p* phi^_p),
-      // A_pq = eps0_p.C0.eps0_q.  It needs the strain's and Q(k)'s k-vectors to agree,
-      // which they do off the Nyquist planes (k_space zeroes b there but not a).
-      W qq = 0;
-#pragma unroll
-      for (int pv = 0; pv < V; ++pv) {
-        qq -= tr[pv] * phr[pv] + ti[pv] * phi_[pv];
-#pragma unroll
-        for (int qv = 0; qv < V; ++qv) qq += aW[pv][qv] * (tr[pv] * tr[qv] + ti[pv] * ti[qv]);
-      }
-      elen += (double)((W)0.5 * w * qq);
-    } else if (a.homog && a.energy) {
-      // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
-      const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
-      W er[6], ei[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const int ii = I1[q], jj = J1[q];
-        W gr, gi;
-        if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
-        else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
-#pragma unroll
-        for (int v = 0; v < V; ++v) { gr -= tr[v] * epW[v][q]; gi -= ti[v] * epW[v][q]; }
-        if (k0) gr += ebW[q];
-        er[q] = gr;
-        ei[q] = gi;
-      }
-      W qq = 0;
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        W cr2 = 0, ci2 = 0;
-#pragma unroll
-        for (int j = 0; j < 6; ++j) { cr2 += c0W[r + j * 6] * er[j]; ci2 += c0W[r + j * 6] * ei[j]; }
-        qq += er[r] * cr2 + ei[r] * ci2;
-      }
-      elen += (double)((W)0.5 * w * qq);
-    }
-    // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
-    W nr = 0, ni = 0;
-    if (!k0) {
-      const double k2d = ad[0] * ad[0] + ad[1] * ad[1] + ad[2] * ad[2];
-      const Damp<W> rden(recip_ge1(1.0 + dmd * kapcd * k2d * k2d));
-      const W dk2 = (W)(dmd * k2d);
-      const W mr = lan_a * cr - hlb * str, mi = lan_a * ci - hlb * sti;
-      nr = rden(cr - dk2 * mr);
-      ni = rden(ci - dk2 * mi);
-    }
-    const C cn = mk((R)nr, (R)ni);
-    a.Kc_out[p * PL + m] = cn;
-    e[V * TM] = cn;
   }
   __syncthreads();
   fz::dit_range<C, N, LN, 1, LS, NT, PV, 1, NS - 1>(buf, tw);
@@ -467,6 +797,8 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
+  step_dep_wait();
+  step_dep_release();
   __syncthreads();
   P::inverse_head(buf, tws, mp);
   // constants of the driving force in registers; pointwise math in the field precision W
@@ -582,6 +914,9 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
   __shared__ double g[V][9];
   __shared__ int sameg;  // every variant has the gradient coefficients of variant 0
   const int64_t m0 = (int64_t)blockIdx.x * TM;
+  // the eta^ state was written by the previous step's Z2, which has completed once this
+  // block runs (PB released it only after its own wait), and PB does not touch it: the
+  // tile load overlaps PB's last blocks (L2 reads, cp.async.cg)
   tile_load<C, N, TM>(ks, LN, 0, a.Keta, NK, PL, m0, V);
   fz::cp_async_commit();
   if (threadIdx.x == 0) {
@@ -594,6 +929,8 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
     sameg = same;
   }
   for (int i = threadIdx.x; i < N * Tw<C>::K; i += NT) tw[i] = a.twz[i];
+  step_dep_wait();
+  step_dep_release();
   __syncthreads();
   // DIF stage 0: butterflies from global memory (column-fastest: coalesced rows)
 #pragma unroll 1
@@ -673,11 +1010,12 @@ __global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restri
 }
 
 // ------------------------------------------------------------------ PI
-// Block (z, f < V): eta_new_f -> real, eta statistics.  Block (z, V): dc_new
-// -> real, concentration statistics.
+// Block (z, f < V): eta_new_f -> real, eta statistics, and theta_f = eta_f^2 -> forward
+// for the next step (which then starts at its column kernel).  The concentration plane
+// and the end of the step are k_lf_pc's.
 template <typename R, int N, int PV, int NTP>
 __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
-    k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
+    k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V) {
   using P = fz::Plane<R, N, NTP, PV>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
@@ -688,57 +1026,92 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
+  step_dep_wait();
+  step_dep_release();
   __syncthreads();
   P::inverse_head(buf, tws, mp);
-  R* dst = (f < V) ? a.eta_next + f * N3 + z * PL : a.c_next + z * PL;
-  double emax = 0.0, s2 = 0.0, cmin = 1.0, cmax = 0.0, csum = 0.0;
-  const double cbar = a.F->cbar;
-  if (f < V) {
-    // new eta_f out, its statistics, and theta_f = eta_f^2 -> forward for the next
-    // step (which then starts at its column kernel)
-    P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
-      C* row = (C*)(dst + (int64_t)y * N);
+  R* dst = a.eta_next + f * N3 + z * PL;
+  double emax = 0.0, s2 = 0.0;
+  P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
+    C* row = (C*)(dst + (int64_t)y * N);
 #pragma unroll
-      for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
-        const C v = x[r];
-        row[n0 + r * dn] = v;
-        emax = fmax(emax, fmax((double)v.x, (double)v.y));
-        s2 += (double)v.x * v.x + (double)v.y * v.y;
-        x[r] = mk((R)((double)v.x * (double)v.x), (R)((double)v.y * (double)v.y));
-      }
-    });
-    P::forward_tail(buf, tws, mp);
-  } else {
-    P::template x_stage0<false>(buf, tws, [&](int y, int n0, int dn, C* x) {
-      C* row = (C*)(dst + (int64_t)y * N);
-#pragma unroll
-      for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
-        const C v = x[r];
-        row[n0 + r * dn] = v;
-        const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
-        cmin = fmin(cmin, fmin(c0, c1));
-        cmax = fmax(cmax, fmax(c0, c1));
-        csum += c0 + c1;
-      }
-    });
-  }
+    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+      const C v = x[r];
+      row[n0 + r * dn] = v;
+      emax = fmax(emax, fmax((double)v.x, (double)v.y));
+      s2 += (double)v.x * v.x + (double)v.y * v.y;
+      x[r] = mk((R)((double)v.x * (double)v.x), (R)((double)v.y * (double)v.y));
+    }
+  });
+  P::forward_tail(buf, tws, mp);
+  // the concentration quantities of this block's partial slot hold their start values
   const int blk = z * (V + 1) + f;
   block_reduce_store(emax, 1, a.partials + LQ_PHIMAX * PSTRIDE + blk);
   block_reduce_store(s2, 0, a.partials + LQ_SOLID * PSTRIDE + blk);
+  if (threadIdx.x == 0) {
+    a.partials[LQ_CMIN * PSTRIDE + blk] = 1.0;
+    a.partials[LQ_CMAX * PSTRIDE + blk] = 0.0;
+    a.partials[LQ_CSUM * PSTRIDE + blk] = 0.0;
+  }
+}
+
+// ------------------------------------------------------------------ PC
+// Block z: dc_new -> real, concentration statistics; the member's last block ends the
+// step.  PC reads only the dc^ spectrum (Z1's) and writes only dc and its partial slots,
+// none of which PI touches, so it runs beside PI: launched right after it with
+// programmatic dependent launch, its blocks take the slots PI's single wave leaves free,
+// and only the member's last block waits for PI (griddepcontrol.wait) before it reduces
+// every block partial of the step in a fixed order into history row *hist_row and
+// advances the row (so graph replays need no host-side row index).  That block's wait
+// also makes PC's completion imply PI's, which the next step's Z1 relies on.
+template <typename R, int N, int PV, int NTP>
+__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
+    k_lf_pc(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
+  using P = fz::Plane<R, N, NTP, PV>;
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw;
+  C* tws = buf + P::ELEMS;
+  const int z = blockIdx.x;
+  constexpr int64_t PL = (int64_t)N * N, NK = (int64_t)N * N * P::NXH;
+  C* mp = a.M + V * NK + z * (int64_t)N * P::NXH;
+  P::load_tw(tws, a.twx, a.twy, a.post);
+  step_dep_release();
+  __syncthreads();
+  P::inverse_head(buf, tws, mp);
+  R* dst = a.c_next + z * PL;
+  double cmin = 1.0, cmax = 0.0, csum = 0.0;
+  const double cbar = a.F->cbar;
+  P::template x_stage0<false>(buf, tws, [&](int y, int n0, int dn, C* x) {
+    C* row = (C*)(dst + (int64_t)y * N);
+#pragma unroll
+    for (int r = 0; r < fz::StageOf<P::LX, 0, PV>::R; ++r) {
+      const C v = x[r];
+      row[n0 + r * dn] = v;
+      const double c0 = cbar + (double)v.x, c1 = cbar + (double)v.y;
+      cmin = fmin(cmin, fmin(c0, c1));
+      cmax = fmax(cmax, fmax(c0, c1));
+      csum += c0 + c1;
+    }
+  });
+  const int blk = z * (V + 1) + V;
+  if (threadIdx.x == 0) {
+    a.partials[LQ_PHIMAX * PSTRIDE + blk] = 0.0;
+    a.partials[LQ_SOLID * PSTRIDE + blk] = 0.0;
+  }
   block_reduce_store(cmin, 2, a.partials + LQ_CMIN * PSTRIDE + blk);
   block_reduce_store(cmax, 1, a.partials + LQ_CMAX * PSTRIDE + blk);
   block_reduce_store(csum, 0, a.partials + LQ_CSUM * PSTRIDE + blk);
-  // ---- finalisation of the step: the member's last PI block reduces every block
-  // partial of the step in a fixed order into history row *hist_row and advances it
-  // (so graph replays need no host-side row index)
   __shared__ int last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    last = atomicAdd(a.ticket, 1) == (int)(gridDim.x * gridDim.y) - 1;
+    last = atomicAdd(a.ticket, 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
   if (!last) return;
+  step_dep_wait();  // PI complete, its partials visible
   __threadfence();
   const int row = *(volatile const int*)a.hist_row;
   // every thread loads its strided share of every quantity at once (all loads in flight
@@ -795,6 +1168,23 @@ struct Scope {
   }
 };
 
+// launch of a per-step kernel, with programmatic dependent launch when `dep` is set
+template <typename... P, typename... Args>
+void launch_step_kernel(void (*k)(P...), dim3 grid, int threads, size_t smem, cudaStream_t st, bool dep,
+                        Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = dep ? 1 : 0;
+  MEU_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
+}
+
 template <typename K>
 void ensure_smem(K fn, size_t bytes) {
   if (bytes <= 48 * 1024) return;
@@ -823,14 +1213,22 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   const double mm = (double)members;
   const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
   const size_t sp = P::smem_bytes();
-  const size_t s1 = sizeof(C) * ((size_t)N * z1_row_stride<R, N, V, TM>() + N * Tw<C>::K);
+  const size_t s1 = z1_smem_base<R, N, V, TM>() + (z1_prefetch<R, N, V, TM>() ? z1_smem_stage<R, N, V, TM>() : 0);
   const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
   const size_t spb = pb_smem<R, N, V, PV, NTP>();
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_pb<R, N, V, PV, NTP>, spb);
   ensure_smem(k_lf_pi<R, N, PV, NTP>, sp);
+  ensure_smem(k_lf_pc<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_z1<R, N, V, PV, TM>, s1);
   ensure_smem(k_lf_z2<R, N, V, PV, TM>, s2);
+  // Programmatic dependent launch of the four step kernels, except with per-kernel timing
+  // (which keeps them apart).  With 256-thread plane kernels (three per SM), letting Z1
+  // start in PI's last wave and PI in Z2's made deck 1 slower (171.6 -> 178.0 us per
+  // step), while PB after Z1 and Z2 after PB gained; with 512-thread plane kernels all
+  // four gain (180.7 -> 174.8 us, FP64 350.7 -> 339.0 us).
+  const bool dep = !(hook && hook->timing());
+  const bool dep_after_plane = dep && NTP >= 512;
   if (opts & LS_QCHECK) {
     Scope s(hook, "lf_qcheck", 0.0, st);
     k_lf_qcheck<R, N><<<dim3(148, 1, members), 256, 0, st>>>(dA);
@@ -844,18 +1242,15 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   }
   {
     Scope s(hook, "lf_z_green_ch", (2.0 * V + 3) * nk * sizeof(C), st);
-    k_lf_z1<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s1, st>>>(dA);
-    MEU_CHECK_LAUNCH();
+    launch_step_kernel(k_lf_z1<R, N, V, PV, TM>, dim3(tiles, 1, members), NT, s1, st, dep_after_plane, dA);
   }
   {
     Scope s(hook, "lf_plane_tdgl_rhs", (2.0 * V) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pb<R, N, V, PV, NTP><<<dim3(V, N, members), NTP, spb, st>>>(dA);
-    MEU_CHECK_LAUNCH();
+    launch_step_kernel(k_lf_pb<R, N, V, PV, NTP>, dim3(V, N, members), NTP, spb, st, dep, dA);
   }
   {
     Scope s(hook, "lf_z_tdgl", 4.0 * V * nk * sizeof(C), st);
-    k_lf_z2<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s2, st>>>(dA);
-    MEU_CHECK_LAUNCH();
+    launch_step_kernel(k_lf_z2<R, N, V, PV, TM>, dim3(tiles, 1, members), NT, s2, st, dep, dA);
   }
   NbList l;
   for (int q = 0; q < Q_TOTAL; ++q) l.nb[q] = 0;
@@ -865,9 +1260,12 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   l.nb[Q_FINT2] = tiles;
   l.nb[Q_CMIN] = l.nb[Q_CMAX] = l.nb[Q_PHIMAX] = l.nb[Q_SOLID] = l.nb[Q_CSUM0] = N * (V + 1);
   {
-    Scope s(hook, "lf_plane_inv_stats_theta", (2.0 * V + 1.0) * nk * sizeof(C) + (V + 1.0) * n3 * sizeof(R), st);
-    k_lf_pi<R, N, PV, NTP><<<dim3(N, V + 1, members), NTP, sp, st>>>(dA, V, l);
-    MEU_CHECK_LAUNCH();
+    Scope s(hook, "lf_plane_inv_stats_theta", (2.0 * V) * nk * sizeof(C) + (double)V * n3 * sizeof(R), st);
+    launch_step_kernel(k_lf_pi<R, N, PV, NTP>, dim3(N, V, members), NTP, sp, st, dep_after_plane, dA, V);
+  }
+  {
+    Scope s(hook, "lf_plane_inv_c_end", nk * sizeof(C) + n3 * sizeof(R), st);
+    launch_step_kernel(k_lf_pc<R, N, PV, NTP>, dim3(N, 1, members), NTP, sp, st, dep, dA, V, l);
   }
   for (int q = 0; q < Q_TOTAL; ++q) nb[q] = l.nb[q];
 }
@@ -892,6 +1290,11 @@ void run_init(const LanFusedArgs<R>* dA, int members, cudaStream_t st, LaunchHoo
   {
     Scope s(hook, "lf_z_state", 2.0 * (V + 1) * nk * sizeof(C), st);
     k_lf_z0<R, N, V, PV, TM><<<dim3(tiles, 1, members), NT, s0, st>>>(dA);
+    MEU_CHECK_LAUNCH();
+  }
+  if constexpr (V == 1) {
+    Scope s(hook, "lf_green_table", nk * sizeof(R), st);
+    k_lf_gtab<R, N, V, PV><<<dim3(2 * 148, 1, members), 256, 0, st>>>(dA);
     MEU_CHECK_LAUNCH();
   }
 }

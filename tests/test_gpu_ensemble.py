@@ -61,10 +61,10 @@ def test_ensemble_launches_per_bucket():
     n0 = ens.launch_count
     ens.run(16)
     buckets = len({(p.nx, p.nvar) for p, _, _ in ms})
-    # per bucket and step, whatever the member count: four kernels, plus the theta
+    # per bucket and step, whatever the member count: five kernels, plus the theta
     # transform on the first step after new fields and, on the ensemble's first step,
     # the one-time condition test of Q(k)
-    assert ens.launch_count - n0 == (6 + 15 * 4) * buckets
+    assert ens.launch_count - n0 == (7 + 15 * 5) * buckets
 
 
 @pytest.mark.gpu
