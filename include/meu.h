@@ -69,6 +69,7 @@ extern "C" {
 #define MEU_ERR_NOMEM 102
 #define MEU_ERR_UNSUPPORTED 103
 #define MEU_ERR_NOT_FINITE 104
+#define MEU_ERR_TIMEOUT 105 /* a bounded device-side wait ran out; the call's results are not valid */
 
 /*
  * Parameters consumed by the step (ModGparams.f:59-90 after the setup of

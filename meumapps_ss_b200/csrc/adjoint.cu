@@ -370,6 +370,7 @@ void Engine<R>::adjoint(int T, int K, const double* cons_tgt, const double* phi_
       a.twy = (const C*)fft->py.tw;
       a.twz = (const C*)fft->pz.tw;
       a.post = (const C*)fft->post_tw;
+      a.err = d_err;
       int nbq[Q_TOTAL];
       if (!adj_step<R>(N, a, st, &prof, nbq)) throw CudaError("adjoint not instantiated", MEU_ERR_UNSUPPORTED);
       NbList l;

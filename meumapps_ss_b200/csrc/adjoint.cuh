@@ -73,6 +73,7 @@ struct AdjArgs {
   const cplx<R>* twy;
   const cplx<R>* twz;
   const cplx<R>* post;
+  int* err;                   // the handle's error word (bounded waits that ran out)
 };
 
 enum AdjQ : int { AQ_X = 0, AQ_Y, AQ_Z, AQ_WG, AQ_EA, ADJ_Q };

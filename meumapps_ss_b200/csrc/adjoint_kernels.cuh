@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(NTP) k_ad_b(AdjArgs<R> a) {
   C* mp = a.M + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
   __syncthreads();
-  P::inverse_head(buf, tws, mp);
+  P::inverse_head(buf, tws, mp, a.err);
   const LanFusedConst& F = *a.F;
   const double dtl = F.dtl, cbar = F.cbar, s0 = F.sig0_ebar[0], A11 = F.A[0][0];
   double wg = 0, ea = 0;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(NTP) k_ad_d(AdjArgs<R> a) {
   C* mp = a.M + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
   __syncthreads();
-  P::inverse_head(buf, tws, mp);
+  P::inverse_head(buf, tws, mp, a.err);
   const int64_t off = z * PL;
   auto lam = [&](int y, int n0, int dn, C* x) {
 #pragma unroll
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(NTP) k_ad_b1_v(AdjArgs<R> a) {
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
   __syncthreads();
-  P::inverse_head(buf, tws, a.M + v * NK + z * (int64_t)N * P::NXH);
+  P::inverse_head(buf, tws, a.M + v * NK + z * (int64_t)N * P::NXH, a.err);
   R* dst = a.wv + v * N3 + z * PL;
   P::template x_stage0<false>(buf, tws, [&](int y, int n0, int dn, C* x) {
 #pragma unroll
@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(NTP) k_ad_d_v(AdjArgs<R> a) {
   C* mp = a.M + q * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
   __syncthreads();
-  P::inverse_head(buf, tws, mp);
+  P::inverse_head(buf, tws, mp, a.err);
   const int64_t off = q * N3 + z * PL;
   auto lam = [&](int y, int n0, int dn, C* x) {
 #pragma unroll

@@ -558,6 +558,7 @@ void Engine<R>::check_err() {
   if (*h_err) {
     int code = *h_err;
     MEU_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    if (code == MEU_ERR_TIMEOUT) throw CudaError("a bounded device-side wait ran out in the step", code);
     throw CudaError("singular matrix in the step (reference err_flag " + std::to_string(code) + ")", code);
   }
 }

@@ -14,6 +14,7 @@
 // between their forward and inverse passes.  Nothing outside the fused step
 // sees this layout.
 #pragma once
+#include "../../include/meu.h"
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -232,6 +233,41 @@ __device__ __forceinline__ void cp_async_span(C* smem, const C* gmem, int n) {
   constexpr int PER = 16 / sizeof(C);
   for (int i = threadIdx.x; i < n / PER; i += NT) cp_async16(smem + i * PER, gmem + i * PER);
 }
+// ------------------------------------------------------- bulk copies (TMA engine)
+// One bulk copy of a contiguous span into shared memory, issued by one thread and
+// completed on an mbarrier (transaction count = bytes).  No multicast: the source is
+// this GPU's own global memory.  Both addresses 16-byte aligned, n a multiple of 16.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init1(uint64_t* mb) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mb)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned n, uint64_t* mb) {
+  // earlier generic-proxy accesses of dst are ordered before the async-proxy writes
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mb)), "r"(n) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(n), "r"(smem_u32(mb))
+               : "memory");
+}
+// Wait for phase `parity` of mb to complete, at most `limit` polls (each try_wait
+// suspends for a bounded time); false if it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity, int limit) {
+  for (int i = 0; i < limit; ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(mb)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+// polls of a bulk-copy wait before the block records MEU_ERR_TIMEOUT (far above any copy)
+constexpr int BULK_WAIT_POLLS = 1 << 18;
+
 // 16-byte vector store of n complex (n even, 16-byte aligned)
 template <typename C, int NT>
 __device__ __forceinline__ void store_span(C* gmem, const C* smem, int n) {
@@ -362,18 +398,27 @@ struct Plane {
   static constexpr int NSX = rplan(LX, PV).ns, NSY = rplan(NY, PV).ns;
 
   // Inverse of an M-form plane in global memory (src) into shared memory, every
-  // stage except the x transform's stage 0.  Ends with a barrier.
-  static __device__ __forceinline__ void inverse_head(C* buf, const C* tws, const C* __restrict__ src) {
+  // stage except the x transform's stage 0.  Ends with a barrier.  Once per block: the
+  // plane arrives by one bulk copy on the block's mbarrier; a wait that runs out records
+  // MEU_ERR_TIMEOUT in *err.
+  static __device__ __forceinline__ void inverse_head(C* buf, const C* tws, const C* __restrict__ src, int* err) {
     const C* twx = tws;
     const C* twy = tws + LX * K;
     const C* post = tws + (LX + NY) * K;
     static_assert(NSY >= 2, "the streaming plane needs a y plan of two stages or more");
     using SY = StageOf<NY, NSY - 1, PV>;  // first executed y stage (M = 1: no twiddles)
-    // the whole plane in flight at once (16-byte asynchronous copies), then the first
-    // stage in place; columns 0 and LX (Hermitian in ky) are packed as X0 + i XN, so the
-    // y transform runs over LX columns; its column 0 then holds x0 + i xN, both real
-    load_m(buf, src);
-    cp_async_wait_all();
+    // the whole plane in one bulk copy, then the first stage in place; columns 0 and LX
+    // (Hermitian in ky) are packed as X0 + i XN, so the y transform runs over LX
+    // columns; its column 0 then holds x0 + i xN, both real
+    static_assert((ELEMS * sizeof(C)) % 16 == 0, "bulk copy size");
+    __shared__ uint64_t mb;
+    if (threadIdx.x == 0) mbar_init1(&mb);
+    __syncthreads();
+    if (threadIdx.x == 0) bulk_load(buf, src, (unsigned)(ELEMS * sizeof(C)), &mb);
+    if (!mbar_wait(&mb, 0, BULK_WAIT_POLLS)) {
+      if (err) atomicMax(err, MEU_ERR_TIMEOUT);
+      mbar_wait(&mb, 0, BULK_WAIT_POLLS);  // the copy's own completion, bounded too
+    }
     __syncthreads();
 #pragma unroll 1
     for (int t = threadIdx.x; t < LX * SY::TASKS; t += NT) {

@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   step_dep_wait();
   step_dep_release();
   __syncthreads();
-  P::inverse_head(buf, tws, mp);
+  P::inverse_head(buf, tws, mp, a.err);
   // constants of the driving force in registers; pointwise math in the field precision W
   using W = R;
   const LanFusedConst& F = *a.F;
@@ -1029,7 +1029,7 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   step_dep_wait();
   step_dep_release();
   __syncthreads();
-  P::inverse_head(buf, tws, mp);
+  P::inverse_head(buf, tws, mp, a.err);
   R* dst = a.eta_next + f * N3 + z * PL;
   double emax = 0.0, s2 = 0.0;
   P::template x_stage0<true>(buf, tws, [&](int y, int n0, int dn, C* x) {
@@ -1079,7 +1079,7 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   P::load_tw(tws, a.twx, a.twy, a.post);
   step_dep_release();
   __syncthreads();
-  P::inverse_head(buf, tws, mp);
+  P::inverse_head(buf, tws, mp, a.err);
   R* dst = a.c_next + z * PL;
   double cmin = 1.0, cmax = 0.0, csum = 0.0;
   const double cbar = a.F->cbar;
