@@ -398,8 +398,19 @@ __device__ __forceinline__ W nyq_strain_energy(const W* tr, const W* ti, const W
 // operator and Cahn-Hilliard update of the dc^ state (read and written in global
 // memory by the k-space pass), z iFFT of phi^_v and dc^ (the last DIT stage
 // straight to global memory).
+// resident Z1 blocks per SM it is compiled for: as many as its shared memory allows
+// (dynamic tile, 2 KB for its static arrays, 1 KB the runtime reserves per block), at
+// most 3 (80 registers a thread).  A bound above what fits would cap the registers for
+// nothing (FP64, 3 variants: 2 blocks fit, and a 3-block bound spilled 480 bytes)
+template <typename R, int N, int V, int TM>
+constexpr int z1_min_blocks() {
+  constexpr size_t bytes = z1_smem_base<R, N, V, TM>() + (z1_prefetch<R, N, V, TM>() ? z1_smem_stage<R, N, V, TM>() : 0);
+  constexpr int by_smem = (int)((228 * 1024) / (bytes + 1024 + 2048));
+  return by_smem < 1 ? 1 : (by_smem < 3 ? by_smem : 3);
+}
+
 template <typename R, int N, int V, int PV, int TM>
-__global__ void __launch_bounds__(NT, 3) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
+__global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM, LV = V * TM;
@@ -896,8 +907,22 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
 // writes straight back; the last DIF stage, the state update and the first DIT
 // stage touch the same elements of one butterfly, so they run on its registers.
 // With a two-stage radix plan a column makes two shared-memory round trips.
+// Z2's shared memory and the resident blocks per SM it is compiled for: as many as its
+// tile allows (with 2 KB for static arrays and the 1 KB runtime reserve), at most 4 (64
+// registers a thread) with up to three variants in FP32, else 3
+template <typename R, int N, int V, int TM>
+constexpr size_t z2_smem() {
+  return sizeof(cplx<R>) * (2 * (size_t)N * V * TM + N * Tw<cplx<R>>::K);
+}
+template <typename R, int N, int V, int TM>
+constexpr int z2_min_blocks() {
+  constexpr int by_smem = (int)(SM_SMEM / (z2_smem<R, N, V, TM>() + BLOCK_RESERVED + 2048));
+  constexpr int cap = (sizeof(R) == 4 && V <= 3) ? 4 : 3;
+  return by_smem < 1 ? 1 : (by_smem < cap ? by_smem : cap);
+}
+
 template <typename R, int N, int V, int PV, int TM>
-__global__ void __launch_bounds__(NT, 3) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
+__global__ void __launch_bounds__(NT, (z2_min_blocks<R, N, V, TM>())) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
   using C = cplx<R>;
   const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NXH = N / 2 + 1, LN = V * TM;
@@ -1214,7 +1239,7 @@ void run_step(const LanFusedArgs<R>* dA, int members, int opts, cudaStream_t st,
   const double n3 = (double)N * N * N * mm, nk = (double)N * N * NXH * mm;
   const size_t sp = P::smem_bytes();
   const size_t s1 = z1_smem_base<R, N, V, TM>() + (z1_prefetch<R, N, V, TM>() ? z1_smem_stage<R, N, V, TM>() : 0);
-  const size_t s2 = sizeof(C) * (2 * (size_t)N * V * TM + N * Tw<C>::K);
+  const size_t s2 = z2_smem<R, N, V, TM>();
   const size_t spb = pb_smem<R, N, V, PV, NTP>();
   ensure_smem(k_lf_pf<R, N, PV, NTP>, sp);
   ensure_smem(k_lf_pb<R, N, V, PV, NTP>, spb);
