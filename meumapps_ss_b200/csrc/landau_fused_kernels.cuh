@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
     // barrier between them): the Cahn-Hilliard update reads theta^ and writes slot V, then
     // the elastic pass overwrites theta^ with phi^.  Split, each pass keeps fewer values live.
     // ---- Cahn-Hilliard on the fluctuation state: mu^ = A dc^ - B/2 sum theta^
-  #pragma unroll 1
+#pragma unroll 1
     for (int i = threadIdx.x; i < N * TM; i += NT) {
       const int p = i / TM, c = i - p * TM;
       const int64_t m = m0 + c;
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
       const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
       C* e = buf + p * LS + c;
       W str = 0, sti = 0;
-  #pragma unroll
+#pragma unroll
       for (int v = 0; v < V; ++v) {
         const W tr = (W)e[v * TM].x * s, ti = (W)e[v * TM].y * s;
         str += tr;
@@ -535,12 +535,12 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
       e[V * TM] = cn;
     }
     // ---- homogeneous elasticity: phi^_v = sum_u T_vu theta^_u from the Green-operator table
-  #pragma unroll 1
+#pragma unroll 1
     for (int i = threadIdx.x; i < N * TM; i += NT) {
       const int p = i / TM, c = i - p * TM;
       C* e = buf + p * LS + c;
       if (!a.homog) {
-  #pragma unroll
+#pragma unroll
         for (int v = 0; v < V; ++v) e[v * TM] = mk((R)0, (R)0);
         continue;
       }
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
       const int kx = fz::kx_of_col<N, PV>(cx), ky = fz::rev<N, PV>(py), kz = fz::rev<N, PV>(p);
       const bool k0 = (kx == 0 && ky == 0 && kz == 0);
       W tr[V], ti[V];
-  #pragma unroll
+#pragma unroll
       for (int v = 0; v < V; ++v) {
         tr[v] = (W)e[v * TM].x * s;
         ti[v] = (W)e[v * TM].y * s;
@@ -558,19 +558,19 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
       {
         W T[V][V];
         int q = 0;
-  #pragma unroll
+#pragma unroll
         for (int v = 0; v < V; ++v)
-  #pragma unroll
+#pragma unroll
           for (int u = v; u < V; ++u) {
             const W t = k0 ? (W)0 : PRE ? (W)lds<R>(gts + (q * N + p) * TM + c) : (W)__ldg(a.gtab + q * NK + p * PL + m);
             T[v][u] = t;
             T[u][v] = t;
             ++q;
           }
-  #pragma unroll
+#pragma unroll
         for (int v = 0; v < V; ++v) {
           W pr = 0, pi = 0;
-  #pragma unroll
+#pragma unroll
           for (int u = 0; u < V; ++u) {
             pr += T[v][u] * tr[u];
             pi += T[v][u] * ti[u];
@@ -589,10 +589,10 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
         // A_pq = eps0_p.C0.eps0_q.  It needs the strain's and Q(k)'s k-vectors to agree,
         // which they do off the Nyquist planes (k_space zeroes b there but not a).
         W qq = 0;
-  #pragma unroll
+#pragma unroll
         for (int pv = 0; pv < V; ++pv) {
           qq -= tr[pv] * phr[pv] + ti[pv] * phi_[pv];
-  #pragma unroll
+#pragma unroll
           for (int qv = 0; qv < V; ++qv) qq += aW[pv][qv] * (tr[pv] * tr[qv] + ti[pv] * ti[qv]);
         }
         elen += (double)((W)0.5 * w * qq);
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
       const W w = (kx == 0 || 2 * kx == N) ? (W)1 : (W)2;
       C* e = buf + p * LS + c;
       W tr[V], ti[V], str = 0, sti = 0;
-  #pragma unroll
+#pragma unroll
       for (int v = 0; v < V; ++v) {
         tr[v] = (W)e[v * TM].x * s;
         ti[v] = (W)e[v * TM].y * s;
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
         sti += ti[v];
       }
       if (a.rec_theta) {
-  #pragma unroll
+#pragma unroll
         for (int v = 0; v < V; ++v) a.rec_theta[v * NK + p * PL + m] = mk((R)tr[v], (R)ti[v]);
       }
       const C cs = a.Kc[p * PL + m];
@@ -640,9 +640,9 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
       W ur[3] = {0, 0, 0}, ui[3] = {0, 0, 0};
       if (a.homog && !k0) {
         W Sr[6] = {0, 0, 0, 0, 0, 0}, Si[6] = {0, 0, 0, 0, 0, 0};
-  #pragma unroll
+#pragma unroll
         for (int v = 0; v < V; ++v)
-  #pragma unroll
+#pragma unroll
           for (int q = 0; q < 6; ++q) { Sr[q] += tr[v] * sgW[v][q]; Si[q] += ti[v] * sgW[v][q]; }
         // R_i = i sum_j b_j S_ij (Voigt: 11,22,33,23,13,12)
         const W t1r = b[0] * Sr[0] + b[1] * Sr[5] + b[2] * Sr[4], t1i = b[0] * Si[0] + b[1] * Si[5] + b[2] * Si[4];
@@ -654,15 +654,15 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
         double Qs[6];
         if (qcub) {
           const double s2 = Kv[0] + Kv[1] + Kv[2];
-  #pragma unroll
+#pragma unroll
           for (int q = 0; q < 3; ++q) Qs[q] = q_other * s2 + (q_own - q_other) * Kv[q];
-  #pragma unroll
+#pragma unroll
           for (int q = 3; q < 6; ++q) Qs[q] = q_off * Kv[q];
         } else {
-  #pragma unroll
+#pragma unroll
           for (int q = 0; q < 6; ++q) {
             double acc = 0;
-  #pragma unroll
+#pragma unroll
             for (int n = 0; n < 6; ++n) acc += qc[q][n] * Kv[n];
             Qs[q] = acc;
           }
@@ -676,14 +676,14 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
         const W Qi[3][3] = {{(W)(i00 * rd), (W)(i01 * rd), (W)(i02 * rd)},
                             {(W)(i01 * rd), (W)(i11 * rd), (W)(i12 * rd)},
                             {(W)(i02 * rd), (W)(i12 * rd), (W)(i22 * rd)}};
-  #pragma unroll
+#pragma unroll
         for (int r = 0; r < 3; ++r) {
           ur[r] = Qi[r][0] * Rr[0] + Qi[r][1] * Rr[1] + Qi[r][2] * Rr[2];
           ui[r] = Qi[r][0] * Ri[0] + Qi[r][1] * Ri[1] + Qi[r][2] * Ri[2];
         }
       }
       W phr[V], phi_[V];
-  #pragma unroll
+#pragma unroll
       for (int v = 0; v < V; ++v) {
         W pr = 0, pi = 0;
         if (a.homog && !k0) {
@@ -706,10 +706,10 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
         // A_pq = eps0_p.C0.eps0_q.  It needs the strain's and Q(k)'s k-vectors to agree,
         // which they do off the Nyquist planes (k_space zeroes b there but not a).
         W qq = 0;
-  #pragma unroll
+#pragma unroll
         for (int pv = 0; pv < V; ++pv) {
           qq -= tr[pv] * phr[pv] + ti[pv] * phi_[pv];
-  #pragma unroll
+#pragma unroll
           for (int qv = 0; qv < V; ++qv) qq += aW[pv][qv] * (tr[pv] * tr[qv] + ti[pv] * ti[qv]);
         }
         elen += (double)((W)0.5 * w * qq);
@@ -717,23 +717,23 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
         // engineering elastic strain e = gamma(u^) - sum_v theta^_v eps0_v (+ e_mean at k = 0)
         const int I1[6] = {0, 1, 2, 1, 0, 0}, J1[6] = {0, 1, 2, 2, 2, 1};
         W er[6], ei[6];
-  #pragma unroll
+#pragma unroll
         for (int q = 0; q < 6; ++q) {
           const int ii = I1[q], jj = J1[q];
           W gr, gi;
           if (q < 3) { gr = -b[ii] * ui[ii]; gi = b[ii] * ur[ii]; }
           else { gr = -(b[ii] * ui[jj] + b[jj] * ui[ii]); gi = b[ii] * ur[jj] + b[jj] * ur[ii]; }
-  #pragma unroll
+#pragma unroll
           for (int v = 0; v < V; ++v) { gr -= tr[v] * epW[v][q]; gi -= ti[v] * epW[v][q]; }
           if (k0) gr += ebW[q];
           er[q] = gr;
           ei[q] = gi;
         }
         W qq = 0;
-  #pragma unroll
+#pragma unroll
         for (int r = 0; r < 6; ++r) {
           W cr2 = 0, ci2 = 0;
-  #pragma unroll
+#pragma unroll
           for (int j = 0; j < 6; ++j) { cr2 += c0W[r + j * 6] * er[j]; ci2 += c0W[r + j * 6] * ei[j]; }
           qq += er[r] * cr2 + ei[r] * ci2;
         }
