@@ -784,12 +784,14 @@ constexpr size_t pb_smem() {
 }
 
 // resident blocks per SM the plane kernels are compiled for: as many as shared memory
-// allows, at most 768 threads (85 registers a thread at 256 threads, 64 at 512)
+// allows, at most 4 of 256 threads (64 registers a thread; 128^3 FP32 planes fit 3, so
+// 80) or 2 of 512 (64).  Four 256-thread blocks on the 32^3-96^3 planes: deck 3
+// 1.798 -> 1.752 ms per step
 template <typename R, int N, int PV, int NTP>
 constexpr int plane_min_blocks() {
   constexpr size_t per = fz::Plane<R, N, NTP, PV>::smem_bytes() + BLOCK_RESERVED;
   constexpr int by_smem = (int)(SM_SMEM / per);
-  constexpr int by_threads = NTP >= 512 ? 2 : 3;
+  constexpr int by_threads = NTP >= 512 ? 2 : 4;
   return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
 }
 
