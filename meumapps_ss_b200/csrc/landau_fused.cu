@@ -112,7 +112,10 @@ LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool
       return it->second;
     }
   }
-  constexpr int WARM = 3, TIMED = 10, REPS = 2;  // best of REPS timings of TIMED steps
+  // Each candidate is timed the way a run executes it: a CUDA graph of GSTEPS steps
+  // (programmatic dependent launch inside), best of REPS replays after one warm replay.
+  // A stream that cannot be captured (the legacy default stream) times eager launches.
+  constexpr int WARM = 3, GSTEPS = 8, REPS = 3;
   cudaEvent_t e0, e1;
   MEU_CUDA(cudaEventCreate(&e0));
   MEU_CUDA(cudaEventCreate(&e1));
@@ -120,21 +123,53 @@ LanSched lan_autotune(int N, int V, const LanFusedArgs<R>* dA, int members, bool
   double best_t = 1e300;
   int nb[Q_TOTAL];
   const int eopt = energy ? LS_ENERGY : 0;
+  const int sopt = eopt | LS_THETA_READY;
   for (const LanSched& s : lan_sched_candidates(N, f64)) {
-    for (int i = 0; i < WARM; ++i)
-      if (!lan_fused_step<R>(N, V, s, dA, members, eopt | (i ? LS_THETA_READY : 0), st, nullptr, nb)) break;
-    for (int r = 0; r < REPS; ++r) {
-      MEU_CUDA(cudaEventRecord(e0, st));
-      for (int i = 0; i < TIMED; ++i) lan_fused_step<R>(N, V, s, dA, members, eopt | LS_THETA_READY, st, nullptr, nb);
-      MEU_CUDA(cudaEventRecord(e1, st));
-      MEU_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms / TIMED < best_t) {
-        best_t = ms / TIMED;
-        best = s;
+    bool ok = true;
+    for (int i = 0; i < WARM && ok; ++i)
+      ok = lan_fused_step<R>(N, V, s, dA, members, eopt | (i ? LS_THETA_READY : 0), st, nullptr, nb);
+    if (!ok) continue;
+    cudaGraphExec_t ge = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      cudaGraph_t g = nullptr;
+      try {
+        for (int i = 0; i < GSTEPS; ++i) lan_fused_step<R>(N, V, s, dA, members, sopt, st, nullptr, nb);
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
       }
+      if (cudaStreamEndCapture(st, &g) == cudaSuccess && g && cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+        ge = nullptr;
+      if (g) cudaGraphDestroy(g);
     }
+    (void)cudaGetLastError();  // a refused capture leaves its (non-sticky) error behind
+    auto steps = [&]() {
+      if (ge) {
+        MEU_CUDA(cudaGraphLaunch(ge, st));
+      } else {
+        for (int i = 0; i < GSTEPS; ++i) lan_fused_step<R>(N, V, s, dA, members, sopt, st, nullptr, nb);
+      }
+    };
+    try {
+      steps();
+      for (int r = 0; r < REPS; ++r) {
+        MEU_CUDA(cudaEventRecord(e0, st));
+        steps();
+        MEU_CUDA(cudaEventRecord(e1, st));
+        MEU_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        MEU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms / GSTEPS < best_t) {
+          best_t = ms / GSTEPS;
+          best = s;
+        }
+      }
+    } catch (...) {
+      if (ge) cudaGraphExecDestroy(ge);
+      throw;
+    }
+    if (ge) cudaGraphExecDestroy(ge);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
