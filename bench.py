@@ -332,17 +332,21 @@ def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0):
     out = {"workload": f"landau-ensemble-{ENS_MEMBERS}x1var"}
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     fields_out = {}
-    for prec in (P.PREC_F32, P.PREC_F64):
+    # legs: per-bucket kernels replayed as graphs (FP32 autotuned, FP64), and the FP32
+    # persistent launch (one launch per run of up to 64 steps, MEU_ENS_PERSISTENT)
+    legs = (("fp32_bulk", P.PREC_F32, True, False), ("fp64_plain", P.PREC_F64, False, False),
+            ("fp32_persistent", P.PREC_F32, False, True))
+    for key, prec, tune, pers in legs:
         ws = CF.ensemble_config(ENS_MEMBERS, precision=prec)
         cells = sum(w.params.nx ** 3 for w in ws)
-        ens = Ensemble([w.params for w in ws], autotune=prec == P.PREC_F32)
+        ens = Ensemble([w.params for w in ws], autotune=tune, persistent=pers)
         ens.set_stream(stream.cuda_stream)
         for i, w in enumerate(ws):
             ens.set_fields(i, *ensemble_fields(w))
         ens.run(W, diag=True)
         sampler = ClockSampler(local)
         torch.cuda.synchronize()
-        if prec == P.PREC_F32:
+        if key == "fp32_bulk":
             sampler.start()
             time.sleep(0.3)
         l0 = ens.launch_count
@@ -352,18 +356,27 @@ def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0):
         b.record(stream)
         stream.synchronize()
         ms = a.elapsed_time(b)
-        key = "fp32_bulk" if prec == P.PREC_F32 else "fp64_plain"
         out[key] = {"value": cells * K / (ms / 1e3) / 1e6, "unit": UNIT, "steps": K, "ms_per_step": ms / K,
                     "gpu_launches_per_step": (ens.launch_count - l0) / K}
-        if prec == P.PREC_F32:
+        if pers:
+            out[key]["schedule"] = list(ens.schedule(0)[:3])
+        if key == "fp32_bulk":
             out["clocks"] = sampler.stop()
             out["cells_per_step"] = cells
-        fields_out[prec] = [ens.get_fields(i)[:2] for i in range(len(ws))]
+        fields_out[key] = [ens.get_fields(i)[:2] for i in range(len(ws))]
         ens.close()
-    worst_c = max(float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64))
-                  for (c32, _), (c64, _) in zip(fields_out[P.PREC_F32], fields_out[P.PREC_F64]))
-    worst_e = max(float(np.linalg.norm(e32 - e64) / max(np.linalg.norm(e64), 1e-300))
-                  for (_, e32), (_, e64) in zip(fields_out[P.PREC_F32], fields_out[P.PREC_F64]))
+
+    def worst(k32):
+        wc = max(float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64))
+                 for (c32, _), (c64, _) in zip(fields_out[k32], fields_out["fp64_plain"]))
+        we = max(float(np.linalg.norm(e32 - e64) / max(np.linalg.norm(e64), 1e-300))
+                 for (_, e32), (_, e64) in zip(fields_out[k32], fields_out["fp64_plain"]))
+        return wc, we
+
+    worst_c, worst_e = worst("fp32_bulk")
+    pc, pe = worst("fp32_persistent")
+    out["fp32_persistent"]["err_vs_fp64"] = {"c_rel_l2_max_member": pc, "eta_rel_l2_max_member": pe,
+                                             "after_steps": W + K}
     out["fp32_speedup"] = out["fp32_bulk"]["value"] / out["fp64_plain"]["value"]
     out["err_vs_fp64"] = {"c_rel_l2_max_member": worst_c, "eta_rel_l2_max_member": worst_e, "after_steps": W + K}
     return out

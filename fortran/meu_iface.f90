@@ -112,7 +112,8 @@ module meu_iface
       type(c_ptr), value :: h
       integer(c_int32_t), intent(in) :: in3(3)
     end function
-    ! ensembles: params(n) decks stepped together (flags: MEU_ENS_AUTOTUNE = 1)
+    ! ensembles: params(n) decks stepped together (flags: MEU_ENS_AUTOTUNE = 1,
+    ! MEU_ENS_PERSISTENT = 2: one persistent launch per run of steps, one order parameter each)
     integer(c_int) function meu_ensemble_create(n, params, flags, e) bind(C, name="meu_ensemble_create")
       import :: c_int, c_int32_t, c_ptr, meu_params
       integer(c_int32_t), value :: n, flags

@@ -226,6 +226,14 @@ typedef struct meu_ensemble meu_ensemble;
 
 /* flags for meu_ensemble_create */
 #define MEU_ENS_AUTOTUNE 1 /* time the schedule variants of each bucket before any field is set */
+/* One persistent launch per run of up to 64 steps: every pass of every member, whatever
+ * its grid size, is a work item that the launch's blocks claim in order, each member's
+ * passes ordered by a device counter (no grid-wide barrier; every wait is bounded and
+ * ends in MEU_ERR_TIMEOUT).  One order parameter per member (MEU_ERR_UNSUPPORTED
+ * otherwise); every member runs the schedule (2, 256, 16 FP32 / 8 FP64) and gives the
+ * results of a single handle on that schedule.  Overrides MEU_ENS_AUTOTUNE.  The first
+ * step after new fields runs as per-bucket launches. */
+#define MEU_ENS_PERSISTENT 2
 
 int meu_ensemble_create(int32_t n_members, const meu_params* params, int32_t flags, meu_ensemble** out);
 /* fields of one member, layouts as meu_set_fields (no u_state: no heterogeneous elasticity) */

@@ -1,0 +1,3 @@
+// Persistent ensemble kernel in float (every grid size of the fused path, one order parameter).
+#include "ens_persist_impl.cuh"
+MEU_PK_INSTANTIATE(float)

@@ -5,13 +5,18 @@
 // branches, and runs of 8, 4, 2 or 1 whole-ensemble steps replay CUDA graphs.
 // An optional autotuner picks each bucket's schedule (radix plan, plane threads,
 // column tile) by timing the candidates on the bucket before the fields are set.
+// With MEU_ENS_PERSISTENT the warm steps of every member instead run as work items of
+// one persistent launch per run of up to PK_MAX_STEPS steps (ens_persist.cuh).
+#include <algorithm>
 #include <map>
 #include <memory>
+#include <numeric>
 #include <string>
 #include <tuple>
 #include <vector>
 
 #include "engine.cuh"
+#include "ens_persist.cuh"
 
 namespace meu {
 
@@ -67,6 +72,16 @@ class EnsembleT : public EnsembleBase {
   cudaGraphExec_t gexec[GRAPH_SLOTS] = {};   // 2^slot whole-ensemble steps
   int64_t graph_launches[GRAPH_SLOTS] = {};  // kernels in each graph
   bool warm = false;
+  // persistent mode: argument records of all members (member order), the work list of
+  // one step, and the launch's counters
+  bool persist = false;
+  std::vector<LanFusedArgs<R>> hAll;
+  LanFusedArgs<R>* dAll = nullptr;
+  PkMember* dMt = nullptr;
+  uint32_t* dItems = nullptr;
+  int* dNeed = nullptr;
+  int* dCtrl = nullptr;
+  int pkL = 0;
 
   void sync_args();
   void step_launches();
@@ -110,6 +125,14 @@ EnsembleT<R>::EnsembleT(int n, const meu_params* ps, int flags) {
     bk[b].idx.push_back(m);
     bucket_of.push_back(b);
   }
+  persist = (flags & MEU_ENS_PERSISTENT) != 0;
+  if (persist) {
+    if (n > PK_MAX_MEMBERS) throw CudaError("persistent ensemble: too many members", MEU_ERR_UNSUPPORTED);
+    for (int m = 0; m < n; ++m)
+      if (ps[m].nvar != PK_V)
+        throw CudaError("persistent ensemble member " + std::to_string(m) + ": one order parameter per member",
+                        MEU_ERR_UNSUPPORTED);
+  }
   MEU_CUDA(cudaStreamCreateWithFlags(&own_st, cudaStreamNonBlocking));
   st = own_st;
   MEU_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -118,9 +141,32 @@ EnsembleT<R>::EnsembleT(int n, const meu_params* ps, int flags) {
     MEU_CUDA(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
     MEU_CUDA(cudaMalloc(&b.dA, sizeof(LanFusedArgs<R>) * b.idx.size()));
   }
+  if (persist) {
+    // one schedule for every size: the persistent kernel's
+    for (Bucket& b : bk) {
+      b.sched.pv = PK_PV;
+      b.sched.ntp = PK_NTP;
+      b.sched.tm = pk_tm<R>();
+    }
+    std::vector<int> Ns(n), en(n);
+    for (int m = 0; m < n; ++m) {
+      Ns[m] = ps[m].nx;
+      en[m] = ps[m].diag_energy != 0 ? 1 : 0;
+    }
+    const PkPlan pl = pk_plan(Ns, en, sizeof(R) == 8);
+    pkL = (int)pl.items.size();
+    MEU_CUDA(cudaMalloc(&dAll, sizeof(LanFusedArgs<R>) * n));
+    MEU_CUDA(cudaMalloc(&dMt, sizeof(PkMember) * n));
+    MEU_CUDA(cudaMalloc(&dItems, sizeof(uint32_t) * pkL));
+    MEU_CUDA(cudaMalloc(&dNeed, sizeof(int) * pkL));
+    MEU_CUDA(cudaMalloc(&dCtrl, sizeof(int) * (2 + (size_t)n)));
+    MEU_CUDA(cudaMemcpy(dMt, pl.mt.data(), sizeof(PkMember) * n, cudaMemcpyHostToDevice));
+    MEU_CUDA(cudaMemcpy(dItems, pl.items.data(), sizeof(uint32_t) * pkL, cudaMemcpyHostToDevice));
+    MEU_CUDA(cudaMemcpy(dNeed, pl.need.data(), sizeof(int) * pkL, cudaMemcpyHostToDevice));
+  }
   for (auto& e : mem) MEU_CUDA(cudaStreamSynchronize(e->st));
   sync_args();
-  if (flags & MEU_ENS_AUTOTUNE) {
+  if ((flags & MEU_ENS_AUTOTUNE) && !persist) {
     for (Bucket& b : bk)
       b.sched = lan_autotune<R>(b.N, b.V, b.dA, (int)b.idx.size(), b.energy, st, nullptr);
     MEU_CUDA(cudaStreamSynchronize(st));
@@ -143,6 +189,8 @@ EnsembleT<R>::~EnsembleT() {
     if (b.bst) cudaStreamDestroy(b.bst);
   }
   if (fork) cudaEventDestroy(fork);
+  for (void* q : {(void*)dAll, (void*)dMt, (void*)dItems, (void*)dNeed, (void*)dCtrl})
+    if (q) cudaFree(q);
   prof.reset();
   mem.clear();
   if (own_st) cudaStreamDestroy(own_st);
@@ -162,6 +210,48 @@ void EnsembleT<R>::sync_args() {
     MEU_CUDA(cudaMemcpyAsync(b.dA, b.hA.data(), sizeof(LanFusedArgs<R>) * b.hA.size(), cudaMemcpyHostToDevice, st));
     MEU_CUDA(cudaStreamSynchronize(st));
   }
+  if (!persist) return;
+  std::vector<LanFusedArgs<R>> all(members);
+  for (const Bucket& b : bk)
+    for (size_t j = 0; j < b.idx.size(); ++j) all[b.idx[j]] = b.hA[j];
+  if (all.size() == hAll.size() && memcmp(all.data(), hAll.data(), sizeof(LanFusedArgs<R>) * all.size()) == 0) return;
+  hAll = all;
+  MEU_CUDA(cudaMemcpyAsync(dAll, hAll.data(), sizeof(LanFusedArgs<R>) * hAll.size(), cudaMemcpyHostToDevice, st));
+  MEU_CUDA(cudaStreamSynchronize(st));
+}
+
+// Work list of one step of the persistent kernel (see ens_persist.cuh): pass-major,
+// members of larger grids first within a pass.  need = the member's items of its earlier
+// passes: Z1 0, PB T, Z2 T + N, PI and PC 2T + N, END 2T + 3N (T column tiles).
+PkPlan pk_plan(const std::vector<int>& N, const std::vector<int>& energy, bool f64) {
+  PkPlan p;
+  const int n = (int)N.size(), tm = f64 ? pk_tm<double>() : pk_tm<float>();
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return N[a] > N[b]; });
+  p.mt.resize(n);
+  for (int m = 0; m < n; ++m) {
+    const int nn = N[m], t = nn * (nn / 2 + 1) / tm;
+    PkMember& q = p.mt[m];
+    q.N = nn;
+    q.per_step = 2 * t + 3 * nn + 1;
+    for (int k = 0; k < Q_TOTAL; ++k) q.nb.nb[k] = 0;
+    q.nb.nb[Q_FCH] = energy[m] ? nn : 0;
+    q.nb.nb[Q_FINT] = q.nb.nb[Q_ELEN] = q.nb.nb[Q_FINT2] = t;
+    q.nb.nb[Q_CMIN] = q.nb.nb[Q_CMAX] = q.nb.nb[Q_PHIMAX] = q.nb.nb[Q_SOLID] = q.nb.nb[Q_CSUM0] = nn * (PK_V + 1);
+  }
+  for (int kind = PK_Z1; kind <= PK_END; ++kind)
+    for (int m : order) {
+      const int nn = N[m], t = nn * (nn / 2 + 1) / tm;
+      const int count = (kind == PK_Z1 || kind == PK_Z2) ? t : kind == PK_END ? 1 : nn;
+      const int need = kind == PK_Z1 ? 0 : kind == PK_PB ? t : kind == PK_Z2 ? t + nn : kind == PK_END ? 2 * t + 3 * nn
+                                                                                                        : 2 * t + nn;
+      for (int i = 0; i < count; ++i) {
+        p.items.push_back(pk_item(m, kind, i));
+        p.need.push_back(need);
+      }
+    }
+  return p;
 }
 
 // one ensemble step: fork to the bucket streams, batched step, join
@@ -250,7 +340,12 @@ void EnsembleT<R>::run(int nsteps, meu_diag* diag) {
             break;
           }
       int k = 1;
-      if (slot >= 0) {
+      if (persist && can_replay()) {
+        k = std::min(chunk - i, PK_MAX_STEPS);
+        while (k > 1 && !homog_stable(k)) --k;
+        pk_launch<R>(dAll, dMt, dItems, dNeed, pkL, k, members, dCtrl, st);
+        prof.launches += 1;
+      } else if (slot >= 0) {
         if (!gexec[slot]) capture_graph(slot);
         MEU_CUDA(cudaGraphLaunch(gexec[slot], st));
         prof.launches += graph_launches[slot];
@@ -278,7 +373,7 @@ void EnsembleT<R>::run(int nsteps, meu_diag* diag) {
     }
     done += chunk;
   }
-  if (can_replay())
+  if (can_replay() && !persist)
     for (int sl = 0; sl < GRAPH_SLOTS; ++sl)
       if (!gexec[sl]) capture_graph(sl);
 }

@@ -242,6 +242,9 @@ __device__ __forceinline__ void mbar_init1(uint64_t* mb) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mb)) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
+__device__ __forceinline__ void mbar_inval(uint64_t* mb) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(mb)) : "memory");
+}
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned n, uint64_t* mb) {
   // earlier generic-proxy accesses of dst are ordered before the async-proxy writes
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -420,6 +423,9 @@ struct Plane {
       mbar_wait(&mb, 0, BULK_WAIT_POLLS);  // the copy's own completion, bounded too
     }
     __syncthreads();
+    // every thread is past its wait: the mbarrier is invalidated, so a block that runs
+    // several planes (the persistent ensemble kernel) initialises it afresh for the next
+    if (threadIdx.x == 0) mbar_inval(&mb);
 #pragma unroll 1
     for (int t = threadIdx.x; t < LX * SY::TASKS; t += NT) {
       const int c = t % LX, b = t / LX;

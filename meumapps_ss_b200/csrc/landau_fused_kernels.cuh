@@ -409,10 +409,11 @@ constexpr int z1_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem < 3 ? by_smem : 3);
 }
 
+// Z1 of column tile bx of one member (the kernel's body; the persistent ensemble kernel
+// runs it as one of its work items)
 template <typename R, int N, int V, int PV, int TM>
-__global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
+__device__ __forceinline__ void lf_z1_body(const LanFusedArgs<R>& a, const int bx) {
   using C = cplx<R>;
-  const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NF = V + 1, NXH = N / 2 + 1, LN = NF * TM, LV = V * TM;
   // row stride of the tile: LN padded so that consecutive rows start half the banks apart
   // (the k-space pass reads TM columns of several rows per warp)
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
   using W = R;
   __shared__ double qc[6][6];
   __shared__ W sgW[V][6], epW[V][6], c0W[36], ebW[6], aW[V][V];
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  const int64_t m0 = (int64_t)bx * TM;
   {
     const LanFusedConst& G = *a.F;
     for (int i = threadIdx.x; i < 36; i += NT) {
@@ -767,8 +768,13 @@ __global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(co
 #pragma unroll
     for (int r = 0; r < S0::R; ++r) dst[(int64_t)(j + r * S0::M) * PL] = x[r];
   }
-  block_reduce_store(fint, 0, a.partials + LQ_FINT * PSTRIDE + blockIdx.x);
-  block_reduce_store(elen, 0, a.partials + LQ_ELEN * PSTRIDE + blockIdx.x);
+  block_reduce_store(fint, 0, a.partials + LQ_FINT * PSTRIDE + bx);
+  block_reduce_store(elen, 0, a.partials + LQ_ELEN * PSTRIDE + bx);
+}
+template <typename R, int N, int V, int PV, int TM>
+__global__ void __launch_bounds__(NT, (z1_min_blocks<R, N, V, TM>())) k_lf_z1(const LanFusedArgs<R>* __restrict__ A) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  lf_z1_body<R, N, V, PV, TM>(a, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ PB
@@ -795,18 +801,16 @@ constexpr int plane_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
 }
 
-template <typename R, int N, int V, int PV, int NTP>
-__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
-    k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
+// PB of variant f, plane z of one member.  COH: the eta and dc planes may have been
+// written earlier in the same launch (the persistent ensemble kernel), so they are read
+// with coherent loads instead of the read-only path.
+template <typename R, int N, int V, int PV, int NTP, bool COH = false>
+__device__ __forceinline__ void lf_pb_body(const LanFusedArgs<R>& a, const int f, const int z) {
   using P = fz::Plane<R, N, NTP, PV>;
-  const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
-  // field index fastest: the V blocks of one plane, which read the same eta and
-  // dc planes, are resident together and share those reads through L2
-  const int f = blockIdx.x, z = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
@@ -890,8 +894,8 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
     const int64_t g0 = z * PL + (int64_t)y * N + 2 * n;
     C ev[V];
 #pragma unroll
-    for (int q = 0; q < V; ++q) ev[q] = __ldg((const C*)(a.eta + q * N3 + g0));
-    const C dcv = __ldg((const C*)(a.c + g0));
+    for (int q = 0; q < V; ++q) ev[q] = COH ? *(const C*)(a.eta + q * N3 + g0) : __ldg((const C*)(a.eta + q * N3 + g0));
+    const C dcv = COH ? *(const C*)(a.c + g0) : __ldg((const C*)(a.c + g0));
     const C ph = buf[y * P::PITCH + n];
     if (rec) ((C*)(rec + (int64_t)y * N))[n] = ph;
     if (bulk) bulk_energy(ev, dcv);
@@ -901,6 +905,14 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   P::x_forward0(buf, tws, [](int, int, int, C*) {});
   if (bulk) block_reduce_store(fch, 0, a.partials + LQ_FCH * PSTRIDE + z);
   P::forward_tail(buf, tws, mp);
+}
+template <typename R, int N, int V, int PV, int NTP>
+__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
+    k_lf_pb(const LanFusedArgs<R>* __restrict__ A) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  // field index fastest: the V blocks of one plane, which read the same eta and
+  // dc planes, are resident together and share those reads through L2
+  lf_pb_body<R, N, V, PV, NTP>(a, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------------ Z2
@@ -923,10 +935,10 @@ constexpr int z2_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem < cap ? by_smem : cap);
 }
 
+// Z2 of column tile bx of one member
 template <typename R, int N, int V, int PV, int TM>
-__global__ void __launch_bounds__(NT, (z2_min_blocks<R, N, V, TM>())) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
+__device__ __forceinline__ void lf_z2_body(const LanFusedArgs<R>& a, const int bx) {
   using C = cplx<R>;
-  const LanFusedArgs<R> a = A[blockIdx.z];
   constexpr int NXH = N / 2 + 1, LN = V * TM;
   constexpr int64_t PL = (int64_t)N * NXH, NK = PL * N;
   constexpr int NS = fz::rplan(N, PV).ns;
@@ -940,7 +952,7 @@ __global__ void __launch_bounds__(NT, (z2_min_blocks<R, N, V, TM>())) k_lf_z2(co
   using W = R;  // working precision of the update (the state's)
   __shared__ double g[V][9];
   __shared__ int sameg;  // every variant has the gradient coefficients of variant 0
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  const int64_t m0 = (int64_t)bx * TM;
   // the eta^ state was written by the previous step's Z2, which has completed once this
   // block runs (PB released it only after its own wait), and PB does not touch it: the
   // tile load overlaps PB's last blocks (L2 reads, cp.async.cg)
@@ -1033,23 +1045,26 @@ __global__ void __launch_bounds__(NT, (z2_min_blocks<R, N, V, TM>())) k_lf_z2(co
 #pragma unroll
     for (int r = 0; r < S0::R; ++r) dst[(int64_t)(j + r * S0::M) * PL] = x[r];
   }
-  block_reduce_store(fint, 0, a.partials + Q_FINT2 * PSTRIDE + blockIdx.x);
+  block_reduce_store(fint, 0, a.partials + Q_FINT2 * PSTRIDE + bx);
+}
+template <typename R, int N, int V, int PV, int TM>
+__global__ void __launch_bounds__(NT, (z2_min_blocks<R, N, V, TM>())) k_lf_z2(const LanFusedArgs<R>* __restrict__ A) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  lf_z2_body<R, N, V, PV, TM>(a, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ PI
 // Block (z, f < V): eta_new_f -> real, eta statistics, and theta_f = eta_f^2 -> forward
 // for the next step (which then starts at its column kernel).  The concentration plane
 // and the end of the step are k_lf_pc's.
+// PI of plane z, variant f of one member
 template <typename R, int N, int PV, int NTP>
-__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
-    k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V) {
+__device__ __forceinline__ void lf_pi_body(const LanFusedArgs<R>& a, const int V, const int z, const int f) {
   using P = fz::Plane<R, N, NTP, PV>;
-  const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
-  const int z = blockIdx.x, f = blockIdx.y;
   constexpr int64_t PL = (int64_t)N * N, N3 = PL * N, NK = (int64_t)N * N * P::NXH;
   C* mp = a.M + f * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
@@ -1081,26 +1096,24 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
     a.partials[LQ_CSUM * PSTRIDE + blk] = 0.0;
   }
 }
+template <typename R, int N, int PV, int NTP>
+__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
+    k_lf_pi(const LanFusedArgs<R>* __restrict__ A, int V) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  lf_pi_body<R, N, PV, NTP>(a, V, blockIdx.x, blockIdx.y);
+}
 
 // ------------------------------------------------------------------ PC
 // Block z: dc_new -> real, concentration statistics; the member's last block ends the
-// step.  PC reads only the dc^ spectrum (Z1's) and writes only dc and its partial slots,
-// none of which PI touches, so it runs beside PI: launched right after it with
-// programmatic dependent launch, its blocks take the slots PI's single wave leaves free,
-// and only the member's last block waits for PI (griddepcontrol.wait) before it reduces
-// every block partial of the step in a fixed order into history row *hist_row and
-// advances the row (so graph replays need no host-side row index).  That block's wait
-// also makes PC's completion imply PI's, which the next step's Z1 relies on.
+// step.
+// PC of plane z of one member: the plane and its partial slots (not the end of the step)
 template <typename R, int N, int PV, int NTP>
-__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
-    k_lf_pc(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
+__device__ __forceinline__ void lf_pc_body(const LanFusedArgs<R>& a, const int V, const int z) {
   using P = fz::Plane<R, N, NTP, PV>;
-  const LanFusedArgs<R> a = A[blockIdx.z];
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* buf = (C*)smraw;
   C* tws = buf + P::ELEMS;
-  const int z = blockIdx.x;
   constexpr int64_t PL = (int64_t)N * N, NK = (int64_t)N * N * P::NXH;
   C* mp = a.M + V * NK + z * (int64_t)N * P::NXH;
   P::load_tw(tws, a.twx, a.twy, a.post);
@@ -1130,20 +1143,16 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
   block_reduce_store(cmin, 2, a.partials + LQ_CMIN * PSTRIDE + blk);
   block_reduce_store(cmax, 1, a.partials + LQ_CMAX * PSTRIDE + blk);
   block_reduce_store(csum, 0, a.partials + LQ_CSUM * PSTRIDE + blk);
-  __shared__ int last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(a.ticket, 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  step_dep_wait();  // PI complete, its partials visible
-  __threadfence();
+}
+
+// The end of a member's step, by one block once every partial of the step is written
+// and visible: every block partial in a fixed order into history row *hist_row, which
+// then advances (so graph replays need no host-side row index).  Every thread loads its
+// strided share of every quantity at once (all loads in flight together: one L2 round
+// trip), then one block reduction of the Q_STEP_COUNT values.
+template <int NTP, typename R>
+__device__ __forceinline__ void lf_step_reduce(const LanFusedArgs<R>& a, const NbList& nb) {
   const int row = *(volatile const int*)a.hist_row;
-  // every thread loads its strided share of every quantity at once (all loads in flight
-  // together: one L2 round trip), then one block reduction of the Q_STEP_COUNT values;
-  // fixed reduction order
   constexpr int QN = Q_STEP_COUNT, NW = NTP / 32;
   auto qop = [](int q) { return (q == Q_CMIN) ? 2 : (q == Q_CMAX || q == Q_PHIMAX) ? 1 : 0; };
   double acc[QN];
@@ -1181,6 +1190,30 @@ __global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
     *a.ticket = 0;
     *a.hist_row = row + 1;
   }
+}
+
+// PC reads only the dc^ spectrum (Z1's) and writes only dc and its partial slots, none
+// of which PI touches, so it runs beside PI: launched right after it with programmatic
+// dependent launch, its blocks take the slots PI's single wave leaves free, and only the
+// member's last block waits for PI (griddepcontrol.wait) before it ends the step
+// (lf_step_reduce).  That block's wait also makes PC's completion imply PI's, which the
+// next step's Z1 relies on.
+template <typename R, int N, int PV, int NTP>
+__global__ void __launch_bounds__(NTP, (plane_min_blocks<R, N, PV, NTP>()))
+    k_lf_pc(const LanFusedArgs<R>* __restrict__ A, int V, NbList nb) {
+  const LanFusedArgs<R> a = A[blockIdx.z];
+  lf_pc_body<R, N, PV, NTP>(a, V, blockIdx.x);
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(a.ticket, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  step_dep_wait();  // PI complete, its partials visible
+  __threadfence();
+  lf_step_reduce<NTP>(a, nb);
 }
 
 // ------------------------------------------------------------------ launch sequence

@@ -199,13 +199,16 @@ class Ensemble:
     """Many independent fused Landau simulations advanced together
     (``meu_ensemble_*``).  ``params`` is a list of decks; member m's fields are
     set and read as for ``Simulation``.  ``autotune`` times the schedule variants
-    of every size bucket at creation."""
+    of every size bucket at creation.  ``persistent`` runs the warm steps of every
+    member as work items of one persistent launch (``MEU_ENS_PERSISTENT``: one order
+    parameter per member, schedule (2, 256, wide tile) for every size)."""
 
-    def __init__(self, params, autotune: bool = False):
+    def __init__(self, params, autotune: bool = False, persistent: bool = False):
         self.params = [p.copy() for p in params]
         arr = (P.MeuParams * len(self.params))(*self.params)
         h = C.c_void_p()
-        st = lib().meu_ensemble_create(len(self.params), arr, 1 if autotune else 0, C.byref(h))
+        flags = (1 if autotune else 0) | (2 if persistent else 0)
+        st = lib().meu_ensemble_create(len(self.params), arr, flags, C.byref(h))
         if st:
             raise MeuError(st, lib().meu_ensemble_last_error(None).decode())
         self.h = h

@@ -8,6 +8,8 @@
   FP64 oracle's fields to 1e-10.
 * The autotuned ensemble picks instantiated schedules and stays within the FP32
   tolerance of the FP64 path.
+* The persistent ensemble (one launch per run of steps, every size's passes as work
+  items) gives each member's single-handle fields on its schedule bit for bit.
 """
 import numpy as np
 import pytest
@@ -50,6 +52,50 @@ def test_ensemble_equals_single_handles(precision):
         for k in ("fint", "fch", "elen", "etot", "cmin", "cmax", "phimax", "solid_now", "cavg"):
             assert np.array_equal(ds[k], de[i][k]), (i, k)
         assert np.array_equal(ds["step"], de[i]["step"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [P.PREC_F32, P.PREC_F64])
+def test_persistent_ensemble_equals_single_handles(precision):
+    """MEU_ENS_PERSISTENT: after the first (per-bucket) step, every pass of every member
+    of five grid sizes runs as work items of one launch per run of up to 64 steps; each
+    member's fields equal those of its own handle on the persistent schedule bit for bit."""
+    sizes = (32, 48, 64, 32, 96, 128)
+    ms = _members(precision, sizes=sizes, nvars=(1,) * len(sizes))
+    ens = Ensemble([m[0] for m in ms], persistent=True)
+    tm = 16 if precision == P.PREC_F32 else 8
+    for i, (p, c, e) in enumerate(ms):
+        assert ens.schedule(i)[:3] == (2, 256, tm)
+        ens.set_fields(i, c, e)
+    n0 = ens.launch_count
+    de = ens.run(70)  # one per-bucket step, then persistent launches of 64 and 5 steps
+    buckets = len(set(sizes))
+    assert ens.launch_count - n0 == 7 * buckets + 2
+    assert ens.step == ms[0][0].step + 70
+    for i, (p, c, e) in enumerate(ms):
+        s = Simulation(p)
+        s.set_schedule(2, 256, tm)
+        s.set_fields(c, e)
+        ds = s.run(70)
+        cs, es, _, _ = s.get_fields()
+        ce, ee, _ = ens.get_fields(i)
+        assert np.array_equal(cs, ce), i
+        assert np.array_equal(es, ee), i
+        # the energies: same sums, but the elastic energy is a difference of two large
+        # quadratic forms, and the compiler fuses multiply-adds differently in the
+        # persistent kernel (a separately compiled body), which the cancellation lifts to
+        # ~1e-9 relative in FP64
+        for k in ("fint", "fch", "elen", "etot", "cmin", "cmax", "phimax", "solid_now", "cavg"):
+            assert np.allclose(ds[k], de[i][k], rtol=1e-8, atol=0.0), (i, k)
+        assert np.array_equal(ds["step"], de[i]["step"])
+
+
+@pytest.mark.gpu
+def test_persistent_ensemble_rules():
+    ms = _members(P.PREC_F32, sizes=(32, 48), nvars=(1, 2))
+    with pytest.raises(_lib.MeuError) as ex:
+        Ensemble([m[0] for m in ms], persistent=True)
+    assert ex.value.code == 103  # MEU_ERR_UNSUPPORTED
 
 
 @pytest.mark.gpu
