@@ -98,8 +98,11 @@ __global__ void __launch_bounds__(PK_NTP, min_blocks<R>())
   const int total = L * nsteps;
   __shared__ int s_item;
   // thread 0 claims the block's next item while the block runs the current one, so the
-  // claim's round trip overlaps work (claims stay in list order per block)
-  int next = 0;
+  // claim's round trip overlaps work (claims stay in list order per block).  It also keeps
+  // the last count it acquired and its member: a later item of that member needing no
+  // more is ordered after the finished items by that acquire already, so it starts
+  // without another round trip.
+  int next = 0, seen_m = -1, seen_v = 0;
   if (threadIdx.x == 0) next = atomicAdd(claim, 1);
   for (;;) {
     if (threadIdx.x == 0) {
@@ -108,9 +111,14 @@ __global__ void __launch_bounds__(PK_NTP, min_blocks<R>())
       if (g < total && !*(volatile const int*)abort_flag) {
         const int s = g / L, i = g - s * L;
         const int m = (int)(items[i] & (PK_MAX_MEMBERS - 1));
-        const int w = wait_done(done + m, s * mt[m].per_step + need[i], abort_flag);
+        const int target = s * mt[m].per_step + need[i];
+        const int w = (m == seen_m && target <= seen_v) ? 1 : wait_done(done + m, target, abort_flag);
         if (w == 1) {
           it = g;
+          if (m != seen_m || target > seen_v) {
+            seen_m = m;
+            seen_v = target;
+          }
         } else if (w == 0) {
           atomicMax(A[m].err, MEU_ERR_TIMEOUT);
           atomicExch(abort_flag, 1);
@@ -132,12 +140,10 @@ __global__ void __launch_bounds__(PK_NTP, min_blocks<R>())
       case 96: run_item<R, 96>(a, mt[m].nb, kind, idx); break;
       default: run_item<R, 128>(a, mt[m].nb, kind, idx); break;
     }
-    // every thread's writes of the item, then one release of the member's counter
+    // every thread's writes of the item (the barrier), then one release of the member's
+    // counter (cumulative: it orders the block's writes before the count)
     __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      atomicAdd(done + m, 1);
-    }
+    if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;\n" ::"l"(done + m) : "memory");
   }
 }
 
