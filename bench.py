@@ -7,7 +7,9 @@ operator, dt = 0.005, FP32 bulk arithmetic (FP64 for Omega(k), the k = 0 mode
 and every reduction).  A "step" is one time step of that grid.
 --config 0 / 2 select the 64^3 single-variant and the 512^3 heterogeneous decks;
 --config 3 the batched ensemble of 96 single-variant runs on 32^3..128^3 grids
-(a "step" advances every member once; cells = the members' grid points).
+(a "step" advances every member once; cells = the members' grid points);
+--config 5 the slab-decomposed FFT of one grid over the ranks (512^2 x 512N, weak
+scaling; a "step" is one forward and one inverse transform).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -1007,8 +1009,71 @@ def run_reference_ensemble(args):
     return 0
 
 
+# ------------------------------------------------- slab-decomposed FFT (multi-GPU)
+def run_slab(args):
+    """--config 5: f_trans + inv_trans of one grid split over the N ranks in z slabs
+    (meu_slab_fft_*, one NCCL all-to-all per transform).  Weak scaling: the grid is
+    512 x 512 x (512 N), so every rank holds a 512^3 slab; FP32.  A step is one forward
+    and one inverse transform; value = grid cells / step time (max over ranks)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from meumapps_ss_b200 import params as P
+    from meumapps_ss_b200.slab_fft import SlabFFT
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's P3DFFT build needs MPI and a "
+                              "Fortran compiler, neither of which this image has"}), flush=True)
+        return 0
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n = args.n or 512
+    nx, ny, nz = n, n, n * world
+    K, W = args.steps, max(3, args.warmup)
+    f = SlabFFT(nx, ny, nz, precision=P.PREC_F32)
+    g = torch.Generator(device="cuda").manual_seed(1 + rank)
+    real = torch.rand(f.real_shape, dtype=torch.float32, device="cuda", generator=g)
+    for _ in range(W):
+        real = f.inverse(f.forward(real))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(K):
+        real = f.inverse(f.forward(real))
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    f.close()
+    if rank == 0:
+        cells = nx * ny * nz
+        print(json.dumps({"metric": "Mcell/s (slab FFT forward + inverse)", "value": cells * K / (ms / 1e3) / 1e6,
+                          "unit": "Mcell/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic (uniform random slabs)",
+                          "config": {"workload": f"slab-fft-{nx}x{ny}x{nz}", "grid": [nx, ny, nz],
+                                     "parallelism": f"z slabs over {world} ranks, NCCL all-to-all"}}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
+    if args.config == 5:
+        return run_slab(args)
     if args.config == 4:
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}), flush=True)

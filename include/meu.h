@@ -309,6 +309,36 @@ int64_t meu_launch_count(const meu_handle* h);
 int meu_fft_roundtrip(int32_t nx, int32_t ny, int32_t nz, int32_t precision, const double* in, double* spec_out,
                       double* back_out);
 
+/* Slab-decomposed f_trans / inv_trans over P GPUs, one process per GPU, for grids
+ * larger than one GPU holds.  Replaces the P3DFFT decomposition of the reference
+ * (Multi_MEUMAPPS.f:124-128 process grid, :241-248 plan; ModFunc.f:15-40 calls) with
+ * one all-to-all per transform, which the caller issues (NCCL all-to-all of P equal
+ * chunks; meumapps_ss_b200/slab_fft.py does it with torch.distributed).  Rank r holds
+ * the real z-planes [r*Nz/P, (r+1)*Nz/P) as [z][y][x] and the spectrum of the ky rows
+ * [r*Ny/P, (r+1)*Ny/P) as the "k-slab" [kz][ky][kx] (kx in [0, Nx/2]), in the field
+ * precision (float / float2 for MEU_PREC_F32, double / double2 for MEU_PREC_F64).
+ * Forward: forward_planes (real slab -> send buffer of P chunks, chunk d for rank d),
+ * all-to-all (chunk q from rank q into slot q of the receive buffer, which is the
+ * k-slab), forward_columns (in place; the result is scaled by 1/(Nx Ny Nz) like
+ * f_trans).  Inverse: inverse_columns (k-slab in place, unscaled; chunk q of it is
+ * rank q's), all-to-all, inverse_planes (receive buffer -> real slab).  Device arrays
+ * are 16-byte aligned; work is queued on `stream` (a cudaStream_t, NULL = legacy
+ * default) and not synchronised.  Ny and Nz are multiples of P; Nx, Ny, Nz, Ny/P and
+ * Nz/P are 2^a 3^b (Nx even); otherwise MEU_ERR_UNSUPPORTED / MEU_ERR_BADARG. */
+typedef struct meu_slab_fft meu_slab_fft;
+int meu_slab_fft_create(int32_t nx, int32_t ny, int32_t nz, int32_t nranks, int32_t rank, int32_t precision,
+                        meu_slab_fft** out);
+/* out4: real slab elements, complex elements of one chunk, complex elements of the
+ * send / receive / k-slab buffers (P chunks), P */
+int meu_slab_fft_sizes(const meu_slab_fft* h, int64_t* out4);
+int meu_slab_fft_forward_planes(meu_slab_fft* h, const void* real_dev, void* send_dev, void* stream);
+int meu_slab_fft_forward_columns(meu_slab_fft* h, void* kslab_dev, void* stream);
+int meu_slab_fft_inverse_columns(meu_slab_fft* h, void* kslab_dev, void* stream);
+int meu_slab_fft_inverse_planes(meu_slab_fft* h, const void* recv_dev, void* real_dev, void* stream);
+int64_t meu_slab_fft_launch_count(const meu_slab_fft* h);
+const char* meu_slab_fft_last_error(const meu_slab_fft* h);
+int meu_slab_fft_destroy(meu_slab_fft* h);
+
 /* Allocation-free variant of meu_fft_roundtrip.  It has no counterpart in the
  * reference.  For callers that cannot call cudaMalloc: a driver whose device
  * memory belongs to its OpenACC / managed-memory runtime, a framework whose

@@ -69,6 +69,17 @@ def lib():
                                           C.POINTER(P.MeuParams)]
     L.meu_fft_roundtrip.argtypes = [i32, i32, i32, i32, dp, dp, dp]
     L.meu_fft_roundtrip_noalloc.argtypes = [i32, i32, i32, i32, vp, vp, vp]
+    L.meu_slab_fft_create.argtypes = [i32, i32, i32, i32, i32, i32, C.POINTER(vp)]
+    L.meu_slab_fft_sizes.argtypes = [vp, C.POINTER(i64)]
+    L.meu_slab_fft_forward_planes.argtypes = [vp, vp, vp, vp]
+    L.meu_slab_fft_forward_columns.argtypes = [vp, vp, vp]
+    L.meu_slab_fft_inverse_columns.argtypes = [vp, vp, vp]
+    L.meu_slab_fft_inverse_planes.argtypes = [vp, vp, vp, vp]
+    L.meu_slab_fft_launch_count.argtypes = [vp]
+    L.meu_slab_fft_launch_count.restype = i64
+    L.meu_slab_fft_last_error.argtypes = [vp]
+    L.meu_slab_fft_last_error.restype = C.c_char_p
+    L.meu_slab_fft_destroy.argtypes = [vp]
     L.meu_set_stream.argtypes = [vp, vp]
     L.meu_timing.argtypes = [vp, i32]
     L.meu_timing_report.argtypes = [vp, i32, C.c_char_p, C.POINTER(i64), dp, dp]
