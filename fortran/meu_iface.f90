@@ -157,6 +157,44 @@ module meu_iface
       integer(c_int32_t), value :: nx, ny, nz, precision
       type(c_ptr), value :: in_dev, spec_dev, back_dev
     end function
+    ! slab-decomposed f_trans / inv_trans over the MPI ranks (one GPU each) in place of
+    ! P3DFFT: planes, then an all-to-all of nranks equal chunks (MPI_Alltoall on device
+    ! buffers, or NCCL), then columns; device pointers, stream = c_null_ptr for the default
+    integer(c_int) function meu_slab_fft_create(nx, ny, nz, nranks, rank, precision, h) &
+        bind(C, name="meu_slab_fft_create")
+      import :: c_int, c_int32_t, c_ptr
+      integer(c_int32_t), value :: nx, ny, nz, nranks, rank, precision
+      type(c_ptr), intent(out) :: h
+    end function
+    integer(c_int) function meu_slab_fft_sizes(h, out4) bind(C, name="meu_slab_fft_sizes")
+      import :: c_int, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), intent(out) :: out4(4)
+    end function
+    integer(c_int) function meu_slab_fft_forward_planes(h, real_dev, send_dev, stream) &
+        bind(C, name="meu_slab_fft_forward_planes")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, real_dev, send_dev, stream
+    end function
+    integer(c_int) function meu_slab_fft_forward_columns(h, kslab_dev, stream) &
+        bind(C, name="meu_slab_fft_forward_columns")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, kslab_dev, stream
+    end function
+    integer(c_int) function meu_slab_fft_inverse_columns(h, kslab_dev, stream) &
+        bind(C, name="meu_slab_fft_inverse_columns")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, kslab_dev, stream
+    end function
+    integer(c_int) function meu_slab_fft_inverse_planes(h, recv_dev, real_dev, stream) &
+        bind(C, name="meu_slab_fft_inverse_planes")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, recv_dev, real_dev, stream
+    end function
+    integer(c_int) function meu_slab_fft_destroy(h) bind(C, name="meu_slab_fft_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
   end interface
 
 contains
