@@ -219,10 +219,13 @@ def elasticity_label(p) -> str:
             f"fixed-point iteration to residual <= {p.el_tol:g} (FP64 residual)")
 
 
-def measure_deck(cfg: int, stream, K: int, W: int, K64: int, local: int):
+def measure_deck(cfg: int, stream, K: int, W: int, K64: int, local: int, peak: float = 0.0):
     """One more deck beside the headline: FP32-bulk and FP64 throughput (CUDA events
     around meu_run, graph capture and autotuning outside the timed region), the
-    FP32 error against FP64 after W + K steps, the clocks during the FP32 window."""
+    FP32 error against FP64 after W + K steps, the clocks during the FP32 window.
+    With peak (GB/s): the FP32 step's algorithmic bytes from two per-kernel-timed
+    steps after the window (scaled to the window's elastic iterations per step when
+    the moduli are heterogeneous) over the window's step time, as a fraction of it."""
     import numpy as np
     import torch
     from meumapps_ss_b200 import configs as CF
@@ -265,6 +268,21 @@ def measure_deck(cfg: int, stream, K: int, W: int, K64: int, local: int):
         if prec == P.PREC_F32:
             out["clocks"] = sampler.stop()
             out["schedule"] = sim.schedule
+            if peak:
+                sim.timing(True)
+                tr = (P.MeuDiag * 2)()
+                sim.run_into(2, tr)
+                rep_t = sim.timing_report()
+                sim.timing(False)
+                sb = sum(v["bytes"] for v in rep_t.values()) / 2
+                if p32.elastic == P.ELAST_HETERO:
+                    it_t = float(np.mean(P.diag_to_dict(list(tr))["el_iters"]))
+                    sb *= out[key]["elastic_iterations_per_step"] / max(it_t, 1e-9)
+                out["step_roofline"] = {"step_algorithmic_bytes": sb, "peak": peak, "unit": "GB/s",
+                                        "achieved": sb / (ms / k / 1e3) / 1e9,
+                                        "step_frac": sb / (ms / k / 1e3) / 1e9 / peak}
+        elif peak:
+            sim.run(2, diag=False)  # the FP32 leg's two timed steps: same step count for the error
         if k < K:
             sim.run(K - k, diag=False)
         fields[prec] = sim.get_fields()[:2]
@@ -273,7 +291,7 @@ def measure_deck(cfg: int, stream, K: int, W: int, K64: int, local: int):
     out["fp32_speedup"] = out["fp32_bulk"]["value"] / out["fp64_plain"]["value"]
     out["err_vs_fp64"] = {"c_rel_l2": float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64)),
                           "eta_rel_l2": float(np.linalg.norm(e32 - e64) / max(np.linalg.norm(e64), 1e-300)),
-                          "after_steps": W + K}
+                          "after_steps": W + K + (2 if peak else 0)}
     return out
 
 
@@ -320,7 +338,7 @@ def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
     return out
 
 
-def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0):
+def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0, peak: float = 0.0):
     """Deck 3 beside the headline: the 96-member ensemble (32^3..128^3 grids, one
     variant) in FP32 bulk and plain FP64, CUDA events around meu_ensemble_run (graph
     capture and autotuning outside the timed region), with the FP32 error against FP64
@@ -365,6 +383,19 @@ def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0):
         if key == "fp32_bulk":
             out["clocks"] = sampler.stop()
             out["cells_per_step"] = cells
+        if peak:
+            # two more steps in every leg (same step count for the errors); in the FP32 leg
+            # with per-kernel timing, for the step's algorithmic bytes
+            if key == "fp32_bulk":
+                ens.timing(True)
+                ens.run(2, diag=False)
+                sb = sum(v["bytes"] for v in ens.timing_report().values()) / 2
+                ens.timing(False)
+                out["step_roofline"] = {"step_algorithmic_bytes": sb, "peak": peak, "unit": "GB/s",
+                                        "achieved": sb / (ms / K / 1e3) / 1e9,
+                                        "step_frac": sb / (ms / K / 1e3) / 1e9 / peak}
+            else:
+                ens.run(2, diag=False)
         fields_out[key] = [ens.get_fields(i)[:2] for i in range(len(ws))]
         ens.close()
 
@@ -378,9 +409,10 @@ def measure_ensemble(stream, K: int = 20, W: int = 5, local: int = 0):
     worst_c, worst_e = worst("fp32_bulk")
     pc, pe = worst("fp32_persistent")
     out["fp32_persistent"]["err_vs_fp64"] = {"c_rel_l2_max_member": pc, "eta_rel_l2_max_member": pe,
-                                             "after_steps": W + K}
+                                             "after_steps": W + K + (2 if peak else 0)}
     out["fp32_speedup"] = out["fp32_bulk"]["value"] / out["fp64_plain"]["value"]
-    out["err_vs_fp64"] = {"c_rel_l2_max_member": worst_c, "eta_rel_l2_max_member": worst_e, "after_steps": W + K}
+    out["err_vs_fp64"] = {"c_rel_l2_max_member": worst_c, "eta_rel_l2_max_member": worst_e,
+                          "after_steps": W + K + (2 if peak else 0)}
     return out
 
 
@@ -561,10 +593,10 @@ def run_ours(args):
     # ---------------- the other single-grid decks, measured in the same run (rank 0, default workload)
     decks = {}
     if rank == 0 and not args.n and args.config == 1 and not args.no_extra:
-        decks["deck0"] = measure_deck(0, stream, K=200, W=W, K64=200, local=local)
-        decks["deck2"] = measure_deck(2, stream, K=10, W=W, K64=10, local=local)
+        decks["deck0"] = measure_deck(0, stream, K=200, W=W, K64=200, local=local, peak=peak)
+        decks["deck2"] = measure_deck(2, stream, K=10, W=W, K64=10, local=local, peak=peak)
         decks["kks"] = measure_kks(stream)
-        decks["deck3"] = measure_ensemble(stream, local=local)
+        decks["deck3"] = measure_ensemble(stream, local=local, peak=peak)
 
     # ---------------- CPU baseline (rank 0, N = 1): the oracle port on host cores
     cpu = None
