@@ -260,6 +260,10 @@ void meu_ran2_init(meu_ran2_state* s, int32_t iseed);
 double meu_ran2(meu_ran2_state* s);
 /* langevin (ModFunc.f:77-100): one N(0,sd) draw by the polar method. */
 double meu_langevin(meu_ran2_state* s, double sd);
+/* n langevin draws into out[0..n-1]: the numbers, and the final state of *s, of n
+ * meu_langevin calls.  The ran_2 chain and the accept test run on the calling thread;
+ * the logarithm and square root of the accepted pairs on up to `threads` host threads. */
+int meu_langevin_fill(meu_ran2_state* s, double sd, int64_t n, double* out, int32_t threads);
 
 /* Uniform-noise initial fields for the Landau decks: per voxel in Fortran
  * order (x fastest), c = c0 + c_amp*(2u-1), then for each variant

@@ -63,6 +63,7 @@ def lib():
     L.meu_ran2.restype = C.c_double
     L.meu_langevin.argtypes = [C.POINTER(Ran2State), C.c_double]
     L.meu_langevin.restype = C.c_double
+    L.meu_langevin_fill.argtypes = [C.POINTER(Ran2State), C.c_double, i64, dp, i32]
     L.meu_init_uniform.argtypes = [C.POINTER(Ran2State), i32, i32, i32, i32, C.c_double, C.c_double, C.c_double, dp, dp]
     L.meu_params_from_gparams.argtypes = [i32, i32, i32, i32, i32, i32, C.POINTER(C.c_int32), i64, i64, i64,
                                           C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp, dp,
@@ -127,6 +128,14 @@ class Ran2:
 
     def langevin(self, sd: float) -> float:
         return lib().meu_langevin(C.byref(self.s), float(sd))
+
+    def langevin_fill(self, sd: float, n: int, threads: int = 4) -> np.ndarray:
+        """n langevin draws at once (meu_langevin_fill): the numbers of n calls."""
+        out = np.empty(n)
+        st = lib().meu_langevin_fill(C.byref(self.s), float(sd), int(n), dptr(out), int(threads))
+        if st:
+            raise MeuError(st, "meu_langevin_fill")
+        return out
 
 
 def init_uniform(nx: int, ny: int, nz: int, nvar: int, seed: int, c0: float, c_amp: float,

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <future>
+#include <thread>
 #include <memory>
 #include <string>
 #include <vector>
@@ -708,9 +709,12 @@ void Engine<R>::run_noise(int nsteps, meu_ran2_state* rng, double sd, meu_diag* 
     }
     noise_dev = dalloc<double>(cnt);
   }
-  auto generate = [rng, sd, cnt](double* dst, cudaEvent_t free_ev) {
+  // the chain on the drawing thread, the transcendental part of its accepted pairs on the
+  // other host threads (meu_langevin_fill: the numbers of cnt meu_langevin calls)
+  const int32_t fill_threads = (int32_t)std::max(1u, std::thread::hardware_concurrency() - 1);
+  auto generate = [rng, sd, cnt, fill_threads](double* dst, cudaEvent_t free_ev) {
     cudaEventSynchronize(free_ev);  // the buffer's previous copy has run
-    for (int64_t i = 0; i < cnt; ++i) dst[i] = meu_langevin(rng, sd);
+    meu_langevin_fill(rng, sd, cnt, dst, fill_threads);
   };
   std::future<void> next;
   if (noisy > 0) next = std::async(std::launch::async, generate, noise_host[0], noise_ev[0]);

@@ -2,8 +2,11 @@
 // ran_2 generator (ran_2.f:1-42) with its SAVE state made explicit, the
 // langevin draw (ModFunc.f:77-100) and the uniform-noise initialiser of the
 // Landau decks.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "../../include/meu.h"
 
@@ -16,10 +19,49 @@ constexpr int32_t kNtab = 32, kNdiv = 1 + kImm1 / kNtab;
 // without overflow): x <- a*(x - k*q) - k*r, then wrap into [0, m).
 inline int32_t schrage(int32_t x, int32_t a, int32_t q, int32_t r, int32_t m) {
   const int32_t k = x / q;
-  int32_t y = a * (x - k * q) - k * r;
-  if (y < 0) y += m;
-  return y;
+  const int32_t y = a * (x - k * q) - k * r;
+  return y + (m & (y >> 31));  // + m when y < 0, without a branch (its sign is random)
 }
+
+// the shuffle-table set-up ran_2 makes on a call with idum <= 0 (ran_2.f:14-24)
+inline void ran2_seed(meu_ran2_state* s) {
+  if (s->idum <= 0) {
+    s->idum = (-s->idum > 1) ? -s->idum : 1;
+    s->idum2 = s->idum;
+    for (int j = kNtab + 8; j >= 1; --j) {
+      s->idum = schrage(s->idum, kIa1, kIq1, kIr1, kIm1);
+      if (j <= kNtab) s->iv[j - 1] = s->idum;
+    }
+    s->iy = s->iv[0];
+  }
+}
+
+// ran_2 on a state held in locals (registers and a stack table) for a run of draws;
+// the same steps as meu_ran2 after its initialisation
+struct Ran2Local {
+  int32_t idum, idum2, iy, iv[kNtab];
+  explicit Ran2Local(const meu_ran2_state& s) : idum(s.idum), idum2(s.idum2), iy(s.iy) {
+    for (int j = 0; j < kNtab; ++j) iv[j] = s.iv[j];
+  }
+  void store(meu_ran2_state& s) const {
+    s.idum = idum;
+    s.idum2 = idum2;
+    s.iy = iy;
+    for (int j = 0; j < kNtab; ++j) s.iv[j] = iv[j];
+  }
+  inline double next() {
+    const double am = (double)(1.0f / (float)kIm1);
+    const double rnmx = 1.0 - 1.2e-7;
+    idum = schrage(idum, kIa1, kIq1, kIr1, kIm1);
+    idum2 = schrage(idum2, kIa2, kIq2, kIr2, kIm2);
+    const int j = iy / kNdiv;
+    iy = iv[j] - idum2;
+    iv[j] = idum;
+    iy += (iy < 1) ? kImm1 : 0;
+    const double v = am * (double)iy;
+    return v < rnmx ? v : rnmx;
+  }
+};
 }  // namespace
 
 extern "C" {
@@ -35,15 +77,7 @@ double meu_ran2(meu_ran2_state* s) {
   // 2^31 - 128 and the quotient is rounded to single before widening
   const double am = (double)(1.0f / (float)kIm1);
   const double rnmx = 1.0 - 1.2e-7;
-  if (s->idum <= 0) {
-    s->idum = (-s->idum > 1) ? -s->idum : 1;
-    s->idum2 = s->idum;
-    for (int j = kNtab + 8; j >= 1; --j) {
-      s->idum = schrage(s->idum, kIa1, kIq1, kIr1, kIm1);
-      if (j <= kNtab) s->iv[j - 1] = s->idum;
-    }
-    s->iy = s->iv[0];
-  }
+  ran2_seed(s);
   s->idum = schrage(s->idum, kIa1, kIq1, kIr1, kIm1);
   s->idum2 = schrage(s->idum2, kIa2, kIq2, kIr2, kIm2);
   const int j = s->iy / kNdiv;  // 0-based slot of the shuffle table
@@ -64,6 +98,49 @@ double meu_langevin(meu_ran2_state* s, double sd) {
       return v2 * rsq * sd;
     }
   }
+}
+
+// n langevin draws, the numbers of n meu_langevin calls: the serial ran_2 chain and the
+// polar method's accept test run on the calling thread (the state in locals), which
+// keeps v2 and rsq of every accepted pair; the transcendental part,
+// v2 * sqrt(-2 log(rsq) / rsq) * sd, then runs on up to `threads` host threads.
+int meu_langevin_fill(meu_ran2_state* s, double sd, int64_t n, double* out, int32_t threads) {
+  if (!s || (!out && n > 0) || n < 0) return MEU_ERR_BADARG;
+  if (n == 0) return MEU_OK;
+  ran2_seed(s);
+  std::vector<double> rsqv((size_t)n);
+  {
+    // every attempt is stored at slot i, which advances only when the pair is accepted
+    // (a rejected attempt is overwritten by the next): no branch on the random test
+    Ran2Local r(*s);
+    int64_t i = 0;
+    while (i < n) {
+      const double v1 = 2.0 * r.next() - 1.0;
+      const double v2 = 2.0 * r.next() - 1.0;
+      const double rsq = v1 * v1 + v2 * v2;
+      out[i] = v2;
+      rsqv[(size_t)i] = rsq;
+      i += (rsq > 0.0) & (rsq < 1.0);
+    }
+    r.store(*s);
+  }
+  auto finish = [&](int64_t a, int64_t b) {
+    for (int64_t i = a; i < b; ++i) {
+      const double rsq = std::sqrt(-2.0 * std::log(rsqv[(size_t)i]) / rsqv[(size_t)i]);
+      out[i] = out[i] * rsq * sd;
+    }
+  };
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(threads > 0 ? threads : 1, n / 65536 + 1));
+  if (nt == 1) {
+    finish(0, n);
+    return MEU_OK;
+  }
+  std::vector<std::thread> pool;
+  const int64_t per = (n + nt - 1) / nt;
+  for (int64_t t = 1; t < nt; ++t) pool.emplace_back(finish, std::min(n, t * per), std::min(n, (t + 1) * per));
+  finish(0, std::min(n, per));
+  for (auto& th : pool) th.join();
+  return MEU_OK;
 }
 
 void meu_init_uniform(meu_ran2_state* s, int32_t nx, int32_t ny, int32_t nz, int32_t nvar, double c0, double c_amp,

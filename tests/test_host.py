@@ -36,6 +36,21 @@ def test_langevin_agrees(oracle):
     assert abs(np.std(vals) - 0.3) < 0.03
 
 
+def test_langevin_fill_equals_serial_draws():
+    # meu_langevin_fill (the chain on one thread, the logarithms on several) gives the
+    # numbers and the final state of as many meu_langevin calls, fresh seed or not
+    for seed, n, threads, pre in ((-5, 300000, 4, 0), (-12, 70001, 3, 17), (-3, 5, 8, 1), (-8, 0, 2, 2)):
+        a, b = _lib.Ran2(seed), _lib.Ran2(seed)
+        for _ in range(pre):
+            a.langevin(0.5)
+            b.langevin(0.5)
+        ser = np.array([a.langevin(0.02) for _ in range(n)])
+        got = b.langevin_fill(0.02, n, threads)
+        assert np.array_equal(ser, got), (seed, n)
+        assert bytes(a.s) == bytes(b.s)
+        assert a() == b()
+
+
 def test_oracle_initialiser_matches_library(oracle):
     # the CPU legs of the benchmark draw their inputs with the oracle's own ran_2
     for args in ((16, 16, 16, 3, -7, 0.2, 0.01, 0.001), (12, 8, 6, 1, -1, 0.15, 0.01, 0.001)):
