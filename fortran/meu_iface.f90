@@ -78,6 +78,15 @@ module meu_iface
       type(meu_ran2_state), intent(inout) :: rng
       real(c_double), value :: sd
     end function
+    ! n langevin(rng, sd) draws into out(1:n), the logarithms on up to `threads` host threads
+    integer(c_int) function meu_langevin_fill(rng, sd, n, out, threads) bind(C, name="meu_langevin_fill")
+      import :: c_int, c_int32_t, c_int64_t, c_double, meu_ran2_state
+      type(meu_ran2_state), intent(inout) :: rng
+      real(c_double), value :: sd
+      integer(c_int64_t), value :: n
+      real(c_double), intent(out) :: out(*)
+      integer(c_int32_t), value :: threads
+    end function
     integer(c_int) function meu_get_fields(h, cons, phi, el_en, u_state) bind(C, name="meu_get_fields")
       import :: c_int, c_ptr
       type(c_ptr), value :: h, cons, phi, el_en, u_state
