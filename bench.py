@@ -314,8 +314,9 @@ def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
     out = {"workload": f"kks-{n}^3-{nvar}var-hetero", "grid": [n, n, n], "variants": nvar, "precision": "f64",
            "elasticity": "heterogeneous cubic moduli, fixed point (ModElastic.f:241-481)",
            "noise_draws_per_step": nvar * n3,
-           "noise_note": ("ran_2 is one serial chain: each step's vartot*N^3 langevin draws are made on one host "
-                          "thread, overlapped with the previous step on the GPU")}
+           "noise_note": ("ran_2 is one serial chain: each step's vartot*N^3 langevin draws walk it on one host "
+                          "thread (the logarithms on the other host threads), overlapped with the previous step "
+                          "on the GPU")}
     for noisy in (False, True):
         q = p.copy()
         q.noise_step = q.step + 10 ** 6 if noisy else 0

@@ -107,8 +107,13 @@ double meu_langevin(meu_ran2_state* s, double sd) {
 int meu_langevin_fill(meu_ran2_state* s, double sd, int64_t n, double* out, int32_t threads) {
   if (!s || (!out && n > 0) || n < 0) return MEU_ERR_BADARG;
   if (n == 0) return MEU_OK;
+  std::vector<double> rsqv;
+  try {
+    rsqv.resize((size_t)n);
+  } catch (...) {
+    return MEU_ERR_NOMEM;
+  }
   ran2_seed(s);
-  std::vector<double> rsqv((size_t)n);
   {
     // every attempt is stored at slot i, which advances only when the pair is accepted
     // (a rejected attempt is overwritten by the next): no branch on the random test
@@ -131,14 +136,16 @@ int meu_langevin_fill(meu_ran2_state* s, double sd, int64_t n, double* out, int3
     }
   };
   const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(threads > 0 ? threads : 1, n / 65536 + 1));
-  if (nt == 1) {
-    finish(0, n);
-    return MEU_OK;
-  }
-  std::vector<std::thread> pool;
   const int64_t per = (n + nt - 1) / nt;
-  for (int64_t t = 1; t < nt; ++t) pool.emplace_back(finish, std::min(n, t * per), std::min(n, (t + 1) * per));
-  finish(0, std::min(n, per));
+  auto part = [&](int64_t t) { finish(std::min(n, t * per), std::min(n, (t + 1) * per)); };
+  std::vector<std::thread> pool;
+  try {
+    for (int64_t t = 1; t < nt; ++t) pool.emplace_back(part, t);
+  } catch (...) {
+    // fewer threads than asked (the system refused one): this thread takes the rest
+  }
+  part(0);
+  for (int64_t t = 1 + (int64_t)pool.size(); t < nt; ++t) part(t);
   for (auto& th : pool) th.join();
   return MEU_OK;
 }

@@ -7,6 +7,7 @@
 // argument record.
 #pragma once
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "landau_fused.cuh"
@@ -1245,21 +1246,23 @@ void launch_step_kernel(void (*k)(P...), dim3 grid, int threads, size_t smem, cu
   MEU_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
 }
 
+// Raises fn's dynamic shared-memory limit to the opt-in maximum once per (kernel,
+// device) and host thread; throws if `bytes` exceeds it.
 template <typename K>
 void ensure_smem(K fn, size_t bytes) {
   if (bytes <= 48 * 1024) return;
-  static thread_local std::vector<const void*> done;
-  for (const void* f : done)
-    if (f == (const void*)fn) return;
+  static thread_local std::vector<std::pair<const void*, int>> done;
   int dev = 0, optin = 0;
   MEU_CUDA(cudaGetDevice(&dev));
+  for (const auto& f : done)
+    if (f.first == (const void*)fn && f.second == dev) return;
   MEU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   cudaFuncAttributes fa;
   MEU_CUDA(cudaFuncGetAttributes(&fa, (const void*)fn));
   const int lim = optin - (int)fa.sharedSizeBytes;
   if ((int)bytes > lim) throw CudaError("fused tile exceeds shared memory", MEU_ERR_UNSUPPORTED);
   MEU_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  done.push_back((const void*)fn);
+  done.emplace_back((const void*)fn, dev);
 }
 
 template <typename R, int N, int V, int PV, int NTP, int TM>
