@@ -191,7 +191,7 @@ void el_rows_launch(const FFT3& f, const PtrList<cplx<R>>& sp, const R* pphi, co
     constexpr int NR = el_rows_per_block(L);
     auto fn = pf ? k_el_rows<R, L, PV, O, true> : k_el_rows<R, L, PV, O, false>;
     const size_t sm = (size_t)(6 * NR + 1) * L * sizeof(C) + (pf ? (size_t)E.nvar * NR * 2 * L * sizeof(R) : 0);
-    if (sm > 48 * 1024 && (int)sm > smem_optin((const void*)fn))
+    if ((int)sm > smem_optin((const void*)fn))  // dynamic + static above 48 KB needs the opt-in
       throw CudaError("fused elastic rows exceed shared memory", MEU_ERR_UNSUPPORTED);
     fn<<<(unsigned)((nrows + NR - 1) / NR), 256, sm, st>>>(sp, pphi, nrows, (const C*)f.px.tw, (const C*)f.post_tw, E,
                                                           n3, (R)cfac, err);

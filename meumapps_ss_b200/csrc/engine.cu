@@ -382,7 +382,9 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
     };
     g_el_k = resident((const void*)k_el_k<R>);
     g_lan_k1 = resident((const void*)k_lan_k1<R>);
-    g_elener = resident((const void*)k_elener<R>);
+    el_ortho_gen = ortho6(hK.c0m);
+    for (int n = 0; n < p.numph; ++n) el_ortho_gen = el_ortho_gen && ortho6(p.sela[n]);
+    g_elener = resident(el_ortho_gen ? (const void*)k_elener<R, true> : (const void*)k_elener<R>);
     if (hK.prop_moduli) {
       ElxProp& X = el_prop;
       for (int i = 0; i < 36; ++i) {
@@ -425,7 +427,7 @@ Engine<R>::Engine(const meu_params& p) : P(p) {
       const int64_t ntiles = (n3 + PF_TILE - 1) / PF_TILE;
       // grid: the blocks that fit at once (each loops over tiles), at most one per tile
       auto fit = [&](const void* fn, size_t smem) {
-        if (smem > 48 * 1024 && (int)smem > smem_optin(fn))
+        if ((int)smem > smem_optin(fn))  // dynamic + static above 48 KB needs the opt-in
           throw CudaError("elastic prefetch tiles exceed shared memory", MEU_ERR_UNSUPPORTED);
         int nb = 0;
         MEU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, PF_TILE, smem));
@@ -815,7 +817,8 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
           KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
                   fn_el_x<<<g_el_x, PF_TILE, sm_el_x, st>>>(el_prop, (int64_t)n3, pphi, strain, xs, cfac, d_err));
         } else
-          KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R), k_el_x<R><<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
+          KLAUNCH("el_x", (double)(V + 12) * n3 * sizeof(R),
+                  (el_ortho_gen ? k_el_x<R, true> : k_el_x<R>)<<<gridr(), 256, 0, st>>>(dK, pphi, strain, xs, cfac, d_err));
         std::vector<const R*> in;
         for (int m = 0; m < 6; ++m) in.push_back(field(xs, m));
         fwd_list(in, 0);
@@ -862,7 +865,8 @@ void Engine<R>::elastic(const R* ph_for_ppr, R* elg, int mode, bool zeroth_only)
             fn_elener<<<g_elener, PF_TILE, sm_elener, st>>>(en_prop, (int64_t)n3, ph_for_ppr, pphi, strain, el_en, elg,
                                                             mode, eta2, partials, d_err));
   } else
-    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R), k_elener<R><<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
+    KLAUNCH("elener", (double)(2 * V + 6 + 1 + V) * n3 * sizeof(R),
+            (el_ortho_gen ? k_elener<R, true> : k_elener<R>)<<<g_elener, RED_THREADS, 0, st>>>(dK, ph_for_ppr, pphi, strain, el_en, elg, mode,
                                                   (P.model == MEU_MODEL_LANDAU && P.eig_coupling == MEU_EIG_ETA2) ? 1 : 0,
                                                   partials, d_err));
 }

@@ -307,6 +307,7 @@ class Engine : public EngineBase {
   void (*fn_elener)(ElenProp, int64_t, const R*, const R*, const R*, R*, R*, int, int, double*, int*) = nullptr;
   size_t sm_el_x = 0, sm_elener = 0;  // their dynamic shared memory (prefetch tiles)
   bool el_ortho = false;              // stiffnesses with decoupled normal / shear blocks
+  bool el_ortho_gen = false;          // general moduli: C0 and every phase's compliance in that pattern
   bool el_fused_rows = false;         // iterations run the x passes and el_x as one kernel
   bool fused_warm = false;
   bool q_checked = false;  // Q(k) of the fused step tested (LS_QCHECK on its first step)

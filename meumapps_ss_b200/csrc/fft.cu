@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(256) k_cols_s(PtrList<cplx<R>> in, PtrList<cpl
 // (227 KB per block on sm_100 minus the kernel's static shared memory).
 template <typename R>
 static void set_smem(const void* fn, size_t bytes) {
-  if (bytes <= 48 * 1024) return;
+  // always: without the opt-in, dynamic plus static shared memory must stay within 48 KB
   if ((int)bytes > smem_optin(fn)) throw CudaError("transform tile exceeds shared memory", 103);
 }
 

@@ -278,6 +278,40 @@ __device__ __forceinline__ int invert6(double* a, int flag) {
   return invert_small<6>(a, 6, flag);
 }
 
+// Inverse of a 6x6 (column-major) whose normal and shear parts decouple and whose shears
+// are independent (nonzero only at i, j < 3 or i == j: every cubic or orthotropic
+// compliance mix in the crystal frame): the 3x3 normal block by its adjugate, the three
+// shears by their reciprocals.  The same singularity test as invert6, on the exact
+// 1-norms of the block-diagonal matrix and of its inverse; a zero determinant or shear
+// returns flag with a unchanged.
+__device__ __forceinline__ int invert6_ortho(double* a, int flag) {
+  const double b00 = a[0], b10 = a[1], b20 = a[2], b01 = a[6], b11 = a[7], b21 = a[8];
+  const double b02 = a[12], b12 = a[13], b22 = a[14];
+  const double s3 = a[21], s4 = a[28], s5 = a[35];
+  const double c00 = b11 * b22 - b12 * b21, c01 = b02 * b21 - b01 * b22, c02 = b01 * b12 - b02 * b11;
+  const double c10 = b12 * b20 - b10 * b22, c11 = b00 * b22 - b02 * b20, c12 = b02 * b10 - b00 * b12;
+  const double c20 = b10 * b21 - b11 * b20, c21 = b01 * b20 - b00 * b21, c22 = b00 * b11 - b01 * b10;
+  const double det = b00 * c00 + b01 * c10 + b02 * c20;
+  if (det == 0.0 || s3 == 0.0 || s4 == 0.0 || s5 == 0.0) return flag;
+  const double anorm = fmax(fmax(fabs(b00) + fabs(b10) + fabs(b20), fabs(b01) + fabs(b11) + fabs(b21)),
+                            fmax(fabs(b02) + fabs(b12) + fabs(b22), fmax(fabs(s3), fmax(fabs(s4), fabs(s5)))));
+  const double r = 1.0 / det;
+  a[0] = c00 * r; a[6] = c01 * r; a[12] = c02 * r;
+  a[1] = c10 * r; a[7] = c11 * r; a[13] = c12 * r;
+  a[2] = c20 * r; a[8] = c21 * r; a[14] = c22 * r;
+  a[21] = 1.0 / s3; a[28] = 1.0 / s4; a[35] = 1.0 / s5;
+  const double inorm = fmax(fmax(fabs(a[0]) + fabs(a[1]) + fabs(a[2]), fabs(a[6]) + fabs(a[7]) + fabs(a[8])),
+                            fmax(fabs(a[12]) + fabs(a[13]) + fabs(a[14]),
+                                 fmax(fabs(a[21]), fmax(fabs(a[28]), fabs(a[35])))));
+  // rcond = 1 / (|A| |A^-1|) <= 1e-16 stops, as the reference's rcond .le. 1e-16 does; a
+  // mix of non-finite values (NaN) fails that comparison there and here alike, so it
+  // goes on to the step's non-finite check (MEU_ERR_NOT_FINITE) instead
+  if (anorm * inorm >= 1e16) return flag;
+  return 0;
+}
+// nonzero pattern of invert6_ortho's matrices (column-major index i + 6 j)
+__host__ __device__ constexpr bool ortho_nz(int k) { return (k % 6 < 3 && k / 6 < 3) || k % 6 == k / 6; }
+
 // 3x3 inverse in closed form (adjugate), column-major; returns 0 or flag.
 __device__ __forceinline__ int invert3(double* q, int flag) {
   const double a = q[0], b = q[3], c = q[6], d = q[1], e = q[4], f = q[7], g = q[2], h = q[5], i = q[8];

@@ -1250,7 +1250,8 @@ void launch_step_kernel(void (*k)(P...), dim3 grid, int threads, size_t smem, cu
 // device) and host thread; throws if `bytes` exceeds it.
 template <typename K>
 void ensure_smem(K fn, size_t bytes) {
-  if (bytes <= 48 * 1024) return;
+  // no shortcut below 48 KB: without the opt-in, dynamic plus static shared memory must
+  // stay within 48 KB, so a 48 KB tile of a kernel with static arrays needs it too
   static thread_local std::vector<std::pair<const void*, int>> done;
   int dev = 0, optin = 0;
   MEU_CUDA(cudaGetDevice(&dev));

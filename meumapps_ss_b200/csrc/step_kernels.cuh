@@ -207,8 +207,10 @@ __global__ void __launch_bounds__(256) k_el_zeroth(const DevConst* __restrict__ 
 // --------------------------------------------------- elastic: polarisation x
 // ModElastic.f:248-327.  strain = engineering gamma (6), xs out (6).  General
 // moduli: the per-voxel mixed compliance is inverted (6x6); the proportional case
-// goes through k_el_x_prop below.
-template <typename R>
+// goes through k_el_x_prop below.  ORTHO: every phase's compliance and C0 have the
+// decoupled normal / shear pattern (cubic or orthotropic in the crystal frame), so the
+// mix is inverted as a 3x3 block and three shears and the zero entries are skipped.
+template <typename R, bool ORTHO = false>
 __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
                                               const R* __restrict__ strain, R* __restrict__ xs, double cfac, int* err) {
   const DevConst& K = *Kp;
@@ -230,13 +232,15 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
           const double pv = (double)pphi[v * n3 + id];
           psum += pv;
 #pragma unroll
-          for (int i = 0; i < 36; ++i) Cm[i] += pv * p.sela[n - 1][i];
+          for (int i = 0; i < 36; ++i)
+            if (!ORTHO || ortho_nz(i)) Cm[i] += pv * p.sela[n - 1][i];
         }
       if (psum < 1.0) {
 #pragma unroll
-        for (int i = 0; i < 36; ++i) Cm[i] += (1.0 - psum) * p.sela[0][i];
+        for (int i = 0; i < 36; ++i)
+          if (!ORTHO || ortho_nz(i)) Cm[i] += (1.0 - psum) * p.sela[0][i];
       }
-      set_err(err, invert6(Cm, MEU_ERR_C_SINGULAR));
+      set_err(err, ORTHO ? invert6_ortho(Cm, MEU_ERR_C_SINGULAR) : invert6(Cm, MEU_ERR_C_SINGULAR));
     }
     double gam[6];
 #pragma unroll
@@ -246,6 +250,7 @@ __global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, c
       double s = 0;
 #pragma unroll
       for (int m = 0; m < 6; ++m) {
+        if (ORTHO && !ortho_nz(r + m * 6)) continue;
         const double c = Cm[r + m * 6];
         s += cfac * (K.c0m[r + m * 6] - c) * gam[m] + c * e0[m];
       }
@@ -446,7 +451,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict
 // -------------------------------------------------------------- elener
 // ModElastic.f:540-687.  mode 0 (KKS): fdiff += el_grad; mode 1 (Landau): elg = el_grad.
 // theta' = 30 f^2 (f^2 - 2f + 1) (KKS and Landau h coupling) or 2 eta (eta^2 coupling).
-template <typename R>
+template <typename R, bool ORTHO = false>
 __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
                                                         const R* __restrict__ pphi, const R* __restrict__ strain,
                                                         R* __restrict__ el_en, R* __restrict__ elg, int mode, int eta2,
@@ -473,18 +478,20 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
     double Cm[36], sig[6];
     {
 #pragma unroll
-      for (int i = 0; i < 36; ++i) Cm[i] = (1.0 - psum) * p.sela[0][i];
+      for (int i = 0; i < 36; ++i) Cm[i] = (!ORTHO || ortho_nz(i)) ? (1.0 - psum) * p.sela[0][i] : 0.0;
       for (int n = 2; n <= p.numph; ++n)
         for (int v = K.ph_lo[n]; v < K.ph_hi[n]; ++v) {
 #pragma unroll
-          for (int i = 0; i < 36; ++i) Cm[i] += P[v] * p.sela[n - 1][i];
+          for (int i = 0; i < 36; ++i)
+            if (!ORTHO || ortho_nz(i)) Cm[i] += P[v] * p.sela[n - 1][i];
         }
-      set_err(err, invert6(Cm, MEU_ERR_C_ELENER_SINGULAR));
+      set_err(err, ORTHO ? invert6_ortho(Cm, MEU_ERR_C_ELENER_SINGULAR) : invert6(Cm, MEU_ERR_C_ELENER_SINGULAR));
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
         double s = 0;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) s += Cm[i + j * 6] * eps[j];
+        for (int j = 0; j < 6; ++j)
+          if (!ORTHO || ortho_nz(i + j * 6)) s += Cm[i + j * 6] * eps[j];
         sig[i] = s;
       }
     }
@@ -493,7 +500,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
     for (int i = 0; i < 6; ++i) {
       double em = 0;
 #pragma unroll
-      for (int j = 0; j < 6; ++j) em += p.sela[0][i + j * 6] * sig[j];
+      for (int j = 0; j < 6; ++j)
+        if (!ORTHO || ortho_nz(i + j * 6)) em += p.sela[0][i + j * 6] * sig[j];
       elmat += sig[i] * em;
     }
     elmat *= 0.5;
@@ -507,7 +515,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restri
           for (int i = 0; i < 6; ++i) {
             double ep = 0;
 #pragma unroll
-            for (int j = 0; j < 6; ++j) ep += p.sela[n - 1][i + j * 6] * sig[j];
+            for (int j = 0; j < 6; ++j)
+              if (!ORTHO || ortho_nz(i + j * 6)) ep += p.sela[n - 1][i + j * 6] * sig[j];
             elp += sig[i] * ep;
           }
           elp *= 0.5;
