@@ -887,7 +887,15 @@ void Engine<R>::kks_step(meu_diag* d) {
     inv_list(V, out);
   }
   // local driving force (:619-845)
-  KLAUNCH("kks_point", (double)(7 * V + 4 * E) * n3 * sizeof(R), k_kks_point<R><<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, phi, c, wr, pphi, fd, fc, partials, d_err));
+  {
+    // compile-time phase and solute counts for the common decks (composition solve in registers)
+    auto kp = k_kks_point<R>;
+    if (P.numph == 2 && P.numel == 1) kp = k_kks_point<R, 2, 1>;
+    else if (P.numph == 3 && P.numel == 1) kp = k_kks_point<R, 3, 1>;
+    else if (P.numph == 2 && P.numel == 2) kp = k_kks_point<R, 2, 2>;
+    KLAUNCH("kks_point", (double)(7 * V + 4 * E) * n3 * sizeof(R),
+            kp<<<RED_BLOCKS, RED_THREADS, 0, st>>>(dK, phi, c, wr, pphi, fd, fc, partials, d_err));
+  }
   // elasticity (:851-880)
   last_iters = 0;
   if (step >= P.elastep0 && P.elastic != MEU_ELAST_NONE) {

@@ -42,15 +42,20 @@ __global__ void __launch_bounds__(256) k_kks_grad(const DevConst* __restrict__ K
 
 // ------------------------------------------------- KKS: local driving force
 // Multi_MEUMAPPS.f:634-845 per voxel.  g4 = [gx_v, gy_v, gz_v, kds_v] per v.
-// Fields in R; the local solve and the energies in FP64.
-template <typename R>
+// Fields in R; the local solve and the energies in FP64.  NPH, NEL > 0: the phase and
+// solute counts are compile-time (the common decks), so the zdim x zdim composition
+// system and its inverse live in registers; 0, 0: any counts, arrays sized for the
+// largest system (local memory).
+template <typename R, int NPH = 0, int NEL = 0>
 __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
                                                            const R* __restrict__ cons, const R* __restrict__ g4,
                                                            R* __restrict__ pphi, R* __restrict__ fdiff,
                                                            R* __restrict__ fc, double* partials, int* err) {
   const DevConst& K = *Kp;
   const meu_params& p = K.p;
-  const int V = p.nvar, numel = p.numel, numph = p.numph, zdim = K.zdim;
+  constexpr bool FIX = NPH > 0 && NEL > 0;
+  constexpr int ZM = FIX ? NPH * NEL : 12;  // largest zdim the arrays hold
+  const int V = p.nvar, numel = FIX ? NEL : p.numel, numph = FIX ? NPH : p.numph, zdim = FIX ? ZM : K.zdim;
   const int64_t n3 = K.n3;
   double fch = 0, fw = 0, fint = 0;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n3; id += (int64_t)gridDim.x * blockDim.x) {
@@ -71,7 +76,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
       }
     Pph[0] = 1.0 - Pph[0];
     // interface compositions (:677-710)
-    double Z[144], Zr[12], X[MEU_MAX_EL][MEU_MAX_PH], Gib[MEU_MAX_PH], MuC[MEU_MAX_EL];
+    double Z[ZM * ZM], Zr[ZM], X[MEU_MAX_EL][MEU_MAX_PH], Gib[MEU_MAX_PH], MuC[MEU_MAX_EL];
     for (int i = 0; i < zdim * zdim; ++i) Z[i] = K.zconst[i];
     for (int i = 0; i < zdim; ++i) Zr[i] = K.zr_const[i];
     for (int e = 1; e <= numel; ++e) {
@@ -79,7 +84,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_kks_point(const DevConst* __res
       Zr[i0 - 1] = (double)cons[(e - 1) * n3 + id];
       for (int n = 1; n <= numph; ++n) Z[(i0 - 1) + (numph * (e - 1) + n - 1) * zdim] = Pph[n - 1];
     }
-    set_err(err, invert_small<12>(Z, zdim, MEU_ERR_Z_SINGULAR));
+    set_err(err, invert_small<ZM>(Z, zdim, MEU_ERR_Z_SINGULAR));
     for (int n = 1; n <= numph; ++n)
       for (int e = 1; e <= numel; ++e) {
         const int i0 = numph * (e - 1) + n;
