@@ -9,7 +9,8 @@ and every reduction).  A "step" is one time step of that grid.
 --config 3 the batched ensemble of 96 single-variant runs on 32^3..128^3 grids
 (a "step" advances every member once; cells = the members' grid points);
 --config 5 the slab-decomposed FFT of one grid over the ranks (512^2 x 512N, weak
-scaling; a "step" is one forward and one inverse transform).
+scaling; a "step" is one forward and one inverse transform); --config 6 the
+reference's own KKS model (128^3, 3 variants, FP64, noise off and on).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -1103,10 +1104,42 @@ def run_slab(args):
     return 0
 
 
+# ------------------------------------------------ the reference's own model (KKS)
+def run_kks(args):
+    """--config 6: the reference's KKS model (plain FP64, 3 variants, heterogeneous
+    cubic moduli, deck in its Input.txt format) on a 128^3 grid (--n to change it),
+    Langevin noise off and on; one rank.  A step is one time step."""
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the Fortran reference cannot be built here "
+                              "(no Fortran compiler, MPI or P3DFFT)"}), flush=True)
+        return 0
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.Stream()
+    n = args.n or 128
+    r = measure_kks(stream, n=n, K=args.steps, W=max(1, args.warmup))
+    off = r["noise_off"]
+    print(json.dumps({"metric": "Mcell-steps/s (KKS, plain FP64)", "value": off["value"], "unit": UNIT, "n_gpus": 1,
+                      "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": off["ms_per_step"],
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic (the reference's InitFields restated, ran_2 with the deck's seed)",
+                      "config": {"workload": r["workload"], "grid": r["grid"], "variants": r["variants"]},
+                      "noise_on": r["noise_on"], "elastic_iterations_per_step": off["elastic_iterations_per_step"]}),
+          flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.config == 5:
         return run_slab(args)
+    if args.config == 6:
+        return run_kks(args)
     if args.config == 4:
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}), flush=True)
