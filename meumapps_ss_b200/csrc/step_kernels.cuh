@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) k_el_zeroth(const DevConst* __restrict__ 
 // decoupled normal / shear pattern (cubic or orthotropic in the crystal frame), so the
 // mix is inverted as a 3x3 block and three shears and the zero entries are skipped.
 template <typename R, bool ORTHO = false>
-__global__ void __launch_bounds__(256) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
+__global__ void __launch_bounds__(256, ORTHO ? 3 : 1) k_el_x(const DevConst* __restrict__ Kp, const R* __restrict__ pphi,
                                               const R* __restrict__ strain, R* __restrict__ xs, double cfac, int* err) {
   const DevConst& K = *Kp;
   const meu_params& p = K.p;
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_el_k(const DevConst* __restrict
 // ModElastic.f:540-687.  mode 0 (KKS): fdiff += el_grad; mode 1 (Landau): elg = el_grad.
 // theta' = 30 f^2 (f^2 - 2f + 1) (KKS and Landau h coupling) or 2 eta (eta^2 coupling).
 template <typename R, bool ORTHO = false>
-__global__ void __launch_bounds__(RED_THREADS) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
+__global__ void __launch_bounds__(RED_THREADS, ORTHO ? 3 : 1) k_elener(const DevConst* __restrict__ Kp, const R* __restrict__ phi,
                                                         const R* __restrict__ pphi, const R* __restrict__ strain,
                                                         R* __restrict__ el_en, R* __restrict__ elg, int mode, int eta2,
                                                         double* partials, int* err) {
