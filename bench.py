@@ -321,6 +321,7 @@ def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
     for noisy in (False, True):
         q = p.copy()
         q.noise_step = q.step + 10 ** 6 if noisy else 0
+        q.flags |= P.FLAG_AUTOTUNE  # the transform passes' radix plan and column tile, timed at meu_create
         with Simulation(q) as g:
             g.set_stream(stream.cuda_stream)
             g.set_fields(cons, phi)
@@ -328,6 +329,7 @@ def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
             _lib.lib().meu_ran2_init(C.byref(st), -abs(deck.iseed) or -1)
             run = (lambda k: g.run_noise(k, st, deck.sd)) if noisy else (lambda k: g.run(k))
             run(W)
+            sched = g.schedule
             torch.cuda.synchronize()
             a.record(stream)
             d = run(K)
@@ -336,7 +338,7 @@ def measure_kks(stream, n: int = 128, nvar: int = 3, K: int = 5, W: int = 2):
             ms = a.elapsed_time(b)
         key = "noise_on" if noisy else "noise_off"
         out[key] = {"value": n3 * K / (ms / 1e3) / 1e6, "unit": UNIT, "steps": K, "ms_per_step": ms / K,
-                    "elastic_iterations_per_step": float(sum(d["el_iters"]) / K)}
+                    "elastic_iterations_per_step": float(sum(d["el_iters"]) / K), "schedule": list(sched)}
     return out
 
 
