@@ -260,8 +260,8 @@ void meu_ran2_init(meu_ran2_state* s, int32_t iseed);
 double meu_ran2(meu_ran2_state* s);
 /* langevin (ModFunc.f:77-100): one N(0,sd) draw by the polar method. */
 double meu_langevin(meu_ran2_state* s, double sd);
-/* n langevin draws into out[0..n-1]: the numbers, and the final state of *s, of n
- * meu_langevin calls.  The ran_2 chain and the accept test run on the calling thread;
+/* n langevin draws into out[0..n-1] (the noise loop of Multi_MEUMAPPS.f:552-566 over
+ * ModFunc.f:77-100): the numbers, and the final state of *s, of n meu_langevin calls.  The ran_2 chain and the accept test run on the calling thread;
  * the logarithm and square root of the accepted pairs on up to `threads` host threads. */
 int meu_langevin_fill(meu_ran2_state* s, double sd, int64_t n, double* out, int32_t threads);
 
