@@ -48,7 +48,8 @@ extern "C" {
 
 /* flags */
 #define MEU_FLAG_GENERIC 1  /* use the generic kernels even where the fused Landau step applies */
-#define MEU_FLAG_AUTOTUNE 2 /* fused Landau step: time the schedule variants in meu_create and keep the fastest */
+#define MEU_FLAG_AUTOTUNE 2 /* time the schedule variants in meu_create and keep the fastest (fused Landau
+                             * step; on the generic path the transforms' radix plan and column tile) */
 
 /* Landau eigenstrain coupling theta(eta) */
 #define MEU_EIG_ETA2 0 /* theta = eta^2 */
