@@ -15,7 +15,9 @@
  *                             uniform fields (uniformity and the k = 0 recurrence),
  *                             mass conservation (Landau and KKS), Khachaturyan's
  *                             closed-form elastic energy of a dilatational inclusion
- *                             in a cubic medium, and a numpy restatement of one
+ *                             in a cubic medium (Landau) and of a tetragonal one in
+ *                             the KKS model (eldis + elener with equal matrix and
+ *                             precipitate moduli), and a numpy restatement of one
  *                             Landau step (1 to 3 variants, eta^2 and h(eta)
  *                             coupling, with and without elasticity) to 1e-12;
  *   tests/test_host.py        ran_2 / langevin against two other restatements.

@@ -206,6 +206,62 @@ def test_inclusion_energy_matches_khachaturyan(oracle):
     assert abs(d["elen"][0] - energy) <= 1e-12 * abs(energy)
 
 
+def _p_inverse(theta):
+    """phi with p(phi) = phi^3 (6 phi^2 - 15 phi + 10) = theta on (0, 1), by bisection."""
+    lo, hi = np.zeros_like(theta), np.ones_like(theta)
+    for _ in range(64):
+        mid = 0.5 * (lo + hi)
+        pm = mid ** 3 * (6 * mid * mid - 15 * mid + 10)
+        lo, hi = np.where(pm < theta, mid, lo), np.where(pm < theta, hi, mid)
+    return 0.5 * (lo + hi)
+
+
+def test_kks_inclusion_energy_matches_khachaturyan(oracle):
+    # The reference's own model: one variant with a tetragonal eigenstrain in a medium whose
+    # matrix and precipitate share one cubic stiffness.  eldis's fixed point then keeps the
+    # zeroth order (ModElastic.f:115-236) and elener's energy (ModElastic.f:493-691),
+    # summed over the grid, is Khachaturyan's 1/2 sum_k B(n_k) |theta^(k)|^2 of the shape
+    # function theta = p(phi), with B(n) = eps0:C:eps0 - (sig0 n) . (n C n)^-1 . (sig0 n)
+    # evaluated here with numpy, independently of the oracle's discrete Q(k)
+    n = 16
+    deck = P.parse_input_txt(CF.kks_input_txt(n, 1, 1, hetero=False))
+    p = P.kks_params(deck)
+    cons, _ = P.init_fields(deck)
+    assert np.array_equal(_mat(p, "cela", 0), _mat(p, "cela", 1))
+    x, y, z = _grid(n)
+    rng = np.random.default_rng(4)
+    theta = 0.5 * np.ones((n, n, n))
+    for m in [(1, 0, 0), (0, 2, 1), (1, 1, 1), (3, -2, 1), (2, 5, -3), (6, 1, 0)]:
+        theta += 0.07 * rng.uniform(0.5, 1.0) * np.cos(2 * np.pi * (m[0] * x + m[1] * y + m[2] * z) / n
+                                                       + rng.uniform(0, 2 * np.pi))
+    assert theta.min() > 0 and theta.max() < 1
+    phi = _p_inverse(theta)
+    o = oracle.OracleSim(p)
+    o.set_fields(cons, phi[None])
+    d = o.run(1)
+    cm = _mat(p, "cela", 1)
+    e0 = np.array(p.trans_ppt[0][:3])
+    assert not any(p.trans_ppt[0][3:6]) and not any(p.e_mean[:])
+    sig0 = cm[:3, :3] @ e0  # normal stress of the eigenstrain (the cubic C has no normal-shear part)
+    w0 = e0 @ sig0
+    th = np.fft.fftn(p_of(phi)) / n ** 3
+    kk = np.stack(np.meshgrid(*(np.fft.fftfreq(n) * 2 * np.pi,) * 3, indexing="ij"), axis=-1)[..., ::-1]
+    kn = np.linalg.norm(kk, axis=-1)
+    b = np.full(kn.shape, w0)  # k = 0: no relaxation (u^(0) = 0, no applied strain)
+    for idx in zip(*np.nonzero(kn > 0)):
+        nv = kk[idx] / kn[idx]
+        g = np.array([[sum(cm[_VO[i][j], _VO[k][l]] * nv[j] * nv[l] for j in range(3) for l in range(3))
+                       for k in range(3)] for i in range(3)])
+        t = sig0 * nv
+        b[idx] = w0 - t @ np.linalg.solve(g, t)
+    energy = n ** 3 * 0.5 * np.sum(b * np.abs(th) ** 2)
+    assert abs(d["elen"][0] - energy) <= 1e-12 * abs(energy), (d["elen"][0], energy)  # measured 2e-16
+
+
+def p_of(phi):
+    return phi ** 3 * (6 * phi * phi - 15 * phi + 10)
+
+
 # ------------------------------------------------------- numpy mirror of a step
 _VO = [[0, 5, 4], [5, 1, 3], [4, 3, 2]]
 
