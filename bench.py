@@ -1114,13 +1114,10 @@ def run_kks(args):
     import torch
 
     rank = int(os.environ.get("RANK", "0"))
-    if args.impl == "reference":
-        if rank == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "the Fortran reference cannot be built here "
-                              "(no Fortran compiler, MPI or P3DFFT)"}), flush=True)
-        return 0
     if rank != 0:
         return 0
+    if args.impl == "reference":
+        return run_kks_reference(args)
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     stream = torch.cuda.Stream()
     n = args.n or 128
@@ -1132,6 +1129,47 @@ def run_kks(args):
                       "data": "synthetic (the reference's InitFields restated, ran_2 with the deck's seed)",
                       "config": {"workload": r["workload"], "grid": r["grid"], "variants": r["variants"]},
                       "noise_on": r["noise_on"], "elastic_iterations_per_step": off["elastic_iterations_per_step"]}),
+          flush=True)
+    return 0
+
+
+def run_kks_reference(args):
+    """--config 6 --impl reference: the oracle port of the reference's KKS step (FP64,
+    all host threads) on the same deck, inputs from the pure-Python set-up mirror; after
+    one untimed step, as many of the K steps as fit about two minutes."""
+    from meumapps_ss_b200 import configs as CF
+    from meumapps_ss_b200 import params as P
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    n = args.n or 128
+    deck = P.parse_input_txt(CF.kks_input_txt(n, 3, 10 ** 6, radius=max(3, n // 10)))
+    p = P.kks_params(deck)
+    p.noise_step = 0
+    cons, phi = P.init_fields(deck)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    s = O.OracleSim(p)
+    s.set_fields(cons, phi)
+    t0 = time.perf_counter()
+    s.run(1)
+    t1 = time.perf_counter() - t0
+    k = max(1, min(args.steps, int(120.0 / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    s.run(k)
+    dt = time.perf_counter() - t0
+    s.close()
+    value = n ** 3 * k / dt / 1e6
+    sample = (f"{k} FP64 KKS time steps of kks-{n}^3-3var-hetero after one untimed step (oracle port, "
+              f"{threads} threads; the Fortran/MPI/P3DFFT reference cannot be built in this image)")
+    print(json.dumps({"impl": "reference", "metric": "Mcell-steps/s (KKS, plain FP64)", "value": value, "unit": UNIT,
+                      "n_gpus": 1, "steps": k, "warmup": 1, "ms_per_step": dt / k * 1e3, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic (the reference's InitFields restated, ran_2 with the deck's seed)",
+                      "config": {"workload": f"kks-{n}^3-3var-hetero", "grid": [n, n, n], "variants": 3},
+                      "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
           flush=True)
     return 0
 
