@@ -713,7 +713,8 @@ void Engine<R>::run_noise(int nsteps, meu_ran2_state* rng, double sd, meu_diag* 
   }
   // the chain on the drawing thread, the transcendental part of its accepted pairs on the
   // other host threads (meu_langevin_fill: the numbers of cnt meu_langevin calls)
-  const int32_t fill_threads = (int32_t)std::max(1u, std::thread::hardware_concurrency() - 1);
+  const unsigned hc = std::thread::hardware_concurrency();  // 0 when unknown
+  const int32_t fill_threads = (int32_t)(hc > 1 ? hc - 1 : 1);
   auto generate = [rng, sd, cnt, fill_threads](double* dst, cudaEvent_t free_ev) {
     cudaEventSynchronize(free_ev);  // the buffer's previous copy has run
     meu_langevin_fill(rng, sd, cnt, dst, fill_threads);
