@@ -20,6 +20,10 @@
  *                             precipitate moduli), and a numpy restatement of one
  *                             Landau step (1 to 3 variants, eta^2 and h(eta)
  *                             coupling, with and without elasticity) to 1e-12;
+ *   tests/test_oracle_kks_mirror.py  a numpy restatement of one KKS step of the
+ *                             reference (gradients, composition solve, driving forces,
+ *                             n_tilda projection, both updates, clip; no elasticity),
+ *                             1 and 3 variants, 1 and 2 solutes, to 1e-12;
  *   tests/test_host.py        ran_2 / langevin against two other restatements.
  *
  * It follows the reference statement by statement:

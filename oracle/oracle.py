@@ -6,7 +6,8 @@ reference artefacts (the reference ships none and its Fortran build is not
 compilable here).  Pinned on the CPU against numpy.fft (tests/test_oracle_fft.py),
 known answers -- single-mode decay, uniform fields, mass conservation,
 Khachaturyan's closed-form inclusion energy (Landau, and the KKS model's eldis +
-elener with equal moduli) -- and a numpy restatement of one
+elener with equal moduli) -- a numpy restatement of one KKS step of the reference
+(tests/test_oracle_kks_mirror.py) and a numpy restatement of one
 Landau step (tests/test_oracle_kat.py).
 """
 from __future__ import annotations
