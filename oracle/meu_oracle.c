@@ -22,7 +22,8 @@
  *                             coupling, with and without elasticity) to 1e-12;
  *   tests/test_oracle_kks_mirror.py  a numpy restatement of one KKS step of the
  *                             reference (gradients, composition solve, driving forces,
- *                             n_tilda projection, both updates, clip; no elasticity),
+ *                             n_tilda projection, both updates, clip; and at the first
+ *                             elastic step eldis and elener with heterogeneous moduli),
  *                             1 and 3 variants, 1 and 2 solutes, to 1e-12;
  *   tests/test_host.py        ran_2 / langevin against two other restatements.
  *
