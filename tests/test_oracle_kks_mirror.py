@@ -381,3 +381,32 @@ def test_numpy_mirror_of_a_kks_step_with_elasticity(oracle, nvar):
     for k in ("fint", "fw", "fch", "elen"):
         assert en[k] != 0.0
         assert abs(d[k][0] - en[k]) <= 1e-12 * abs(en[k]), (k, d[k][0], en[k])
+
+
+@pytest.mark.parametrize("scale", [0.5, 1.5])
+def test_numpy_mirror_of_the_elastic_fixed_point_under_contrast(oracle, scale):
+    # a precipitate stiffness 1/scale of the deck's, with its C12 raised by 30% (not
+    # proportional to the matrix): the fixed point needs 9 iterations (scale 0.5) or stops
+    # at the reference's cap of 10 (scale 1.5, ModElastic.f:462-467)
+    deck = P.parse_input_txt(CF.kks_input_txt(16, 1, 5, hetero=True))
+    p = P.kks_params(deck)
+    for k in range(p.numph):
+        p.wellph[k] = 1.0e8 * (k + 1)
+    c2 = _mat(p, "cela", 1) / scale
+    c2[0, 1] *= 1.3
+    c2[1, 0] *= 1.3
+    p.set_matrix("cela", 1, c2)
+    p.set_matrix("sela", 1, np.linalg.inv(c2))
+    rng = np.random.default_rng(5)
+    cons0, phi0 = P.init_fields(deck)
+    phi = np.clip(phi0 + rng.uniform(0.0, 0.3, phi0.shape) * (rng.uniform(size=phi0.shape) > 0.15), 0.0, 1.0)
+    cons = cons0 + 0.02 * rng.uniform(-1, 1, cons0.shape)
+    c1, f1, en = numpy_kks_step(p, cons, phi, elastic=True)
+    o = oracle.OracleSim(p)
+    o.set_fields(cons, phi)
+    d = o.run(1)
+    co, fo, _, _ = o.get_fields()
+    assert int(d["el_iters"][0]) == en["iters"] and en["iters"] > 4
+    assert np.max(np.abs(co - c1)) <= 1e-12 * np.max(np.abs(c1))
+    assert np.max(np.abs(fo - f1)) <= 1e-12
+    assert abs(d["elen"][0] - en["elen"]) <= 1e-12 * abs(en["elen"])
